@@ -1,0 +1,167 @@
+/*
+ * rang_wgridder.h — C ABI of the B200 (sm_100a) w-gridder.
+ *
+ * Part 1 is the reference's C ABI for the exact gridder, symbol for symbol:
+ * rang-core `core/src/ffi_wgridder.rs`. Every array is a HOST array owned by
+ * the caller and borrowed for the call; the library copies it to the GPU,
+ * runs the CUDA pipeline and copies the outputs back. Status codes are the
+ * reference's: 0 success; 1 invalid arguments (the message is kept per thread
+ * for rang_core_wgridder_last_error); 2 an internal failure (a CUDA error, no
+ * device memory; the message is kept likewise). Outputs are zeroed by the
+ * callee. `info` receives 14 doubles: kernel_index, supp, nu, nv, nplanes,
+ * nvis, wmin_d, wmax_d, nm1min, nm1max, nshift, dw, wmin, ofactor
+ * (core/src/wgridder.rs:469-511).
+ *
+ * Part 2 extends the ABI for callers whose data already lives on the GPU
+ * (the PyTorch autograd wrapper, FISTA): a persistent plan on device
+ * pointers, the reference's `Prepared` (core/src/wgridder.rs:3170-3499).
+ */
+#ifndef RANG_WGRIDDER_H
+#define RANG_WGRIDDER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* core/src/ffi_wgridder.rs:22-42 (#[repr(C)] WgridderOptions), same layout. */
+typedef struct WgridderOptions {
+  size_t nx, ny;
+  double pixsize_x, pixsize_y, epsilon, center_x, center_y, sigma_min, sigma_max;
+  int32_t do_wgridding, divide_by_n, flip_u, flip_v, flip_w, allow_nshift;
+  int64_t kernel_index; /* < 0: the cost model chooses */
+  size_t nu, nv;
+} WgridderOptions;
+
+/* Kinds of the _ex entry points (ffi_wgridder.rs:297-310). */
+#define WGRIDDER_VIS_UNIT 0
+#define WGRIDDER_VIS_C64 1
+#define WGRIDDER_VIS_C128 2
+#define WGRIDDER_WGT_NONE 0
+#define WGRIDDER_WGT_F32 1
+#define WGRIDDER_WGT_F64 2
+#define WGRIDDER_WGT_F32_PRODUCT 3
+
+/* ---------------------------------------------------------------- part 1 */
+
+/* ffi_wgridder.rs:155 — visibilities (nrow * nchan interleaved complex
+ * doubles) to the dirty image (nx * ny doubles, first axis l); wgt and mask
+ * may be null. */
+int32_t rang_core_wgridder_vis2dirty_f64(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                         const double* uvw, const double* freq, const double* vis,
+                                         const double* wgt, const uint8_t* mask, double* dirty,
+                                         double* info);
+/* ffi_wgridder.rs:191 — as above in single precision. */
+int32_t rang_core_wgridder_vis2dirty_f32(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                         const double* uvw, const double* freq, const float* vis,
+                                         const float* wgt, const uint8_t* mask, float* dirty,
+                                         double* info);
+/* ffi_wgridder.rs:228 — the image to visibilities (written). */
+int32_t rang_core_wgridder_dirty2vis_f64(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                         const double* uvw, const double* freq, const double* dirty,
+                                         const double* wgt, const uint8_t* mask, double* vis,
+                                         double* info);
+/* ffi_wgridder.rs:264 — as above in single precision. */
+int32_t rang_core_wgridder_dirty2vis_f32(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                         const double* uvw, const double* freq, const float* dirty,
+                                         const float* wgt, const uint8_t* mask, float* vis,
+                                         double* info);
+/* ffi_wgridder.rs:454 — data of kind vis_kind, weights of kind wgt_kind read
+ * in place; dirty and/or psf (either may be null, not both). With a PSF both
+ * images use the plan of wgt * mask != 0. */
+int32_t rang_core_wgridder_vis2dirty_ex_f64(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                            const double* uvw, const double* freq, const void* vis,
+                                            int32_t vis_kind, const void* wgt, int32_t wgt_kind,
+                                            const uint8_t* mask, double* dirty, double* psf,
+                                            double* info);
+/* ffi_wgridder.rs:496 */
+int32_t rang_core_wgridder_vis2dirty_ex_f32(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                            const double* uvw, const double* freq, const void* vis,
+                                            int32_t vis_kind, const void* wgt, int32_t wgt_kind,
+                                            const uint8_t* mask, float* dirty, float* psf,
+                                            double* info);
+/* ffi_wgridder.rs:542 — with WGRIDDER_WGT_F32_PRODUCT the weight is the
+ * float product wgt[i] * wgt2[i]. */
+int32_t rang_core_wgridder_vis2dirty_ex2_f64(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                             const double* uvw, const double* freq, const void* vis,
+                                             int32_t vis_kind, const void* wgt, const void* wgt2,
+                                             int32_t wgt_kind, const uint8_t* mask, double* dirty,
+                                             double* psf, double* info);
+/* ffi_wgridder.rs:573 */
+int32_t rang_core_wgridder_vis2dirty_ex2_f32(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                             const double* uvw, const double* freq, const void* vis,
+                                             int32_t vis_kind, const void* wgt, const void* wgt2,
+                                             int32_t wgt_kind, const uint8_t* mask, float* dirty,
+                                             float* psf, double* info);
+/* ffi_wgridder.rs:668 */
+int32_t rang_core_wgridder_dirty2vis_ex_f64(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                            const double* uvw, const double* freq, const double* dirty,
+                                            const void* wgt, int32_t wgt_kind, const uint8_t* mask,
+                                            double* vis, double* info);
+/* ffi_wgridder.rs:695 */
+int32_t rang_core_wgridder_dirty2vis_ex_f32(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                            const double* uvw, const double* freq, const float* dirty,
+                                            const void* wgt, int32_t wgt_kind, const uint8_t* mask,
+                                            float* vis, double* info);
+/* ffi_wgridder.rs:722 — row `index` of the kernel table into out[7] (W,
+ * ofactor, epsilon, beta, e0, ndim, singleprec); 1 past the end. */
+int32_t rang_core_wgridder_kernel_row(size_t index, double* out);
+/* ffi_wgridder.rs:749 — this thread's last failure message into buf (at most
+ * len bytes, not terminated); returns its full length. */
+size_t rang_core_wgridder_last_error(uint8_t* buf, size_t len);
+
+/* ---------------------------------------------------------------- part 2 */
+
+/* A persistent plan on DEVICE pointers (no counterpart symbol in the
+ * reference; it is the reference's Prepared, wgridder.rs:3170-3222, whose
+ * active set is wgt * mask != 0, or |vis|^2 wgt mask != 0 with with_vis).
+ * `uvw_dev` (nrow * 3 doubles) is copied; `freq` is a HOST array; the
+ * activity arrays are read during the call only. `single` selects float
+ * working precision. `stream` is a cudaStream_t (null: the legacy stream).
+ * The plan's buffers live on `stream`'s device; destroy the plan before the
+ * stream. */
+typedef struct RangWgridPlan RangWgridPlan;
+int32_t rang_b200_wgridder_plan_create(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                       const double* uvw_dev, const double* freq, const void* vis_dev,
+                                       int32_t vis_kind, const void* wgt_dev, const void* wgt2_dev,
+                                       int32_t wgt_kind, const uint8_t* mask_dev, int32_t with_vis,
+                                       int32_t single, void* stream, RangWgridPlan** plan,
+                                       double* info);
+/* vis2dirty with the plan into image_dev (nx * ny, the plan's precision):
+ * unit = 0 grids the data (vis_dev of vis_kind), unit = 1 unit visibilities
+ * (the PSF); weights as in the _ex2 entry points. Asynchronous on `stream`. */
+int32_t rang_b200_wgridder_plan_grid(RangWgridPlan* plan, const void* vis_dev, int32_t vis_kind,
+                                     const void* wgt_dev, const void* wgt2_dev, int32_t wgt_kind,
+                                     int32_t unit, void* image_dev, void* stream);
+/* dirty2vis with the plan: image_dev (nx * ny) to vis_dev (nrow * nchan
+ * interleaved complex, overwritten; inactive visibilities zero), times the
+ * weights. Asynchronous on `stream`. */
+int32_t rang_b200_wgridder_plan_degrid(RangWgridPlan* plan, const void* image_dev, const void* wgt_dev,
+                                       int32_t wgt_kind, void* vis_dev, void* stream);
+/* Waits for `stream` and reports a failure the kernels detected (status 2)
+ * or 0. */
+int32_t rang_b200_wgridder_plan_status(RangWgridPlan* plan, void* stream);
+/* The plan's 14 info doubles. */
+int32_t rang_b200_wgridder_plan_info(const RangWgridPlan* plan, double* info);
+void rang_b200_wgridder_plan_destroy(RangWgridPlan* plan);
+
+/* The visibility binning of a call on HOST arrays, for parity tests: per
+ * visibility (row-major) iu0, iv0 (-1 when inactive) and the bin key
+ * tile * max(nplanes, 1) + first plane (0xffffffff when inactive), and the
+ * sorted order (`sorted`, nrow * nchan entries of room; `nsorted` receives
+ * the active count). Arguments as rang_core_wgridder_vis2dirty_ex2_*;
+ * with_vis selects the activity |vis|^2 wgt mask != 0. */
+int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                   const double* uvw, const double* freq, const void* vis,
+                                   int32_t vis_kind, const void* wgt, const void* wgt2, int32_t wgt_kind,
+                                   const uint8_t* mask, int32_t with_vis, int32_t single, int64_t* iu0,
+                                   int64_t* iv0, uint32_t* key, uint32_t* sorted, size_t* nsorted,
+                                   double* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RANG_WGRIDDER_H */

@@ -1,0 +1,416 @@
+// The C ABI of include/rang_wgridder.h.
+//
+// Part 1 restates the reference's `core/src/ffi_wgridder.rs` entry points
+// (argument checks, messages, status codes) on top of the CUDA pipeline: the
+// host arrays are copied to the device on a per-thread stream, planned,
+// gridded or degridded there, and the outputs copied back. Part 2 exposes the
+// device-resident plan.
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "wgrid_plan.h"
+
+using namespace wg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+int32_t guarded(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const InvalidArgument& e) {
+    g_last_error = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return 2;
+  } catch (...) {
+    g_last_error = "internal failure in the gridder";
+    return 2;
+  }
+}
+
+// Keeps freed device memory in the stream-ordered pool (set once per device),
+// so a call does not pay for cudaMalloc of the previous call's buffers again.
+void configure_pool(int dev) {
+  static std::mutex mu;
+  static std::map<int, bool> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  check_cuda(cudaDeviceGetDefaultMemPool(&pool, dev), "memory pool");
+  uint64_t keep = UINT64_MAX;
+  check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
+  done[dev] = true;
+}
+
+// The library's own stream for host-array calls: one per thread and device.
+cudaStream_t call_stream() {
+  static thread_local std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "no CUDA device");
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  configure_pool(dev);
+  cudaStream_t s;
+  check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+  streams[dev] = s;
+  return s;
+}
+
+size_t vis_bytes(int kind, const void* p) {  // ffi_wgridder.rs:319-336
+  switch (kind) {
+    case VIS_UNIT:
+      return 0;
+    case VIS_C64:
+      if (p) return 8;
+      break;
+    case VIS_C128:
+      if (p) return 16;
+      break;
+  }
+  throw InvalidArgument("invalid visibility array or kind");
+}
+
+size_t wgt_bytes(int kind, const void* p, const void* p2) {  // ffi_wgridder.rs:344-371
+  switch (kind) {
+    case WGT_NONE:
+      return 0;
+    case WGT_F32:
+      if (p) return 4;
+      break;
+    case WGT_F64:
+      if (p) return 8;
+      break;
+    case WGT_F32_PRODUCT:
+      if (p && p2) return 4;
+      break;
+  }
+  throw InvalidArgument("invalid weight array or kind");
+}
+
+DevBuf upload(const void* host, size_t bytes, cudaStream_t s) {
+  DevBuf b;
+  if (host && bytes) {
+    b.alloc(bytes, s);
+    check_cuda(cudaMemcpyAsync(b.get(), host, bytes, cudaMemcpyHostToDevice, s), "copy to device");
+  }
+  return b;
+}
+
+struct Uploaded {
+  DevBuf uvw, vis, wgt, wgt2, mask;
+  Inputs in;
+};
+
+Uploaded upload_inputs(size_t nrow, size_t nchan, const double* uvw, const void* vis, int vis_kind,
+                       const void* wgt, const void* wgt2, int wgt_kind, const uint8_t* mask, cudaStream_t s) {
+  size_t n = nrow * nchan;
+  size_t vb = vis_bytes(vis_kind, vis), wb = wgt_bytes(wgt_kind, wgt, wgt2);
+  Uploaded u;
+  u.uvw = upload(uvw, nrow * 3 * sizeof(double), s);
+  u.vis = upload(vis_kind == VIS_UNIT ? nullptr : vis, n * vb, s);
+  u.wgt = upload(wgt_kind == WGT_NONE ? nullptr : wgt, n * wb, s);
+  u.wgt2 = upload(wgt_kind == WGT_F32_PRODUCT ? wgt2 : nullptr, n * 4, s);
+  u.mask = upload(mask, n, s);
+  u.in.vis = u.vis.get();
+  u.in.vis_kind = vis_kind;
+  u.in.wgt = u.wgt.get();
+  u.in.wgt2 = u.wgt2.get();
+  u.in.wgt_kind = wgt_kind;
+  u.in.mask = u.mask.as<uint8_t>();
+  return u;
+}
+
+template <class T>
+void finish(Plan<T>& plan, cudaStream_t s) {
+  check_cuda(cudaStreamSynchronize(s), "gridder");
+  if (plan.kernel_errors(s)) throw DeviceError("a visibility fell outside its uv tile (internal inconsistency)");
+}
+
+// vis2dirty_multi (wgridder.rs:2436-2496) on host arrays.
+template <class T>
+void host_vis2dirty(const WgridderOptions* o, size_t nrow, size_t nchan, const double* uvw, const double* freq,
+                    const void* vis, int vis_kind, const void* wgt, const void* wgt2, int wgt_kind,
+                    const uint8_t* mask, T* dirty, T* psf, double* info) {
+  if (!o) throw InvalidArgument("null options");
+  if (!uvw || !freq || !info || (!dirty && !psf)) throw InvalidArgument("null array");
+  vis_bytes(vis_kind, vis);
+  wgt_bytes(wgt_kind, wgt, wgt2);
+  check_common(*o, nrow, nchan);
+  f_over_c(freq, nchan);  // the frequency checks, before any device work
+  size_t npix = o->nx * o->ny;
+  cudaStream_t s = call_stream();
+  Uploaded u = upload_inputs(nrow, nchan, uvw, vis, vis_kind, wgt, wgt2, wgt_kind, mask, s);
+  Plan<T> plan(*o, nrow, nchan, u.uvw.as<double>(), freq, u.in, psf == nullptr, s);
+  if (dirty) std::memset(dirty, 0, npix * sizeof(T));
+  if (psf) std::memset(psf, 0, npix * sizeof(T));
+  std::memcpy(info, plan.info().v, sizeof(plan.info().v));
+  if (plan.empty()) return;
+  DevBuf img(npix * sizeof(T), s);
+  if (dirty) {
+    plan.grid(u.in, VALUE_DATA, img.as<T>(), s);
+    check_cuda(cudaMemcpyAsync(dirty, img.get(), npix * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
+  }
+  if (psf) {
+    plan.grid(u.in, VALUE_UNIT, img.as<T>(), s);
+    check_cuda(cudaMemcpyAsync(psf, img.get(), npix * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
+  }
+  finish(plan, s);
+}
+
+// dirty2vis_multi (wgridder.rs:2998-3041) on host arrays.
+template <class T>
+void host_dirty2vis(const WgridderOptions* o, size_t nrow, size_t nchan, const double* uvw, const double* freq,
+                    const T* dirty, const void* wgt, int wgt_kind, const uint8_t* mask, T* vis, double* info) {
+  if (!o) throw InvalidArgument("null options");
+  if (!uvw || !freq || !vis || !dirty || !info) throw InvalidArgument("null array");
+  wgt_bytes(wgt_kind, wgt, nullptr);
+  check_common(*o, nrow, nchan);
+  f_over_c(freq, nchan);
+  size_t n = nrow * nchan, npix = o->nx * o->ny;
+  cudaStream_t s = call_stream();
+  Uploaded u = upload_inputs(nrow, nchan, uvw, nullptr, VIS_UNIT, wgt, nullptr, wgt_kind, mask, s);
+  Plan<T> plan(*o, nrow, nchan, u.uvw.as<double>(), freq, u.in, false, s);
+  std::memcpy(info, plan.info().v, sizeof(plan.info().v));
+  if (plan.empty()) {
+    std::memset(vis, 0, n * 2 * sizeof(T));
+    return;
+  }
+  DevBuf img = upload(dirty, npix * sizeof(T), s);
+  DevBuf out(n * 2 * sizeof(T), s);
+  plan.degrid(img.as<T>(), u.in, out.as<T>(), s);
+  check_cuda(cudaMemcpyAsync(vis, out.get(), n * 2 * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
+  finish(plan, s);
+}
+
+}  // namespace
+
+struct RangWgridPlan {
+  int single = 0;
+  std::unique_ptr<Plan<float>> f;
+  std::unique_ptr<Plan<double>> d;
+};
+
+extern "C" {
+
+int32_t rang_core_wgridder_vis2dirty_f64(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                         const double* freq, const double* vis, const double* wgt,
+                                         const uint8_t* mask, double* dirty, double* info) {
+  return guarded([&] {
+    if (!vis) throw InvalidArgument("null array");
+    host_vis2dirty<double>(opts, nrow, nchan, uvw, freq, vis, VIS_C128, wgt, nullptr, wgt ? WGT_F64 : WGT_NONE,
+                           mask, dirty, nullptr, info);
+  });
+}
+
+int32_t rang_core_wgridder_vis2dirty_f32(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                         const double* freq, const float* vis, const float* wgt,
+                                         const uint8_t* mask, float* dirty, double* info) {
+  return guarded([&] {
+    if (!vis) throw InvalidArgument("null array");
+    host_vis2dirty<float>(opts, nrow, nchan, uvw, freq, vis, VIS_C64, wgt, nullptr, wgt ? WGT_F32 : WGT_NONE, mask,
+                          dirty, nullptr, info);
+  });
+}
+
+int32_t rang_core_wgridder_dirty2vis_f64(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                         const double* freq, const double* dirty, const double* wgt,
+                                         const uint8_t* mask, double* vis, double* info) {
+  return guarded([&] {
+    host_dirty2vis<double>(opts, nrow, nchan, uvw, freq, dirty, wgt, wgt ? WGT_F64 : WGT_NONE, mask, vis, info);
+  });
+}
+
+int32_t rang_core_wgridder_dirty2vis_f32(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                         const double* freq, const float* dirty, const float* wgt,
+                                         const uint8_t* mask, float* vis, double* info) {
+  return guarded([&] {
+    host_dirty2vis<float>(opts, nrow, nchan, uvw, freq, dirty, wgt, wgt ? WGT_F32 : WGT_NONE, mask, vis, info);
+  });
+}
+
+int32_t rang_core_wgridder_vis2dirty_ex_f64(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                            const double* freq, const void* vis, int32_t vis_kind, const void* wgt,
+                                            int32_t wgt_kind, const uint8_t* mask, double* dirty, double* psf,
+                                            double* info) {
+  return guarded([&] {
+    if (wgt_kind == WGT_F32_PRODUCT) throw InvalidArgument("invalid weight array or kind");
+    host_vis2dirty<double>(opts, nrow, nchan, uvw, freq, vis, vis_kind, wgt, nullptr, wgt_kind, mask, dirty, psf,
+                           info);
+  });
+}
+
+int32_t rang_core_wgridder_vis2dirty_ex_f32(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                            const double* freq, const void* vis, int32_t vis_kind, const void* wgt,
+                                            int32_t wgt_kind, const uint8_t* mask, float* dirty, float* psf,
+                                            double* info) {
+  return guarded([&] {
+    if (wgt_kind == WGT_F32_PRODUCT) throw InvalidArgument("invalid weight array or kind");
+    host_vis2dirty<float>(opts, nrow, nchan, uvw, freq, vis, vis_kind, wgt, nullptr, wgt_kind, mask, dirty, psf,
+                          info);
+  });
+}
+
+int32_t rang_core_wgridder_vis2dirty_ex2_f64(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                             const double* uvw, const double* freq, const void* vis, int32_t vis_kind,
+                                             const void* wgt, const void* wgt2, int32_t wgt_kind, const uint8_t* mask,
+                                             double* dirty, double* psf, double* info) {
+  return guarded([&] {
+    host_vis2dirty<double>(opts, nrow, nchan, uvw, freq, vis, vis_kind, wgt, wgt2, wgt_kind, mask, dirty, psf, info);
+  });
+}
+
+int32_t rang_core_wgridder_vis2dirty_ex2_f32(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                             const double* uvw, const double* freq, const void* vis, int32_t vis_kind,
+                                             const void* wgt, const void* wgt2, int32_t wgt_kind, const uint8_t* mask,
+                                             float* dirty, float* psf, double* info) {
+  return guarded([&] {
+    host_vis2dirty<float>(opts, nrow, nchan, uvw, freq, vis, vis_kind, wgt, wgt2, wgt_kind, mask, dirty, psf, info);
+  });
+}
+
+int32_t rang_core_wgridder_dirty2vis_ex_f64(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                            const double* freq, const double* dirty, const void* wgt,
+                                            int32_t wgt_kind, const uint8_t* mask, double* vis, double* info) {
+  return guarded([&] {
+    if (wgt_kind == WGT_F32_PRODUCT) throw InvalidArgument("invalid weight array or kind");
+    host_dirty2vis<double>(opts, nrow, nchan, uvw, freq, dirty, wgt, wgt_kind, mask, vis, info);
+  });
+}
+
+int32_t rang_core_wgridder_dirty2vis_ex_f32(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                            const double* freq, const float* dirty, const void* wgt,
+                                            int32_t wgt_kind, const uint8_t* mask, float* vis, double* info) {
+  return guarded([&] {
+    if (wgt_kind == WGT_F32_PRODUCT) throw InvalidArgument("invalid weight array or kind");
+    host_dirty2vis<float>(opts, nrow, nchan, uvw, freq, dirty, wgt, wgt_kind, mask, vis, info);
+  });
+}
+
+int32_t rang_core_wgridder_kernel_row(size_t index, double* out) {
+  const KernelRow* r = kernel_row(index);
+  if (!r || !out) return 1;
+  double v[7] = {(double)r->w, r->ofactor, r->epsilon, r->beta, r->e0, (double)r->ndim, (double)r->single};
+  std::memcpy(out, v, sizeof(v));
+  return 0;
+}
+
+size_t rang_core_wgridder_last_error(uint8_t* buf, size_t len) {
+  if (buf) std::memcpy(buf, g_last_error.data(), std::min(len, g_last_error.size()));
+  return g_last_error.size();
+}
+
+int32_t rang_b200_wgridder_plan_create(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw_dev,
+                                       const double* freq, const void* vis_dev, int32_t vis_kind, const void* wgt_dev,
+                                       const void* wgt2_dev, int32_t wgt_kind, const uint8_t* mask_dev,
+                                       int32_t with_vis, int32_t single, void* stream, RangWgridPlan** plan,
+                                       double* info) {
+  return guarded([&] {
+    if (!opts || !plan) throw InvalidArgument("null options");
+    if ((!uvw_dev && nrow) || !freq || !info) throw InvalidArgument("null array");
+    vis_bytes(vis_kind, vis_dev);
+    wgt_bytes(wgt_kind, wgt_dev, wgt2_dev);
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "no CUDA device");
+    configure_pool(dev);
+    Inputs in{vis_dev, vis_kind, wgt_dev, wgt2_dev, wgt_kind, mask_dev};
+    cudaStream_t s = (cudaStream_t)stream;
+    auto p = std::make_unique<RangWgridPlan>();
+    p->single = single ? 1 : 0;
+    if (single) {
+      p->f = std::make_unique<Plan<float>>(*opts, nrow, nchan, uvw_dev, freq, in, with_vis != 0, s);
+      std::memcpy(info, p->f->info().v, sizeof(p->f->info().v));
+    } else {
+      p->d = std::make_unique<Plan<double>>(*opts, nrow, nchan, uvw_dev, freq, in, with_vis != 0, s);
+      std::memcpy(info, p->d->info().v, sizeof(p->d->info().v));
+    }
+    *plan = p.release();
+  });
+}
+
+int32_t rang_b200_wgridder_plan_grid(RangWgridPlan* plan, const void* vis_dev, int32_t vis_kind, const void* wgt_dev,
+                                     const void* wgt2_dev, int32_t wgt_kind, int32_t unit, void* image_dev,
+                                     void* stream) {
+  return guarded([&] {
+    if (!plan || !image_dev) throw InvalidArgument("null array");
+    if (!unit) vis_bytes(vis_kind, vis_dev);
+    wgt_bytes(wgt_kind, wgt_dev, wgt2_dev);
+    Inputs in{vis_dev, vis_kind, wgt_dev, wgt2_dev, wgt_kind, nullptr};
+    ValueMode m = unit ? VALUE_UNIT : VALUE_DATA;
+    if (plan->single)
+      plan->f->grid(in, m, (float*)image_dev, (cudaStream_t)stream);
+    else
+      plan->d->grid(in, m, (double*)image_dev, (cudaStream_t)stream);
+  });
+}
+
+int32_t rang_b200_wgridder_plan_degrid(RangWgridPlan* plan, const void* image_dev, const void* wgt_dev,
+                                       int32_t wgt_kind, void* vis_dev, void* stream) {
+  return guarded([&] {
+    if (!plan || !image_dev || !vis_dev) throw InvalidArgument("null array");
+    wgt_bytes(wgt_kind, wgt_dev, nullptr);
+    Inputs in{nullptr, VIS_UNIT, wgt_dev, nullptr, wgt_kind, nullptr};
+    if (plan->single)
+      plan->f->degrid((const float*)image_dev, in, (float*)vis_dev, (cudaStream_t)stream);
+    else
+      plan->d->degrid((const double*)image_dev, in, (double*)vis_dev, (cudaStream_t)stream);
+  });
+}
+
+int32_t rang_b200_wgridder_plan_status(RangWgridPlan* plan, void* stream) {
+  return guarded([&] {
+    if (!plan) throw InvalidArgument("null plan");
+    int e = plan->single ? plan->f->kernel_errors((cudaStream_t)stream) : plan->d->kernel_errors((cudaStream_t)stream);
+    if (e) throw DeviceError("a visibility fell outside its uv tile (internal inconsistency)");
+  });
+}
+
+int32_t rang_b200_wgridder_plan_info(const RangWgridPlan* plan, double* info) {
+  if (!plan || !info) return 1;
+  const PlanInfo& pi = plan->single ? plan->f->info() : plan->d->info();
+  std::memcpy(info, pi.v, sizeof(pi.v));
+  return 0;
+}
+
+void rang_b200_wgridder_plan_destroy(RangWgridPlan* plan) { delete plan; }
+
+int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                   const double* freq, const void* vis, int32_t vis_kind, const void* wgt,
+                                   const void* wgt2, int32_t wgt_kind, const uint8_t* mask, int32_t with_vis,
+                                   int32_t single, int64_t* iu0, int64_t* iv0, uint32_t* key, uint32_t* sorted,
+                                   size_t* nsorted, double* info) {
+  return guarded([&] {
+    if (!opts) throw InvalidArgument("null options");
+    if (!uvw || !freq || !info || !iu0 || !iv0 || !key || !sorted || !nsorted) throw InvalidArgument("null array");
+    check_common(*opts, nrow, nchan);
+    size_t n = nrow * nchan;
+    cudaStream_t s = call_stream();
+    Uploaded u = upload_inputs(nrow, nchan, uvw, vis, vis_kind, wgt, wgt2, wgt_kind, mask, s);
+    auto run = [&](auto& plan) {
+      std::memcpy(info, plan.info().v, sizeof(plan.info().v));
+      *nsorted = plan.nvis();
+      for (size_t i = 0; i < n; i++) {
+        iu0[i] = iv0[i] = -1;
+        key[i] = 0xffffffffu;
+      }
+      plan.export_binning(key, sorted, s);
+      plan.export_pixels(u.in, with_vis != 0, iu0, iv0, s);
+    };
+    if (single) {
+      Plan<float> plan(*opts, nrow, nchan, u.uvw.as<double>(), freq, u.in, with_vis != 0, s);
+      run(plan);
+    } else {
+      Plan<double> plan(*opts, nrow, nchan, u.uvw.as<double>(), freq, u.in, with_vis != 0, s);
+      run(plan);
+    }
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,1029 @@
+// The B200 w-gridder pipeline.
+//
+//   scan        active count and |w| range (one pass over the visibilities)
+//   plan        kernel, grid and w-planes on the host (wgrid_setup.cpp)
+//   binning     counting sort of the active visibilities by (uv tile, first
+//               w-plane): per-visibility key, bin counts, exclusive scan,
+//               scatter; then a task list of <= TASK_CHUNK visibilities of
+//               one tile each
+//   gridding    one CTA per task: the visibilities' ES-kernel footprints on
+//               all their w-planes accumulate in a shared-memory window of
+//               the tile (tile + support - 1 cells square per plane), which
+//               is then added to the HBM-resident w-planes
+//   FFT         cuFFT: inverse along v on every grid row, along u on the
+//               image columns only
+//   project     per pixel, the planes' w-screens applied and summed in
+//               plane order, then the global correction
+// and the adjoint for degridding (corrected image times w-screen placed on
+// the grid, forward FFTs, then one CTA per task gathering each visibility's
+// footprint from a shared-memory copy of the tile's planes).
+//
+// All w-planes of a call stay resident in HBM when they fit (a 9450^2
+// complex64 plane is 714 MB), so every visibility is read once per
+// direction and the footprint on all of its planes is formed in one pass.
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+
+#include "wgrid_plan.h"
+
+namespace wg {
+
+namespace {
+
+constexpr uint32_t INACTIVE = 0xffffffffu;
+constexpr uint32_t TASK_CHUNK = 2048;
+constexpr int GRID_THREADS = 256;
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr size_t SMEM_WINDOW_BYTES = 100 * 1024;
+
+unsigned blocks_for(uint64_t n, int threads, unsigned cap = 148u * 32u) {
+  uint64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  return (unsigned)std::min<uint64_t>(b, cap);
+}
+
+// ------------------------------------------------------------------ scan
+
+struct ScanOut {
+  unsigned long long count;    // active visibilities
+  unsigned long long finite;   // of which with a non-NaN |w|
+  unsigned long long lo_bits;  // min |w| as the bits of a non-negative double
+  unsigned long long hi_bits;  // max |w|
+};
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// scan (wgridder.rs:1051-1077): the count is exact and min/max are order
+// independent, so the result is the reference's bit for bit.
+template <class T>
+__global__ void k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__ uvw,
+                       const double* __restrict__ foc, double fw, Inputs in, int with_vis, ScanOut* out) {
+  uint64_t n = (uint64_t)nrow * nchan;
+  unsigned long long cnt = 0, fin = 0;
+  double lo = 1e300, hi = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (is_active<T>(in, with_vis != 0, i)) {
+      uint32_t row = (uint32_t)(i / nchan);
+      uint32_t ch = (uint32_t)(i - (uint64_t)row * nchan);
+      double w = fabs(fw * uvw[3 * (uint64_t)row + 2] * foc[ch]);
+      cnt++;
+      if (!isnan(w)) {
+        fin++;
+        lo = fmin(lo, w);
+        hi = fmax(hi, w);
+      }
+    }
+  }
+  cnt = warp_sum(cnt);
+  fin = warp_sum(fin);
+  lo = warp_min(lo);
+  hi = warp_max(hi);
+  if ((threadIdx.x & 31) == 0 && cnt) {
+    atomicAdd(&out->count, cnt);
+    if (fin) {
+      atomicAdd(&out->finite, fin);
+      atomicMin(&out->lo_bits, (unsigned long long)__double_as_longlong(lo));
+      atomicMax(&out->hi_bits, (unsigned long long)__double_as_longlong(hi));
+    }
+  }
+}
+
+// ------------------------------------------------------------------ binning
+
+// Setup::locate (wgridder.rs:1244-1255) as one key: tile * nbuckets + plane.
+template <class T>
+__device__ __forceinline__ uint32_t bin_of(const Geom<T>& g, const double* __restrict__ uvw,
+                                           const double* __restrict__ foc, uint32_t idx, int64_t* piu0 = nullptr,
+                                           int64_t* piv0 = nullptr) {
+  uint32_t nchan = (uint32_t)g.nchan;
+  uint32_t row = idx / nchan, ch = idx - row * nchan;
+  double b[3];
+  row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+  double f = foc[ch];
+  double u = b[0] * f, v = b[1] * f, w = b[2] * f;
+  double uf, vf;
+  int64_t iu0, iv0;
+  getpix(g, u, v, uf, vf, iu0, iv0);
+  uint32_t tu = (uint32_t)shifted(iu0, g.nu) >> g.log2tile;
+  uint32_t tv = (uint32_t)shifted(iv0, g.nv) >> g.log2tile;
+  if (piu0) *piu0 = iu0;
+  if (piv0) *piv0 = iv0;
+  return (tu * (uint32_t)g.ntv + tv) * (uint32_t)g.nbuckets + (uint32_t)minplane(g, w);
+}
+
+// One atomic per distinct counter in the warp; each active lane gets the
+// counter's old value plus its rank among the lanes with the same counter.
+__device__ __forceinline__ uint32_t warp_aggregated_add(uint32_t* counters, uint32_t key, bool active) {
+  unsigned mask = __ballot_sync(0xffffffffu, active);
+  uint32_t res = 0;
+  if (active) {
+    unsigned peers = __match_any_sync(mask, key);
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(peers) - 1;
+    unsigned rank = __popc(peers & ((1u << lane) - 1));
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(&counters[key], (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    res = base + rank;
+  }
+  return res;
+}
+
+template <class T>
+__global__ void k_bin_count(const __grid_constant__ Geom<T> g, const double* __restrict__ uvw,
+                            const double* __restrict__ foc, Inputs in, int with_vis, uint32_t* __restrict__ key,
+                            uint32_t* __restrict__ counts) {
+  uint64_t n = g.nrow * g.nchan;
+  uint64_t nround = (n + 31) & ~31ull;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nround; i += (uint64_t)gridDim.x * blockDim.x) {
+    bool act = false;
+    uint32_t k = INACTIVE;
+    if (i < n) {
+      act = is_active<T>(in, with_vis != 0, i);
+      if (act) k = bin_of(g, uvw, foc, (uint32_t)i);
+      key[i] = k;
+    }
+    warp_aggregated_add(counts, k, act);
+  }
+}
+
+__global__ void k_bin_scatter(uint64_t n, const uint32_t* __restrict__ key, uint32_t* __restrict__ cursor,
+                              uint32_t* __restrict__ sorted) {
+  uint64_t nround = (n + 31) & ~31ull;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nround; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t k = i < n ? key[i] : INACTIVE;
+    bool act = k != INACTIVE;
+    uint32_t pos = warp_aggregated_add(cursor, k, act);
+    if (act) sorted[pos] = (uint32_t)i;
+  }
+}
+
+// ------------------------------------------------------------------ exclusive scan (u32)
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+  __shared__ uint32_t warp_tot[SCAN_THREADS / 32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    uint32_t t = lane < nw ? warp_tot[lane] : 0;
+    uint32_t s = t;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < nw) warp_tot[lane] = s - t;
+    if (lane == nw - 1) *total = s;
+  }
+  __syncthreads();
+  uint32_t r = x - v + warp_tot[wid];
+  __syncthreads();
+  return r;
+}
+
+__global__ void k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t n,
+                             uint32_t* __restrict__ tile_sums) {
+  uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+  uint32_t v[SCAN_ITEMS];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = base + k < n ? in[base + k] : 0;
+    s += v[k];
+  }
+  __shared__ uint32_t total;
+  uint32_t run = block_exclusive_scan(s, &total);
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint64_t n, const uint32_t* __restrict__ offs) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += offs[i / SCAN_TILE];
+}
+
+// out[i] = sum of in[0..i) for i < n (in and out may alias).
+void exclusive_scan(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t s) {
+  uint64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  DevBuf sums(ntiles * 4, s);
+  k_scan_tiles<<<(unsigned)ntiles, SCAN_THREADS, 0, s>>>(in, out, n, sums.as<uint32_t>());
+  check_cuda(cudaGetLastError(), "scan");
+  if (ntiles > 1) {
+    exclusive_scan(sums.as<uint32_t>(), sums.as<uint32_t>(), ntiles, s);
+    k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, sums.as<uint32_t>());
+    check_cuda(cudaGetLastError(), "scan");
+  }
+}
+
+// ------------------------------------------------------------------ tasks
+
+__global__ void k_task_count(const uint32_t* __restrict__ starts, uint32_t nb, uint32_t ntiles,
+                             uint32_t* __restrict__ ntask) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < ntiles) {
+    uint32_t c = starts[(uint64_t)(t + 1) * nb] - starts[(uint64_t)t * nb];
+    ntask[t] = (c + TASK_CHUNK - 1) / TASK_CHUNK;
+  } else if (t == ntiles) {
+    ntask[t] = 0;
+  }
+}
+
+__device__ __forceinline__ uint32_t plane_at(const uint32_t* starts, uint64_t b0, uint32_t nb, uint32_t k) {
+  uint32_t m = 0;
+  while (m + 1 < nb && starts[b0 + m + 1] <= k) m++;
+  return m;
+}
+
+__global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t nb, uint32_t ntiles,
+                            const uint32_t* __restrict__ off, Task* __restrict__ tasks, uint32_t* __restrict__ ntotal) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  uint64_t b0 = (uint64_t)t * nb;
+  uint32_t s = starts[b0], e = starts[b0 + nb];
+  uint32_t q0 = off[t];
+  for (uint32_t k0 = s, q = q0; k0 < e; k0 += TASK_CHUNK, q++) {
+    uint32_t k1 = min(k0 + TASK_CHUNK, e);
+    Task tk;
+    tk.tile = t;
+    tk.k0 = k0;
+    tk.k1 = k1;
+    tk.plo = (uint16_t)plane_at(starts, b0, nb, k0);
+    tk.phi = (uint16_t)plane_at(starts, b0, nb, k1 - 1);
+    tasks[q] = tk;
+  }
+  if (t == ntiles - 1) *ntotal = off[ntiles];
+}
+
+// ------------------------------------------------------------------ gridding
+
+template <class T, int S>
+__global__ void __launch_bounds__(GRID_THREADS)
+    k_grid(const __grid_constant__ Geom<T> g, Inputs in, int mode, const double* __restrict__ uvw,
+           const double* __restrict__ foc, const uint32_t* __restrict__ sorted, const Task* __restrict__ tasks,
+           const uint32_t* __restrict__ ntasks, cplx<T>* __restrict__ grids, int pg0, int npg, int gmax,
+           int* __restrict__ err) {
+  if (blockIdx.x >= *ntasks) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int L = g.L, LL = L * L;
+  T* bre = reinterpret_cast<T*>(smem);
+  T* bim = bre + (size_t)gmax * LL;
+  const Task t = tasks[blockIdx.x];
+  const int tu = (int)(t.tile / (uint32_t)g.ntv), tv = (int)(t.tile - (uint32_t)tu * (uint32_t)g.ntv);
+  const int bu = tu << g.log2tile, bv = tv << g.log2tile;
+  const unsigned tilesz = 1u << g.log2tile;
+  int lo = 0, hi = 0;
+  if (g.do_wgridding) {
+    lo = max((int)t.plo, pg0);
+    hi = min((int)t.phi + S - 1, pg0 + npg - 1);
+  }
+  const uint32_t nchan = (uint32_t)g.nchan;
+  for (int w0 = lo; w0 <= hi; w0 += gmax) {
+    const int gw = min(gmax, hi - w0 + 1);
+    for (int c = threadIdx.x; c < gw * LL; c += blockDim.x) {
+      bre[c] = (T)0;
+      bim[c] = (T)0;
+    }
+    __syncthreads();
+    for (uint32_t k = t.k0 + threadIdx.x; k < t.k1; k += blockDim.x) {
+      const uint32_t idx = sorted[k];
+      const uint32_t row = idx / nchan, ch = idx - row * nchan;
+      double b[3];
+      const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+      const double f = foc[ch];
+      const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
+      const int mp = minplane(g, w);
+      const int plo = g.do_wgridding ? max(mp, w0) : 0;
+      const int phi = g.do_wgridding ? min(mp + S - 1, w0 + gw - 1) : 0;
+      if (plo > phi) continue;
+      double uf, vf;
+      int64_t iu0, iv0;
+      getpix(g, u, v, uf, vf, iu0, iv0);
+      const int ou = offset_in(iu0, g.nu, bu), ov = offset_in(iv0, g.nv, bv);
+      if ((unsigned)ou >= tilesz || (unsigned)ov >= tilesz) {
+        atomicOr(err, 1);
+        continue;
+      }
+      T ku[S], kv[S];
+      const T x0 = (T)(-uf * 2.0 + ((double)S - 1.0));
+      const T y0 = (T)(-vf * 2.0 + ((double)S - 1.0));
+      eval_taps2<T, S>(g.coeff, g.ne, x0, y0, ku, kv);
+      cplx<T> val = unit_value<T>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<T>(in, idx));
+      if (mode == VALUE_DATA) val = data_value<T>(vis_get<T>(in, idx), val, (T)imflip);
+      for (int p = plo; p <= phi; p++) {
+        T kk[S];
+        if (g.do_wgridding) {
+          const T kw = w_factor<T, S>(g, p - mp, p, w);
+#pragma unroll
+          for (int cu = 0; cu < S; cu++) kk[cu] = ku[cu] * kw;
+        } else {
+#pragma unroll
+          for (int cu = 0; cu < S; cu++) kk[cu] = ku[cu];
+        }
+        T* pr = bre + (size_t)(p - w0) * LL + ou * L + ov;
+        T* pi = bim + (size_t)(p - w0) * LL + ou * L + ov;
+#pragma unroll
+        for (int cu = 0; cu < S; cu++) {
+          const T tr = val.re * kk[cu], ti = val.im * kk[cu];
+#pragma unroll
+          for (int cv = 0; cv < S; cv++) {
+            atomicAdd(pr + cu * L + cv, tr * kv[cv]);
+            atomicAdd(pi + cu * L + cv, ti * kv[cv]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < gw * LL; c += blockDim.x) {
+      const T re = bre[c], im = bim[c];
+      if (re == (T)0 && im == (T)0) continue;
+      const int pl = c / LL, rem = c - pl * LL, i = rem / L, j = rem - i * L;
+      const int row = (bu + i + g.nu / 2) % g.nu, col = (bv + j + g.nv / 2) % g.nv;
+      cplx<T>* dst = grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col;
+      atomicAdd(&dst->re, re);
+      atomicAdd(&dst->im, im);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ degridding
+
+template <class T, int S>
+__global__ void __launch_bounds__(GRID_THREADS)
+    k_degrid(const __grid_constant__ Geom<T> g, Inputs wts, const double* __restrict__ uvw,
+             const double* __restrict__ foc, const uint32_t* __restrict__ sorted, const Task* __restrict__ tasks,
+             const uint32_t* __restrict__ ntasks, const cplx<T>* __restrict__ grids, int pg0, int npg, int gmax,
+             cplx<T>* __restrict__ vis, int first_group, int last_group, int* __restrict__ err) {
+  if (blockIdx.x >= *ntasks) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int L = g.L, LL = L * L;
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem);
+  const Task t = tasks[blockIdx.x];
+  const int tu = (int)(t.tile / (uint32_t)g.ntv), tv = (int)(t.tile - (uint32_t)tu * (uint32_t)g.ntv);
+  const int bu = tu << g.log2tile, bv = tv << g.log2tile;
+  const unsigned tilesz = 1u << g.log2tile;
+  int lo = 0, hi = 0;
+  if (g.do_wgridding) {
+    lo = max((int)t.plo, pg0);
+    hi = min((int)t.phi + S - 1, pg0 + npg - 1);
+  }
+  const int nwin = lo <= hi ? (hi - lo + gmax) / gmax : 0;
+  const int nloop = max(nwin, last_group ? 1 : 0);
+  const uint32_t nchan = (uint32_t)g.nchan;
+  for (int wi = 0; wi < nloop; wi++) {
+    const int w0 = lo + wi * gmax;
+    const int gw = wi < nwin ? min(gmax, hi - w0 + 1) : 0;
+    for (int c = threadIdx.x; c < gw * LL; c += blockDim.x) {
+      const int pl = c / LL, rem = c - pl * LL, i = rem / L, j = rem - i * L;
+      const int row = (bu + i + g.nu / 2) % g.nu, col = (bv + j + g.nv / 2) % g.nv;
+      buf[c] = grids[((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col];
+    }
+    __syncthreads();
+    const bool finalize = last_group && wi == nloop - 1;
+    const bool fresh = first_group && wi == 0;
+    for (uint32_t k = t.k0 + threadIdx.x; k < t.k1; k += blockDim.x) {
+      const uint32_t idx = sorted[k];
+      const uint32_t row = idx / nchan, ch = idx - row * nchan;
+      double b[3];
+      const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+      const double f = foc[ch];
+      const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
+      const int mp = minplane(g, w);
+      const int plo = g.do_wgridding ? max(mp, w0) : 0;
+      const int phi = g.do_wgridding ? min(mp + S - 1, w0 + gw - 1) : (gw > 0 ? 0 : -1);
+      cplx<T> acc = fresh ? cplx<T>{(T)0, (T)0} : vis[idx];
+      if (plo <= phi) {
+        double uf, vf;
+        int64_t iu0, iv0;
+        getpix(g, u, v, uf, vf, iu0, iv0);
+        const int ou = offset_in(iu0, g.nu, bu), ov = offset_in(iv0, g.nv, bv);
+        if ((unsigned)ou >= tilesz || (unsigned)ov >= tilesz) {
+          atomicOr(err, 1);
+          continue;
+        }
+        T ku[S], kv[S];
+        const T x0 = (T)(-uf * 2.0 + ((double)S - 1.0));
+        const T y0 = (T)(-vf * 2.0 + ((double)S - 1.0));
+        eval_taps2<T, S>(g.coeff, g.ne, x0, y0, ku, kv);
+        for (int p = plo; p <= phi; p++) {
+          T kk[S];
+          if (g.do_wgridding) {
+            const T kw = w_factor<T, S>(g, p - mp, p, w);
+#pragma unroll
+            for (int cu = 0; cu < S; cu++) kk[cu] = ku[cu] * kw;
+          } else {
+#pragma unroll
+            for (int cu = 0; cu < S; cu++) kk[cu] = ku[cu];
+          }
+          const cplx<T>* src = buf + (size_t)(p - w0) * LL + ou * L + ov;
+          T rr = 0, ri = 0;
+#pragma unroll
+          for (int cu = 0; cu < S; cu++) {
+            T tr = 0, tim = 0;
+#pragma unroll
+            for (int cv = 0; cv < S; cv++) {
+              const cplx<T> c = src[cu * L + cv];
+              tr = fma_t(kv[cv], c.re, tr);
+              tim = fma_t(kv[cv], c.im, tim);
+            }
+            rr = fma_t(kk[cu], tr, rr);
+            ri = fma_t(kk[cu], tim, ri);
+          }
+          acc = {rr + acc.re, ri * (T)imflip + acc.im};
+        }
+      }
+      if (finalize) {  // wgridder.rs:3146-3159
+        const T tw = wgt_get<T>(wts, idx);
+        if (g.shifting) {
+          const cplx<T> ph = shift_phase<T>(g, b, imflip, f, -1.0);
+          acc = cmul(acc, cplx<T>{ph.re * tw, ph.im * tw});
+        } else {
+          acc = {acc.re * tw, acc.im * tw};
+        }
+      }
+      vis[idx] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ per-pixel stages
+
+struct CorrNodes {
+  int n;
+  double x[32], w[32];
+};
+
+__device__ __forceinline__ double corfunc_dev(const CorrNodes& c, double v) {
+  double s = 0.0;
+  for (int i = 0; i < c.n; i++) s += c.w[i] * cos(c.x[i] * v);
+  return 1.0 / s;
+}
+
+// nm1 + r_l x + r_m y + nshift of the pixel's table entry (wgridder.rs:589-599, 806-818).
+template <class T>
+__device__ __forceinline__ double screen_arg(const Geom<T>& g, int i, int j) {
+  int ti = g.lmshift ? i : min(i, g.nx - i), tj = g.lmshift ? j : min(j, g.ny - j);
+  double x = g.x0 + (double)ti * g.pixsize_x, y = g.y0 + (double)tj * g.pixsize_y;
+  double xsq = x * x, ysq = y * y;
+  double tmp = 1.0 - xsq - ysq;
+  double nm1 = tmp >= 0.0 ? (-xsq - ysq) / (sqrt(tmp) + 1.0) : -sqrt(-tmp) - 1.0;
+  return nm1 + g.r_l * x + g.r_m * y + g.nshift;
+}
+
+// The w-screen of plane p at one pixel (screen_par, wgridder.rs:2296-2314).
+template <class T>
+__device__ __forceinline__ cplx<T> screen(const Geom<T>& g, double s, int p, bool adjoint) {
+  double w0 = g.wmin + (double)p * g.dw;
+  double phs = w0 * s;
+  if (adjoint) phs *= -1.0;
+  T ang;
+  if (sizeof(T) == 4)
+    ang = (T)(2.0 * PI * (phs - floor(phs)));
+  else
+    ang = (T)(2.0 * PI * phs);
+  T sn, cs;
+  sincos_t(ang, &sn, &cs);
+  return {cs, sn};
+}
+
+// global_corrections (wgridder.rs:822-861) per pixel, full image.
+template <class T>
+__global__ void k_corr(const __grid_constant__ Geom<T> g, const __grid_constant__ CorrNodes cn,
+                       const double* __restrict__ cfu, const double* __restrict__ cfv, double* __restrict__ corr) {
+  uint64_t npix = (uint64_t)g.nx * g.ny;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < npix; q += (uint64_t)gridDim.x * blockDim.x) {
+    int i = (int)(q / g.ny), j = (int)(q - (uint64_t)i * g.ny);
+    int ti = g.lmshift ? i : min(i, g.nx - i), tj = g.lmshift ? j : min(j, g.ny - j);
+    double x = g.x0 + (double)ti * g.pixsize_x, y = g.y0 + (double)tj * g.pixsize_y;
+    double xsq = x * x, ysq = y * y;
+    double tmp = 1.0 - xsq - ysq;
+    double fct;
+    if (tmp >= 0.0) {
+      double nm1 = (-xsq - ysq) / (sqrt(tmp) + 1.0);
+      double fv = corfunc_dev(cn, (nm1 + g.r_l * x + g.r_m * y + g.nshift) * g.dw);
+      if (g.divide_by_n) fv /= nm1 + 1.0;
+      fct = fv;
+    } else if (g.divide_by_n) {
+      fct = 0.0;
+    } else {
+      fct = corfunc_dev(cn, (-sqrt(-tmp) - 1.0 + g.nshift) * g.dw);
+    }
+    int iu = g.nx / 2 - min(ti, g.nx - ti), iv = g.ny / 2 - min(tj, g.ny - tj);
+    fct *= cfu[iu] * cfv[iv];
+    corr[q] = fct;
+  }
+}
+
+// After the FFTs of a plane group: each pixel's planes, w-screened, summed in
+// plane order into `acc`; on the last group the correction gives the image
+// (grid_to_image's projection and correct_image, wgridder.rs:2371-2428).
+template <class T>
+__global__ void k_project(const __grid_constant__ Geom<T> g, const cplx<T>* __restrict__ grids, int pg0, int npg,
+                          T* __restrict__ acc, int first, int last, const double* __restrict__ corr,
+                          const double* __restrict__ cfu, const double* __restrict__ cfv, T* __restrict__ out) {
+  uint64_t npix = (uint64_t)g.nx * g.ny;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < npix; q += (uint64_t)gridDim.x * blockDim.x) {
+    int i = (int)(q / g.ny), j = (int)(q - (uint64_t)i * g.ny);
+    int ix = (g.nu - g.nx / 2 + i) % g.nu, jx = (g.nv - g.ny / 2 + j) % g.nv;
+    T a = first ? (T)0 : acc[q];
+    double s = g.do_wgridding ? screen_arg(g, i, j) : 0.0;
+    for (int p = pg0; p < pg0 + npg; p++) {
+      cplx<T> gv = grids[((size_t)(p - pg0) * g.nu + ix) * g.nv + jx];
+      T term;
+      if (g.do_wgridding) {
+        cplx<T> ph = screen<T>(g, s, p, true);
+        term = gv.re * ph.re - gv.im * ph.im;
+      } else {
+        term = gv.re;
+      }
+      a = a + term;
+    }
+    if (!last) {
+      acc[q] = a;
+    } else if (g.do_wgridding) {
+      out[q] = a * (T)corr[q];
+    } else {
+      int iu = g.nx / 2 - min(i, g.nx - i), iv = g.ny / 2 - min(j, g.ny - j);
+      out[q] = (T)((double)a * cfu[iu] * cfv[iv]);
+    }
+  }
+}
+
+// The corrected image of a degridding call (wgridder.rs:3064-3091).
+template <class T>
+__global__ void k_correct_input(const __grid_constant__ Geom<T> g, const T* __restrict__ dirty,
+                                const double* __restrict__ corr, const double* __restrict__ cfu,
+                                const double* __restrict__ cfv, T* __restrict__ out) {
+  uint64_t npix = (uint64_t)g.nx * g.ny;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < npix; q += (uint64_t)gridDim.x * blockDim.x) {
+    if (g.do_wgridding) {
+      out[q] = dirty[q] * (T)corr[q];
+    } else {
+      int i = (int)(q / g.ny), j = (int)(q - (uint64_t)i * g.ny);
+      int iu = g.nx / 2 - min(i, g.nx - i), iv = g.ny / 2 - min(j, g.ny - j);
+      out[q] = dirty[q] * (T)(cfu[iu] * cfv[iv]);
+    }
+  }
+}
+
+// The corrected image times plane p's w-screen, placed on the (zeroed) grid
+// at the image rows and columns (image_to_grid, wgridder.rs:2937-2963).
+template <class T>
+__global__ void k_place(const __grid_constant__ Geom<T> g, const T* __restrict__ img, int p,
+                        cplx<T>* __restrict__ grid) {
+  uint64_t npix = (uint64_t)g.nx * g.ny;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < npix; q += (uint64_t)gridDim.x * blockDim.x) {
+    int i = (int)(q / g.ny), j = (int)(q - (uint64_t)i * g.ny);
+    int ix = (g.nu - g.nx / 2 + i) % g.nu, jx = (g.nv - g.ny / 2 + j) % g.nv;
+    T d = img[q];
+    cplx<T> v;
+    if (g.do_wgridding) {
+      cplx<T> ph = screen<T>(g, screen_arg(g, i, j), p, false);
+      v = {d * ph.re, d * ph.im};
+    } else {
+      v = {d, (T)0};
+    }
+    grid[(size_t)ix * g.nv + jx] = v;
+  }
+}
+
+template <class T>
+__global__ void k_pixels(const __grid_constant__ Geom<T> g, const double* __restrict__ uvw,
+                         const double* __restrict__ foc, Inputs in, int with_vis, int64_t* __restrict__ iu0,
+                         int64_t* __restrict__ iv0) {
+  uint64_t n = g.nrow * g.nchan;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (is_active<T>(in, with_vis != 0, i)) {
+      bin_of(g, uvw, foc, (uint32_t)i, &iu0[i], &iv0[i]);
+    } else {
+      iu0[i] = -1;
+      iv0[i] = -1;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ cuFFT plans
+
+template <class T>
+struct FftTraits;
+template <>
+struct FftTraits<float> {
+  static constexpr cufftType type = CUFFT_C2C;
+  static cufftResult exec(cufftHandle h, cplx<float>* p, int dir) {
+    return cufftExecC2C(h, reinterpret_cast<cufftComplex*>(p), reinterpret_cast<cufftComplex*>(p), dir);
+  }
+};
+template <>
+struct FftTraits<double> {
+  static constexpr cufftType type = CUFFT_Z2Z;
+  static cufftResult exec(cufftHandle h, cplx<double>* p, int dir) {
+    return cufftExecZ2Z(h, reinterpret_cast<cufftDoubleComplex*>(p), reinterpret_cast<cufftDoubleComplex*>(p), dir);
+  }
+};
+
+struct FftPair {
+  cufftHandle rows = 0, cols = 0;
+  std::mutex mu;
+};
+
+void check_fft(cufftResult r, const char* what) {
+  if (r != CUFFT_SUCCESS) throw DeviceError(std::string("cuFFT ") + what + " failed (" + std::to_string((int)r) + ")");
+}
+
+// Row transforms (length nv, nu rows) and image-column transforms (length nu,
+// ny/2 columns of stride nv) of one grid size, per device, kept for the life
+// of the process.
+template <class T>
+FftPair& fft_plans(int nu, int nv, int ny) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int>, std::unique_ptr<FftPair>> cache;
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "device");
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_tuple(dev, nu, nv, ny);
+  auto& slot = cache[key];
+  if (!slot) {
+    auto p = std::make_unique<FftPair>();
+    int n_row[1] = {nv};
+    check_fft(cufftPlanMany(&p->rows, 1, n_row, nullptr, 1, nv, nullptr, 1, nv, FftTraits<T>::type, nu), "row plan");
+    int n_col[1] = {nu};
+    int emb[1] = {nu};
+    check_fft(cufftPlanMany(&p->cols, 1, n_col, emb, nv, 1, emb, nv, 1, FftTraits<T>::type, ny / 2), "column plan");
+    slot = std::move(p);
+  }
+  return *slot;
+}
+
+// The image-column transforms of one plane: columns [nv - ny/2, nv) and [0, ny/2).
+template <class T>
+void fft_cols(FftPair& f, cplx<T>* plane, int nv, int ny, int dir, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(f.mu);
+  check_fft(cufftSetStream(f.cols, s), "stream");
+  check_fft(FftTraits<T>::exec(f.cols, plane + (nv - ny / 2), dir), "columns");
+  check_fft(FftTraits<T>::exec(f.cols, plane, dir), "columns");
+}
+
+template <class T>
+void fft_rows(FftPair& f, cplx<T>* plane, int dir, cudaStream_t s) {
+  std::lock_guard<std::mutex> lock(f.mu);
+  check_fft(cufftSetStream(f.rows, s), "stream");
+  check_fft(FftTraits<T>::exec(f.rows, plane, dir), "rows");
+}
+
+template <class T, int S>
+void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, const Inputs& in, int mode,
+                 const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
+                 const uint32_t* ntasks, cplx<T>* grids, int pg0, int npg, int gmax, int* err) {
+  check_cuda(cudaFuncSetAttribute(k_grid<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
+  k_grid<T, S><<<nblocks, GRID_THREADS, smem, s>>>(g, in, mode, uvw, foc, sorted, tasks, ntasks, grids, pg0, npg,
+                                                   gmax, err);
+  check_cuda(cudaGetLastError(), "grid kernel");
+}
+
+template <class T, int S>
+void launch_degrid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, const Inputs& wts,
+                   const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
+                   const uint32_t* ntasks, const cplx<T>* grids, int pg0, int npg, int gmax, cplx<T>* vis,
+                   int first, int last, int* err) {
+  check_cuda(cudaFuncSetAttribute(k_degrid<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
+  k_degrid<T, S><<<nblocks, GRID_THREADS, smem, s>>>(g, wts, uvw, foc, sorted, tasks, ntasks, grids, pg0, npg, gmax,
+                                                     vis, first, last, err);
+  check_cuda(cudaGetLastError(), "degrid kernel");
+}
+
+// Dispatch on the support (the reference's with_supp!, wgridder.rs:2225-2244).
+template <class F>
+void with_supp_float(int supp, F&& f) {
+  switch (supp) {
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 5: f(std::integral_constant<int, 5>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 7: f(std::integral_constant<int, 7>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    default: throw InvalidArgument("kernel support outside 4..=8 in single precision");
+  }
+}
+template <class F>
+void with_supp_double(int supp, F&& f) {
+  switch (supp) {
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 5: f(std::integral_constant<int, 5>{}); break;
+    case 6: f(std::integral_constant<int, 6>{}); break;
+    case 7: f(std::integral_constant<int, 7>{}); break;
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 9: f(std::integral_constant<int, 9>{}); break;
+    case 10: f(std::integral_constant<int, 10>{}); break;
+    case 11: f(std::integral_constant<int, 11>{}); break;
+    case 12: f(std::integral_constant<int, 12>{}); break;
+    case 13: f(std::integral_constant<int, 13>{}); break;
+    case 14: f(std::integral_constant<int, 14>{}); break;
+    case 15: f(std::integral_constant<int, 15>{}); break;
+    case 16: f(std::integral_constant<int, 16>{}); break;
+    default: throw InvalidArgument("kernel support outside 4..=16");
+  }
+}
+}  // namespace
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw DeviceError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
+  if (this != &o) {
+    release();
+    p_ = o.p_;
+    n_ = o.n_;
+    s_ = o.s_;
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  return *this;
+}
+
+void DevBuf::alloc(size_t bytes, cudaStream_t s) {
+  release();
+  if (bytes == 0) return;
+  check_cuda(cudaMallocAsync(&p_, bytes, s), "device memory");
+  n_ = bytes;
+  s_ = s;
+}
+
+void DevBuf::release() {
+  if (p_) cudaFreeAsync(p_, s_);
+  p_ = nullptr;
+  n_ = 0;
+}
+
+int max_window_planes(int L, size_t cell_bytes) {
+  size_t per = (size_t)L * L * cell_bytes;
+  return (int)std::max<size_t>(1, SMEM_WINDOW_BYTES / per);
+}
+
+template <class T>
+Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw_dev, const double* freq_host,
+              const Inputs& act, bool with_vis, cudaStream_t s)
+    : o_(o), nrow_(nrow), nchan_(nchan), n_(nrow * nchan) {
+  check_common(o, nrow, nchan);
+  if (n_ >= 0xffffffffull) throw InvalidArgument("too many visibilities for one call (at most 2^32 - 2)");
+  recentring(o, r_l_, r_m_);
+  std::vector<double> foc = f_over_c(freq_host, nchan);
+  uvw_.alloc(nrow * 3 * sizeof(double), s);
+  foc_.alloc(nchan * sizeof(double), s);
+  if (nrow) check_cuda(cudaMemcpyAsync(uvw_.get(), uvw_dev, nrow * 3 * sizeof(double), cudaMemcpyDeviceToDevice, s), "copy uvw");
+  check_cuda(cudaMemcpyAsync(foc_.get(), foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, s), "copy freq");
+  err_.alloc(sizeof(int), s);
+  check_cuda(cudaMemsetAsync(err_.get(), 0, sizeof(int), s), "memset");
+  // Scan.
+  DevBuf so(sizeof(ScanOut), s);
+  ScanOut init{0, 0, 0, 0};
+  const double big = 1e300;
+  std::memcpy(&init.lo_bits, &big, sizeof(big));
+  check_cuda(cudaMemcpyAsync(so.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s), "copy");
+  double fw = o.flip_w ? 1.0 : -1.0;
+  if (n_) {
+    k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw_.as<double>(),
+                                                  foc_.as<double>(), fw, act, with_vis ? 1 : 0, so.as<ScanOut>());
+    check_cuda(cudaGetLastError(), "scan kernel");
+  }
+  ScanOut r;
+  check_cuda(cudaMemcpyAsync(&r, so.get(), sizeof(r), cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaStreamSynchronize(s), "scan");
+  nvis_ = r.count;
+  double wmin_d = 1e300, wmax_d = -1e300;
+  if (r.finite) {
+    std::memcpy(&wmin_d, &r.lo_bits, sizeof(double));
+    std::memcpy(&wmax_d, &r.hi_bits, sizeof(double));
+  }
+  if (nvis_ == 0) {
+    std::memset(&info_, 0, sizeof(info_));
+    return;
+  }
+  make_geom<T>(o, nrow, nchan, nvis_, wmin_d, wmax_d, r_l_, r_m_, g_, info_, kernel_);
+  build_layout(act, with_vis, s);
+}
+
+template <class T>
+void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
+  ntiles_ = (size_t)g_.ntu * g_.ntv;
+  nbins_ = ntiles_ * (size_t)g_.nbuckets;
+  if (nbins_ >= 0xffffffffull) throw InvalidArgument("too many uv tiles and w-planes for one call");
+  key_.alloc(n_ * 4, s);
+  starts_.alloc((nbins_ + 1) * 4, s);
+  check_cuda(cudaMemsetAsync(starts_.get(), 0, (nbins_ + 1) * 4, s), "memset");
+  k_bin_count<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act,
+                                                      with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>());
+  check_cuda(cudaGetLastError(), "bin count");
+  exclusive_scan(starts_.as<uint32_t>(), starts_.as<uint32_t>(), nbins_ + 1, s);
+  {
+    DevBuf cursor((nbins_ + 1) * 4, s);
+    check_cuda(cudaMemcpyAsync(cursor.get(), starts_.get(), (nbins_ + 1) * 4, cudaMemcpyDeviceToDevice, s), "copy");
+    sorted_.alloc(nvis_ * 4, s);
+    k_bin_scatter<<<blocks_for(n_, 256), 256, 0, s>>>(n_, key_.as<uint32_t>(), cursor.as<uint32_t>(),
+                                                       sorted_.as<uint32_t>());
+    check_cuda(cudaGetLastError(), "bin scatter");
+  }
+  // Tasks.
+  max_tasks_ = nvis_ / TASK_CHUNK + ntiles_ + 1;
+  DevBuf ntask((ntiles_ + 1) * 4, s);
+  k_task_count<<<(unsigned)((ntiles_ + 1 + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(), (uint32_t)g_.nbuckets,
+                                                                     (uint32_t)ntiles_, ntask.as<uint32_t>());
+  check_cuda(cudaGetLastError(), "tasks");
+  exclusive_scan(ntask.as<uint32_t>(), ntask.as<uint32_t>(), ntiles_ + 1, s);
+  tasks_.alloc(max_tasks_ * sizeof(Task), s);
+  ntasks_.alloc(4, s);
+  k_task_emit<<<(unsigned)((ntiles_ + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(), (uint32_t)g_.nbuckets,
+                                                                (uint32_t)ntiles_, ntask.as<uint32_t>(),
+                                                                tasks_.as<Task>(), ntasks_.as<uint32_t>());
+  check_cuda(cudaGetLastError(), "tasks");
+  corrections(s);
+}
+
+template <class T>
+void Plan<T>::corrections(cudaStream_t s) {
+  // cfu, cfv tables on the host (corfunc_table, wgridder.rs:353-355).
+  size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
+  std::vector<double> tab(nu2 + nv2);
+  for (size_t i = 0; i < nu2; i++) tab[i] = kernel_->corfunc((double)i * (1.0 / (double)g_.nu));
+  for (size_t j = 0; j < nv2; j++) tab[nu2 + j] = kernel_->corfunc((double)j * (1.0 / (double)g_.nv));
+  size_t npix = (size_t)g_.nx * g_.ny;
+  corr_.alloc((nu2 + nv2 + (g_.do_wgridding ? npix : 0)) * sizeof(double), s);
+  check_cuda(cudaMemcpyAsync(corr_.get(), tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, s), "copy");
+  // The stream must not outlive `tab`.
+  check_cuda(cudaStreamSynchronize(s), "corrections");
+  if (g_.do_wgridding) {
+    CorrNodes cn{};
+    cn.n = (int)kernel_->corr_x.size();
+    if (cn.n > 32) throw DeviceError("correction quadrature too long");
+    for (int i = 0; i < cn.n; i++) {
+      cn.x[i] = kernel_->corr_x[i];
+      cn.w[i] = kernel_->corr_w[i];
+    }
+    double* base = corr_.as<double>();
+    k_corr<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, cn, base, base + nu2, base + nu2 + nv2);
+    check_cuda(cudaGetLastError(), "corrections");
+  }
+}
+
+template <class T>
+size_t Plan<T>::plane_group(size_t cell_bytes) const {
+  size_t nplanes = (size_t)std::max(g_.nplanes, 1);
+  size_t plane = (size_t)g_.nu * g_.nv * cell_bytes;
+  size_t freeb = 0, total = 0;
+  check_cuda(cudaMemGetInfo(&freeb, &total), "memory info");
+  size_t budget = std::min<size_t>(freeb / 2, (size_t)64 << 30);
+  size_t group = std::max<size_t>(1, budget / plane);
+  return std::min(group, nplanes);
+}
+
+template <class T>
+void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s) {
+  size_t npix = (size_t)o_.nx * o_.ny;
+  if (nvis_ == 0) {
+    check_cuda(cudaMemsetAsync(image, 0, npix * sizeof(T), s), "memset");
+    return;
+  }
+  const size_t cell = sizeof(cplx<T>);
+  const size_t nplanes = (size_t)std::max(g_.nplanes, 1);
+  const size_t group = plane_group(cell);
+  const size_t plane = (size_t)g_.nu * g_.nv;
+  DevBuf grids(group * plane * cell, s);
+  DevBuf acc(group < nplanes ? npix * sizeof(T) : 0, s);
+  FftPair& fft = fft_plans<T>(g_.nu, g_.nv, g_.ny);
+  const int gmax = std::min<int>(max_window_planes(g_.L, 2 * sizeof(T)), (int)std::min<size_t>(nplanes, 64));
+  const int smem = gmax * g_.L * g_.L * 2 * (int)sizeof(T);
+  const double* corr = corr_.as<double>();
+  const size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
+  for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
+    int n = (int)std::min(group, nplanes - pg0);
+    check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
+    auto run = [&](auto S) {
+      launch_grid<T, decltype(S)::value>(smem, (unsigned)max_tasks_, s, g_, data, (int)mode, uvw_.as<double>(),
+                                         foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>(),
+                                         ntasks_.as<uint32_t>(), grids.as<cplx<T>>(), (int)pg0, n, gmax,
+                                         err_.as<int>());
+    };
+    if constexpr (sizeof(T) == 4)
+      with_supp_float(g_.supp, run);
+    else
+      with_supp_double(g_.supp, run);
+    for (int p = 0; p < n; p++) {
+      cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
+      fft_rows<T>(fft, pl, CUFFT_INVERSE, s);
+      fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_INVERSE, s);
+    }
+    bool first = pg0 == 0, last = pg0 + n >= nplanes;
+    k_project<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, grids.as<cplx<T>>(), (int)pg0, n, acc.as<T>(), first,
+                                                       last, g_.do_wgridding ? corr + nu2 + nv2 : nullptr, corr,
+                                                       corr + nu2, image);
+    check_cuda(cudaGetLastError(), "project");
+  }
+}
+
+template <class T>
+void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s) {
+  check_cuda(cudaMemsetAsync(vis, 0, n_ * 2 * sizeof(T), s), "memset");
+  if (nvis_ == 0) return;
+  const size_t npix = (size_t)o_.nx * o_.ny;
+  const size_t cell = sizeof(cplx<T>);
+  const size_t nplanes = (size_t)std::max(g_.nplanes, 1);
+  const size_t group = plane_group(cell);
+  const size_t plane = (size_t)g_.nu * g_.nv;
+  DevBuf grids(group * plane * cell, s);
+  DevBuf img(npix * sizeof(T), s);
+  FftPair& fft = fft_plans<T>(g_.nu, g_.nv, g_.ny);
+  const double* corr = corr_.as<double>();
+  const size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
+  k_correct_input<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, image, g_.do_wgridding ? corr + nu2 + nv2 : nullptr,
+                                                           corr, corr + nu2, img.as<T>());
+  check_cuda(cudaGetLastError(), "correct");
+  const int gmax = std::min<int>(max_window_planes(g_.L, sizeof(cplx<T>)), (int)std::min<size_t>(nplanes, 64));
+  const int smem = gmax * g_.L * g_.L * (int)sizeof(cplx<T>);
+  for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
+    int n = (int)std::min(group, nplanes - pg0);
+    check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
+    for (int p = 0; p < n; p++) {
+      cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
+      k_place<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, img.as<T>(), (int)pg0 + p, pl);
+      check_cuda(cudaGetLastError(), "place");
+      fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_FORWARD, s);
+      fft_rows<T>(fft, pl, CUFFT_FORWARD, s);
+    }
+    bool first = pg0 == 0, last = pg0 + n >= nplanes;
+    auto run = [&](auto S) {
+      launch_degrid<T, decltype(S)::value>(smem, (unsigned)max_tasks_, s, g_, wts, uvw_.as<double>(),
+                                           foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>(),
+                                           ntasks_.as<uint32_t>(), grids.as<cplx<T>>(), (int)pg0, n, gmax,
+                                           reinterpret_cast<cplx<T>*>(vis), first, last, err_.as<int>());
+    };
+    if constexpr (sizeof(T) == 4)
+      with_supp_float(g_.supp, run);
+    else
+      with_supp_double(g_.supp, run);
+  }
+}
+
+template <class T>
+int Plan<T>::kernel_errors(cudaStream_t s) const {
+  int e = 0;
+  if (!err_.get()) return 0;
+  check_cuda(cudaMemcpyAsync(&e, err_.get(), sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaStreamSynchronize(s), "stream");
+  return e;
+}
+
+template <class T>
+void Plan<T>::export_binning(uint32_t* key_host, uint32_t* sorted_host, cudaStream_t s) const {
+  if (nvis_ == 0) return;
+  check_cuda(cudaMemcpyAsync(key_host, key_.get(), n_ * 4, cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaMemcpyAsync(sorted_host, sorted_.get(), nvis_ * 4, cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaStreamSynchronize(s), "copy");
+}
+
+template <class T>
+void Plan<T>::export_pixels(const Inputs& act, bool with_vis, int64_t* iu0_host, int64_t* iv0_host,
+                            cudaStream_t s) const {
+  if (nvis_ == 0) return;
+  DevBuf a(n_ * 8, s), b(n_ * 8, s);
+  k_pixels<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act, with_vis ? 1 : 0,
+                                                  a.as<int64_t>(), b.as<int64_t>());
+  check_cuda(cudaGetLastError(), "pixels");
+  check_cuda(cudaMemcpyAsync(iu0_host, a.get(), n_ * 8, cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaMemcpyAsync(iv0_host, b.get(), n_ * 8, cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaStreamSynchronize(s), "copy");
+}
+
+template class Plan<float>;
+template class Plan<double>;
+
+}  // namespace wg

@@ -1,0 +1,117 @@
+// The device-resident plan of a gridder call: scan, kernel choice, the
+// visibility binning by (uv tile, first w-plane), and the task list of the
+// gridding and degridding kernels. A plan is built once per set of
+// coordinates, weights and mask and can then grid and degrid any number of
+// times (the reference's `Prepared`, core/src/wgridder.rs:3170-3499).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "wgrid_common.h"
+#include "wgrid_device.cuh"
+#include "wgrid_setup.h"
+
+namespace wg {
+
+// A gridding task: visibilities [k0, k1) of the sorted order, all in one uv
+// tile, with first planes in [plo, phi].
+struct Task {
+  uint32_t tile, k0, k1;
+  uint16_t plo, phi;
+};
+
+// Failures inside a library call that are not the caller's arguments
+// (CUDA errors, device memory) map to status 2.
+struct DeviceError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void check_cuda(cudaError_t e, const char* what);
+
+// Device memory taken from the stream-ordered pool and returned on release.
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(size_t bytes, cudaStream_t s) { alloc(bytes, s); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_) { o.p_ = nullptr; }
+  DevBuf& operator=(DevBuf&& o) noexcept;
+  ~DevBuf() { release(); }
+  void alloc(size_t bytes, cudaStream_t s);
+  void release();
+  template <class U>
+  U* as() const { return reinterpret_cast<U*>(p_); }
+  void* get() const { return p_; }
+  size_t size() const { return n_; }
+
+ private:
+  void* p_ = nullptr;
+  size_t n_ = 0;
+  cudaStream_t s_ = nullptr;
+};
+
+// How a gridding pass forms each visibility's value.
+enum ValueMode : int { VALUE_DATA = 0, VALUE_UNIT = 1 };
+
+template <class T>
+class Plan {
+ public:
+  // Scan the active set (`with_vis`: |vis|^2 wgt mask != 0, else wgt mask
+  // != 0), choose kernel and grid, and bin the active visibilities. `uvw`
+  // and the arrays of `act` are device pointers; `freq` is on the host.
+  Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw_dev, const double* freq_host,
+       const Inputs& act, bool with_vis, cudaStream_t s);
+
+  bool empty() const { return nvis_ == 0; }
+  const PlanInfo& info() const { return info_; }
+  size_t nvis() const { return nvis_; }
+  const Geom<T>& geom() const { return g_; }
+
+  // vis2dirty into `image` (nx * ny, device): `data` gives the data and the
+  // weights; VALUE_UNIT grids unit visibilities (the PSF).
+  void grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s);
+  // dirty2vis of `image` into `vis` (nrow * nchan interleaved complex,
+  // device, overwritten; inactive visibilities zero), times the weights of
+  // `wts`.
+  void degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s);
+
+  // Waits for `s` and returns the inconsistencies the kernels flagged (0: none).
+  int kernel_errors(cudaStream_t s) const;
+
+  // For the tests: per visibility (row-major) the bin key tile * nbuckets +
+  // first plane (0xffffffff inactive), and the sorted order.
+  void export_binning(uint32_t* key_host, uint32_t* sorted_host, cudaStream_t s) const;
+  // Per visibility iu0, iv0 (int64) from the device arithmetic, for the tests.
+  void export_pixels(const Inputs& act, bool with_vis, int64_t* iu0_host, int64_t* iv0_host, cudaStream_t s) const;
+
+ private:
+  void build_layout(const Inputs& act, bool with_vis, cudaStream_t s);
+  void corrections(cudaStream_t s);
+  size_t plane_group(size_t cell_bytes) const;
+
+  WgridderOptions o_;
+  size_t nrow_, nchan_, n_;
+  size_t nvis_ = 0;
+  double r_l_ = 0, r_m_ = 0;
+  Geom<T> g_;
+  PlanInfo info_{};
+  EsKernel* kernel_ = nullptr;
+  DevBuf uvw_, foc_;
+  DevBuf key_;      // u32 per visibility: bin or 0xffffffff
+  DevBuf starts_;   // u32 per bin + 1: exclusive offsets
+  DevBuf sorted_;   // u32 per active visibility: linear index
+  DevBuf tasks_;    // Task, at most max_tasks_
+  DevBuf ntasks_;   // u32: tasks in use
+  DevBuf corr_;     // double per pixel: the global correction
+  DevBuf err_;      // int: kernel-detected inconsistencies
+  size_t nbins_ = 0, ntiles_ = 0, max_tasks_ = 0;
+};
+
+// The largest shared-memory tile window (planes) per CTA.
+int max_window_planes(int L, size_t cell_bytes);
+
+}  // namespace wg

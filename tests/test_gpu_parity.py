@@ -1,0 +1,252 @@
+"""Parity of the CUDA path (through `rang._core`, the C ABI) with the CPU
+oracle and the FP64 DFT.
+
+Tolerances: the integer binning (iu0, iv0, tile, first plane, plan) must be
+bit-identical to the oracle's; images and visibilities agree with the
+oracle's to 1e-10 (f64) and 2e-5 (f32) relative L-inf (the two differ only in
+accumulation order and FFT rounding), and with the DFT to the reference's
+own gates (10 eps, research/df1-wgridder.md:179-203)."""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from cases import lcg_case, meerkat_like, rel_linf, small_case
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+TOL = {True: 2e-5, False: 1e-10}
+
+
+@pytest.fixture(scope="module")
+def cw():
+    from rang import core_wgridder
+
+    return core_wgridder
+
+
+def _info_equal(a, b):
+    assert a.keys() == b.keys()
+    for k in a:
+        assert a[k] == b[k], (k, a[k], b[k])
+
+
+def test_vis2dirty_matches_dft_both_precisions(cw):
+    # reference tests/test_core_wgridder.py:75-95
+    uvw, freq, vis, wgt, nx, ny, dx = small_case()
+    ref = oracle.dft_dirty(uvw, freq, vis * wgt, nx, ny, dx, dx)
+    common = dict(uvw=uvw, freq=freq, npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx)
+    d64, info = cw.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-9, return_info=True, **common)
+    assert rel_linf(d64, ref) < 1e-8
+    assert info["nvis"] == vis.size and info["nplanes"] > info["supp"]
+    _, oinfo = oracle.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-9, return_info=True, **common)
+    _info_equal(info, oinfo)
+    d32 = cw.vis2dirty(vis=vis.astype(np.complex64), wgt=wgt.astype(np.float32), epsilon=1e-4, **common)
+    assert d32.dtype == np.float32 and rel_linf(d32, ref) < 1e-3
+
+
+def test_lcg_cases_match_dft(cw):
+    # core/src/wgridder.rs:4667-4686
+    for nx, ny, field, wmax in [(32, 32, 0.2, 500.0), (32, 16, 0.05, 50.0)]:
+        uvw, freq, vis, wgt, dx = lcg_case(nx, ny, field, wmax, 60, 7)
+        d = cw.vis2dirty(uvw=uvw, freq=freq, vis=vis, wgt=wgt, npix_x=nx, npix_y=ny, pixsize_x=dx,
+                         pixsize_y=dx, epsilon=1e-9)
+        assert rel_linf(d, oracle.dft_dirty(uvw, freq, vis * wgt, nx, ny, dx, dx)) < 1e-8
+
+
+def test_adjoint_and_dirty2vis(cw):
+    # reference tests/test_core_wgridder.py:98-125
+    uvw, freq, vis, wgt, nx, ny, dx = small_case(seed=8)
+    x = np.random.default_rng(1).standard_normal((nx, ny))
+    common = dict(uvw=uvw, freq=freq, wgt=wgt, pixsize_x=dx, pixsize_y=dx, epsilon=1e-9)
+    ax = cw.dirty2vis(dirty=x, **common)
+    aty = cw.vis2dirty(vis=vis, npix_x=nx, npix_y=ny, **common)
+    lhs = np.real(np.vdot(ax, vis))
+    assert abs(lhs - np.sum(x * aty)) / (np.linalg.norm(ax) * np.linalg.norm(vis)) < 1e-12
+    img = np.zeros((nx, ny))
+    img[5, 20] = 2.0
+    got = cw.dirty2vis(dirty=img, **common)
+    assert rel_linf(got, oracle.dft_vis(uvw, freq, img, dx, dx) * wgt) < 1e-8
+
+
+def test_zero_weights_and_bad_input(cw):
+    # reference tests/test_core_wgridder.py:128-147
+    uvw, freq, vis, wgt, nx, ny, dx = small_case(nrow=6)
+    common = dict(uvw=uvw, freq=freq, npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx)
+    empty, info = cw.vis2dirty(vis=vis, wgt=np.zeros_like(wgt), epsilon=1e-6, return_info=True, **common)
+    assert not empty.any() and info["nvis"] == 0
+    with pytest.raises(ValueError, match="ascending"):
+        cw.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-6, **{**common, "freq": freq[::-1]})
+    with pytest.raises(ValueError, match="kernel"):
+        cw.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-14, **common)
+    with pytest.raises(ValueError, match="even"):
+        cw.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-6, **{**common, "npix_x": 31})
+    v = cw.dirty2vis(dirty=np.ones((nx, ny)), uvw=uvw, freq=freq, wgt=np.zeros_like(wgt), pixsize_x=dx,
+                     pixsize_y=dx, epsilon=1e-6)
+    assert not v.any()
+
+
+@pytest.fixture(scope="module")
+def df1():
+    data = np.load(GOLDEN / "df1_cases.npz")
+    names = sorted({k.split("/")[0] for k in data.files})
+    return {n: {k.split("/")[1]: data[k] for k in data.files if k.startswith(n + "/")} for n in names}
+
+
+@pytest.mark.parametrize("eps,single", [(1e-5, True), (1e-5, False), (1e-7, False), (1e-9, False)])
+def test_golden_df1_cases(cw, df1, eps, single):
+    """Within 10 eps of the golden FP64 DFT, and equal to the oracle to
+    rounding, in both directions."""
+    for name, c in df1.items():
+        nx, ny, dx, dy = int(c["nx"]), int(c["ny"]), float(c["dx"]), float(c["dy"])
+        vis = c["vis"].astype(np.complex64) if single else c["vis"]
+        wgt = c["wgt"].astype(np.float32) if single else c["wgt"]
+        kw = dict(uvw=c["uvw"], freq=c["freq"], wgt=wgt, pixsize_x=dx, pixsize_y=dy, epsilon=eps)
+        d, info = cw.vis2dirty(vis=vis, npix_x=nx, npix_y=ny, return_info=True, **kw)
+        od, oinfo = oracle.vis2dirty(vis=vis, npix_x=nx, npix_y=ny, return_info=True, **kw)
+        _info_equal(info, oinfo)
+        assert rel_linf(d, c["dft_dirty"]) < 10 * eps, name
+        assert rel_linf(d, od) < TOL[single], name
+        img = c["image"].astype(np.float32) if single else c["image"]
+        v = cw.dirty2vis(dirty=img, **kw)
+        assert rel_linf(v, c["dft_vis"]) < 10 * eps, name
+        assert rel_linf(v, oracle.dirty2vis(dirty=img, **kw)) < TOL[single], name
+
+
+OPTION_SETS = [
+    {},
+    {"flip_u": True, "flip_v": True},
+    {"flip_w": True},
+    {"center_x": 0.01, "center_y": -0.02},
+    {"center_x": -0.005, "flip_u": True, "allow_nshift": False},
+    {"divide_by_n": True},
+    {"do_wgridding": False},
+    {"sigma_min": 1.5, "sigma_max": 2.0},
+]
+
+
+@pytest.mark.parametrize("single", [True, False])
+@pytest.mark.parametrize("opts", OPTION_SETS, ids=lambda o: ",".join(o) or "default")
+def test_options_match_oracle(cw, opts, single):
+    uvw, freq = meerkat_like(nant=16, ntime=6, nchan=8, seed=3)
+    rng = np.random.default_rng(11)
+    shape = (uvw.shape[0], freq.size)
+    vis = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+    wgt = rng.uniform(0.5, 1.5, shape)
+    mask = (rng.uniform(size=shape) > 0.2).astype(np.uint8)
+    if single:
+        vis, wgt = vis.astype(np.complex64), wgt.astype(np.float32)
+    nx, ny, dx = 96, 64, 2.0e-4
+    eps = 1e-5 if single else 1e-10
+    kw = dict(uvw=uvw, freq=freq, wgt=wgt, mask=mask, pixsize_x=dx, pixsize_y=dx * 1.1, epsilon=eps, **opts)
+    d, info = cw.vis2dirty(vis=vis, npix_x=nx, npix_y=ny, return_info=True, **kw)
+    od, oinfo = oracle.vis2dirty(vis=vis, npix_x=nx, npix_y=ny, return_info=True, **kw)
+    _info_equal(info, oinfo)
+    assert rel_linf(d, od) < TOL[single]
+    x = rng.standard_normal((nx, ny)).astype(np.float32 if single else np.float64)
+    v = cw.dirty2vis(dirty=x, **kw)
+    ov = oracle.dirty2vis(dirty=x, **kw)
+    assert rel_linf(v, ov) < TOL[single]
+    assert not v[mask == 0].any()
+
+
+@pytest.mark.parametrize("single", [True, False])
+def test_binning_is_bit_exact(cw, single):
+    """iu0, iv0, tile and first plane of every visibility equal the oracle's
+    (the reference's index arithmetic), and the GPU's order is the oracle's
+    up to the order inside a (tile, plane) bin."""
+    uvw, freq = meerkat_like(nant=24, ntime=8, nchan=32, seed=5)
+    rng = np.random.default_rng(2)
+    shape = (uvw.shape[0], freq.size)
+    vis = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+    vis.ravel()[::17] = 0.0
+    wgt = rng.uniform(0.5, 1.5, shape)
+    wgt.ravel()[::13] = 0.0
+    for opts in ({}, {"center_x": 0.003, "flip_v": True}, {"do_wgridding": False}):
+        for with_vis in (True, False):
+            kw = dict(uvw=uvw, freq=freq, vis=vis, wgt=wgt, npix_x=512, npix_y=384, pixsize_x=1.5e-5,
+                      pixsize_y=1.5e-5, epsilon=1e-5 if single else 1e-7, single=single, with_vis=with_vis,
+                      **opts)
+            g = cw.binning(**kw)
+            o = oracle.binning(**kw)
+            _info_equal(g["info"], o["info"])
+            nb = max(o["info"]["nplanes"], 1)
+            act = o["tile"] >= 0
+            okey = np.where(act, o["tile"] * nb + o["minplane"], 0xFFFFFFFF).astype(np.uint32)
+            assert np.array_equal(g["key"], okey)
+            assert np.array_equal(g["iu0"][act], o["iu0"][act])
+            assert np.array_equal(g["iv0"][act], o["iv0"][act])
+            gs = g["sorted"].astype(np.int64)
+            assert gs.size == o["sorted"].size
+            gk = g["key"][gs]
+            assert np.all(np.diff(gk.astype(np.int64)) >= 0)
+            assert np.array_equal(gs[np.lexsort((gs, gk))], o["sorted"].astype(np.int64))
+
+
+def test_psf_mode_and_weight_kinds(cw):
+    # reference tests/test_core_wgridder.py:215-261 (to rounding: the GPU
+    # accumulates with atomics, so sums are not bit-reproducible)
+    uvw, freq, vis, wgt, nx, ny, dx = small_case(seed=21, nrow=50)
+    vis64 = vis.astype(np.complex64)
+    wgt32 = wgt.astype(np.float32)
+    wgt32[3, 1] = 0.0
+    common = dict(uvw=uvw, freq=freq, npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx, epsilon=1e-7)
+    dirty, psf = cw.dirty_psf(vis=vis64, wgt=wgt32, **common)
+    odirty, opsf = oracle.dirty_psf(vis=vis64, wgt=wgt32, **common)
+    assert rel_linf(dirty, odirty) < 1e-10 and rel_linf(psf, opsf) < 1e-10
+    sep = cw.vis2dirty(vis=vis64.astype(np.complex128), wgt=wgt32.astype(np.float64), **common)
+    assert rel_linf(dirty, sep) < 1e-12
+    b = np.random.default_rng(99).uniform(0.1, 1.1, wgt32.shape).astype(np.float32)
+    one = cw.dirty_psf(vis=vis64, wgt=wgt32 * b, single=True, **{**common, "epsilon": 1e-5})
+    two = cw.dirty_psf(vis=vis64, wgt=wgt32, wgt2=b, single=True, **{**common, "epsilon": 1e-5})
+    assert rel_linf(one[0], two[0]) < 1e-6 and rel_linf(one[1], two[1]) < 1e-6
+    x = np.random.default_rng(2).standard_normal((nx, ny))
+    kw = {k: common[k] for k in ("uvw", "freq", "pixsize_x", "pixsize_y", "epsilon")}
+    assert np.array_equal(cw.dirty2vis(dirty=x, wgt=wgt32, **kw),
+                          cw.dirty2vis(dirty=x, wgt=wgt32.astype(np.float64), **kw))
+
+
+def test_fits_image_orientation(cw):
+    """A unit point source off centre lands, after `fits_image`, at its
+    WSClean FITS pixel with value 1 (the PSF centre normalisation)."""
+    rng = np.random.default_rng(4)
+    width, scale = 48, 60.0
+    freq = np.array([1.2e9, 1.4e9])
+    lam = freq.max() / oracle.C_LIGHT
+    cell = scale * np.pi / 648000.0
+    uvw = np.stack([rng.uniform(-0.4, 0.4, 60) / cell / lam, rng.uniform(-0.4, 0.4, 60) / cell / lam,
+                    rng.uniform(-100, 100, 60) / lam], axis=1)
+    l0, m0 = 7 * cell, -4 * cell
+    n0 = np.sqrt(1 - l0**2 - m0**2) - 1
+    u, v, w = (uvw[:, i, None] * freq / oracle.C_LIGHT for i in range(3))
+    # WSClean's image is rang's with v and w flipped, transposed.
+    data = np.exp(-2j * np.pi * (u * l0 - v * m0 - w * n0)).astype(np.complex64)
+    weights = np.ones(data.shape, np.float32)
+    got = cw.fits_image(uvw, freq, data, weights, width, width, scale, epsilon=1e-7)
+    assert abs(got["psf"][width // 2, width // 2] - 1.0) < 1e-12
+    peak = np.unravel_index(np.argmax(got["dirty"]), got["dirty"].shape)
+    assert peak == (width // 2 - 4, width // 2 + 7)
+    assert abs(got["dirty"][peak] - 1.0) < 1e-5
+
+
+def test_larger_case_matches_oracle(cw):
+    """A MeerKAT-shaped case with flags at eps 1e-5 (single) and 1e-7
+    (double), against the oracle and, on a few pixels, the DFT."""
+    uvw, freq = meerkat_like(nant=64, ntime=8, nchan=16, seed=1)
+    rng = np.random.default_rng(5)
+    shape = (uvw.shape[0], freq.size)
+    vis = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    mask = (rng.uniform(size=shape) > 0.2).astype(np.uint8)
+    nx = ny = 256
+    dx = 1.5 * np.pi / 648000.0
+    for single, eps in ((True, 1e-5), (False, 1e-7)):
+        v = vis.astype(np.complex64) if single else vis
+        kw = dict(uvw=uvw, freq=freq, mask=mask, pixsize_x=dx, pixsize_y=dx, epsilon=eps)
+        d = cw.vis2dirty(vis=v, npix_x=nx, npix_y=ny, **kw)
+        od = oracle.vis2dirty(vis=v, npix_x=nx, npix_y=ny, **kw)
+        assert rel_linf(d, od) < TOL[single] * 5
+        x = rng.standard_normal((nx, ny)).astype(np.float32 if single else np.float64)
+        assert rel_linf(cw.dirty2vis(dirty=x, **kw), oracle.dirty2vis(dirty=x, **kw)) < TOL[single] * 5

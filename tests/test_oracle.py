@@ -1,0 +1,167 @@
+"""The CPU oracle against the reference's own known answers and the golden
+FP64 DFT fixtures (no GPU). These pin the oracle before it is trusted as the
+checker of the CUDA path."""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from cases import lcg_case, rel_linf, small_case
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+KERNEL_ROWS_SHA256 = "0427f5940e0faa20efc615a1f4fb73eadbf754465f483f216c11b317f4ae3831"
+
+
+def test_kernel_table_matches_pinned_rows():
+    # reference tests/test_core_wgridder.py:55-73 and wgridder.rs:4628-4640
+    pinned = json.loads((GOLDEN / "kernel_rows.json").read_text())
+    assert pinned["sha256"] == KERNEL_ROWS_SHA256
+    table = oracle.kernel_table()
+    assert len(table) == 939
+    assert [tuple(r) for r in pinned["rows"]] == table
+    assert table[0] == (4, 1.2, 0.027638471, 1.30709338717990464, 0.588199361165364421, 2, True)
+    assert table[-1][0] == 16 and table[-1][5] == 3 and table[-1][6] is False
+
+
+def test_good_size_known_answers():
+    # wgridder.rs:4635-4639
+    assert [oracle.good_size(n) for n in (13, 97, 181, 1025, 7)] == [14, 98, 189, 1029, 7]
+
+
+def test_gauss_legendre_integrates_polynomials():
+    # wgridder.rs:4643-4651
+    x, w = oracle.gauss_legendre(10)
+    assert abs(np.sum(w * x**8) - 2.0 / 9.0) < 1e-14
+    assert abs(w.sum() - 2.0) < 1e-14
+
+
+@pytest.mark.parametrize("index", [0, 200, 500, 938])
+def test_polynomial_kernel_matches_es(index):
+    # wgridder.rs:4653-4665
+    v = -1.0 + 2.0 * np.arange(2001) / 2000.0
+    worst = np.abs(oracle.kernel_eval(index, "poly", v) - oracle.kernel_eval(index, "phi", v)).max()
+    assert worst < max(oracle.kernel_row(index)[2], 1e-13)
+
+
+@pytest.mark.parametrize("n", [2, 12, 14, 98, 189, 2376, 1029 * 2])
+def test_fft_matches_numpy(n):
+    a = np.random.default_rng(n).standard_normal(n) + 1j * np.random.default_rng(n + 1).standard_normal(n)
+    assert np.abs(oracle.fft(a) - np.fft.fft(a)).max() < 1e-12 * n
+    assert np.abs(oracle.fft(a, inverse=True) - np.fft.ifft(a) * n).max() < 1e-12 * n
+
+
+def test_vis2dirty_matches_dft_lcg_cases():
+    # wgridder.rs:4667-4686: rel L-inf < 1e-8 at eps 1e-9
+    for nx, ny, field, wmax in [(32, 32, 0.2, 500.0), (32, 16, 0.05, 50.0)]:
+        uvw, freq, vis, wgt, dx = lcg_case(nx, ny, field, wmax, 60, 7)
+        d = oracle.vis2dirty(uvw=uvw, freq=freq, vis=vis, wgt=wgt, npix_x=nx, npix_y=ny, pixsize_x=dx,
+                             pixsize_y=dx, epsilon=1e-9)
+        assert rel_linf(d, oracle.dft_dirty(uvw, freq, vis * wgt, nx, ny, dx, dx)) < 1e-8
+
+
+def test_vis2dirty_matches_dft_both_precisions():
+    # tests/test_core_wgridder.py:75-95
+    uvw, freq, vis, wgt, nx, ny, dx = small_case()
+    ref = oracle.dft_dirty(uvw, freq, vis * wgt, nx, ny, dx, dx)
+    common = dict(uvw=uvw, freq=freq, npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx)
+    d64, info = oracle.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-9, return_info=True, **common)
+    assert rel_linf(d64, ref) < 1e-8
+    assert info["nvis"] == vis.size and info["nplanes"] > info["supp"]
+    d32 = oracle.vis2dirty(vis=vis.astype(np.complex64), wgt=wgt.astype(np.float32), epsilon=1e-4, **common)
+    assert d32.dtype == np.float32 and rel_linf(d32, ref) < 1e-3
+
+
+def test_adjoint_and_one_pixel():
+    # tests/test_core_wgridder.py:98-125
+    uvw, freq, vis, wgt, nx, ny, dx = small_case(seed=8)
+    x = np.random.default_rng(1).standard_normal((nx, ny))
+    common = dict(uvw=uvw, freq=freq, wgt=wgt, pixsize_x=dx, pixsize_y=dx, epsilon=1e-9)
+    ax = oracle.dirty2vis(dirty=x, **common)
+    aty = oracle.vis2dirty(vis=vis, npix_x=nx, npix_y=ny, **common)
+    lhs = np.real(np.vdot(ax, vis))
+    assert abs(lhs - np.sum(x * aty)) / (np.linalg.norm(ax) * np.linalg.norm(vis)) < 1e-12
+    img = np.zeros((nx, ny))
+    img[5, 20] = 2.0
+    got = oracle.dirty2vis(dirty=img, **common)
+    ref = oracle.dft_vis(uvw, freq, img, dx, dx) * wgt
+    assert rel_linf(got, ref) < 1e-8
+
+
+def test_zero_weights_and_bad_input():
+    # tests/test_core_wgridder.py:128-147
+    uvw, freq, vis, wgt, nx, ny, dx = small_case(nrow=6)
+    common = dict(uvw=uvw, freq=freq, npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx)
+    assert not oracle.vis2dirty(vis=vis, wgt=np.zeros_like(wgt), epsilon=1e-6, **common).any()
+    with pytest.raises(ValueError, match="ascending"):
+        oracle.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-6, **{**common, "freq": freq[::-1]})
+    with pytest.raises(ValueError, match="kernel"):
+        oracle.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-14, **common)
+    with pytest.raises(ValueError, match="even"):
+        oracle.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-6, **{**common, "npix_x": 31})
+
+
+def test_psf_mode_matches_separate_calls():
+    # tests/test_core_wgridder.py:215-246: bit identity of the one-pass PSF
+    uvw, freq, vis, wgt, nx, ny, dx = small_case(seed=21, nrow=50)
+    vis64 = vis.astype(np.complex64)
+    wgt32 = wgt.astype(np.float32)
+    wgt32[3, 1] = 0.0
+    common = dict(uvw=uvw, freq=freq, npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx, epsilon=1e-7)
+    dirty, psf = oracle.dirty_psf(vis=vis64, wgt=wgt32, **common)
+    sep = oracle.vis2dirty(vis=vis64.astype(np.complex128), wgt=wgt32.astype(np.float64), **common)
+    ones = np.where(wgt32 != 0, 1.0, 0.0).astype(np.complex128)
+    sep_psf = oracle.vis2dirty(vis=ones, wgt=wgt32.astype(np.float64), **common)
+    assert np.array_equal(dirty, sep) and np.array_equal(psf, sep_psf)
+
+
+def test_product_weights_match_their_product():
+    # wgridder.rs:4812-4871
+    uvw, freq, vis, wgt, dx = lcg_case(32, 24, 0.2, 400.0, 40, 7)
+    a = wgt.astype(np.float32)
+    b = np.random.default_rng(99).uniform(0.1, 1.1, a.shape).astype(np.float32)
+    b.ravel()[::7] = 0.0
+    common = dict(uvw=uvw, freq=freq, vis=vis.astype(np.complex64), npix_x=32, npix_y=24, pixsize_x=dx,
+                  pixsize_y=dx, epsilon=1e-6)
+    one = oracle.dirty_psf(wgt=a * b, return_info=True, **common)
+    two = oracle.dirty_psf(wgt=a, wgt2=b, return_info=True, **common)
+    assert np.array_equal(one[0], two[0]) and np.array_equal(one[1], two[1]) and one[2] == two[2]
+
+
+@pytest.fixture(scope="module")
+def df1():
+    data = np.load(GOLDEN / "df1_cases.npz")
+    names = sorted({k.split("/")[0] for k in data.files})
+    return {n: {k.split("/")[1]: data[k] for k in data.files if k.startswith(n + "/")} for n in names}
+
+
+@pytest.mark.parametrize("eps,single", [(1e-5, True), (1e-5, False), (1e-7, False), (1e-9, False)])
+def test_golden_df1_cases(df1, eps, single):
+    """DF1's first criterion (research/df1-wgridder.md:179-203): within 10 eps
+    of the FP64 DFT, both directions, on the four seeded cases."""
+    for name, c in df1.items():
+        nx, ny, dx, dy = int(c["nx"]), int(c["ny"]), float(c["dx"]), float(c["dy"])
+        vis = c["vis"].astype(np.complex64) if single else c["vis"]
+        wgt = c["wgt"].astype(np.float32) if single else c["wgt"]
+        d = oracle.vis2dirty(uvw=c["uvw"], freq=c["freq"], vis=vis, wgt=wgt, npix_x=nx, npix_y=ny,
+                             pixsize_x=dx, pixsize_y=dy, epsilon=eps)
+        assert rel_linf(d, c["dft_dirty"]) < 10 * eps, name
+        img = c["image"].astype(np.float32) if single else c["image"]
+        v = oracle.dirty2vis(uvw=c["uvw"], freq=c["freq"], dirty=img, wgt=wgt, pixsize_x=dx, pixsize_y=dy,
+                             epsilon=eps)
+        assert rel_linf(v, c["dft_vis"]) < 10 * eps, name
+
+
+def test_binning_is_a_stable_sort_by_tile_and_plane():
+    """The layout (wgridder.rs:1261-1376) is the active visibilities sorted by
+    (tile, first plane, row, channel)."""
+    uvw, freq, vis, wgt, nx, ny, dx = small_case(nrow=300, seed=5)
+    b = oracle.binning(uvw=uvw, freq=freq, vis=vis, wgt=wgt, npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx,
+                       epsilon=1e-5, single=True, with_vis=True)
+    nb = max(b["info"]["nplanes"], 1)
+    key = b["tile"] * nb + b["minplane"]
+    act = np.flatnonzero(b["tile"] >= 0)
+    expect = act[np.lexsort((act, key[act]))]
+    assert np.array_equal(b["sorted"], expect)
