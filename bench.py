@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Benchmark: ms2dirty + dirty2ms round trip on synthetic MeerKAT-shaped data.
+
+Workload (default): 64 antennas (2016 baselines) x 512 integrations of 8 s x
+1024 channels over 856-1712 MHz = 1,056,964,608 complex64 visibilities, the
+sum of 50 seeded point sources plus complex Gaussian noise (sigma 0.1), 20 %
+seeded random flags, unit weights; image 4096 x 4096 at 1.0 arcsec;
+epsilon 1e-5, single-precision working type (the kernel table's
+single-precision rows).
+
+One step = vis2dirty (scan, plan, binning, gridding, FFT, projection) then
+dirty2vis (scan, plan, binning, w-screens, FFT, degridding) of the same
+visibilities and mask: the reference's two stateless calls.
+
+* `value`: Mvis/s of the step with inputs resident in HBM (device API,
+  CUDA events on torch's current stream, max over ranks).
+* `e2e`: the same through the reference-facing C ABI (`rang._core`) with
+  pinned host arrays: host-to-device copies of the inputs and the
+  device-to-host copies of the image and the visibilities are inside the
+  timed region (host clock around the synchronous calls).
+* `roofline`: the dominant kernel's algorithmic HBM bytes per launch over its
+  event-timed average launch, against the measured copy bandwidth.
+* `cpu_baseline`: the CPU oracle (a C++/OpenMP restatement of the
+  reference's Rust wgridder; the reference itself cannot be built here) on
+  the first eighth of the integrations with all host threads.
+* `accuracy`: the step's outputs against a float64 run at epsilon 1e-7.
+
+`--impl reference` times the CPU oracle alone, on the same workload sample.
+Multi-GPU (`--gpus N` under torchrun): independent replicas, one per GPU.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "rang-core_b200"))
+
+from rang import synth  # noqa: E402
+
+WORKLOAD = "ms2dirty+dirty2ms 1.06G vis 4096^2"
+METRIC = "Mvis/s ms2dirty+dirty2ms @eps=1e-5 vs FP64"
+UNIT = "Mvis/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD, choices=sorted(synth.WORKLOADS))
+    ap.add_argument("--epsilon", type=float, default=1e-5)
+    ap.add_argument("--cpu-fraction", type=float, default=0.125)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of this GPU during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_observation(wl, seed=0):
+    uvw = synth.uvw_tracks(nant=64, ntime=wl["ntime"], tint=8.0, dec_deg=-30.0)
+    freq = synth.channels(wl["nchan"])
+    sky = synth.point_sky(wl["npix"], nsrc=50, seed=11 + seed)
+    return uvw, freq, sky
+
+
+# ------------------------------------------------------------------ CPU (oracle)
+
+
+def cpu_round_trip(oracle, uvw, freq, vis, mask, npix, cell, eps):
+    kw = dict(uvw=uvw, freq=freq, mask=mask, pixsize_x=cell, pixsize_y=cell, epsilon=eps)
+    t0 = time.perf_counter()
+    dirty = oracle.vis2dirty(vis=vis, npix_x=npix, npix_y=npix, **kw)
+    oracle.dirty2vis(dirty=dirty, **kw)
+    return time.perf_counter() - t0
+
+
+def cpu_sample(wl, fraction, seed=0):
+    """Host data of the first `fraction` of the integrations: visibilities
+    predicted from the point sky by the oracle's own degridder (float64,
+    epsilon 1e-6) plus seeded noise and flags."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle
+
+    uvw, freq, sky = make_observation(wl, seed)
+    nbl = 2016
+    nt = max(1, int(round(wl["ntime"] * fraction)))
+    uvw = uvw[: nt * nbl]
+    cell = wl["cell_arcsec"] * synth.ARCSEC
+    model = oracle.dirty2vis(uvw=uvw, freq=freq, dirty=sky.astype(np.float32), pixsize_x=cell, pixsize_y=cell,
+                             epsilon=1e-5)
+    rng = np.random.default_rng(1000 + seed)
+    shape = model.shape
+    vis = (model + 0.1 * (rng.standard_normal(shape) + 1j * rng.standard_normal(shape))).astype(np.complex64)
+    mask = (rng.uniform(size=shape) >= wl["flag"]).astype(np.uint8)
+    return oracle, uvw, freq, vis, mask, nt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl = synth.WORKLOADS[args.workload]
+    oracle, uvw, freq, vis, mask, nt = cpu_sample(wl, args.cpu_fraction)
+    threads = oracle.set_threads(os.cpu_count() or 1)
+    cell = wl["cell_arcsec"] * synth.ARCSEC
+    for _ in range(args.warmup):
+        cpu_round_trip(oracle, uvw, freq, vis, mask, wl["npix"], cell, args.epsilon)
+    times = [cpu_round_trip(oracle, uvw, freq, vis, mask, wl["npix"], cell, args.epsilon) for _ in range(args.steps)]
+    t = sum(times)
+    value = vis.size * args.steps / t / 1e6
+    sample = f"first {nt} of {wl['ntime']} integrations ({vis.size} visibilities), full image and grid"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "epsilon": args.epsilon},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU
+
+
+def run_b200(args):
+    import torch
+
+    from rang import core, wgrid_torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    ext = core.extension()
+    wl = synth.WORKLOADS[args.workload]
+    npix, cell, eps = wl["npix"], wl["cell_arcsec"] * synth.ARCSEC, args.epsilon
+
+    uvw_np, freq, sky = make_observation(wl)
+    nrow, nchan = uvw_np.shape[0], freq.size
+    nvis = nrow * nchan
+    uvw = torch.from_numpy(uvw_np).to(dev)
+    common = dict(npix_x=npix, npix_y=npix, pixsize_x=cell, pixsize_y=cell)
+
+    # Synthetic data on the device: the point sky predicted by the degridder
+    # (float32, epsilon 1e-6), seeded noise and flags.
+    gen = wgrid_torch.DevicePlan(uvw, freq, epsilon=1e-6, single=True, **common)
+    vis = gen.degrid(torch.from_numpy(sky).to(dev, torch.float32))
+    gen.close()
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+    for a in range(0, nrow, 65536):
+        b = min(nrow, a + 65536)
+        vis[a:b] += 0.1 * torch.randn((b - a, nchan), dtype=torch.complex64, device=dev, generator=g) * np.sqrt(2.0)
+    mask = (torch.rand((nrow, nchan), device=dev, generator=g) >= wl["flag"]).to(torch.uint8)
+    torch.cuda.synchronize()
+
+    def step():
+        p1 = wgrid_torch.DevicePlan(uvw, freq, vis=vis, mask=mask, epsilon=eps, single=True, **common)
+        dirty = p1.grid(vis)
+        p2 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=eps, single=True, **common)
+        out = p2.degrid(dirty)
+        return p1, p2, dirty, out
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        keep = step()
+        keep[0].status()
+        del keep
+    barrier()
+    stream = torch.cuda.current_stream(dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local)
+    clocks.start()
+    n0 = ext.wgridder_launch_count()
+    ext.wgridder_profile_read()
+    ext.wgridder_profile(1)
+    last = None
+    start.record(stream)
+    for _ in range(args.steps):
+        last = None  # releases the previous step's plans and outputs
+        last = step()
+    end.record(stream)
+    barrier()
+    ext.wgridder_profile(0)
+    prof = ext.wgridder_profile_read()
+    launches = ext.wgridder_launch_count() - n0
+    clk = clocks.stop()
+    plan_info = last[0].info
+    dirty32, vis32 = last[2], last[3]
+    last[0].status()
+    last[1].status()
+    last = None
+    ms = start.elapsed_time(end)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nvis * args.steps / (ms / 1e3) / 1e6
+
+    # Dominant kernel and its roofline (algorithmic bytes per launch).
+    hbm, peak_kind = peaks()
+    nact = int(plan_info["nvis"])
+    nplanes = max(int(plan_info["nplanes"]), 1)
+    grid_bytes = nplanes * plan_info["nu"] * plan_info["nv"] * 8
+    alg = {"grid": nact * (8 + 4) + nrow * 24 + grid_bytes, "degrid": nact * (8 + 4) + nrow * 24 + grid_bytes}
+    dom = max(("grid", "degrid"), key=lambda k: prof[k][1])
+    dom_launches, dom_ms = prof[dom]
+    per_launch_s = dom_ms / max(dom_launches, 1) / 1e3
+    achieved = alg[dom] / per_launch_s / 1e9
+    total_prof = sum(v[1] for v in prof.values())
+    roofline = {"bound": "hbm", "kernel": f"k_{dom}", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": alg[dom], "avg_launch_ms": per_launch_s * 1e3,
+                "share_of_step": dom_ms / max(total_prof, 1e-9)}
+
+    # End to end through the C ABI with pinned host arrays.
+    e2e = None
+    if not args.no_e2e:
+        from rang.core_wgridder import options_list
+
+        vis_h = torch.empty((nrow, nchan), dtype=torch.complex64, pin_memory=True)
+        vis_h.copy_(vis)
+        mask_h = torch.empty((nrow, nchan), dtype=torch.uint8, pin_memory=True)
+        mask_h.copy_(mask)
+        out_h = torch.empty((nrow, nchan), dtype=torch.complex64, pin_memory=True)
+        dirty_h = torch.empty((npix, npix), dtype=torch.float32, pin_memory=True)
+        vis_np, mask_np, out_np, dirty_np = vis_h.numpy(), mask_h.numpy(), out_h.numpy(), dirty_h.numpy()
+        opts = options_list(npix, npix, cell, cell, eps, {})
+        info = np.empty(14)
+
+        def e2e_step():
+            st = ext.wgridder_vis2dirty_f32(opts, uvw_np, freq, vis_np, None, None, mask_np, dirty_np, None, info)
+            assert st == 0, ext.wgridder_last_error()
+            st = ext.wgridder_dirty2vis_f32(opts, uvw_np, freq, dirty_np, None, mask_np, out_np.view(np.float32),
+                                            info)
+            assert st == 0, ext.wgridder_last_error()
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        te = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        h2d = 2 * (uvw_np.nbytes + freq.nbytes + mask_np.nbytes) + vis_np.nbytes + dirty_np.nbytes
+        d2h = dirty_np.nbytes + out_np.nbytes
+        e2e = {"value": world * nvis * args.steps / te / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te / args.steps}
+        del vis_h, mask_h, out_h, dirty_h
+
+    # Error of the float32 step against a float64 run at epsilon 1e-7.
+    accuracy = None
+    if not args.no_accuracy:
+        p64 = wgrid_torch.DevicePlan(uvw, freq, vis=vis, mask=mask, epsilon=1e-7, single=False, **common)
+        d64 = p64.grid(vis)
+        p64.close()
+        dd = (dirty32.double() - d64)
+        peak = d64.abs().max()
+        q64 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=1e-7, single=False, **common)
+        v64 = q64.degrid(dirty32.double())
+        q64.close()
+        dv = vis32.to(torch.complex128) - v64
+        vpeak = v64.abs().max()
+        accuracy = {
+            "reference": "float64 GPU run at epsilon 1e-7 on the same inputs",
+            "dirty_rel_linf": float(dd.abs().max() / peak), "dirty_rel_rms": float(dd.pow(2).mean().sqrt() / peak),
+            "vis_rel_linf": float(dv.abs().max() / vpeak),
+            "vis_rel_rms": float(dv.abs().pow(2).mean().sqrt() / vpeak),
+        }
+        del d64, v64, dd, dv
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        oracle, suvw, sfreq, svis, smask, nt = cpu_sample(wl, args.cpu_fraction)
+        threads = oracle.set_threads(os.cpu_count() or 1)
+        t = cpu_round_trip(oracle, suvw, sfreq, svis, smask, npix, cell, eps)
+        cpu = {"value": svis.size / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"first {nt} of {wl['ntime']} integrations ({svis.size} visibilities), one round trip, "
+                         f"full {npix}^2 image and grid, {threads} threads"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "visibilities": nvis, "active": nact, "image": [npix, npix],
+                       "cell_arcsec": wl["cell_arcsec"], "epsilon": eps, "flags": wl["flag"],
+                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (8.5 GB of visibilities)",
+                       "plan": {k: plan_info[k] for k in ("kernel_index", "supp", "nu", "nv", "nplanes")}},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk, "accuracy": accuracy,
+            "stages_ms": {k: round(v[1], 3) for k, v in prof.items() if v[0]},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -160,6 +160,25 @@ int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, siz
                                    int64_t* iv0, uint32_t* key, uint32_t* sorted, size_t* nsorted,
                                    double* info);
 
+/* Instrumentation (no counterpart in the reference, whose timing report is
+ * RANG_WGRIDDER_TIMING on stderr, wgridder.rs:1773-1812). The launch count
+ * is the number of this library's own CUDA kernels launched so far (cuFFT's
+ * are not counted). While profiling is on, every stage of the pipeline is
+ * bracketed by CUDA events on its stream; profile_read waits for them and
+ * returns per stage the launches and the summed device milliseconds since the
+ * previous read, in the order of stage_name(0 .. n-1). */
+int64_t rang_b200_wgridder_launch_count(void);
+/* How single-precision gridding forms its sums (no counterpart in the
+ * reference, whose RANG_WGRIDDER_SIMD selects CPU instruction sets,
+ * wgridder.rs:1593-1627): 1 split-precision 3 x TF32 tensor-core products
+ * with FP32 accumulation (the default), 0 plain FP32 FMAs on the CUDA cores.
+ * Process-wide; RANG_WGRIDDER_GPU_METHOD=fp32|tf32x3 sets the initial value.
+ * Returns the previous method. */
+int32_t rang_b200_wgridder_set_method(int32_t method);
+void rang_b200_wgridder_profile(int32_t on);
+int32_t rang_b200_wgridder_profile_read(int64_t* launches, double* ms, int32_t n);
+const char* rang_b200_wgridder_stage_name(int32_t index);
+
 #ifdef __cplusplus
 }
 #endif

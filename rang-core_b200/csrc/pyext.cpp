@@ -276,6 +276,21 @@ PYBIND11_MODULE(_core, m) {
     py::gil_scoped_release release;
     rang_b200_wgridder_plan_destroy(reinterpret_cast<RangWgridPlan*>(plan));
   });
+  m.def("wgridder_set_method", [](int m) { return (int)rang_b200_wgridder_set_method(m); });
+  m.def("wgridder_launch_count", []() { return (long long)rang_b200_wgridder_launch_count(); });
+  m.def("wgridder_profile", [](int on) { rang_b200_wgridder_profile(on); });
+  m.def("wgridder_profile_read", []() {
+    int64_t l[64];
+    double t[64];
+    int n;
+    {
+      py::gil_scoped_release release;
+      n = rang_b200_wgridder_profile_read(l, t, 64);
+    }
+    py::dict out;
+    for (int i = 0; i < n; i++) out[py::str(rang_b200_wgridder_stage_name(i))] = py::make_tuple(l[i], t[i]);
+    return out;
+  });
   m.def(
       "wgridder_binning",
       [](std::vector<double> opts, py::object uvw, py::object freq, py::object vis, py::object wgt, py::object wgt2,

@@ -413,4 +413,29 @@ int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, siz
   });
 }
 
+int64_t rang_b200_wgridder_launch_count(void) { return launch_count(); }
+
+int32_t rang_b200_wgridder_set_method(int32_t method) {
+  int old = grid_method();
+  set_grid_method(method == GRID_FP32 ? GRID_FP32 : GRID_TF32X3);
+  return old;
+}
+
+void rang_b200_wgridder_profile(int32_t on) { profile_enable(on != 0); }
+
+int32_t rang_b200_wgridder_profile_read(int64_t* launches, double* ms, int32_t n) {
+  long long l[N_STAGES];
+  double t[N_STAGES];
+  profile_read(l, t);
+  for (int i = 0; i < n && i < N_STAGES; i++) {
+    if (launches) launches[i] = l[i];
+    if (ms) ms[i] = t[i];
+  }
+  return N_STAGES;
+}
+
+const char* rang_b200_wgridder_stage_name(int32_t index) {
+  return index >= 0 && index < N_STAGES ? STAGE_NAMES[index] : nullptr;
+}
+
 }  // extern "C"

@@ -24,6 +24,8 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -38,12 +40,12 @@ namespace wg {
 namespace {
 
 constexpr uint32_t INACTIVE = 0xffffffffu;
-constexpr uint32_t TASK_CHUNK = 2048;
+constexpr uint32_t TASK_CHUNK = 16384;
 constexpr int GRID_THREADS = 256;
 constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
-constexpr size_t SMEM_WINDOW_BYTES = 100 * 1024;
+constexpr size_t SMEM_WINDOW_BYTES = 80 * 1024;
 
 unsigned blocks_for(uint64_t n, int threads, unsigned cap = 148u * 32u) {
   uint64_t b = (n + threads - 1) / threads;
@@ -110,7 +112,11 @@ __global__ void k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__
 
 // ------------------------------------------------------------------ binning
 
-// Setup::locate (wgridder.rs:1244-1255) as one key: tile * nbuckets + plane.
+// Setup::locate (wgridder.rs:1244-1255) as one key: the tile and first plane
+// of the reference's layout, refined by the 8 x 8 sub-tile of the first tap:
+// ((tile * nbuckets + plane) * nsub + sub-tile). Sorting by it keeps the
+// reference's (tile, plane) order and groups each plane's visibilities by
+// sub-tile, which the tensor-core gridder contracts block by block.
 template <class T>
 __device__ __forceinline__ uint32_t bin_of(const Geom<T>& g, const double* __restrict__ uvw,
                                            const double* __restrict__ foc, uint32_t idx, int64_t* piu0 = nullptr,
@@ -124,11 +130,13 @@ __device__ __forceinline__ uint32_t bin_of(const Geom<T>& g, const double* __res
   double uf, vf;
   int64_t iu0, iv0;
   getpix(g, u, v, uf, vf, iu0, iv0);
-  uint32_t tu = (uint32_t)shifted(iu0, g.nu) >> g.log2tile;
-  uint32_t tv = (uint32_t)shifted(iv0, g.nv) >> g.log2tile;
+  const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
+  const uint32_t tu = su >> g.log2tile, tv = sv >> g.log2tile;
+  const uint32_t mask = (1u << g.log2tile) - 1u;
+  const uint32_t sub = ((su & mask) >> 3) * (uint32_t)g.nsub_side + ((sv & mask) >> 3);
   if (piu0) *piu0 = iu0;
   if (piv0) *piv0 = iv0;
-  return (tu * (uint32_t)g.ntv + tv) * (uint32_t)g.nbuckets + (uint32_t)minplane(g, w);
+  return ((tu * (uint32_t)g.ntv + tv) * (uint32_t)g.nbuckets + (uint32_t)minplane(g, w)) * (uint32_t)g.nsub + sub;
 }
 
 // One atomic per distinct counter in the warp; each active lane gets the
@@ -236,40 +244,56 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, uint64_t n, const uint32_
 void exclusive_scan(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t s) {
   uint64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
   DevBuf sums(ntiles * 4, s);
-  k_scan_tiles<<<(unsigned)ntiles, SCAN_THREADS, 0, s>>>(in, out, n, sums.as<uint32_t>());
+  {
+    StageTimer timer_(ST_PREFIX, s);
+    k_scan_tiles<<<(unsigned)ntiles, SCAN_THREADS, 0, s>>>(in, out, n, sums.as<uint32_t>());
+  }
   check_cuda(cudaGetLastError(), "scan");
   if (ntiles > 1) {
     exclusive_scan(sums.as<uint32_t>(), sums.as<uint32_t>(), ntiles, s);
-    k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, sums.as<uint32_t>());
+    {
+      StageTimer timer_(ST_PREFIX, s);
+      k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, sums.as<uint32_t>());
+    }
     check_cuda(cudaGetLastError(), "scan");
   }
 }
 
 // ------------------------------------------------------------------ tasks
 
-__global__ void k_task_count(const uint32_t* __restrict__ starts, uint32_t nb, uint32_t ntiles,
+// Tasks per tile; `stride` bins per tile (nbuckets * nsub).
+__global__ void k_task_count(const uint32_t* __restrict__ starts, uint32_t stride, uint32_t ntiles,
                              uint32_t* __restrict__ ntask) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < ntiles) {
-    uint32_t c = starts[(uint64_t)(t + 1) * nb] - starts[(uint64_t)t * nb];
+    uint32_t c = starts[(uint64_t)(t + 1) * stride] - starts[(uint64_t)t * stride];
     ntask[t] = (c + TASK_CHUNK - 1) / TASK_CHUNK;
   } else if (t == ntiles) {
     ntask[t] = 0;
   }
 }
 
-__device__ __forceinline__ uint32_t plane_at(const uint32_t* starts, uint64_t b0, uint32_t nb, uint32_t k) {
-  uint32_t m = 0;
-  while (m + 1 < nb && starts[b0 + m + 1] <= k) m++;
-  return m;
+// The first plane of sorted visibility k of the tile whose bins start at b0:
+// the bin m with starts[b0 + m] <= k < starts[b0 + m + 1] (binary search).
+__device__ __forceinline__ uint32_t plane_at(const uint32_t* starts, uint64_t b0, uint32_t stride, uint32_t nsub,
+                                             uint32_t k) {
+  uint32_t lo = 0, hi = stride - 1;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (starts[b0 + mid] <= k)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo / nsub;
 }
 
-__global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t nb, uint32_t ntiles,
+__global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t stride, uint32_t nsub, uint32_t ntiles,
                             const uint32_t* __restrict__ off, Task* __restrict__ tasks, uint32_t* __restrict__ ntotal) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntiles) return;
-  uint64_t b0 = (uint64_t)t * nb;
-  uint32_t s = starts[b0], e = starts[b0 + nb];
+  uint64_t b0 = (uint64_t)t * stride;
+  uint32_t s = starts[b0], e = starts[b0 + stride];
   uint32_t q0 = off[t];
   for (uint32_t k0 = s, q = q0; k0 < e; k0 += TASK_CHUNK, q++) {
     uint32_t k1 = min(k0 + TASK_CHUNK, e);
@@ -277,8 +301,8 @@ __global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t nb, ui
     tk.tile = t;
     tk.k0 = k0;
     tk.k1 = k1;
-    tk.plo = (uint16_t)plane_at(starts, b0, nb, k0);
-    tk.phi = (uint16_t)plane_at(starts, b0, nb, k1 - 1);
+    tk.plo = (uint16_t)plane_at(starts, b0, stride, nsub, k0);
+    tk.phi = (uint16_t)plane_at(starts, b0, stride, nsub, k1 - 1);
     tasks[q] = tk;
   }
   if (t == ntiles - 1) *ntotal = off[ntiles];
@@ -286,17 +310,92 @@ __global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t nb, ui
 
 // ------------------------------------------------------------------ gridding
 
+// One grid cell += (re, im): a single 8-byte vector reduction in L2 for
+// complex float, two scalar ones for complex double.
+__device__ __forceinline__ void add_cell(cplx<float>* dst, float re, float im) {
+  atomicAdd(reinterpret_cast<float2*>(dst), make_float2(re, im));
+}
+__device__ __forceinline__ void add_cell(cplx<double>* dst, double re, double im) {
+  atomicAdd(&dst->re, re);
+  atomicAdd(&dst->im, im);
+}
+
+// Thread layout of the gridding kernel. Thread (x, y, z) owns the window
+// cells whose u index is x mod S, v index y mod S and plane (z + k Z) mod S:
+// every footprint (S x S cells on each of S planes) holds exactly one cell of
+// each owner and plane residue, so the threads accumulate in shared memory
+// without atomics and in a fixed order (the visibilities' sorted order).
+template <int S>
+struct GridLayout {
+  static constexpr int S2 = S * S;
+  // At most 512 threads (128 registers each) for the large f64 supports.
+  static constexpr int Z = S2 * S <= 512 ? S : (512 / S2 > 0 ? 512 / S2 : 1);  // plane-residue groups
+  static constexpr int NOWN = S2 * Z;                        // owning threads
+  static constexpr int THREADS = (NOWN + 31) / 32 * 32;
+  static constexpr int JPER = (S + Z - 1) / Z;  // plane residues per thread
+};
+
+// Staging of one batch of visibilities, in two phases. Phase 1 (one thread
+// per visibility): the offsets of its first taps in the tile window, its
+// first plane, its u and v taps and its value times the w tap of each plane
+// (the reference's taps_uv, w_factor, unit_value and data_value,
+// wgridder.rs:1565-1591, 1414-1435). Phase 2 (all threads): per visibility
+// and owner (x, y) the window offset of the owner's cell and the tap product
+// ku * kv there, and per plane residue r the plane's window index and value.
 template <class T, int S>
-__global__ void __launch_bounds__(GRID_THREADS)
+struct GridStaging {
+  struct Cell {
+    int off;
+    T kk;
+  };
+  struct PlaneVal {
+    T re, im;
+    int pl;  // plane index in the window, -1 outside it
+    int pad;
+  };
+  int* meta;     // [B] ou | ov << 8, or -1: not gridded in this window
+  int* mp;       // [B] first plane
+  T* ku;         // [B][S]
+  T* kv;         // [B][S]
+  cplx<T>* cw;   // [B][S] value * kw(plane mp + j), zero outside the window
+  Cell* rc;      // [B][S*S]
+  PlaneVal* pw;  // [B][S]
+  static constexpr size_t bytes_per_vis() {
+    return 2 * sizeof(int) + 2 * S * sizeof(T) + S * sizeof(cplx<T>) + S * S * sizeof(Cell) + S * sizeof(PlaneVal);
+  }
+  __device__ void carve(unsigned char* base, int B) {
+    // Largest alignment first.
+    pw = reinterpret_cast<PlaneVal*>(base);
+    rc = reinterpret_cast<Cell*>(pw + (size_t)B * S);
+    cw = reinterpret_cast<cplx<T>*>(rc + (size_t)B * S * S);
+    ku = reinterpret_cast<T*>(cw + (size_t)B * S);
+    kv = ku + (size_t)B * S;
+    meta = reinterpret_cast<int*>(kv + (size_t)B * S);
+    mp = meta + B;
+  }
+};
+
+template <class T, int S>
+int staging_batch() {
+  int b = (int)(28672 / GridStaging<T, S>::bytes_per_vis());
+  return std::max(1, std::min(b, GridLayout<S>::THREADS));
+}
+
+template <class T, int S>
+__global__ void __launch_bounds__(GridLayout<S>::THREADS)
     k_grid(const __grid_constant__ Geom<T> g, Inputs in, int mode, const double* __restrict__ uvw,
            const double* __restrict__ foc, const uint32_t* __restrict__ sorted, const Task* __restrict__ tasks,
-           const uint32_t* __restrict__ ntasks, cplx<T>* __restrict__ grids, int pg0, int npg, int gmax,
+           const uint32_t* __restrict__ ntasks, cplx<T>* __restrict__ grids, int pg0, int npg, int gmax, int batch,
            int* __restrict__ err) {
+  using Lay = GridLayout<S>;
+  using St = GridStaging<T, S>;
+  constexpr int S2 = S * S;
   if (blockIdx.x >= *ntasks) return;
   extern __shared__ __align__(16) unsigned char smem[];
   const int L = g.L, LL = L * L;
-  T* bre = reinterpret_cast<T*>(smem);
-  T* bim = bre + (size_t)gmax * LL;
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem);
+  St st;
+  st.carve(smem + (size_t)gmax * LL * sizeof(cplx<T>), batch);
   const Task t = tasks[blockIdx.x];
   const int tu = (int)(t.tile / (uint32_t)g.ntv), tv = (int)(t.tile - (uint32_t)tu * (uint32_t)g.ntv);
   const int bu = tu << g.log2tile, bv = tv << g.log2tile;
@@ -307,70 +406,375 @@ __global__ void __launch_bounds__(GRID_THREADS)
     hi = min((int)t.phi + S - 1, pg0 + npg - 1);
   }
   const uint32_t nchan = (uint32_t)g.nchan;
+  const int tid = threadIdx.x;
+  const bool owner = tid < Lay::NOWN;
+  const int oz = tid % Lay::Z, oxy = tid / Lay::Z;
   for (int w0 = lo; w0 <= hi; w0 += gmax) {
     const int gw = min(gmax, hi - w0 + 1);
-    for (int c = threadIdx.x; c < gw * LL; c += blockDim.x) {
-      bre[c] = (T)0;
-      bim[c] = (T)0;
+    for (int c = tid; c < gw * LL; c += blockDim.x) buf[c] = cplx<T>{(T)0, (T)0};
+    // The owner's running sums: consecutive contributions to one cell are
+    // added in registers and the sum added to the window when the cell changes.
+    cplx<T> acc[Lay::JPER];
+    int cur[Lay::JPER];
+#pragma unroll
+    for (int jj = 0; jj < Lay::JPER; jj++) {
+      acc[jj] = cplx<T>{(T)0, (T)0};
+      cur[jj] = -1;
     }
-    __syncthreads();
-    for (uint32_t k = t.k0 + threadIdx.x; k < t.k1; k += blockDim.x) {
-      const uint32_t idx = sorted[k];
-      const uint32_t row = idx / nchan, ch = idx - row * nchan;
-      double b[3];
-      const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
-      const double f = foc[ch];
-      const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
-      const int mp = minplane(g, w);
-      const int plo = g.do_wgridding ? max(mp, w0) : 0;
-      const int phi = g.do_wgridding ? min(mp + S - 1, w0 + gw - 1) : 0;
-      if (plo > phi) continue;
-      double uf, vf;
-      int64_t iu0, iv0;
-      getpix(g, u, v, uf, vf, iu0, iv0);
-      const int ou = offset_in(iu0, g.nu, bu), ov = offset_in(iv0, g.nv, bv);
-      if ((unsigned)ou >= tilesz || (unsigned)ov >= tilesz) {
-        atomicOr(err, 1);
-        continue;
-      }
-      T ku[S], kv[S];
-      const T x0 = (T)(-uf * 2.0 + ((double)S - 1.0));
-      const T y0 = (T)(-vf * 2.0 + ((double)S - 1.0));
-      eval_taps2<T, S>(g.coeff, g.ne, x0, y0, ku, kv);
-      cplx<T> val = unit_value<T>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<T>(in, idx));
-      if (mode == VALUE_DATA) val = data_value<T>(vis_get<T>(in, idx), val, (T)imflip);
-      for (int p = plo; p <= phi; p++) {
-        T kk[S];
-        if (g.do_wgridding) {
-          const T kw = w_factor<T, S>(g, p - mp, p, w);
+    for (uint32_t kb = t.k0; kb < t.k1; kb += (uint32_t)batch) {
+      const int nb = (int)min((uint32_t)batch, t.k1 - kb);
+      __syncthreads();
+      if (tid < nb) {  // phase 1
+        int meta = -1, mpq = 0;
+        const uint32_t idx = sorted[kb + tid];
+        const uint32_t row = idx / nchan, ch = idx - row * nchan;
+        double b[3];
+        const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+        const double f = foc[ch];
+        const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
+        const int mp = minplane(g, w);
+        if (!g.do_wgridding || (mp <= w0 + gw - 1 && mp + S - 1 >= w0)) {
+          double uf, vf;
+          int64_t iu0, iv0;
+          getpix(g, u, v, uf, vf, iu0, iv0);
+          const int ou = offset_in(iu0, g.nu, bu), ov = offset_in(iv0, g.nv, bv);
+          if ((unsigned)ou >= tilesz || (unsigned)ov >= tilesz) {
+            atomicOr(err, 1);
+          } else {
+            T ku[S], kv[S];
+            const T x0 = (T)(-uf * 2.0 + ((double)S - 1.0));
+            const T y0 = (T)(-vf * 2.0 + ((double)S - 1.0));
+            eval_taps2<T, S>(g.coeff, g.ne, x0, y0, ku, kv);
+            cplx<T> val = unit_value<T>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<T>(in, idx));
+            if (mode == VALUE_DATA) val = data_value<T>(vis_get<T>(in, idx), val, (T)imflip);
 #pragma unroll
-          for (int cu = 0; cu < S; cu++) kk[cu] = ku[cu] * kw;
-        } else {
-#pragma unroll
-          for (int cu = 0; cu < S; cu++) kk[cu] = ku[cu];
+            for (int j = 0; j < S; j++) {
+              st.ku[tid * S + j] = ku[j];
+              st.kv[tid * S + j] = kv[j];
+              T kw = (T)0;
+              if (g.do_wgridding) {
+                const int p = mp + j;
+                if (p >= w0 && p < w0 + gw) kw = w_factor<T, S>(g, j, p, w);
+              } else if (j == 0) {
+                kw = (T)1;
+              }
+              st.cw[tid * S + j] = cplx<T>{val.re * kw, val.im * kw};
+            }
+            meta = ou | (ov << 8);
+            mpq = mp;
+          }
         }
-        T* pr = bre + (size_t)(p - w0) * LL + ou * L + ov;
-        T* pi = bim + (size_t)(p - w0) * LL + ou * L + ov;
+        st.meta[tid] = meta;
+        st.mp[tid] = mpq;
+      }
+      __syncthreads();
+      for (int e = tid; e < nb * (S2 + S); e += blockDim.x) {  // phase 2
+        if (e < nb * S2) {
+          const int q = e / S2, xy = e - q * S2, x = xy / S, y = xy - x * S;
+          const int m = st.meta[q];
+          typename St::Cell c{0, (T)0};
+          if (m >= 0) {
+            const int ou = m & 255, ov = m >> 8;
+            const int cu = (x - ou % S + S) % S, cv = (y - ov % S + S) % S;
+            c.off = (ou + cu) * L + ov + cv;
+            c.kk = st.ku[q * S + cu] * st.kv[q * S + cv];
+          }
+          st.rc[e] = c;
+        } else {
+          const int e2 = e - nb * S2, q = e2 / S, r = e2 - q * S;
+          const int mp = st.mp[q];
+          const int j = (r - mp % S + S) % S;
+          const int p = mp + j;
+          typename St::PlaneVal pv;
+          pv.pad = 0;
+          const bool in_win = g.do_wgridding ? (p >= w0 && p < w0 + gw) : (j == 0);
+          pv.pl = st.meta[q] >= 0 && in_win ? p - w0 : -1;
+          pv.re = st.cw[q * S + j].re;
+          pv.im = st.cw[q * S + j].im;
+          st.pw[e2] = pv;
+        }
+      }
+      __syncthreads();
+      if (owner) {  // accumulation, in sorted order
+        for (int q = 0; q < nb; q++) {
+          if (st.meta[q] < 0) continue;
+          const typename St::Cell c = st.rc[q * S2 + oxy];
 #pragma unroll
-        for (int cu = 0; cu < S; cu++) {
-          const T tr = val.re * kk[cu], ti = val.im * kk[cu];
-#pragma unroll
-          for (int cv = 0; cv < S; cv++) {
-            atomicAdd(pr + cu * L + cv, tr * kv[cv]);
-            atomicAdd(pi + cu * L + cv, ti * kv[cv]);
+          for (int jj = 0; jj < Lay::JPER; jj++) {
+            const int r = oz + jj * Lay::Z;
+            if (r >= S) break;
+            const typename St::PlaneVal pv = st.pw[q * S + r];
+            if (pv.pl < 0) continue;
+            const int at = pv.pl * LL + c.off;
+            if (at != cur[jj]) {
+              if (cur[jj] >= 0) {
+                cplx<T> o = buf[cur[jj]];
+                buf[cur[jj]] = cplx<T>{o.re + acc[jj].re, o.im + acc[jj].im};
+              }
+              cur[jj] = at;
+              acc[jj] = cplx<T>{(T)0, (T)0};
+            }
+            acc[jj].re = fma_t(pv.re, c.kk, acc[jj].re);
+            acc[jj].im = fma_t(pv.im, c.kk, acc[jj].im);
           }
         }
       }
     }
+    if (owner) {
+#pragma unroll
+      for (int jj = 0; jj < Lay::JPER; jj++)
+        if (cur[jj] >= 0) {
+          cplx<T> o = buf[cur[jj]];
+          buf[cur[jj]] = cplx<T>{o.re + acc[jj].re, o.im + acc[jj].im};
+        }
+    }
     __syncthreads();
-    for (int c = threadIdx.x; c < gw * LL; c += blockDim.x) {
-      const T re = bre[c], im = bim[c];
-      if (re == (T)0 && im == (T)0) continue;
+    for (int c = tid; c < gw * LL; c += blockDim.x) {
+      const cplx<T> v = buf[c];
+      if (v.re == (T)0 && v.im == (T)0) continue;
       const int pl = c / LL, rem = c - pl * LL, i = rem / L, j = rem - i * L;
       const int row = (bu + i + g.nu / 2) % g.nu, col = (bv + j + g.nv / 2) % g.nv;
       cplx<T>* dst = grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col;
-      atomicAdd(&dst->re, re);
-      atomicAdd(&dst->im, im);
+      add_cell(dst, v.re, v.im);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ tensor-core gridding (3 x TF32)
+
+// The separable footprint of a block of K visibilities on one plane is a
+// rank-K product: T[i][n] += sum_k A[i][k] B[k][n] with A[i][k] the u taps of
+// visibility k placed at its row in a 16-row sub-tile window and
+// B[k][n] = value_k * kw_k(plane) * kv_k[n - offset], so one warp that owns
+// one w-plane of the tile window accumulates each 8 x 8 sub-tile's 16 x 16
+// window with mma.sync m16n8k8 (TF32 inputs, FP32 accumulation). Each
+// operand is split as x = hi + lo in TF32 and the product formed as
+// hi*hi + hi*lo + lo*hi (3 x TF32), which keeps about 21 bits of each
+// factor. Operands come straight from the staged taps into registers: the
+// footprint is sparse (S of 16 rows per column), so forming it costs less
+// than staging it through shared memory for tcgen05.
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+constexpr int TC_DRAIN = 8;
+
+template <int S>
+struct TcStaging {
+  int* grp;       // [B] (first plane << 4 | sub-tile), or -1: not gridded in this window
+  int* duv;       // [B] offsets of the first taps inside the sub-tile: du | dv << 8
+  float* ku;      // [B][S]
+  float* kv;      // [B][S]
+  cplx<float>* cw;  // [B][S] value * kw(plane first + j), zero outside the window
+  static constexpr size_t bytes_per_vis() { return 2 * sizeof(int) + 2 * S * sizeof(float) + S * sizeof(cplx<float>); }
+  __device__ void carve(unsigned char* base, int B) {
+    cw = reinterpret_cast<cplx<float>*>(base);
+    ku = reinterpret_cast<float*>(cw + (size_t)B * S);
+    kv = ku + (size_t)B * S;
+    grp = reinterpret_cast<int*>(kv + (size_t)B * S);
+    duv = grp + B;
+  }
+};
+
+// Adds one warp's 16 x 16 sub-tile accumulators (real and imaginary parts) to
+// its plane of the window.
+__device__ __forceinline__ void tc_flush(cplx<float>* plane, int L, int a8, int b8, const float (&c)[2][2][4]) {
+  const int lane = threadIdx.x & 31, gq = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int row = a8 + gq + (r >= 2 ? 8 : 0), col = b8 + 8 * nt + 2 * t + (r & 1);
+      const float re = c[0][nt][r], im = c[1][nt][r];
+      if (row < L && col < L && (re != 0.0f || im != 0.0f)) {
+        cplx<float>* d = plane + row * L + col;
+        cplx<float> o = *d;
+        *d = cplx<float>{o.re + re, o.im + im};
+      }
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256)
+    k_grid_tc(const __grid_constant__ Geom<float> g, Inputs in, int mode, const double* __restrict__ uvw,
+              const double* __restrict__ foc, const uint32_t* __restrict__ sorted, const Task* __restrict__ tasks,
+              const uint32_t* __restrict__ ntasks, cplx<float>* __restrict__ grids, int pg0, int npg, int gmax,
+              int* __restrict__ err) {
+  static_assert(S <= 8, "sub-tile windows hold 8 + S - 1 <= 16 rows");
+  using St = TcStaging<S>;
+  if (blockIdx.x >= *ntasks) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int L = g.L, LL = L * L;
+  const int batch = blockDim.x;
+  cplx<float>* buf = reinterpret_cast<cplx<float>*>(smem);
+  St st;
+  st.carve(smem + (size_t)gmax * LL * sizeof(cplx<float>), batch);
+  const Task t = tasks[blockIdx.x];
+  const int tu = (int)(t.tile / (uint32_t)g.ntv), tv = (int)(t.tile - (uint32_t)tu * (uint32_t)g.ntv);
+  const int bu = tu << g.log2tile, bv = tv << g.log2tile;
+  const unsigned tilesz = 1u << g.log2tile;
+  int lo = 0, hi = 0;
+  if (g.do_wgridding) {
+    lo = max((int)t.plo, pg0);
+    hi = min((int)t.phi + S - 1, pg0 + npg - 1);
+  }
+  const uint32_t nchan = (uint32_t)g.nchan;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, tq = lane & 3;
+  for (int w0 = lo; w0 <= hi; w0 += gmax) {
+    const int gw = min(gmax, hi - w0 + 1);
+    for (int c = tid; c < gw * LL; c += blockDim.x) buf[c] = cplx<float>{0.0f, 0.0f};
+    float acc[2][2][4];
+    int gcur = -2, a8 = 0, b8 = 0, jpl = 0, blocks = 0;
+    bool act = false;
+    for (uint32_t kb = t.k0; kb < t.k1; kb += (uint32_t)batch) {
+      const int nb = (int)min((uint32_t)batch, t.k1 - kb);
+      __syncthreads();
+      if (tid < nb) {  // staging: one visibility per thread
+        int grp = -1, duv = 0;
+        const uint32_t idx = sorted[kb + tid];
+        const uint32_t row = idx / nchan, ch = idx - row * nchan;
+        double b[3];
+        const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+        const double f = foc[ch];
+        const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
+        const int mp = minplane(g, w);
+        if (!g.do_wgridding || (mp <= w0 + gw - 1 && mp + S - 1 >= w0)) {
+          double uf, vf;
+          int64_t iu0, iv0;
+          getpix(g, u, v, uf, vf, iu0, iv0);
+          const int ou = offset_in(iu0, g.nu, bu), ov = offset_in(iv0, g.nv, bv);
+          if ((unsigned)ou >= tilesz || (unsigned)ov >= tilesz) {
+            atomicOr(err, 1);
+          } else {
+            float ku[S], kv[S];
+            const float x0 = (float)(-uf * 2.0 + ((double)S - 1.0));
+            const float y0 = (float)(-vf * 2.0 + ((double)S - 1.0));
+            eval_taps2<float, S>(g.coeff, g.ne, x0, y0, ku, kv);
+            cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
+            if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+              st.ku[tid * S + j] = ku[j];
+              st.kv[tid * S + j] = kv[j];
+              float kw = 0.0f;
+              if (g.do_wgridding) {
+                const int p = mp + j;
+                if (p >= w0 && p < w0 + gw) kw = w_factor<float, S>(g, j, p, w);
+              } else if (j == 0) {
+                kw = 1.0f;
+              }
+              st.cw[tid * S + j] = cplx<float>{val.re * kw, val.im * kw};
+            }
+            const int sub = (ou >> 3) * g.nsub_side + (ov >> 3);
+            grp = (mp << 4) | sub;
+            duv = (ou & 7) | ((ov & 7) << 8);
+          }
+        }
+        st.grp[tid] = grp;
+        st.duv[tid] = duv;
+      }
+      __syncthreads();
+      if (warp < gw) {  // this warp's plane: w0 + warp
+        const int p = w0 + warp;
+        int q = 0;
+        while (q < nb) {
+          const int gqv = st.grp[q];
+          // The tensor cores' FP32 accumulation does not round to nearest, so
+          // long sums drift: every TC_DRAIN blocks the accumulators are added
+          // to the window (rounded FP32 adds) and restarted from zero.
+          if (gqv != gcur || blocks == TC_DRAIN) {
+            if (act) tc_flush(buf + (size_t)warp * LL, L, a8, b8, acc);
+            blocks = 0;
+            gcur = gqv;
+#pragma unroll
+            for (int c2 = 0; c2 < 2; c2++)
+#pragma unroll
+              for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+                for (int r = 0; r < 4; r++) acc[c2][nt][r] = 0.0f;
+            act = false;
+            if (gqv >= 0) {
+              const int mpg = gqv >> 4, sub = gqv & 15;
+              a8 = (sub / g.nsub_side) * 8;
+              b8 = (sub % g.nsub_side) * 8;
+              jpl = p - mpg;
+              act = g.do_wgridding ? (jpl >= 0 && jpl < S) : (jpl == 0);
+            }
+          }
+          // The block: the leading visibilities (at most 8) of the current group.
+          const bool same = lane < 8 && q + lane < nb && st.grp[q + lane] == gcur;
+          const unsigned m = __ballot_sync(0xffffffffu, same);
+          const int kbk = __ffs(~m) - 1;
+          if (act) {
+            uint32_t ah[4], al[4];
+            float bv[2][2][2];  // [k half][comp][n tile]
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+              const int k = tq + 4 * h;
+              float a_lo = 0.0f, a_hi = 0.0f;
+              float kvv[2] = {0.0f, 0.0f};
+              cplx<float> w = {0.0f, 0.0f};
+              if (k < kbk) {
+                const int e = q + k;
+                const int d = st.duv[e];
+                const int du = d & 255, dv = d >> 8;
+                const int cu0 = gq - du, cu1 = gq + 8 - du;
+                if (cu0 >= 0 && cu0 < S) a_lo = st.ku[e * S + cu0];
+                if (cu1 >= 0 && cu1 < S) a_hi = st.ku[e * S + cu1];
+#pragma unroll
+                for (int nt = 0; nt < 2; nt++) {
+                  const int cv = gq + 8 * nt - dv;
+                  if (cv >= 0 && cv < S) kvv[nt] = st.kv[e * S + cv];
+                }
+                w = st.cw[e * S + jpl];
+              }
+              split_tf32(a_lo, ah[2 * h], al[2 * h]);      // rows gq: a0 (k = tq) / a2 (k = tq + 4)
+              split_tf32(a_hi, ah[2 * h + 1], al[2 * h + 1]);  // rows gq + 8: a1 / a3
+#pragma unroll
+              for (int nt = 0; nt < 2; nt++) {
+                bv[h][0][nt] = w.re * kvv[nt];
+                bv[h][1][nt] = w.im * kvv[nt];
+              }
+            }
+#pragma unroll
+            for (int c2 = 0; c2 < 2; c2++)
+#pragma unroll
+              for (int nt = 0; nt < 2; nt++) {
+                uint32_t bh0, bl0, bh1, bl1;
+                split_tf32(bv[0][c2][nt], bh0, bl0);
+                split_tf32(bv[1][c2][nt], bh1, bl1);
+                mma_tf32(acc[c2][nt], ah, bh0, bh1);
+                mma_tf32(acc[c2][nt], ah, bl0, bl1);
+                mma_tf32(acc[c2][nt], al, bh0, bh1);
+              }
+            blocks++;
+          }
+          q += kbk;
+        }
+      }
+    }
+    if (warp < gw && act) tc_flush(buf + (size_t)warp * LL, L, a8, b8, acc);
+    __syncthreads();
+    for (int c = tid; c < gw * LL; c += blockDim.x) {
+      const cplx<float> v = buf[c];
+      if (v.re == 0.0f && v.im == 0.0f) continue;
+      const int pl = c / LL, rem = c - pl * LL, i = rem / L, j = rem - i * L;
+      const int row = (bu + i + g.nu / 2) % g.nu, col = (bv + j + g.nv / 2) % g.nv;
+      add_cell(grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col, v.re, v.im);
     }
     __syncthreads();
   }
@@ -705,10 +1109,30 @@ template <class T, int S>
 void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, const Inputs& in, int mode,
                  const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
                  const uint32_t* ntasks, cplx<T>* grids, int pg0, int npg, int gmax, int* err) {
-  check_cuda(cudaFuncSetAttribute(k_grid<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
-  k_grid<T, S><<<nblocks, GRID_THREADS, smem, s>>>(g, in, mode, uvw, foc, sorted, tasks, ntasks, grids, pg0, npg,
-                                                   gmax, err);
+  const int batch = staging_batch<T, S>();
+  const int total = smem + batch * (int)GridStaging<T, S>::bytes_per_vis();
+  check_cuda(cudaFuncSetAttribute(k_grid<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, total), "smem");
+  {
+    StageTimer timer_(ST_GRID, s);
+    k_grid<T, S><<<nblocks, GridLayout<S>::THREADS, total, s>>>(g, in, mode, uvw, foc, sorted, tasks, ntasks, grids,
+                                                                pg0, npg, gmax, batch, err);
+  }
   check_cuda(cudaGetLastError(), "grid kernel");
+}
+
+template <int S>
+void launch_grid_tc(int gmax, unsigned nblocks, cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode,
+                    const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
+                    const uint32_t* ntasks, cplx<float>* grids, int pg0, int npg, int* err) {
+  const int threads = 32 * std::max(gmax, 4);
+  const int smem = gmax * g.L * g.L * (int)sizeof(cplx<float>) + threads * (int)TcStaging<S>::bytes_per_vis();
+  check_cuda(cudaFuncSetAttribute(k_grid_tc<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
+  {
+    StageTimer timer_(ST_GRID, s);
+    k_grid_tc<S><<<nblocks, threads, smem, s>>>(g, in, mode, uvw, foc, sorted, tasks, ntasks, grids, pg0, npg, gmax,
+                                                err);
+  }
+  check_cuda(cudaGetLastError(), "grid kernel (tensor cores)");
 }
 
 template <class T, int S>
@@ -717,8 +1141,11 @@ void launch_degrid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g,
                    const uint32_t* ntasks, const cplx<T>* grids, int pg0, int npg, int gmax, cplx<T>* vis,
                    int first, int last, int* err) {
   check_cuda(cudaFuncSetAttribute(k_degrid<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
-  k_degrid<T, S><<<nblocks, GRID_THREADS, smem, s>>>(g, wts, uvw, foc, sorted, tasks, ntasks, grids, pg0, npg, gmax,
-                                                     vis, first, last, err);
+  {
+    StageTimer timer_(ST_DEGRID, s);
+    k_degrid<T, S><<<nblocks, GRID_THREADS, smem, s>>>(g, wts, uvw, foc, sorted, tasks, ntasks, grids, pg0, npg, gmax,
+                                                       vis, first, last, err);
+  }
   check_cuda(cudaGetLastError(), "degrid kernel");
 }
 
@@ -759,6 +1186,69 @@ void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw DeviceError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+const char* const STAGE_NAMES[N_STAGES] = {"scan", "bin_count", "prefix", "bin_scatter", "tasks", "corr", "grid",
+                                           "fft", "project", "correct_input", "place", "degrid", "other"};
+
+namespace {
+struct Profiler {
+  std::atomic<bool> on{false};
+  std::atomic<long long> launches{0};
+  std::mutex mu;
+  struct Rec {
+    int stage;
+    int n;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  long long counts[N_STAGES] = {};
+};
+Profiler& profiler() {
+  static Profiler p;
+  return p;
+}
+}  // namespace
+
+StageTimer::StageTimer(Stage st, cudaStream_t s, int launches) : st_(st), s_(s) {
+  Profiler& p = profiler();
+  if (st != ST_FFT) p.launches += launches;
+  if (p.on.load()) {
+    check_cuda(cudaEventCreate(&a_), "event");
+    check_cuda(cudaEventCreate(&b_), "event");
+    check_cuda(cudaEventRecord(a_, s_), "event");
+    std::lock_guard<std::mutex> lock(p.mu);
+    p.counts[st] += launches;
+  }
+}
+
+StageTimer::~StageTimer() {
+  if (!a_) return;
+  Profiler& p = profiler();
+  cudaEventRecord(b_, s_);
+  std::lock_guard<std::mutex> lock(p.mu);
+  p.recs.push_back({(int)st_, 0, a_, b_});
+}
+
+void profile_enable(bool on) { profiler().on = on; }
+
+long long launch_count() { return profiler().launches.load(); }
+
+void profile_read(long long* launches, double* ms) {
+  Profiler& p = profiler();
+  std::lock_guard<std::mutex> lock(p.mu);
+  for (int i = 0; i < N_STAGES; i++) {
+    launches[i] = p.counts[i];
+    ms[i] = 0.0;
+    p.counts[i] = 0;
+  }
+  for (auto& r : p.recs) {
+    float t = 0.0f;
+    if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) ms[r.stage] += t;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  p.recs.clear();
+}
+
 DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
   if (this != &o) {
     release();
@@ -784,6 +1274,22 @@ void DevBuf::release() {
   p_ = nullptr;
   n_ = 0;
 }
+
+namespace {
+std::atomic<int> g_method{-1};
+}
+
+int grid_method() {
+  int m = g_method.load();
+  if (m < 0) {
+    const char* e = std::getenv("RANG_WGRIDDER_GPU_METHOD");
+    m = (e && std::string(e) == "fp32") ? GRID_FP32 : GRID_TF32X3;
+    g_method = m;
+  }
+  return m;
+}
+
+void set_grid_method(int m) { g_method = m; }
 
 int max_window_planes(int L, size_t cell_bytes) {
   size_t per = (size_t)L * L * cell_bytes;
@@ -812,8 +1318,11 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   check_cuda(cudaMemcpyAsync(so.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s), "copy");
   double fw = o.flip_w ? 1.0 : -1.0;
   if (n_) {
-    k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw_.as<double>(),
-                                                  foc_.as<double>(), fw, act, with_vis ? 1 : 0, so.as<ScanOut>());
+    {
+      StageTimer timer_(ST_SCAN, s);
+      k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw_.as<double>(),
+                                                    foc_.as<double>(), fw, act, with_vis ? 1 : 0, so.as<ScanOut>());
+    }
     check_cuda(cudaGetLastError(), "scan kernel");
   }
   ScanOut r;
@@ -836,35 +1345,49 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
 template <class T>
 void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
   ntiles_ = (size_t)g_.ntu * g_.ntv;
-  nbins_ = ntiles_ * (size_t)g_.nbuckets;
+  nbins_ = ntiles_ * (size_t)g_.nbuckets * (size_t)g_.nsub;
   if (nbins_ >= 0xffffffffull) throw InvalidArgument("too many uv tiles and w-planes for one call");
   key_.alloc(n_ * 4, s);
   starts_.alloc((nbins_ + 1) * 4, s);
   check_cuda(cudaMemsetAsync(starts_.get(), 0, (nbins_ + 1) * 4, s), "memset");
-  k_bin_count<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act,
-                                                      with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>());
+  {
+    StageTimer timer_(ST_BIN_COUNT, s);
+    k_bin_count<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act,
+                                                        with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>());
+  }
   check_cuda(cudaGetLastError(), "bin count");
   exclusive_scan(starts_.as<uint32_t>(), starts_.as<uint32_t>(), nbins_ + 1, s);
   {
     DevBuf cursor((nbins_ + 1) * 4, s);
     check_cuda(cudaMemcpyAsync(cursor.get(), starts_.get(), (nbins_ + 1) * 4, cudaMemcpyDeviceToDevice, s), "copy");
     sorted_.alloc(nvis_ * 4, s);
-    k_bin_scatter<<<blocks_for(n_, 256), 256, 0, s>>>(n_, key_.as<uint32_t>(), cursor.as<uint32_t>(),
-                                                       sorted_.as<uint32_t>());
+    {
+      StageTimer timer_(ST_BIN_SCATTER, s);
+      k_bin_scatter<<<blocks_for(n_, 256), 256, 0, s>>>(n_, key_.as<uint32_t>(), cursor.as<uint32_t>(),
+                                                         sorted_.as<uint32_t>());
+    }
     check_cuda(cudaGetLastError(), "bin scatter");
   }
   // Tasks.
   max_tasks_ = nvis_ / TASK_CHUNK + ntiles_ + 1;
   DevBuf ntask((ntiles_ + 1) * 4, s);
-  k_task_count<<<(unsigned)((ntiles_ + 1 + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(), (uint32_t)g_.nbuckets,
-                                                                     (uint32_t)ntiles_, ntask.as<uint32_t>());
+  {
+    StageTimer timer_(ST_TASKS, s);
+    k_task_count<<<(unsigned)((ntiles_ + 1 + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(),
+                                                                       (uint32_t)(g_.nbuckets * g_.nsub),
+                                                                       (uint32_t)ntiles_, ntask.as<uint32_t>());
+  }
   check_cuda(cudaGetLastError(), "tasks");
   exclusive_scan(ntask.as<uint32_t>(), ntask.as<uint32_t>(), ntiles_ + 1, s);
   tasks_.alloc(max_tasks_ * sizeof(Task), s);
   ntasks_.alloc(4, s);
-  k_task_emit<<<(unsigned)((ntiles_ + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(), (uint32_t)g_.nbuckets,
-                                                                (uint32_t)ntiles_, ntask.as<uint32_t>(),
-                                                                tasks_.as<Task>(), ntasks_.as<uint32_t>());
+  {
+    StageTimer timer_(ST_TASKS, s);
+    k_task_emit<<<(unsigned)((ntiles_ + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(),
+                                                                  (uint32_t)(g_.nbuckets * g_.nsub), (uint32_t)g_.nsub,
+                                                                  (uint32_t)ntiles_, ntask.as<uint32_t>(),
+                                                                  tasks_.as<Task>(), ntasks_.as<uint32_t>());
+  }
   check_cuda(cudaGetLastError(), "tasks");
   corrections(s);
 }
@@ -890,7 +1413,10 @@ void Plan<T>::corrections(cudaStream_t s) {
       cn.w[i] = kernel_->corr_w[i];
     }
     double* base = corr_.as<double>();
-    k_corr<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, cn, base, base + nu2, base + nu2 + nv2);
+    {
+      StageTimer timer_(ST_CORR, s);
+      k_corr<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, cn, base, base + nu2, base + nu2 + nv2);
+    }
     check_cuda(cudaGetLastError(), "corrections");
   }
 }
@@ -920,18 +1446,26 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s)
   DevBuf grids(group * plane * cell, s);
   DevBuf acc(group < nplanes ? npix * sizeof(T) : 0, s);
   FftPair& fft = fft_plans<T>(g_.nu, g_.nv, g_.ny);
-  const int gmax = std::min<int>(max_window_planes(g_.L, 2 * sizeof(T)), (int)std::min<size_t>(nplanes, 64));
-  const int smem = gmax * g_.L * g_.L * 2 * (int)sizeof(T);
+  const int gmax = std::min<int>(max_window_planes(g_.L, sizeof(cplx<T>)), (int)std::min<size_t>(nplanes, 64));
+  const int smem = gmax * g_.L * g_.L * (int)sizeof(cplx<T>);
   const double* corr = corr_.as<double>();
   const size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
   for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
     int n = (int)std::min(group, nplanes - pg0);
     check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
     auto run = [&](auto S) {
-      launch_grid<T, decltype(S)::value>(smem, (unsigned)max_tasks_, s, g_, data, (int)mode, uvw_.as<double>(),
-                                         foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>(),
-                                         ntasks_.as<uint32_t>(), grids.as<cplx<T>>(), (int)pg0, n, gmax,
-                                         err_.as<int>());
+      constexpr int SV = decltype(S)::value;
+      if constexpr (sizeof(T) == 4) {
+        if (grid_method() == GRID_TF32X3) {
+          launch_grid_tc<SV>(gmax, (unsigned)max_tasks_, s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(),
+                             sorted_.as<uint32_t>(), tasks_.as<Task>(), ntasks_.as<uint32_t>(), grids.as<cplx<T>>(),
+                             (int)pg0, n, err_.as<int>());
+          return;
+        }
+      }
+      launch_grid<T, SV>(smem, (unsigned)max_tasks_, s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(),
+                         sorted_.as<uint32_t>(), tasks_.as<Task>(), ntasks_.as<uint32_t>(), grids.as<cplx<T>>(),
+                         (int)pg0, n, gmax, err_.as<int>());
     };
     if constexpr (sizeof(T) == 4)
       with_supp_float(g_.supp, run);
@@ -939,13 +1473,17 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s)
       with_supp_double(g_.supp, run);
     for (int p = 0; p < n; p++) {
       cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
+      StageTimer timer_(ST_FFT, s, 3);
       fft_rows<T>(fft, pl, CUFFT_INVERSE, s);
       fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_INVERSE, s);
     }
     bool first = pg0 == 0, last = pg0 + n >= nplanes;
-    k_project<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, grids.as<cplx<T>>(), (int)pg0, n, acc.as<T>(), first,
-                                                       last, g_.do_wgridding ? corr + nu2 + nv2 : nullptr, corr,
-                                                       corr + nu2, image);
+    {
+      StageTimer timer_(ST_PROJECT, s);
+      k_project<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, grids.as<cplx<T>>(), (int)pg0, n, acc.as<T>(), first,
+                                                         last, g_.do_wgridding ? corr + nu2 + nv2 : nullptr, corr,
+                                                         corr + nu2, image);
+    }
     check_cuda(cudaGetLastError(), "project");
   }
 }
@@ -964,8 +1502,11 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s) 
   FftPair& fft = fft_plans<T>(g_.nu, g_.nv, g_.ny);
   const double* corr = corr_.as<double>();
   const size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
-  k_correct_input<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, image, g_.do_wgridding ? corr + nu2 + nv2 : nullptr,
-                                                           corr, corr + nu2, img.as<T>());
+  {
+    StageTimer timer_(ST_CORRECT_INPUT, s);
+    k_correct_input<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, image, g_.do_wgridding ? corr + nu2 + nv2 : nullptr,
+                                                             corr, corr + nu2, img.as<T>());
+  }
   check_cuda(cudaGetLastError(), "correct");
   const int gmax = std::min<int>(max_window_planes(g_.L, sizeof(cplx<T>)), (int)std::min<size_t>(nplanes, 64));
   const int smem = gmax * g_.L * g_.L * (int)sizeof(cplx<T>);
@@ -974,10 +1515,16 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s) 
     check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
     for (int p = 0; p < n; p++) {
       cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
-      k_place<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, img.as<T>(), (int)pg0 + p, pl);
+      {
+        StageTimer timer_(ST_PLACE, s);
+        k_place<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, img.as<T>(), (int)pg0 + p, pl);
+      }
       check_cuda(cudaGetLastError(), "place");
-      fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_FORWARD, s);
-      fft_rows<T>(fft, pl, CUFFT_FORWARD, s);
+      {
+        StageTimer timer_(ST_FFT, s, 3);
+        fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_FORWARD, s);
+        fft_rows<T>(fft, pl, CUFFT_FORWARD, s);
+      }
     }
     bool first = pg0 == 0, last = pg0 + n >= nplanes;
     auto run = [&](auto S) {
@@ -1008,6 +1555,9 @@ void Plan<T>::export_binning(uint32_t* key_host, uint32_t* sorted_host, cudaStre
   check_cuda(cudaMemcpyAsync(key_host, key_.get(), n_ * 4, cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaMemcpyAsync(sorted_host, sorted_.get(), nvis_ * 4, cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaStreamSynchronize(s), "copy");
+  // The reference's key, tile * nbuckets + plane, without the sub-tile.
+  for (size_t i = 0; i < n_; i++)
+    if (key_host[i] != INACTIVE) key_host[i] /= (uint32_t)g_.nsub;
 }
 
 template <class T>
@@ -1015,8 +1565,11 @@ void Plan<T>::export_pixels(const Inputs& act, bool with_vis, int64_t* iu0_host,
                             cudaStream_t s) const {
   if (nvis_ == 0) return;
   DevBuf a(n_ * 8, s), b(n_ * 8, s);
-  k_pixels<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act, with_vis ? 1 : 0,
-                                                  a.as<int64_t>(), b.as<int64_t>());
+  {
+    StageTimer timer_(ST_OTHER, s);
+    k_pixels<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act, with_vis ? 1 : 0,
+                                                    a.as<int64_t>(), b.as<int64_t>());
+  }
   check_cuda(cudaGetLastError(), "pixels");
   check_cuda(cudaMemcpyAsync(iu0_host, a.get(), n_ * 8, cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaMemcpyAsync(iv0_host, b.get(), n_ * 8, cudaMemcpyDeviceToHost, s), "copy");

@@ -82,8 +82,8 @@ class Plan {
   // Waits for `s` and returns the inconsistencies the kernels flagged (0: none).
   int kernel_errors(cudaStream_t s) const;
 
-  // For the tests: per visibility (row-major) the bin key tile * nbuckets +
-  // first plane (0xffffffff inactive), and the sorted order.
+  // For the tests: per visibility (row-major) the reference's bin key
+  // tile * nbuckets + first plane (0xffffffff inactive), and the sorted order.
   void export_binning(uint32_t* key_host, uint32_t* sorted_host, cudaStream_t s) const;
   // Per visibility iu0, iv0 (int64) from the device arithmetic, for the tests.
   void export_pixels(const Inputs& act, bool with_vis, int64_t* iu0_host, int64_t* iv0_host, cudaStream_t s) const;
@@ -111,7 +111,40 @@ class Plan {
   size_t nbins_ = 0, ntiles_ = 0, max_tasks_ = 0;
 };
 
+// How single-precision gridding accumulates footprints: split-precision
+// 3 x TF32 tensor-core products (default) or plain FP32 CUDA-core FMAs.
+// Double precision always uses FP64 CUDA-core FMAs. The environment
+// variable RANG_WGRIDDER_GPU_METHOD (fp32 | tf32x3) sets the default.
+enum GridMethod : int { GRID_FP32 = 0, GRID_TF32X3 = 1 };
+int grid_method();
+void set_grid_method(int method);
+
 // The largest shared-memory tile window (planes) per CTA.
 int max_window_planes(int L, size_t cell_bytes);
+
+// Stages of the pipeline, for the launch counter and the event profiler.
+enum Stage : int {
+  ST_SCAN = 0, ST_BIN_COUNT, ST_PREFIX, ST_BIN_SCATTER, ST_TASKS, ST_CORR, ST_GRID, ST_FFT, ST_PROJECT,
+  ST_CORRECT_INPUT, ST_PLACE, ST_DEGRID, ST_OTHER, N_STAGES
+};
+extern const char* const STAGE_NAMES[N_STAGES];
+
+// Brackets the launches of one stage on `s`: counts them and, while the
+// profiler is on, records a CUDA event pair around them.
+class StageTimer {
+ public:
+  StageTimer(Stage st, cudaStream_t s, int launches = 1);
+  ~StageTimer();
+
+ private:
+  Stage st_;
+  cudaStream_t s_;
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+};
+
+void profile_enable(bool on);
+// Totals per stage since the last read (waits for the recorded events).
+void profile_read(long long* launches, double* ms);
+long long launch_count();
 
 }  // namespace wg

@@ -329,6 +329,8 @@ void make_geom(const WgridderOptions& o, size_t nrow, size_t nchan, size_t nvis,
   g.ntu = (int32_t)((nu + tile - 1) / tile);
   g.ntv = (int32_t)((nv + tile - 1) / tile);
   g.L = tile + (int32_t)supp - 1;
+  g.nsub_side = tile >> 3;
+  g.nsub = g.nsub_side * g.nsub_side;
   g.do_wgridding = wgrid;
   g.lmshift = lmshift;
   g.shifting = lmshift || nshift != 0.0;

@@ -3,9 +3,10 @@ oracle and the FP64 DFT.
 
 Tolerances: the integer binning (iu0, iv0, tile, first plane, plan) must be
 bit-identical to the oracle's; images and visibilities agree with the
-oracle's to 1e-10 (f64) and 2e-5 (f32) relative L-inf (the two differ only in
-accumulation order and FFT rounding), and with the DFT to the reference's
-own gates (10 eps, research/df1-wgridder.md:179-203)."""
+oracle's to 1e-9 (f64) and 2e-5 (f32) relative L-inf (the two differ only in
+accumulation order and FFT rounding, which the wide-field correction factors
+amplify up to ~1e5 at the image corners of the 0.3 rad cases), and with the
+DFT to the reference's own gates (10 eps, research/df1-wgridder.md:179-203)."""
 
 from pathlib import Path
 
@@ -18,7 +19,7 @@ from cases import lcg_case, meerkat_like, rel_linf, small_case
 pytestmark = pytest.mark.gpu
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-TOL = {True: 2e-5, False: 1e-10}
+TOL = {True: 2e-5, False: 1e-9}
 
 
 @pytest.fixture(scope="module")
@@ -250,3 +251,39 @@ def test_larger_case_matches_oracle(cw):
         assert rel_linf(d, od) < TOL[single] * 5
         x = rng.standard_normal((nx, ny)).astype(np.float32 if single else np.float64)
         assert rel_linf(cw.dirty2vis(dirty=x, **kw), oracle.dirty2vis(dirty=x, **kw)) < TOL[single] * 5
+
+
+@pytest.fixture
+def method():
+    """Runs a test under one single-precision gridding method and restores
+    the default afterwards."""
+    ext = __import__("rang._core", fromlist=["_core"])
+    old = ext.wgridder_set_method(1)
+    yield ext
+    ext.wgridder_set_method(old)
+
+
+@pytest.mark.parametrize("which", [0, 1], ids=["fp32-cuda-cores", "3xtf32-tensor-cores"])
+def test_single_precision_methods_match_oracle(cw, method, df1, which):
+    """Both single-precision gridding paths, the plain FP32 CUDA-core one and
+    the split-precision 3 x TF32 tensor-core one, stay within the f32
+    tolerance of the oracle and within 10 eps of the FP64 DFT."""
+    method.wgridder_set_method(which)
+    for name, c in df1.items():
+        nx, ny, dx, dy = int(c["nx"]), int(c["ny"]), float(c["dx"]), float(c["dy"])
+        kw = dict(uvw=c["uvw"], freq=c["freq"], wgt=c["wgt"].astype(np.float32), npix_x=nx, npix_y=ny,
+                  pixsize_x=dx, pixsize_y=dy, epsilon=1e-5)
+        vis = c["vis"].astype(np.complex64)
+        d = cw.vis2dirty(vis=vis, **kw)
+        assert rel_linf(d, c["dft_dirty"]) < 1e-4, name
+        assert rel_linf(d, oracle.vis2dirty(vis=vis, **kw)) < TOL[True], name
+    uvw, freq = meerkat_like(nant=64, ntime=8, nchan=16, seed=1)
+    rng = np.random.default_rng(5)
+    shape = (uvw.shape[0], freq.size)
+    vis = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    kw = dict(uvw=uvw, freq=freq, mask=(rng.uniform(size=shape) > 0.2).astype(np.uint8), npix_x=256, npix_y=192,
+              pixsize_x=7e-6, pixsize_y=7e-6, epsilon=1e-5)
+    for opts in ({}, {"do_wgridding": False}, {"center_x": 1e-4}):
+        d, psf = cw.dirty_psf(vis=vis, single=True, **kw, **opts)
+        od, opsf = oracle.dirty_psf(vis=vis, single=True, **kw, **opts)
+        assert rel_linf(d, od) < TOL[True] and rel_linf(psf, opsf) < TOL[True]
