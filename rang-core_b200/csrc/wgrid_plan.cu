@@ -564,7 +564,7 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) 
   lo = to_tf32(x - __uint_as_float(hi));
 }
 __device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
       "{%0,%1,%2,%3};\n"
       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
@@ -750,17 +750,27 @@ __global__ void __launch_bounds__(256)
                 bv[h][1][nt] = w.im * kvv[nt];
               }
             }
+            uint32_t bh[2][2][2], bl[2][2][2];  // [comp][n tile][k half]
 #pragma unroll
             for (int c2 = 0; c2 < 2; c2++)
 #pragma unroll
-              for (int nt = 0; nt < 2; nt++) {
-                uint32_t bh0, bl0, bh1, bl1;
-                split_tf32(bv[0][c2][nt], bh0, bl0);
-                split_tf32(bv[1][c2][nt], bh1, bl1);
-                mma_tf32(acc[c2][nt], ah, bh0, bh1);
-                mma_tf32(acc[c2][nt], ah, bl0, bl1);
-                mma_tf32(acc[c2][nt], al, bh0, bh1);
-              }
+              for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) split_tf32(bv[h][c2][nt], bh[c2][nt][h], bl[c2][nt][h]);
+            // Independent products first: hi * hi on the four accumulators, then
+            // the two cross terms.
+#pragma unroll
+            for (int c2 = 0; c2 < 2; c2++)
+#pragma unroll
+              for (int nt = 0; nt < 2; nt++) mma_tf32(acc[c2][nt], ah, bh[c2][nt][0], bh[c2][nt][1]);
+#pragma unroll
+            for (int c2 = 0; c2 < 2; c2++)
+#pragma unroll
+              for (int nt = 0; nt < 2; nt++) mma_tf32(acc[c2][nt], ah, bl[c2][nt][0], bl[c2][nt][1]);
+#pragma unroll
+            for (int c2 = 0; c2 < 2; c2++)
+#pragma unroll
+              for (int nt = 0; nt < 2; nt++) mma_tf32(acc[c2][nt], al, bh[c2][nt][0], bh[c2][nt][1]);
             blocks++;
           }
           q += kbk;
