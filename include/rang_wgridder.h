@@ -160,6 +160,33 @@ int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, siz
                                    int64_t* iv0, uint32_t* key, uint32_t* sorted, size_t* nsorted,
                                    double* info);
 
+/* The visibility binning of rang_b200_wgridder_plan_create (scan, kernel and
+ * grid choice, counting sort by uv tile and first w-plane) without any
+ * device allocation. It has no counterpart in the reference. It is for
+ * callers that cannot call cudaMalloc: an application whose device memory is
+ * all handed out by its own allocator under a fixed budget, or a path that
+ * must not take the CUDA allocator's locks or wait on it. Every temporary
+ * lives in one 16 MiB array that the library holds on each GPU that loads it
+ * (NOALLOC_SCRATCH_BYTES); a call whose bin counters and scan do not fit in
+ * it fails with status 1 and says how many bytes it needed. The first call on
+ * a device looks up that array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture. All calls share the array, so
+ * calls whose GPU work overlaps race: run them on one stream, or wait for one
+ * before starting another. The call clears what must start at zero and
+ * returns when its work on `stream` is done.
+ * Inputs: uvw_dev (nrow * 3 doubles) and the optional weights wgt_dev
+ * (WGRIDDER_WGT_NONE, _F32 or _F64) and mask_dev (nrow * nchan) are device
+ * arrays; freq is a host array; the active set is wgt * mask != 0 (as for
+ * degridding). Outputs, device arrays of nrow * nchan entries: key_dev, per
+ * visibility (row-major) tile * max(nplanes, 1) + first plane, 0xffffffff
+ * when inactive; sorted_dev, the active visibilities' linear indices in
+ * (tile, first plane) order, *nsorted of them; info, the plan's 14
+ * doubles. */
+int32_t rang_b200_wgridder_bin_noalloc(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                       const double* uvw_dev, const double* freq, const void* wgt_dev,
+                                       int32_t wgt_kind, const uint8_t* mask_dev, int32_t single, void* stream,
+                                       uint32_t* key_dev, uint32_t* sorted_dev, size_t* nsorted, double* info);
+
 /* Instrumentation (no counterpart in the reference, whose timing report is
  * RANG_WGRIDDER_TIMING on stderr, wgridder.rs:1773-1812). The launch count
  * is the number of this library's own CUDA kernels launched so far (cuFFT's

@@ -192,6 +192,8 @@ void host_dirty2vis(const WgridderOptions* o, size_t nrow, size_t nchan, const d
 
 }  // namespace
 
+std::string* wg::last_error_slot() { return &g_last_error; }
+
 struct RangWgridPlan {
   int single = 0;
   std::unique_ptr<Plan<float>> f;

@@ -1590,3 +1590,159 @@ template class Plan<float>;
 template class Plan<double>;
 
 }  // namespace wg
+
+// ------------------------------------------------------------------ binning without allocation
+
+// The visibility binning of a call with every temporary in one file-scope
+// device array instead of allocated memory, for callers that must not
+// allocate device memory. The array is NOALLOC_SCRATCH_BYTES on every device
+// that loads the library, for the life of the process. Its address is taken
+// once per device with cudaGetSymbolAddress (a symbol's host-side name is not
+// a device address). All calls share it: the counters are cleared on every
+// call, and calls whose work overlaps on the GPU race on it.
+namespace wg {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = 16u << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+// The scratch address on the current device, looked up on first use.
+unsigned char* noalloc_scratch() {
+  static std::mutex mu;
+  static std::map<int, unsigned char*> addr;
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "no CUDA device");
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = addr.find(dev);
+  if (it != addr.end()) return it->second;
+  void* p = nullptr;
+  check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "no-allocation scratch address");
+  addr[dev] = static_cast<unsigned char*>(p);
+  return addr[dev];
+}
+
+// exclusive_scan with the tile sums of every level in `tmp` (no allocation).
+void exclusive_scan_in(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* tmp, cudaStream_t s) {
+  uint64_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  k_scan_tiles<<<(unsigned)ntiles, SCAN_THREADS, 0, s>>>(in, out, n, tmp);
+  check_cuda(cudaGetLastError(), "scan");
+  if (ntiles > 1) {
+    exclusive_scan_in(tmp, tmp, ntiles, tmp + ntiles, s);
+    k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, tmp);
+    check_cuda(cudaGetLastError(), "scan");
+  }
+}
+
+uint64_t scan_tmp_words(uint64_t n) {
+  uint64_t words = 0;
+  for (uint64_t m = (n + SCAN_TILE - 1) / SCAN_TILE; m > 1; m = (m + SCAN_TILE - 1) / SCAN_TILE) words += m;
+  return words + 2;
+}
+
+__global__ void k_reference_key(uint64_t n, uint32_t nsub, uint32_t* __restrict__ key) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    if (key[i] != INACTIVE) key[i] /= nsub;
+}
+
+template <class T>
+void bin_noalloc(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw, const double* freq,
+                 const Inputs& act, cudaStream_t s, uint32_t* key, uint32_t* sorted, size_t* nsorted, double* info) {
+  check_common(o, nrow, nchan);
+  const uint64_t n = (uint64_t)nrow * nchan;
+  if (n >= 0xffffffffull) throw InvalidArgument("too many visibilities for one call (at most 2^32 - 2)");
+  double r_l, r_m;
+  recentring(o, r_l, r_m);
+  std::vector<double> foc = f_over_c(freq, nchan);
+  // Scratch layout: the scan result, the channel factors, then u32 words.
+  unsigned char* base = noalloc_scratch();
+  const size_t foc_off = 256, words_off = (foc_off + nchan * sizeof(double) + 255) / 256 * 256;
+  if (words_off > NOALLOC_SCRATCH_BYTES)
+    throw InvalidArgument("too many channels for the no-allocation scratch (" +
+                          std::to_string(NOALLOC_SCRATCH_BYTES) + " bytes)");
+  ScanOut* so = reinterpret_cast<ScanOut*>(base);
+  double* dfoc = reinterpret_cast<double*>(base + foc_off);
+  ScanOut init{0, 0, 0, 0};
+  const double big = 1e300;
+  std::memcpy(&init.lo_bits, &big, sizeof(big));
+  check_cuda(cudaMemcpyAsync(so, &init, sizeof(init), cudaMemcpyHostToDevice, s), "copy");
+  check_cuda(cudaMemcpyAsync(dfoc, foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, s), "copy");
+  const double fw = o.flip_w ? 1.0 : -1.0;
+  if (n) {
+    k_scan<T><<<blocks_for(n, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw, dfoc, fw, act, 0, so);
+    check_cuda(cudaGetLastError(), "scan kernel");
+  }
+  ScanOut r;
+  check_cuda(cudaMemcpyAsync(&r, so, sizeof(r), cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaStreamSynchronize(s), "scan");
+  *nsorted = r.count;
+  if (r.count == 0) {
+    std::memset(info, 0, N_INFO * sizeof(double));
+    if (n) check_cuda(cudaMemsetAsync(key, 0xff, n * sizeof(uint32_t), s), "memset");
+    check_cuda(cudaStreamSynchronize(s), "binning");
+    return;
+  }
+  double wmin_d = 1e300, wmax_d = -1e300;
+  if (r.finite) {
+    std::memcpy(&wmin_d, &r.lo_bits, sizeof(double));
+    std::memcpy(&wmax_d, &r.hi_bits, sizeof(double));
+  }
+  Geom<T> g;
+  PlanInfo pi;
+  EsKernel* kernel = nullptr;
+  make_geom<T>(o, nrow, nchan, r.count, wmin_d, wmax_d, r_l, r_m, g, pi, kernel);
+  const uint64_t nbins = (uint64_t)g.ntu * g.ntv * g.nbuckets * g.nsub;
+  const uint64_t need_words = 2 * (nbins + 1) + scan_tmp_words(nbins + 1);
+  const uint64_t have_words = (NOALLOC_SCRATCH_BYTES - words_off) / sizeof(uint32_t);
+  if (need_words > have_words)
+    throw InvalidArgument("the binning needs " + std::to_string(words_off + need_words * 4) +
+                          " bytes of scratch; the no-allocation scratch holds " +
+                          std::to_string(NOALLOC_SCRATCH_BYTES) + " bytes");
+  uint32_t* counts = reinterpret_cast<uint32_t*>(base + words_off);
+  uint32_t* cursor = counts + (nbins + 1);
+  uint32_t* tmp = cursor + (nbins + 1);
+  check_cuda(cudaMemsetAsync(counts, 0, (nbins + 1) * sizeof(uint32_t), s), "memset");
+  k_bin_count<T><<<blocks_for(n, 256), 256, 0, s>>>(g, uvw, dfoc, act, 0, key, counts);
+  check_cuda(cudaGetLastError(), "bin count");
+  exclusive_scan_in(counts, counts, nbins + 1, tmp, s);
+  check_cuda(cudaMemcpyAsync(cursor, counts, (nbins + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s), "copy");
+  k_bin_scatter<<<blocks_for(n, 256), 256, 0, s>>>(n, key, cursor, sorted);
+  check_cuda(cudaGetLastError(), "bin scatter");
+  k_reference_key<<<blocks_for(n, 256), 256, 0, s>>>(n, (uint32_t)g.nsub, key);
+  check_cuda(cudaGetLastError(), "keys");
+  check_cuda(cudaStreamSynchronize(s), "binning");
+  std::memcpy(info, pi.v, sizeof(pi.v));
+}
+
+}  // namespace
+}  // namespace wg
+
+extern "C" int32_t rang_b200_wgridder_bin_noalloc(const WgridderOptions* opts, size_t nrow, size_t nchan,
+                                                  const double* uvw_dev, const double* freq, const void* wgt_dev,
+                                                  int32_t wgt_kind, const uint8_t* mask_dev, int32_t single,
+                                                  void* stream, uint32_t* key_dev, uint32_t* sorted_dev,
+                                                  size_t* nsorted, double* info) {
+  using namespace wg;
+  std::string* err = last_error_slot();
+  try {
+    if (!opts) throw InvalidArgument("null options");
+    if ((!uvw_dev && nrow) || !freq || !info || !nsorted || ((!key_dev || !sorted_dev) && nrow))
+      throw InvalidArgument("null array");
+    if (!((wgt_kind == WGT_NONE) || (wgt_dev && (wgt_kind == WGT_F32 || wgt_kind == WGT_F64))))
+      throw InvalidArgument("invalid weight array or kind");
+    Inputs act{nullptr, VIS_UNIT, wgt_dev, nullptr, wgt_kind, mask_dev};
+    if (single)
+      bin_noalloc<float>(*opts, nrow, nchan, uvw_dev, freq, act, (cudaStream_t)stream, key_dev, sorted_dev, nsorted,
+                         info);
+    else
+      bin_noalloc<double>(*opts, nrow, nchan, uvw_dev, freq, act, (cudaStream_t)stream, key_dev, sorted_dev, nsorted,
+                          info);
+    return 0;
+  } catch (const InvalidArgument& e) {
+    *err = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    *err = e.what();
+    return 2;
+  }
+}

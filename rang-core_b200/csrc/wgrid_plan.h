@@ -143,6 +143,8 @@ class StageTimer {
 };
 
 void profile_enable(bool on);
+// This thread's last-error message of the C ABI.
+std::string* last_error_slot();
 // Totals per stage since the last read (waits for the recorded events).
 void profile_read(long long* launches, double* ms);
 long long launch_count();
