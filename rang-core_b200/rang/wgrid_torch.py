@@ -116,6 +116,28 @@ class DevicePlan:
                                                      _stream(self.device)))
         return out
 
+    def residual(self, data, wgt, model=None, mask=None, out=None):
+        """The residual image of `data` against the image `model` (None: the
+        data alone), gridded with weights `wgt`, and the misfit
+        sum w |data - A model|^2 over the active visibilities (the
+        reference's Prepared::residual, core/src/wgridder.rs:3232-3395: the
+        prediction is degridded without weights, the residual gridded with
+        them). Returns (image, misfit as a Python float)."""
+        r = data if model is None else data - self.degrid(model)
+        w = torch.ones_like(r.real) if wgt is None else wgt.to(r.real.dtype)
+        act = w != 0
+        if mask is not None:
+            act = act & (mask != 0)
+        q = torch.sum(torch.where(act, w.double() * (r.real.double() ** 2 + r.imag.double() ** 2), 0.0))
+        r = r.to(self.cplx).contiguous()
+        return self.grid(r, wgt, out=out), float(q)
+
+    def gram(self, x, wgt=None, out=None):
+        """A^H W A x: the image of the unweighted prediction of `x`, gridded
+        with the weights (the reference's gram_apply,
+        core/src/clean_certified.rs:233-236)."""
+        return self.grid(self.degrid(x).contiguous(), wgt, out=out)
+
     def status(self):
         """Waits for the stream; raises if a kernel flagged an inconsistency."""
         _check(core.extension().wgridder_plan_status(self._handle, _stream(self.device)))
@@ -128,8 +150,9 @@ class Degrid(torch.autograd.Function):
     @staticmethod
     def forward(ctx, image, plan, wgt):
         ctx.plan = plan
-        ctx.save_for_backward(wgt) if wgt is not None else None
         ctx.has_wgt = wgt is not None
+        if wgt is not None:
+            ctx.save_for_backward(wgt)
         return plan.degrid(image, wgt)
 
     @staticmethod
