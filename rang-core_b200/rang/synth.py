@@ -69,6 +69,32 @@ def point_sky(npix, nsrc=50, smin=1e-3, smax=1.0, index=-1.5, seed=11, margin=8)
     return img
 
 
+def extended_sky(npix, npoint=300, ngauss=40, smin=1e-3, smax=1.0, index=-1.5, seed=21, margin=40):
+    """An (npix, npix) float32 sky: `npoint` point sources and `ngauss`
+    elliptical Gaussians (FWHM 3-30 pixels along each axis, random
+    orientation), all inside `margin` pixels of the edge. Every source's
+    integrated flux follows the power law of `point_sky`."""
+    rng = np.random.default_rng(seed)
+    img = point_sky(npix, nsrc=npoint, smin=smin, smax=smax, index=index, seed=seed + 1, margin=margin)
+    a = index + 1.0
+    yy, xx = np.mgrid[0:npix, 0:npix].astype(np.float32)
+    for _ in range(ngauss):
+        flux = (smin**a + rng.uniform() * (smax**a - smin**a)) ** (1.0 / a)
+        fx, fy = rng.uniform(3.0, 30.0, 2)
+        th = rng.uniform(0.0, np.pi)
+        cx, cy = rng.uniform(margin, npix - margin, 2)
+        sx, sy = fx / 2.3548, fy / 2.3548
+        ct, st = np.cos(th), np.sin(th)
+        h = int(4 * max(sx, sy)) + 1
+        x0, x1 = int(max(cx - h, 0)), int(min(cx + h + 1, npix))
+        y0, y1 = int(max(cy - h, 0)), int(min(cy + h + 1, npix))
+        dx, dy = xx[y0:y1, x0:x1] - cx, yy[y0:y1, x0:x1] - cy
+        u = (ct * dx + st * dy) / sx
+        v = (-st * dx + ct * dy) / sy
+        img[y0:y1, x0:x1] += flux / (2.0 * np.pi * sx * sy) * np.exp(-0.5 * (u * u + v * v))
+    return img.astype(np.float32)
+
+
 # The workloads of the benchmark configurations.
 WORKLOADS = {
     # 64 antennas x 512 integrations x 1024 channels: 1,056,964,608 visibilities,
@@ -77,4 +103,8 @@ WORKLOADS = {
     # 64 antennas x 128 integrations x 64 channels: 16.5 M visibilities, no flags,
     # 1024^2 image at 1.5 arcsec.
     "ms2dirty 16.5M vis 1024^2": dict(ntime=128, nchan=64, npix=1024, cell_arcsec=1.5, flag=0.0),
+    # The round trip's field of view at a quarter of the pixels and an eighth of
+    # the integrations (132 M visibilities, 2048^2 at 2.0 arcsec): a profiling
+    # case a few GB in size.
+    "ms2dirty+dirty2ms 132M vis 2048^2": dict(ntime=64, nchan=1024, npix=2048, cell_arcsec=2.0, flag=0.2),
 }
