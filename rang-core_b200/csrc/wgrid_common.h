@@ -41,7 +41,9 @@ struct Geom {
   int32_t nx, ny, nu, nv;
   int32_t supp, nplanes, nbuckets;  // nbuckets = max(nplanes, 1)
   int32_t log2tile, ntu, ntv, L;    // L = tile + supp - 1
-  int32_t nsub_side, nsub;          // 8-cell sub-tiles of a tile: per side and in all
+  // Sub-tiles of a tile, 8 cells along u by 2^log2subv along v: nsub_side
+  // along u, nsub_v along v, nsub in all.
+  int32_t nsub_side, nsub_v, log2subv, nsub;
   int32_t ne;                       // rows of even (and of odd) coefficients
   int32_t do_wgridding, shifting, lmshift, divide_by_n;
   double fu, fv, fw;  // +-1: flips (w already negated as the reference does)

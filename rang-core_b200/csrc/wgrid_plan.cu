@@ -133,7 +133,7 @@ __device__ __forceinline__ uint32_t bin_of(const Geom<T>& g, const double* __res
   const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
   const uint32_t tu = su >> g.log2tile, tv = sv >> g.log2tile;
   const uint32_t mask = (1u << g.log2tile) - 1u;
-  const uint32_t sub = ((su & mask) >> 3) * (uint32_t)g.nsub_side + ((sv & mask) >> 3);
+  const uint32_t sub = ((su & mask) >> 3) * (uint32_t)g.nsub_v + ((sv & mask) >> g.log2subv);
   if (piu0) *piu0 = iu0;
   if (piv0) *piv0 = iv0;
   return ((tu * (uint32_t)g.ntv + tv) * (uint32_t)g.nbuckets + (uint32_t)minplane(g, w)) * (uint32_t)g.nsub + sub;
@@ -543,25 +543,67 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
 
 // ------------------------------------------------------------------ tensor-core gridding (3 x TF32)
 
-// The separable footprint of a block of K visibilities on one plane is a
-// rank-K product: T[i][n] += sum_k A[i][k] B[k][n] with A[i][k] the u taps of
-// visibility k placed at its row in a 16-row sub-tile window and
-// B[k][n] = value_k * kw_k(plane) * kv_k[n - offset], so one warp that owns
-// one w-plane of the tile window accumulates each 8 x 8 sub-tile's 16 x 16
-// window with mma.sync m16n8k8 (TF32 inputs, FP32 accumulation). Each
-// operand is split as x = hi + lo in TF32 and the product formed as
-// hi*hi + hi*lo + lo*hi (3 x TF32), which keeps about 21 bits of each
-// factor. Operands come straight from the staged taps into registers: the
-// footprint is sparse (S of 16 rows per column), so forming it costs less
-// than staging it through shared memory for tcgen05.
+// The footprints of K visibilities that share a sub-tile and first w-plane
+// (one bin of the sorted order) form, on each of their planes j, a rank-K
+// update of one 16 x 8 window of the grid:
+//   W_j[i][n] += sum_k A_j[i][k] B[k][n],
+//   A_j[i][k] = kw_k(j) ku_k[i - du_k],   B[k][n] = value_k kv_k[n - dv_k],
+// with du_k, dv_k the visibility's first tap inside the window. One warp
+// takes the bins of a contiguous range of the sorted visibilities, 8 at a
+// time, and issues mma.sync m16n8k8 (TF32 inputs, FP32 accumulation) for the
+// real and imaginary parts of every plane, keeping all planes' windows in
+// registers until the bin ends; the window is then added to the HBM-resident
+// planes with float2 atomics. Operands are split as x = hi + lo in TF32 and
+// each product formed as hi*hi + hi*lo + lo*hi (3 x TF32), keeping about 21
+// bits of each factor. The tensor cores' FP32 accumulation does not round to
+// nearest, so every TC_DRAIN blocks the accumulators are added, with rounded
+// FP32 adds, into a second register copy and restarted from zero.
+//
+// Staging (one visibility per lane) stores, per slot, the u taps at [8, 8+S)
+// of a zero-padded 24-entry column, the pre-split B entries at [8, 8+S) of a
+// 16-entry column, and the S w-taps; the zero padding makes every operand
+// fetch a plain load at index (row - du + 8). Slot TC_BATCH is all zero and
+// stands in for the missing visibilities of a short block.
+constexpr int TC_BATCH = 32;
+constexpr int TC_DRAIN = 8;
+constexpr uint32_t TC_CHUNK = 8192;  // sorted visibilities per warp
+constexpr int TC_UPAD = 24;
+constexpr int TC_VPAD = 16;
+// Slot stride of the B columns in float4s: 2 mod 8, so the 8 lanes of one
+// 128-bit load phase (two rows, four slots) hit distinct bank groups.
+constexpr int TC_VSTRIDE = 18;
+
+struct TcSlots {
+  float4* kb;     // [TC_BATCH + 1][TC_VSTRIDE], TC_VPAD used: (re hi, re lo, im hi, im lo) of value * kv
+  float* ku;      // [TC_BATCH + 1][TC_UPAD]
+  float* kw;      // [TC_BATCH + 1][8]
+  uint32_t* key;  // [TC_BATCH + 1]
+  uint32_t* duv;  // [TC_BATCH + 1]: du | dv << 8
+  // Rounded up to whole float4s, all of which the kernel zeroes.
+  __host__ __device__ static constexpr size_t bytes() {
+    return ((size_t)(TC_BATCH + 1) * (TC_VSTRIDE * sizeof(float4) + TC_UPAD * sizeof(float) + 8 * sizeof(float) + 8) +
+            15) / 16 * 16;
+  }
+  __device__ void carve(unsigned char* base) {
+    kb = reinterpret_cast<float4*>(base);
+    ku = reinterpret_cast<float*>(kb + (TC_BATCH + 1) * TC_VSTRIDE);
+    kw = ku + (TC_BATCH + 1) * TC_UPAD;
+    key = reinterpret_cast<uint32_t*>(kw + (TC_BATCH + 1) * 8);
+    duv = key + (TC_BATCH + 1);
+  }
+};
+
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return r;
 }
-__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
-  hi = to_tf32(x);
-  lo = to_tf32(x - __uint_as_float(hi));
+// x = hi + lo with hi rounded to TF32 (to nearest, ties away; a carry out of
+// the mantissa moves into the exponent as rounding requires); lo is exact in
+// FP32 and the tensor core reads its leading TF32 bits.
+__device__ __forceinline__ void split_fast(float x, uint32_t& hi, uint32_t& lo) {
+  hi = (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
+  lo = __float_as_uint(x - __uint_as_float(hi));
 }
 __device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
   asm(
@@ -571,223 +613,197 @@ __device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-constexpr int TC_DRAIN = 8;
+// The window origin (grid row and column of cell (0, 0)) and first plane of a bin key.
+__device__ __forceinline__ void tc_decode(const Geom<float>& g, uint32_t key, int& su0, int& sv0, int& mp) {
+  const uint32_t sub = key % (uint32_t)g.nsub, t = key / (uint32_t)g.nsub;
+  mp = (int)(t % (uint32_t)g.nbuckets);
+  const uint32_t tile = t / (uint32_t)g.nbuckets;
+  const uint32_t tu = tile / (uint32_t)g.ntv, tv = tile - tu * (uint32_t)g.ntv;
+  // Tiles are laid out on the shifted indices (i0 + n/2) mod n; the grid
+  // itself is stored unshifted.
+  su0 = (int)(((tu << g.log2tile) + (sub / (uint32_t)g.nsub_v) * 8u + (uint32_t)(g.nu - g.nu / 2)) %
+              (uint32_t)g.nu);
+  sv0 = (int)(((tv << g.log2tile) + ((sub % (uint32_t)g.nsub_v) << g.log2subv) + (uint32_t)(g.nv - g.nv / 2)) %
+              (uint32_t)g.nv);
+}
 
+// Adds a bin's windows (both register copies) to its planes of the grid.
 template <int S>
-struct TcStaging {
-  int* grp;       // [B] (first plane << 4 | sub-tile), or -1: not gridded in this window
-  int* duv;       // [B] offsets of the first taps inside the sub-tile: du | dv << 8
-  float* ku;      // [B][S]
-  float* kv;      // [B][S]
-  cplx<float>* cw;  // [B][S] value * kw(plane first + j), zero outside the window
-  static constexpr size_t bytes_per_vis() { return 2 * sizeof(int) + 2 * S * sizeof(float) + S * sizeof(cplx<float>); }
-  __device__ void carve(unsigned char* base, int B) {
-    cw = reinterpret_cast<cplx<float>*>(base);
-    ku = reinterpret_cast<float*>(cw + (size_t)B * S);
-    kv = ku + (size_t)B * S;
-    grp = reinterpret_cast<int*>(kv + (size_t)B * S);
-    duv = grp + B;
-  }
-};
-
-// Adds one warp's 16 x 16 sub-tile accumulators (real and imaginary parts) to
-// its plane of the window.
-__device__ __forceinline__ void tc_flush(cplx<float>* plane, int L, int a8, int b8, const float (&c)[2][2][4]) {
-  const int lane = threadIdx.x & 31, gq = lane >> 2, t = lane & 3;
+__device__ __forceinline__ void tc_flush(const Geom<float>& g, cplx<float>* __restrict__ grids, int pg0, int su0,
+                                         int sv0, int mp, unsigned pact, const float (&acc)[S][2][4],
+                                         const float (&mst)[S][2][4]) {
+  const int lane = threadIdx.x & 31, gq = lane >> 2, tq = lane & 3;
+  const size_t plane = (size_t)g.nu * g.nv;
 #pragma unroll
-  for (int nt = 0; nt < 2; nt++)
+  for (int j = 0; j < S; j++) {
+    if (!((pact >> j) & 1u)) continue;
+    cplx<float>* pl = grids + (size_t)(mp + j - pg0) * plane;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-      const int row = a8 + gq + (r >= 2 ? 8 : 0), col = b8 + 8 * nt + 2 * t + (r & 1);
-      const float re = c[0][nt][r], im = c[1][nt][r];
-      if (row < L && col < L && (re != 0.0f || im != 0.0f)) {
-        cplx<float>* d = plane + row * L + col;
-        cplx<float> o = *d;
-        *d = cplx<float>{o.re + re, o.im + im};
-      }
+      const float re = mst[j][0][r] + acc[j][0][r], im = mst[j][1][r] + acc[j][1][r];
+      if (re == 0.0f && im == 0.0f) continue;
+      int row = su0 + gq + (r >= 2 ? 8 : 0), col = sv0 + 2 * tq + (r & 1);
+      while (row >= g.nu) row -= g.nu;
+      while (col >= g.nv) col -= g.nv;
+      atomicAdd(reinterpret_cast<float2*>(pl + (size_t)row * g.nv + col), make_float2(re, im));
     }
+  }
 }
 
 template <int S>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(TC_BATCH)
     k_grid_tc(const __grid_constant__ Geom<float> g, Inputs in, int mode, const double* __restrict__ uvw,
-              const double* __restrict__ foc, const uint32_t* __restrict__ sorted, const Task* __restrict__ tasks,
-              const uint32_t* __restrict__ ntasks, cplx<float>* __restrict__ grids, int pg0, int npg, int gmax,
-              int* __restrict__ err) {
-  static_assert(S <= 8, "sub-tile windows hold 8 + S - 1 <= 16 rows");
-  using St = TcStaging<S>;
-  if (blockIdx.x >= *ntasks) return;
+              const double* __restrict__ foc, const uint32_t* __restrict__ sorted, uint64_t nsorted,
+              cplx<float>* __restrict__ grids, int pg0, int npg) {
+  static_assert(S <= 8, "windows hold 8 + S - 1 <= 16 rows");
   extern __shared__ __align__(16) unsigned char smem[];
-  const int L = g.L, LL = L * L;
-  const int batch = blockDim.x;
-  cplx<float>* buf = reinterpret_cast<cplx<float>*>(smem);
-  St st;
-  st.carve(smem + (size_t)gmax * LL * sizeof(cplx<float>), batch);
-  const Task t = tasks[blockIdx.x];
-  const int tu = (int)(t.tile / (uint32_t)g.ntv), tv = (int)(t.tile - (uint32_t)tu * (uint32_t)g.ntv);
-  const int bu = tu << g.log2tile, bv = tv << g.log2tile;
-  const unsigned tilesz = 1u << g.log2tile;
-  int lo = 0, hi = 0;
-  if (g.do_wgridding) {
-    lo = max((int)t.plo, pg0);
-    hi = min((int)t.phi + S - 1, pg0 + npg - 1);
-  }
+  TcSlots st;
+  st.carve(smem);
+  const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
+  for (int c = lane; c < (int)(TcSlots::bytes() / 16); c += TC_BATCH)
+    reinterpret_cast<float4*>(smem)[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  __syncwarp();
+  const uint64_t k0 = (uint64_t)blockIdx.x * TC_CHUNK;
+  const uint64_t k1 = min(nsorted, k0 + TC_CHUNK);
   const uint32_t nchan = (uint32_t)g.nchan;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, tq = lane & 3;
-  for (int w0 = lo; w0 <= hi; w0 += gmax) {
-    const int gw = min(gmax, hi - w0 + 1);
-    for (int c = tid; c < gw * LL; c += blockDim.x) buf[c] = cplx<float>{0.0f, 0.0f};
-    float acc[2][2][4];
-    int gcur = -2, a8 = 0, b8 = 0, jpl = 0, blocks = 0;
-    bool act = false;
-    for (uint32_t kb = t.k0; kb < t.k1; kb += (uint32_t)batch) {
-      const int nb = (int)min((uint32_t)batch, t.k1 - kb);
-      __syncthreads();
-      if (tid < nb) {  // staging: one visibility per thread
-        int grp = -1, duv = 0;
-        const uint32_t idx = sorted[kb + tid];
-        const uint32_t row = idx / nchan, ch = idx - row * nchan;
-        double b[3];
-        const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
-        const double f = foc[ch];
-        const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
-        const int mp = minplane(g, w);
-        if (!g.do_wgridding || (mp <= w0 + gw - 1 && mp + S - 1 >= w0)) {
-          double uf, vf;
-          int64_t iu0, iv0;
-          getpix(g, u, v, uf, vf, iu0, iv0);
-          const int ou = offset_in(iu0, g.nu, bu), ov = offset_in(iv0, g.nv, bv);
-          if ((unsigned)ou >= tilesz || (unsigned)ov >= tilesz) {
-            atomicOr(err, 1);
-          } else {
-            float ku[S], kv[S];
-            const float x0 = (float)(-uf * 2.0 + ((double)S - 1.0));
-            const float y0 = (float)(-vf * 2.0 + ((double)S - 1.0));
-            eval_taps2<float, S>(g.coeff, g.ne, x0, y0, ku, kv);
-            cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
-            if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
+  const int np = g.do_wgridding ? S : 1;
+  const uint32_t tmask = (1u << g.log2tile) - 1u;
+  const uint32_t vmask = (1u << g.log2subv) - 1u;
+
+  float acc[S][2][4], mst[S][2][4];
 #pragma unroll
-            for (int j = 0; j < S; j++) {
-              st.ku[tid * S + j] = ku[j];
-              st.kv[tid * S + j] = kv[j];
-              float kw = 0.0f;
-              if (g.do_wgridding) {
-                const int p = mp + j;
-                if (p >= w0 && p < w0 + gw) kw = w_factor<float, S>(g, j, p, w);
-              } else if (j == 0) {
-                kw = 1.0f;
-              }
-              st.cw[tid * S + j] = cplx<float>{val.re * kw, val.im * kw};
-            }
-            const int sub = (ou >> 3) * g.nsub_side + (ov >> 3);
-            grp = (mp << 4) | sub;
-            duv = (ou & 7) | ((ov & 7) << 8);
-          }
+  for (int j = 0; j < S; j++)
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+      for (int r = 0; r < 4; r++) acc[j][c][r] = mst[j][c][r] = 0.0f;
+  uint32_t gcur = INACTIVE;
+  int su0 = 0, sv0 = 0, mpc = 0, blocks = 0;
+  unsigned pact = 0;
+
+  for (uint64_t kb = k0; kb < k1; kb += TC_BATCH) {
+    const int nb = (int)min((uint64_t)TC_BATCH, k1 - kb);
+    __syncwarp();
+    if (lane < nb) {  // staging: one visibility per lane
+      uint32_t key = INACTIVE, duv = 0;
+      const uint32_t idx = sorted[kb + lane];
+      const uint32_t row = idx / nchan, ch = idx - row * nchan;
+      double b[3];
+      const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+      const double f = foc[ch];
+      const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
+      const int mp = minplane(g, w);
+      if (!g.do_wgridding || (mp <= pg0 + npg - 1 && mp + S - 1 >= pg0)) {
+        double uf, vf;
+        int64_t iu0, iv0;
+        getpix(g, u, v, uf, vf, iu0, iv0);
+        const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
+        const uint32_t sub = ((su & tmask) >> 3) * (uint32_t)g.nsub_v + ((sv & tmask) >> g.log2subv);
+        key = (((su >> g.log2tile) * (uint32_t)g.ntv + (sv >> g.log2tile)) * (uint32_t)g.nbuckets + (uint32_t)mp) *
+                  (uint32_t)g.nsub + sub;
+        duv = (su & 7u) | ((sv & vmask) << 8);
+        float ku[S], kv[S];
+        const float x0 = (float)(-uf * 2.0 + ((double)S - 1.0));
+        const float y0 = (float)(-vf * 2.0 + ((double)S - 1.0));
+        eval_taps2<float, S>(g.coeff, g.ne, x0, y0, ku, kv);
+        cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
+        if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
+        float* cu = st.ku + lane * TC_UPAD + 8;
+        float4* cb = st.kb + lane * TC_VSTRIDE + 8;
+        float* cw = st.kw + lane * 8;
+#pragma unroll
+        for (int i = 0; i < S; i++) {
+          cu[i] = ku[i];
+          const float re = val.re * kv[i], im = val.im * kv[i];
+          const float rh = __uint_as_float(to_tf32(re)), ih = __uint_as_float(to_tf32(im));
+          cb[i] = make_float4(rh, re - rh, ih, im - ih);
         }
-        st.grp[tid] = grp;
-        st.duv[tid] = duv;
-      }
-      __syncthreads();
-      if (warp < gw) {  // this warp's plane: w0 + warp
-        const int p = w0 + warp;
-        int q = 0;
-        while (q < nb) {
-          const int gqv = st.grp[q];
-          // The tensor cores' FP32 accumulation does not round to nearest, so
-          // long sums drift: every TC_DRAIN blocks the accumulators are added
-          // to the window (rounded FP32 adds) and restarted from zero.
-          if (gqv != gcur || blocks == TC_DRAIN) {
-            if (act) tc_flush(buf + (size_t)warp * LL, L, a8, b8, acc);
-            blocks = 0;
-            gcur = gqv;
+        if (g.do_wgridding) {
 #pragma unroll
-            for (int c2 = 0; c2 < 2; c2++)
-#pragma unroll
-              for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-                for (int r = 0; r < 4; r++) acc[c2][nt][r] = 0.0f;
-            act = false;
-            if (gqv >= 0) {
-              const int mpg = gqv >> 4, sub = gqv & 15;
-              a8 = (sub / g.nsub_side) * 8;
-              b8 = (sub % g.nsub_side) * 8;
-              jpl = p - mpg;
-              act = g.do_wgridding ? (jpl >= 0 && jpl < S) : (jpl == 0);
-            }
+          for (int j = 0; j < S; j++) {
+            const int p = mp + j;
+            cw[j] = (p >= pg0 && p < pg0 + npg) ? w_factor<float, S>(g, j, p, w) : 0.0f;
           }
-          // The block: the leading visibilities (at most 8) of the current group.
-          const bool same = lane < 8 && q + lane < nb && st.grp[q + lane] == gcur;
-          const unsigned m = __ballot_sync(0xffffffffu, same);
-          const int kbk = __ffs(~m) - 1;
-          if (act) {
-            uint32_t ah[4], al[4];
-            float bv[2][2][2];  // [k half][comp][n tile]
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              const int k = tq + 4 * h;
-              float a_lo = 0.0f, a_hi = 0.0f;
-              float kvv[2] = {0.0f, 0.0f};
-              cplx<float> w = {0.0f, 0.0f};
-              if (k < kbk) {
-                const int e = q + k;
-                const int d = st.duv[e];
-                const int du = d & 255, dv = d >> 8;
-                const int cu0 = gq - du, cu1 = gq + 8 - du;
-                if (cu0 >= 0 && cu0 < S) a_lo = st.ku[e * S + cu0];
-                if (cu1 >= 0 && cu1 < S) a_hi = st.ku[e * S + cu1];
-#pragma unroll
-                for (int nt = 0; nt < 2; nt++) {
-                  const int cv = gq + 8 * nt - dv;
-                  if (cv >= 0 && cv < S) kvv[nt] = st.kv[e * S + cv];
-                }
-                w = st.cw[e * S + jpl];
-              }
-              split_tf32(a_lo, ah[2 * h], al[2 * h]);      // rows gq: a0 (k = tq) / a2 (k = tq + 4)
-              split_tf32(a_hi, ah[2 * h + 1], al[2 * h + 1]);  // rows gq + 8: a1 / a3
-#pragma unroll
-              for (int nt = 0; nt < 2; nt++) {
-                bv[h][0][nt] = w.re * kvv[nt];
-                bv[h][1][nt] = w.im * kvv[nt];
-              }
-            }
-            uint32_t bh[2][2][2], bl[2][2][2];  // [comp][n tile][k half]
-#pragma unroll
-            for (int c2 = 0; c2 < 2; c2++)
-#pragma unroll
-              for (int nt = 0; nt < 2; nt++)
-#pragma unroll
-                for (int h = 0; h < 2; h++) split_tf32(bv[h][c2][nt], bh[c2][nt][h], bl[c2][nt][h]);
-            // Independent products first: hi * hi on the four accumulators, then
-            // the two cross terms.
-#pragma unroll
-            for (int c2 = 0; c2 < 2; c2++)
-#pragma unroll
-              for (int nt = 0; nt < 2; nt++) mma_tf32(acc[c2][nt], ah, bh[c2][nt][0], bh[c2][nt][1]);
-#pragma unroll
-            for (int c2 = 0; c2 < 2; c2++)
-#pragma unroll
-              for (int nt = 0; nt < 2; nt++) mma_tf32(acc[c2][nt], ah, bl[c2][nt][0], bl[c2][nt][1]);
-#pragma unroll
-            for (int c2 = 0; c2 < 2; c2++)
-#pragma unroll
-              for (int nt = 0; nt < 2; nt++) mma_tf32(acc[c2][nt], al, bh[c2][nt][0], bh[c2][nt][1]);
-            blocks++;
-          }
-          q += kbk;
+        } else {
+          cw[0] = 1.0f;
         }
       }
+      st.key[lane] = key;
+      st.duv[lane] = duv;
     }
-    if (warp < gw && act) tc_flush(buf + (size_t)warp * LL, L, a8, b8, acc);
-    __syncthreads();
-    for (int c = tid; c < gw * LL; c += blockDim.x) {
-      const cplx<float> v = buf[c];
-      if (v.re == 0.0f && v.im == 0.0f) continue;
-      const int pl = c / LL, rem = c - pl * LL, i = rem / L, j = rem - i * L;
-      const int row = (bu + i + g.nu / 2) % g.nu, col = (bv + j + g.nv / 2) % g.nv;
-      add_cell(grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col, v.re, v.im);
+    __syncwarp();
+    int q = 0;
+    while (q < nb) {
+      const uint32_t gk = st.key[q];
+      if (gk != gcur) {
+        if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc, mst);
+#pragma unroll
+        for (int j = 0; j < S; j++)
+#pragma unroll
+          for (int c = 0; c < 2; c++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) acc[j][c][r] = mst[j][c][r] = 0.0f;
+        blocks = 0;
+        gcur = gk;
+        pact = 0;
+        if (gk != INACTIVE) {
+          tc_decode(g, gk, su0, sv0, mpc);
+          for (int j = 0; j < np; j++)
+            if (mpc + j >= pg0 && mpc + j < pg0 + npg) pact |= 1u << j;
+        }
+      }
+      // The block: the leading visibilities (at most 8) of the current bin.
+      const bool same = lane < 8 && q + lane < nb && st.key[q + lane] == gk;
+      const unsigned m = __ballot_sync(0xffffffffu, same);
+      const int kbk = __ffs(~m) - 1;
+      if (gk != INACTIVE) {
+        const int e0 = tq < kbk ? q + tq : TC_BATCH, e1 = tq + 4 < kbk ? q + tq + 4 : TC_BATCH;
+        const uint32_t d0 = st.duv[e0], d1 = st.duv[e1];
+        const int du0 = (int)(d0 & 255u), dv0 = (int)(d0 >> 8), du1 = (int)(d1 & 255u), dv1 = (int)(d1 >> 8);
+        const float* u0 = st.ku + e0 * TC_UPAD + gq - du0 + 8;
+        const float* u1 = st.ku + e1 * TC_UPAD + gq - du1 + 8;
+        const float ku00 = u0[0], ku01 = u0[8], ku10 = u1[0], ku11 = u1[8];
+        const float4 b0 = st.kb[e0 * TC_VSTRIDE + gq - dv0 + 8];
+        const float4 b1 = st.kb[e1 * TC_VSTRIDE + gq - dv1 + 8];
+        const uint32_t brh0 = __float_as_uint(b0.x), brl0 = __float_as_uint(b0.y);
+        const uint32_t bih0 = __float_as_uint(b0.z), bil0 = __float_as_uint(b0.w);
+        const uint32_t brh1 = __float_as_uint(b1.x), brl1 = __float_as_uint(b1.y);
+        const uint32_t bih1 = __float_as_uint(b1.z), bil1 = __float_as_uint(b1.w);
+        const float* w0p = st.kw + e0 * 8;
+        const float* w1p = st.kw + e1 * 8;
+#pragma unroll
+        for (int j = 0; j < S; j++) {
+          if (!((pact >> j) & 1u)) continue;
+          const float w0 = w0p[j], w1 = w1p[j];
+          uint32_t ah[4], al[4];
+          split_fast(w0 * ku00, ah[0], al[0]);  // A[gq][tq]
+          split_fast(w0 * ku01, ah[1], al[1]);  // A[gq + 8][tq]
+          split_fast(w1 * ku10, ah[2], al[2]);  // A[gq][tq + 4]
+          split_fast(w1 * ku11, ah[3], al[3]);  // A[gq + 8][tq + 4]
+          mma_tf32(acc[j][0], ah, brh0, brh1);
+          mma_tf32(acc[j][1], ah, bih0, bih1);
+          mma_tf32(acc[j][0], ah, brl0, brl1);
+          mma_tf32(acc[j][1], ah, bil0, bil1);
+          mma_tf32(acc[j][0], al, brh0, brh1);
+          mma_tf32(acc[j][1], al, bih0, bih1);
+        }
+        if (++blocks == TC_DRAIN) {
+#pragma unroll
+          for (int j = 0; j < S; j++)
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+#pragma unroll
+              for (int r = 0; r < 4; r++) {
+                mst[j][c][r] += acc[j][c][r];
+                acc[j][c][r] = 0.0f;
+              }
+          blocks = 0;
+        }
+      }
+      q += kbk;
     }
-    __syncthreads();
   }
+  if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc, mst);
 }
 
 // ------------------------------------------------------------------ degridding
@@ -1131,16 +1147,14 @@ void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, c
 }
 
 template <int S>
-void launch_grid_tc(int gmax, unsigned nblocks, cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode,
-                    const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
-                    const uint32_t* ntasks, cplx<float>* grids, int pg0, int npg, int* err) {
-  const int threads = 32 * std::max(gmax, 4);
-  const int smem = gmax * g.L * g.L * (int)sizeof(cplx<float>) + threads * (int)TcStaging<S>::bytes_per_vis();
+void launch_grid_tc(cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode, const double* uvw,
+                    const double* foc, const uint32_t* sorted, uint64_t nsorted, cplx<float>* grids, int pg0, int npg) {
+  const int smem = (int)TcSlots::bytes();
+  const unsigned nblocks = (unsigned)((nsorted + TC_CHUNK - 1) / TC_CHUNK);
   check_cuda(cudaFuncSetAttribute(k_grid_tc<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
   {
     StageTimer timer_(ST_GRID, s);
-    k_grid_tc<S><<<nblocks, threads, smem, s>>>(g, in, mode, uvw, foc, sorted, tasks, ntasks, grids, pg0, npg, gmax,
-                                                err);
+    k_grid_tc<S><<<nblocks, TC_BATCH, smem, s>>>(g, in, mode, uvw, foc, sorted, nsorted, grids, pg0, npg);
   }
   check_cuda(cudaGetLastError(), "grid kernel (tensor cores)");
 }
@@ -1467,9 +1481,8 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s)
       constexpr int SV = decltype(S)::value;
       if constexpr (sizeof(T) == 4) {
         if (grid_method() == GRID_TF32X3) {
-          launch_grid_tc<SV>(gmax, (unsigned)max_tasks_, s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(),
-                             sorted_.as<uint32_t>(), tasks_.as<Task>(), ntasks_.as<uint32_t>(), grids.as<cplx<T>>(),
-                             (int)pg0, n, err_.as<int>());
+          launch_grid_tc<SV>(s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(), sorted_.as<uint32_t>(),
+                             nvis_, grids.as<cplx<T>>(), (int)pg0, n);
           return;
         }
       }
