@@ -116,9 +116,13 @@ __device__ __forceinline__ int minplane(const Geom<T>& g, double w) {
   return min(mp, g.nbuckets - 1);
 }
 
-// `shifted` (wgridder.rs:1177-1179).
+// `shifted` (wgridder.rs:1177-1179). getpix leaves i0 in [-supp/2, n), so
+// i0 + n/2 is almost always in [0, 2n) and one compare replaces the 64-bit
+// remainder; other values take the remainder, with the same result.
 __device__ __forceinline__ int shifted(int64_t i0, int n) {
-  int64_t r = (i0 + n / 2) % n;
+  int64_t r = i0 + n / 2;
+  if (r >= 0 && r < 2 * (int64_t)n) return (int)(r >= n ? r - n : r);
+  r %= n;
   return (int)(r < 0 ? r + n : r);
 }
 
@@ -132,10 +136,17 @@ __device__ __forceinline__ int offset_in(int64_t i0, int n, int base) {
   return (int)d;
 }
 
+// Rows of even (and of odd) coefficients of the support-S kernel: its
+// polynomials have degree S + 3, padded to odd.
+__host__ __device__ constexpr int coeff_rows(int S) { return (((S + 3) | 1) + 1) / 2; }
+
 // The u and v taps by Horner's rule in x^2 on the even/odd split, first
 // ceil(S/2) taps evaluated and the rest mirrored (wgridder.rs:1514-1543).
+// `ne` is coeff_rows(S), which the host checks; the loops run to the
+// compile-time count so that they unroll onto constant-bank operands.
 template <class T, int S>
-__device__ __forceinline__ void eval_taps2(const T* __restrict__ c, int ne, T x, T y, T* ru, T* rv) {
+__device__ __forceinline__ void eval_taps2(const T* __restrict__ c, int /*ne*/, T x, T y, T* ru, T* rv) {
+  constexpr int ne = coeff_rows(S);
   constexpr int H = (S + 1) / 2;
   T x2 = x * x, y2 = y * y;
   T ex[H], ey[H], ox[H], oy[H];
@@ -144,6 +155,7 @@ __device__ __forceinline__ void eval_taps2(const T* __restrict__ c, int ne, T x,
     ex[i] = ey[i] = c[i];
     ox[i] = oy[i] = c[ne * S + i];
   }
+#pragma unroll
   for (int k = 1; k < ne; k++) {
 #pragma unroll
     for (int i = 0; i < H; i++) {
@@ -168,7 +180,8 @@ __device__ __forceinline__ void eval_taps2(const T* __restrict__ c, int ne, T x,
 
 // One tap (wgridder.rs:1548-1560).
 template <class T, int S>
-__device__ __forceinline__ T eval_tap(const T* __restrict__ c, int ne, int i, T x) {
+__device__ __forceinline__ T eval_tap(const T* __restrict__ c, int /*ne*/, int i, T x) {
+  constexpr int ne = coeff_rows(S);
   constexpr int H = (S + 1) / 2;
   if (i >= H) {
     i = S - 1 - i;
@@ -176,6 +189,7 @@ __device__ __forceinline__ T eval_tap(const T* __restrict__ c, int ne, int i, T 
   }
   T x2 = x * x;
   T e = c[i], o = c[ne * S + i];
+#pragma unroll
   for (int k = 1; k < ne; k++) {
     e = fma_t(e, x2, c[k * S + i]);
     o = fma_t(o, x2, c[(ne + k) * S + i]);

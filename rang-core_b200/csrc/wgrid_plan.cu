@@ -572,23 +572,27 @@ constexpr int TC_VPAD = 16;
 // Slot stride of the B columns in float4s: 2 mod 8, so the 8 lanes of one
 // 128-bit load phase (two rows, four slots) hit distinct bank groups.
 constexpr int TC_VSTRIDE = 18;
+// Odd slot strides of the u taps and w taps: the lanes' staging stores (one
+// slot each) and the operand loads (four slots) fall in distinct banks.
+constexpr int TC_USTRIDE = 25;
+constexpr int TC_WSTRIDE = 9;
 
 struct TcSlots {
   float4* kb;     // [TC_BATCH + 1][TC_VSTRIDE], TC_VPAD used: (re hi, re lo, im hi, im lo) of value * kv
-  float* ku;      // [TC_BATCH + 1][TC_UPAD]
-  float* kw;      // [TC_BATCH + 1][8]
+  float* ku;      // [TC_BATCH + 1][TC_USTRIDE], TC_UPAD used
+  float* kw;      // [TC_BATCH + 1][TC_WSTRIDE], S used
   uint32_t* key;  // [TC_BATCH + 1]
   uint32_t* duv;  // [TC_BATCH + 1]: du | dv << 8
   // Rounded up to whole float4s, all of which the kernel zeroes.
   __host__ __device__ static constexpr size_t bytes() {
-    return ((size_t)(TC_BATCH + 1) * (TC_VSTRIDE * sizeof(float4) + TC_UPAD * sizeof(float) + 8 * sizeof(float) + 8) +
+    return ((size_t)(TC_BATCH + 1) * (TC_VSTRIDE * sizeof(float4) + (TC_USTRIDE + TC_WSTRIDE) * sizeof(float) + 8) +
             15) / 16 * 16;
   }
   __device__ void carve(unsigned char* base) {
     kb = reinterpret_cast<float4*>(base);
     ku = reinterpret_cast<float*>(kb + (TC_BATCH + 1) * TC_VSTRIDE);
-    kw = ku + (TC_BATCH + 1) * TC_UPAD;
-    key = reinterpret_cast<uint32_t*>(kw + (TC_BATCH + 1) * 8);
+    kw = ku + (TC_BATCH + 1) * TC_USTRIDE;
+    key = reinterpret_cast<uint32_t*>(kw + (TC_BATCH + 1) * TC_WSTRIDE);
     duv = key + (TC_BATCH + 1);
   }
 };
@@ -708,9 +712,9 @@ __global__ void __launch_bounds__(TC_BATCH)
         eval_taps2<float, S>(g.coeff, g.ne, x0, y0, ku, kv);
         cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
         if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
-        float* cu = st.ku + lane * TC_UPAD + 8;
+        float* cu = st.ku + lane * TC_USTRIDE + 8;
         float4* cb = st.kb + lane * TC_VSTRIDE + 8;
-        float* cw = st.kw + lane * 8;
+        float* cw = st.kw + lane * TC_WSTRIDE;
 #pragma unroll
         for (int i = 0; i < S; i++) {
           cu[i] = ku[i];
@@ -760,8 +764,8 @@ __global__ void __launch_bounds__(TC_BATCH)
         const int e0 = tq < kbk ? q + tq : TC_BATCH, e1 = tq + 4 < kbk ? q + tq + 4 : TC_BATCH;
         const uint32_t d0 = st.duv[e0], d1 = st.duv[e1];
         const int du0 = (int)(d0 & 255u), dv0 = (int)(d0 >> 8), du1 = (int)(d1 & 255u), dv1 = (int)(d1 >> 8);
-        const float* u0 = st.ku + e0 * TC_UPAD + gq - du0 + 8;
-        const float* u1 = st.ku + e1 * TC_UPAD + gq - du1 + 8;
+        const float* u0 = st.ku + e0 * TC_USTRIDE + gq - du0 + 8;
+        const float* u1 = st.ku + e1 * TC_USTRIDE + gq - du1 + 8;
         const float ku00 = u0[0], ku01 = u0[8], ku10 = u1[0], ku11 = u1[8];
         const float4 b0 = st.kb[e0 * TC_VSTRIDE + gq - dv0 + 8];
         const float4 b1 = st.kb[e1 * TC_VSTRIDE + gq - dv1 + 8];
@@ -769,8 +773,8 @@ __global__ void __launch_bounds__(TC_BATCH)
         const uint32_t bih0 = __float_as_uint(b0.z), bil0 = __float_as_uint(b0.w);
         const uint32_t brh1 = __float_as_uint(b1.x), brl1 = __float_as_uint(b1.y);
         const uint32_t bih1 = __float_as_uint(b1.z), bil1 = __float_as_uint(b1.w);
-        const float* w0p = st.kw + e0 * 8;
-        const float* w1p = st.kw + e1 * 8;
+        const float* w0p = st.kw + e0 * TC_WSTRIDE;
+        const float* w1p = st.kw + e1 * TC_WSTRIDE;
 #pragma unroll
         for (int j = 0; j < S; j++) {
           if (!((pact >> j) & 1u)) continue;

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <stdexcept>
 #include <unordered_map>
 
 namespace wg {
