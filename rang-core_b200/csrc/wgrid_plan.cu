@@ -556,31 +556,31 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
 // planes with float2 atomics. Operands are split as x = hi + lo in TF32 and
 // each product formed as hi*hi + hi*lo + lo*hi (3 x TF32), keeping about 21
 // bits of each factor. The tensor cores' FP32 accumulation does not round to
-// nearest, so every TC_DRAIN blocks the accumulators are added, with rounded
-// FP32 adds, into a second register copy and restarted from zero.
+// nearest, so each block's three products start from zero and are added to
+// the window with rounded FP32 adds: no sum is carried inside the tensor core
+// from one block to the next.
 //
 // Staging (one visibility per lane) stores, per slot, the u taps at [8, 8+S)
-// of a zero-padded 24-entry column, the pre-split B entries at [8, 8+S) of a
-// 16-entry column, and the S w-taps; the zero padding makes every operand
-// fetch a plain load at index (row - du + 8). Slot TC_BATCH is all zero and
-// stands in for the missing visibilities of a short block.
+// of a zero-padded 24-entry column, the pre-split B entries at [3, 3+S) of an
+// 11-entry column, and the S w-taps; the zero padding makes every operand
+// fetch a plain load (at row - du + 8, column - dv + 3). Slot TC_BATCH is all
+// zero and stands in for the missing visibilities of a short block.
 constexpr int TC_BATCH = 32;
-constexpr int TC_DRAIN = 8;
 constexpr uint32_t TC_CHUNK = 8192;  // sorted visibilities per warp
+// u-tap columns: 24 entries, taps at [8, 8 + S), read at row - du + 8; the
+// slot stride is odd so that the lanes' stores and loads fall in distinct banks.
 constexpr int TC_UPAD = 24;
-constexpr int TC_VPAD = 16;
-// Slot stride of the B columns in float4s: 2 mod 8, so the 8 lanes of one
-// 128-bit load phase (two rows, four slots) hit distinct bank groups.
-constexpr int TC_VSTRIDE = 18;
-// Odd slot strides of the u taps and w taps: the lanes' staging stores (one
-// slot each) and the operand loads (four slots) fall in distinct banks.
 constexpr int TC_USTRIDE = 25;
-constexpr int TC_WSTRIDE = 9;
+// B columns: 11 float4 entries, taps at [3, 3 + S), read at column - dv + 3
+// (dv < 4); a slot stride of 6 mod 8 float4s puts the 8 lanes of one 128-bit
+// load phase (two columns, four slots) in distinct bank groups.
+constexpr int TC_VSTRIDE = 14;
+constexpr int TC_WSTRIDE = 9;  // w taps, odd stride as the u taps
 
 struct TcSlots {
-  float4* kb;     // [TC_BATCH + 1][TC_VSTRIDE], TC_VPAD used: (re hi, re lo, im hi, im lo) of value * kv
-  float* ku;      // [TC_BATCH + 1][TC_USTRIDE], TC_UPAD used
-  float* kw;      // [TC_BATCH + 1][TC_WSTRIDE], S used
+  float4* kb;     // [TC_BATCH + 1][TC_VSTRIDE]: (re hi, re lo, im hi, im lo) of value * kv
+  float* ku;      // [TC_BATCH + 1][TC_USTRIDE]
+  float* kw;      // [TC_BATCH + 1][TC_WSTRIDE]
   uint32_t* key;  // [TC_BATCH + 1]
   uint32_t* duv;  // [TC_BATCH + 1]: du | dv << 8
   // Rounded up to whole float4s, all of which the kernel zeroes.
@@ -631,11 +631,10 @@ __device__ __forceinline__ void tc_decode(const Geom<float>& g, uint32_t key, in
               (uint32_t)g.nv);
 }
 
-// Adds a bin's windows (both register copies) to its planes of the grid.
+// Adds a bin's windows to its planes of the grid.
 template <int S>
 __device__ __forceinline__ void tc_flush(const Geom<float>& g, cplx<float>* __restrict__ grids, int pg0, int su0,
-                                         int sv0, int mp, unsigned pact, const float (&acc)[S][2][4],
-                                         const float (&mst)[S][2][4]) {
+                                         int sv0, int mp, unsigned pact, const float (&acc)[S][2][4]) {
   const int lane = threadIdx.x & 31, gq = lane >> 2, tq = lane & 3;
   const size_t plane = (size_t)g.nu * g.nv;
 #pragma unroll
@@ -644,7 +643,7 @@ __device__ __forceinline__ void tc_flush(const Geom<float>& g, cplx<float>* __re
     cplx<float>* pl = grids + (size_t)(mp + j - pg0) * plane;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-      const float re = mst[j][0][r] + acc[j][0][r], im = mst[j][1][r] + acc[j][1][r];
+      const float re = acc[j][0][r], im = acc[j][1][r];
       if (re == 0.0f && im == 0.0f) continue;
       int row = su0 + gq + (r >= 2 ? 8 : 0), col = sv0 + 2 * tq + (r & 1);
       while (row >= g.nu) row -= g.nu;
@@ -674,15 +673,15 @@ __global__ void __launch_bounds__(TC_BATCH)
   const uint32_t tmask = (1u << g.log2tile) - 1u;
   const uint32_t vmask = (1u << g.log2subv) - 1u;
 
-  float acc[S][2][4], mst[S][2][4];
+  float acc[S][2][4];
 #pragma unroll
   for (int j = 0; j < S; j++)
 #pragma unroll
     for (int c = 0; c < 2; c++)
 #pragma unroll
-      for (int r = 0; r < 4; r++) acc[j][c][r] = mst[j][c][r] = 0.0f;
+      for (int r = 0; r < 4; r++) acc[j][c][r] = 0.0f;
   uint32_t gcur = INACTIVE;
-  int su0 = 0, sv0 = 0, mpc = 0, blocks = 0;
+  int su0 = 0, sv0 = 0, mpc = 0;
   unsigned pact = 0;
 
   for (uint64_t kb = k0; kb < k1; kb += TC_BATCH) {
@@ -713,7 +712,7 @@ __global__ void __launch_bounds__(TC_BATCH)
         cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
         if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
         float* cu = st.ku + lane * TC_USTRIDE + 8;
-        float4* cb = st.kb + lane * TC_VSTRIDE + 8;
+        float4* cb = st.kb + lane * TC_VSTRIDE + 3;
         float* cw = st.kw + lane * TC_WSTRIDE;
 #pragma unroll
         for (int i = 0; i < S; i++) {
@@ -740,14 +739,13 @@ __global__ void __launch_bounds__(TC_BATCH)
     while (q < nb) {
       const uint32_t gk = st.key[q];
       if (gk != gcur) {
-        if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc, mst);
+        if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
 #pragma unroll
         for (int j = 0; j < S; j++)
 #pragma unroll
           for (int c = 0; c < 2; c++)
 #pragma unroll
-            for (int r = 0; r < 4; r++) acc[j][c][r] = mst[j][c][r] = 0.0f;
-        blocks = 0;
+            for (int r = 0; r < 4; r++) acc[j][c][r] = 0.0f;
         gcur = gk;
         pact = 0;
         if (gk != INACTIVE) {
@@ -767,8 +765,8 @@ __global__ void __launch_bounds__(TC_BATCH)
         const float* u0 = st.ku + e0 * TC_USTRIDE + gq - du0 + 8;
         const float* u1 = st.ku + e1 * TC_USTRIDE + gq - du1 + 8;
         const float ku00 = u0[0], ku01 = u0[8], ku10 = u1[0], ku11 = u1[8];
-        const float4 b0 = st.kb[e0 * TC_VSTRIDE + gq - dv0 + 8];
-        const float4 b1 = st.kb[e1 * TC_VSTRIDE + gq - dv1 + 8];
+        const float4 b0 = st.kb[e0 * TC_VSTRIDE + gq - dv0 + 3];
+        const float4 b1 = st.kb[e1 * TC_VSTRIDE + gq - dv1 + 3];
         const uint32_t brh0 = __float_as_uint(b0.x), brl0 = __float_as_uint(b0.y);
         const uint32_t bih0 = __float_as_uint(b0.z), bil0 = __float_as_uint(b0.w);
         const uint32_t brh1 = __float_as_uint(b1.x), brl1 = __float_as_uint(b1.y);
@@ -784,33 +782,34 @@ __global__ void __launch_bounds__(TC_BATCH)
           split_fast(w0 * ku01, ah[1], al[1]);  // A[gq + 8][tq]
           split_fast(w1 * ku10, ah[2], al[2]);  // A[gq][tq + 4]
           split_fast(w1 * ku11, ah[3], al[3]);  // A[gq + 8][tq + 4]
-          mma_tf32(acc[j][0], ah, brh0, brh1);
-          mma_tf32(acc[j][1], ah, bih0, bih1);
-          mma_tf32(acc[j][0], ah, brl0, brl1);
-          mma_tf32(acc[j][1], ah, bil0, bil1);
-          mma_tf32(acc[j][0], al, brh0, brh1);
-          mma_tf32(acc[j][1], al, bih0, bih1);
-        }
-        if (++blocks == TC_DRAIN) {
+          float d0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, d1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+          mma_tf32(d0, ah, brh0, brh1);
+          mma_tf32(d1, ah, bih0, bih1);
+          mma_tf32(d0, ah, brl0, brl1);
+          mma_tf32(d1, ah, bil0, bil1);
+          mma_tf32(d0, al, brh0, brh1);
+          mma_tf32(d1, al, bih0, bih1);
 #pragma unroll
-          for (int j = 0; j < S; j++)
-#pragma unroll
-            for (int c = 0; c < 2; c++)
-#pragma unroll
-              for (int r = 0; r < 4; r++) {
-                mst[j][c][r] += acc[j][c][r];
-                acc[j][c][r] = 0.0f;
-              }
-          blocks = 0;
+          for (int r = 0; r < 4; r++) {
+            acc[j][0][r] += d0[r];
+            acc[j][1][r] += d1[r];
+          }
         }
       }
       q += kbk;
     }
   }
-  if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc, mst);
+  if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
 }
 
 // ------------------------------------------------------------------ degridding
+
+// Row stride of the degridder's shared-memory window: the smallest stride of
+// at least L cells that is 2 mod 4. The lanes of a warp mostly read one
+// 8 x 2 sub-tile's footprints, at offsets du * stride + dv (du < 8, dv < 2)
+// from a common cell; with such a stride those 16 offsets of 8-byte cells
+// fall in 16 distinct bank pairs.
+__host__ __device__ __forceinline__ int window_stride(int L) { return L + (6 - L % 4) % 4; }
 
 template <class T, int S>
 __global__ void __launch_bounds__(GRID_THREADS)
@@ -820,7 +819,7 @@ __global__ void __launch_bounds__(GRID_THREADS)
              cplx<T>* __restrict__ vis, int first_group, int last_group, int* __restrict__ err) {
   if (blockIdx.x >= *ntasks) return;
   extern __shared__ __align__(16) unsigned char smem[];
-  const int L = g.L, LL = L * L;
+  const int L = g.L, Lp = window_stride(L), LLp = L * Lp;
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem);
   const Task t = tasks[blockIdx.x];
   const int tu = (int)(t.tile / (uint32_t)g.ntv), tv = (int)(t.tile - (uint32_t)tu * (uint32_t)g.ntv);
@@ -837,10 +836,18 @@ __global__ void __launch_bounds__(GRID_THREADS)
   for (int wi = 0; wi < nloop; wi++) {
     const int w0 = lo + wi * gmax;
     const int gw = wi < nwin ? min(gmax, hi - w0 + 1) : 0;
-    for (int c = threadIdx.x; c < gw * LL; c += blockDim.x) {
-      const int pl = c / LL, rem = c - pl * LL, i = rem / L, j = rem - i * L;
-      const int row = (bu + i + g.nu / 2) % g.nu, col = (bv + j + g.nv / 2) % g.nv;
-      buf[c] = grids[((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col];
+    // One warp per window row, lanes along the row.
+    for (int rr = threadIdx.x >> 5; rr < gw * L; rr += blockDim.x >> 5) {
+      const int pl = rr / L, i = rr - pl * L;
+      int row = bu + i + g.nu / 2;
+      while (row >= g.nu) row -= g.nu;
+      const cplx<T>* srow = grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv;
+      cplx<T>* drow = buf + ((size_t)pl * L + i) * Lp;
+      for (int j = threadIdx.x & 31; j < L; j += 32) {
+        int col = bv + j + g.nv / 2;
+        while (col >= g.nv) col -= g.nv;
+        drow[j] = srow[col];
+      }
     }
     __syncthreads();
     const bool finalize = last_group && wi == nloop - 1;
@@ -879,14 +886,14 @@ __global__ void __launch_bounds__(GRID_THREADS)
 #pragma unroll
             for (int cu = 0; cu < S; cu++) kk[cu] = ku[cu];
           }
-          const cplx<T>* src = buf + (size_t)(p - w0) * LL + ou * L + ov;
+          const cplx<T>* src = buf + (size_t)(p - w0) * LLp + ou * Lp + ov;
           T rr = 0, ri = 0;
 #pragma unroll
           for (int cu = 0; cu < S; cu++) {
             T tr = 0, tim = 0;
 #pragma unroll
             for (int cv = 0; cv < S; cv++) {
-              const cplx<T> c = src[cu * L + cv];
+              const cplx<T> c = src[cu * Lp + cv];
               tr = fma_t(kv[cv], c.re, tr);
               tim = fma_t(kv[cv], c.im, tim);
             }
@@ -1535,8 +1542,11 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s) 
                                                              corr, corr + nu2, img.as<T>());
   }
   check_cuda(cudaGetLastError(), "correct");
-  const int gmax = std::min<int>(max_window_planes(g_.L, sizeof(cplx<T>)), (int)std::min<size_t>(nplanes, 64));
-  const int smem = gmax * g_.L * g_.L * (int)sizeof(cplx<T>);
+  const int Lp = window_stride(g_.L);
+  const int gmax = std::min<int>(
+      std::max<int>(1, (int)(SMEM_WINDOW_BYTES / ((size_t)g_.L * Lp * sizeof(cplx<T>)))),
+      (int)std::min<size_t>(nplanes, 64));
+  const int smem = gmax * g_.L * Lp * (int)sizeof(cplx<T>);
   for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
     int n = (int)std::min(group, nplanes - pg0);
     check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
