@@ -192,9 +192,10 @@ def run_fista(dev, max_iterations=200, sigma=0.05):
     iterations) on 2048^2 at 1.5 arcsec: 300 point sources and 40 elliptical
     Gaussians predicted by the degridder onto the 64-antenna coverage of 128
     integrations at 256 channels (66 M visibilities), noise sigma 0.05 per
-    component. Reports the time until the visibility residual RMS (per real
-    component) reaches 1.2 sigma, on the GPU clock, plan and power iteration
-    included."""
+    component. Reports the GPU time until the visibility residual RMS (per
+    real component) first reaches 1.2 sigma (null if it does not within the
+    iterations), plan and power iteration included, and the RMS every 20
+    iterations."""
     import torch
 
     from rang import fista, wgrid_torch
@@ -213,30 +214,44 @@ def run_fista(dev, max_iterations=200, sigma=0.05):
     nvis = vis.numel()
     target = 1.2 * sigma
     torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
     plan = wgrid_torch.DevicePlan(uvw, freq, epsilon=1e-5, single=True, **common)
     dirty, q = plan.residual(vis, None)
+    ev[1].record()
     lmax, _ = fista.power_iteration(plan.gram, plan.shape, dev, max_iterations=30)
-    reached = {}
+    ev[2].record()
+    trajectory, reached = [], {}
+    t_first = {}
 
     def stop(k, misfit):
         rms = float(np.sqrt(max(2.0 * misfit, 0.0) / (2 * nvis)))
+        if k % 20 == 0 or k == max_iterations:
+            trajectory.append([k, rms])
         reached["rms"], reached["k"] = rms, k
-        return rms <= target
+        if rms <= target and "event" not in t_first:
+            t_first["event"] = torch.cuda.Event(enable_timing=True)
+            t_first["event"].record()
+            t_first["k"] = k
+        return False  # all iterations run; the first one at the target is timed
 
     lam = 1e-4 * float(dirty.max())
     x, gx, k, restarts = fista.solve(plan.gram, dirty, lam, 1.0 / lmax, max_iterations, q0=0.5 * q, stop=stop)
-    end.record()
+    ev[3].record()
     torch.cuda.synchronize()
-    t = start.elapsed_time(end) / 1e3
+    t_setup = ev[0].elapsed_time(ev[1]) / 1e3
+    t_power = ev[1].elapsed_time(ev[2]) / 1e3
+    t_iter = ev[2].elapsed_time(ev[3]) / 1e3
+    t_target = ev[0].elapsed_time(t_first["event"]) / 1e3 if "event" in t_first else None
     err = float((x - sky).norm() / sky.norm())
     plan.close()
-    ok = bool(reached.get("rms", 1e9) <= target)
-    return {"config": "2048^2 at 1.5 arcsec, 300 points + 40 Gaussians, 66 M visibilities, sigma 0.05",
-            "target_rms": target, "final_rms": reached.get("rms"), "iterations": int(reached.get("k", -1)),
-            "restarts": int(restarts), "time_s": t if ok else None, "elapsed_s": t, "lambda": lam,
-            "model_rel_error": err, "reached": ok,
+    return {"config": "2048^2 at 1.5 arcsec, 300 points + 40 Gaussians, 66 M visibilities, sigma 0.05, "
+                      "L1 with positivity, lambda 1e-4 max(dirty), step 1/||A^H A|| from 30 power iterations",
+            "target_rms": target, "time_to_target_s": t_target, "iterations_to_target": t_first.get("k"),
+            "iterations": max_iterations, "final_rms": reached.get("rms"), "rms_trajectory": trajectory,
+            "restarts": int(restarts), "plan_and_dirty_s": t_setup, "power_iteration_s": t_power,
+            "fista_s": t_iter, "ms_per_iteration": 1e3 * t_iter / (max_iterations + 1),
+            "model_rel_error": err,
             "learned": None, "learned_note": "the learned U-Net preconditioner is not built"}
 
 
