@@ -75,6 +75,26 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
+// Row and channel of a grid-stride loop's linear index, advanced by the
+// constant stride without a division per element.
+struct RowCh {
+  uint32_t row, ch, srow, sch;
+  __device__ RowCh(uint64_t i, uint32_t nchan, uint64_t stride) {
+    row = (uint32_t)(i / nchan);
+    ch = (uint32_t)(i - (uint64_t)row * nchan);
+    srow = (uint32_t)(stride / nchan);
+    sch = (uint32_t)(stride - (uint64_t)srow * nchan);
+  }
+  __device__ __forceinline__ void next(uint32_t nchan) {
+    row += srow;
+    ch += sch;
+    if (ch >= nchan) {
+      ch -= nchan;
+      row++;
+    }
+  }
+};
+
 // scan (wgridder.rs:1051-1077): the count is exact and min/max are order
 // independent, so the result is the reference's bit for bit.
 template <class T>
@@ -83,10 +103,11 @@ __global__ void k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__
   uint64_t n = (uint64_t)nrow * nchan;
   unsigned long long cnt = 0, fin = 0;
   double lo = 1e300, hi = 0.0;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  RowCh rc(i, nchan, (uint64_t)gridDim.x * blockDim.x);
+  for (; i < n; i += (uint64_t)gridDim.x * blockDim.x, rc.next(nchan)) {
     if (is_active<T>(in, with_vis != 0, i)) {
-      uint32_t row = (uint32_t)(i / nchan);
-      uint32_t ch = (uint32_t)(i - (uint64_t)row * nchan);
+      const uint32_t row = rc.row, ch = rc.ch;
       double w = fabs(fw * uvw[3 * (uint64_t)row + 2] * foc[ch]);
       cnt++;
       if (!isnan(w)) {
@@ -118,11 +139,9 @@ __global__ void k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__
 // reference's (tile, plane) order and groups each plane's visibilities by
 // sub-tile, which the tensor-core gridder contracts block by block.
 template <class T>
-__device__ __forceinline__ uint32_t bin_of(const Geom<T>& g, const double* __restrict__ uvw,
-                                           const double* __restrict__ foc, uint32_t idx, int64_t* piu0 = nullptr,
-                                           int64_t* piv0 = nullptr) {
-  uint32_t nchan = (uint32_t)g.nchan;
-  uint32_t row = idx / nchan, ch = idx - row * nchan;
+__device__ __forceinline__ uint32_t bin_of_rc(const Geom<T>& g, const double* __restrict__ uvw,
+                                              const double* __restrict__ foc, uint32_t row, uint32_t ch,
+                                              int64_t* piu0 = nullptr, int64_t* piv0 = nullptr) {
   double b[3];
   row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
   double f = foc[ch];
@@ -137,6 +156,14 @@ __device__ __forceinline__ uint32_t bin_of(const Geom<T>& g, const double* __res
   if (piu0) *piu0 = iu0;
   if (piv0) *piv0 = iv0;
   return ((tu * (uint32_t)g.ntv + tv) * (uint32_t)g.nbuckets + (uint32_t)minplane(g, w)) * (uint32_t)g.nsub + sub;
+}
+template <class T>
+__device__ __forceinline__ uint32_t bin_of(const Geom<T>& g, const double* __restrict__ uvw,
+                                           const double* __restrict__ foc, uint32_t idx, int64_t* piu0 = nullptr,
+                                           int64_t* piv0 = nullptr) {
+  const uint32_t nchan = (uint32_t)g.nchan;
+  const uint32_t row = idx / nchan, ch = idx - row * nchan;
+  return bin_of_rc(g, uvw, foc, row, ch, piu0, piv0);
 }
 
 // One atomic per distinct counter in the warp; each active lane gets the
@@ -163,12 +190,14 @@ __global__ void k_bin_count(const __grid_constant__ Geom<T> g, const double* __r
                             uint32_t* __restrict__ counts) {
   uint64_t n = g.nrow * g.nchan;
   uint64_t nround = (n + 31) & ~31ull;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nround; i += (uint64_t)gridDim.x * blockDim.x) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  RowCh rc(i, (uint32_t)g.nchan, (uint64_t)gridDim.x * blockDim.x);
+  for (; i < nround; i += (uint64_t)gridDim.x * blockDim.x, rc.next((uint32_t)g.nchan)) {
     bool act = false;
     uint32_t k = INACTIVE;
     if (i < n) {
       act = is_active<T>(in, with_vis != 0, i);
-      if (act) k = bin_of(g, uvw, foc, (uint32_t)i);
+      if (act) k = bin_of_rc(g, uvw, foc, rc.row, rc.ch);
       key[i] = k;
     }
     warp_aggregated_add(counts, k, act);
@@ -568,8 +597,7 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
 constexpr int TC_BATCH = 32;
 constexpr uint32_t TC_CHUNK = 8192;  // sorted visibilities per warp
 // u-tap columns: 24 entries, taps at [8, 8 + S), read at row - du + 8; the
-// slot stride is odd so that the lanes' stores and loads fall in distinct banks.
-constexpr int TC_UPAD = 24;
+// slot stride (25) is odd so that the lanes' stores fall in distinct banks.
 constexpr int TC_USTRIDE = 25;
 // B columns: 11 float4 entries, taps at [3, 3 + S), read at column - dv + 3
 // (dv < 4); a slot stride of 6 mod 8 float4s puts the 8 lanes of one 128-bit
@@ -773,27 +801,53 @@ __global__ void __launch_bounds__(TC_BATCH)
         const uint32_t bih1 = __float_as_uint(b1.z), bil1 = __float_as_uint(b1.w);
         const float* w0p = st.kw + e0 * TC_WSTRIDE;
         const float* w1p = st.kw + e1 * TC_WSTRIDE;
+        // Planes in pairs: four independent accumulator chains in flight.
 #pragma unroll
-        for (int j = 0; j < S; j++) {
-          if (!((pact >> j) & 1u)) continue;
-          const float w0 = w0p[j], w1 = w1p[j];
-          uint32_t ah[4], al[4];
-          split_fast(w0 * ku00, ah[0], al[0]);  // A[gq][tq]
-          split_fast(w0 * ku01, ah[1], al[1]);  // A[gq + 8][tq]
-          split_fast(w1 * ku10, ah[2], al[2]);  // A[gq][tq + 4]
-          split_fast(w1 * ku11, ah[3], al[3]);  // A[gq + 8][tq + 4]
-          float d0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, d1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-          mma_tf32(d0, ah, brh0, brh1);
-          mma_tf32(d1, ah, bih0, bih1);
-          mma_tf32(d0, ah, brl0, brl1);
-          mma_tf32(d1, ah, bil0, bil1);
-          mma_tf32(d0, al, brh0, brh1);
-          mma_tf32(d1, al, bih0, bih1);
+        for (int j = 0; j < S; j += 2) {
+          const bool two = j + 1 < S;
+          if (!((pact >> j) & (two ? 3u : 1u))) continue;
+          uint32_t ah[2][4], al[2][4];
+          float d[2][2][4];
 #pragma unroll
-          for (int r = 0; r < 4; r++) {
-            acc[j][0][r] += d0[r];
-            acc[j][1][r] += d1[r];
+          for (int h = 0; h < 2; h++) {
+            if (h == 1 && !two) break;
+            const float w0 = w0p[j + h], w1 = w1p[j + h];
+            split_fast(w0 * ku00, ah[h][0], al[h][0]);  // A[gq][tq]
+            split_fast(w0 * ku01, ah[h][1], al[h][1]);  // A[gq + 8][tq]
+            split_fast(w1 * ku10, ah[h][2], al[h][2]);  // A[gq][tq + 4]
+            split_fast(w1 * ku11, ah[h][3], al[h][3]);  // A[gq + 8][tq + 4]
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+#pragma unroll
+              for (int r = 0; r < 4; r++) d[h][c][r] = 0.0f;
           }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (h == 0 || two) {
+              mma_tf32(d[h][0], ah[h], brh0, brh1);
+              mma_tf32(d[h][1], ah[h], bih0, bih1);
+            }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (h == 0 || two) {
+              mma_tf32(d[h][0], ah[h], brl0, brl1);
+              mma_tf32(d[h][1], ah[h], bil0, bil1);
+            }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (h == 0 || two) {
+              mma_tf32(d[h][0], al[h], brh0, brh1);
+              mma_tf32(d[h][1], al[h], bih0, bih1);
+            }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (h == 0 || two) {
+#pragma unroll
+              for (int r = 0; r < 4; r++) {
+                acc[j + h][0][r] += d[h][0][r];
+                acc[j + h][1][r] += d[h][1][r];
+              }
+            }
         }
       }
       q += kbk;
