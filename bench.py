@@ -47,6 +47,12 @@ sys.path.insert(0, str(REPO / "rang-core_b200"))
 from rang import synth  # noqa: E402
 
 WORKLOAD = "ms2dirty+dirty2ms 1.06G vis 4096^2"
+# DRAM bytes (read + written) of one launch of the dominant kernels, measured
+# with ncu on a B200 (profiles/dram_grid_degrid_1.06G_4096.md).
+DRAM_TRAFFIC = {
+    (WORKLOAD, 1e-5, "k_grid_tc"): 19.83e9 + 0.571e9,
+    (WORKLOAD, 1e-5, "k_degrid"): 9.61e9 + 9.51e9,
+}
 METRIC = "Mvis/s ms2dirty+dirty2ms @eps=1e-5 vs FP64"
 UNIT = "Mvis/s"
 
@@ -352,17 +358,30 @@ def run_b200(args):
     hbm, peak_kind = peaks()
     nact = int(plan_info["nvis"])
     nplanes = max(int(plan_info["nplanes"]), 1)
+    supp = int(plan_info["supp"])
     grid_bytes = nplanes * plan_info["nu"] * plan_info["nv"] * 8
     alg = {"grid": nact * (8 + 4) + nrow * 24 + grid_bytes, "degrid": nact * (8 + 4) + nrow * 24 + grid_bytes}
     dom = max(("grid", "degrid"), key=lambda k: prof[k][1])
+    kernel = {"grid": "k_grid_tc", "degrid": "k_degrid"}[dom]
     dom_launches, dom_ms = prof[dom]
     per_launch_s = dom_ms / max(dom_launches, 1) / 1e3
     achieved = alg[dom] / per_launch_s / 1e9
     total_prof = sum(v[1] for v in prof.values())
-    roofline = {"bound": "hbm", "kernel": f"k_{dom}", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+    # Useful arithmetic: S^3 complex-by-real multiply-adds per visibility
+    # (4 flops each), against the FP32 CUDA-core FMA peak at the maximum SM
+    # clock; the HBM bound and this bound together are the kernel's roofline.
+    flops = 4.0 * supp**3 * nact
+    fp32_peak = 148 * 128 * 2 * 1965e6 / 1e12
+    traffic = DRAM_TRAFFIC.get((args.workload, args.epsilon, kernel))
+    roofline = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind,
+                "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                                      "one launch of this workload" if traffic else None,
                 "algorithmic_bytes_per_launch": alg[dom], "avg_launch_ms": per_launch_s * 1e3,
-                "share_of_step": dom_ms / max(total_prof, 1e-9)}
+                "share_of_step": dom_ms / max(total_prof, 1e-9),
+                "compute": {"useful_tflop_per_launch": flops / 1e12, "achieved_tflops": flops / per_launch_s / 1e12,
+                            "fp32_fma_peak_tflops": fp32_peak, "peak_kind": "nominal (148 SMs x 128 FMA x 1965 MHz)",
+                            "frac": flops / per_launch_s / 1e12 / fp32_peak}}
 
     # End to end through the C ABI with pinned host arrays.
     e2e = None
