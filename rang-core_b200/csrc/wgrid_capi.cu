@@ -7,6 +7,9 @@
 // device-resident plan.
 #include <cstring>
 #include <map>
+#include <algorithm>
+#include <vector>
+#include <cstdlib>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -63,6 +66,43 @@ cudaStream_t call_stream() {
   streams[dev] = s;
   return s;
 }
+
+// A second per-thread stream for the host <-> device copies of the pipelined calls.
+cudaStream_t copy_stream() {
+  static thread_local std::map<int, cudaStream_t> streams;
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "no CUDA device");
+  auto it = streams.find(dev);
+  if (it != streams.end()) return it->second;
+  cudaStream_t s;
+  check_cuda(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+  streams[dev] = s;
+  return s;
+}
+
+// Row chunks of a host call whose visibilities take `bytes`: the copies of
+// one chunk overlap the gridding or degridding of another. Small calls are
+// not split. RANG_WGRIDDER_ROW_CHUNKS overrides (1: no pipelining).
+int host_row_chunks(size_t bytes) {
+  const char* e = std::getenv("RANG_WGRIDDER_ROW_CHUNKS");
+  const int env = e ? std::atoi(e) : 0;
+  if (env > 0) return std::min(env, 64);
+  return bytes >= ((size_t)256 << 20) ? 8 : 1;
+}
+
+// Events without timing, destroyed with the holder.
+struct Events {
+  std::vector<cudaEvent_t> e;
+  explicit Events(int n) : e((size_t)n, nullptr) {
+    for (auto& x : e) check_cuda(cudaEventCreateWithFlags(&x, cudaEventDisableTiming), "event");
+  }
+  ~Events() {
+    for (auto x : e)
+      if (x) cudaEventDestroy(x);
+  }
+  Events(const Events&) = delete;
+  Events& operator=(const Events&) = delete;
+};
 
 size_t vis_bytes(int kind, const void* p) {  // ffi_wgridder.rs:319-336
   switch (kind) {
@@ -134,6 +174,65 @@ void finish(Plan<T>& plan, cudaStream_t s) {
   if (plan.kernel_errors(s)) throw DeviceError("a visibility fell outside its uv tile (internal inconsistency)");
 }
 
+// vis2dirty of host data with the visibility copy overlapped: coordinates,
+// weights and mask go first and are planned on with the active set they
+// give (weight * mask != 0) while the visibilities follow in row chunks on a
+// second stream; each chunk is gridded as soon as it is on the device. The
+// reference's active set also drops visibilities that are exactly zero, so
+// the plan stands only if a scan of the full active set finds the same count
+// and |w| range (then kernel, grid and planes are the same, and the extra
+// visibilities, all zero, add nothing); otherwise the call is planned and
+// gridded again on the full active set.
+template <class T>
+void host_vis2dirty_pipelined(const WgridderOptions* o, size_t nrow, size_t nchan, const double* uvw,
+                              const double* freq, const void* vis, int vis_kind, const void* wgt, const void* wgt2,
+                              int wgt_kind, const uint8_t* mask, T* dirty, double* info, int chunks) {
+  const size_t npix = o->nx * o->ny, vb = vis_bytes(vis_kind, vis), rowb = nchan * vb;
+  cudaStream_t s = call_stream(), sc = copy_stream();
+  Uploaded u = upload_inputs(nrow, nchan, uvw, nullptr, VIS_UNIT, wgt, wgt2, wgt_kind, mask, s);
+  // The plan's row chunks: rows [c * rpc, (c + 1) * rpc).
+  const size_t rpc = Plan<T>::chunk_rows(nrow, chunks);
+  const int nchunk = (int)((std::max<size_t>(nrow, 1) + rpc - 1) / rpc);
+  Events ready(nchunk);
+  DevBuf visd(nrow * rowb, sc);
+  for (int c = 0; c < nchunk; c++) {
+    const size_t r0 = (size_t)c * rpc, r1 = std::min(nrow, r0 + rpc);
+    check_cuda(cudaMemcpyAsync(visd.as<unsigned char>() + r0 * rowb, static_cast<const unsigned char*>(vis) + r0 * rowb,
+                               (r1 - r0) * rowb, cudaMemcpyHostToDevice, sc),
+               "copy to device");
+    check_cuda(cudaEventRecord(ready.e[c], sc), "record");
+  }
+  Plan<T> plan(*o, nrow, nchan, u.uvw.as<double>(), freq, u.in, false, s, chunks);
+  std::memset(dirty, 0, npix * sizeof(T));
+  Inputs data = u.in;
+  data.vis = visd.get();
+  data.vis_kind = vis_kind;
+  if (plan.empty()) {  // nothing passes the weights and mask: nothing is active
+    check_cuda(cudaStreamSynchronize(sc), "copy");
+    std::memcpy(info, plan.info().v, sizeof(plan.info().v));
+    return;
+  }
+  DevBuf img(npix * sizeof(T), s);
+  if (plan.chunks() == nchunk) {
+    plan.grid(data, VALUE_DATA, img.as<T>(), s, ready.e.data());
+  } else {  // the plan kept one chunk (too many bins): wait for all rows
+    check_cuda(cudaStreamWaitEvent(s, ready.e[nchunk - 1], 0), "wait");
+    plan.grid(data, VALUE_DATA, img.as<T>(), s);
+  }
+  if (plan.same_scan(data, true, s)) {
+    std::memcpy(info, plan.info().v, sizeof(plan.info().v));
+    check_cuda(cudaMemcpyAsync(dirty, img.get(), npix * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
+    finish(plan, s);
+    return;
+  }
+  Plan<T> exact(*o, nrow, nchan, u.uvw.as<double>(), freq, data, true, s);
+  std::memcpy(info, exact.info().v, sizeof(exact.info().v));
+  if (exact.empty()) return;
+  exact.grid(data, VALUE_DATA, img.as<T>(), s);
+  check_cuda(cudaMemcpyAsync(dirty, img.get(), npix * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
+  finish(exact, s);
+}
+
 // vis2dirty_multi (wgridder.rs:2436-2496) on host arrays.
 template <class T>
 void host_vis2dirty(const WgridderOptions* o, size_t nrow, size_t nchan, const double* uvw, const double* freq,
@@ -147,6 +246,13 @@ void host_vis2dirty(const WgridderOptions* o, size_t nrow, size_t nchan, const d
   f_over_c(freq, nchan);  // the frequency checks, before any device work
   size_t npix = o->nx * o->ny;
   cudaStream_t s = call_stream();
+  const size_t vb = vis_bytes(vis_kind, vis);
+  const int chunks = host_row_chunks(nrow * nchan * vb);
+  if (dirty && !psf && vb && chunks > 1) {
+    host_vis2dirty_pipelined<T>(o, nrow, nchan, uvw, freq, vis, vis_kind, wgt, wgt2, wgt_kind, mask, dirty, info,
+                                chunks);
+    return;
+  }
   Uploaded u = upload_inputs(nrow, nchan, uvw, vis, vis_kind, wgt, wgt2, wgt_kind, mask, s);
   Plan<T> plan(*o, nrow, nchan, u.uvw.as<double>(), freq, u.in, psf == nullptr, s);
   if (dirty) std::memset(dirty, 0, npix * sizeof(T));
@@ -177,7 +283,7 @@ void host_dirty2vis(const WgridderOptions* o, size_t nrow, size_t nchan, const d
   size_t n = nrow * nchan, npix = o->nx * o->ny;
   cudaStream_t s = call_stream();
   Uploaded u = upload_inputs(nrow, nchan, uvw, nullptr, VIS_UNIT, wgt, nullptr, wgt_kind, mask, s);
-  Plan<T> plan(*o, nrow, nchan, u.uvw.as<double>(), freq, u.in, false, s);
+  Plan<T> plan(*o, nrow, nchan, u.uvw.as<double>(), freq, u.in, false, s, host_row_chunks(n * 2 * sizeof(T)));
   std::memcpy(info, plan.info().v, sizeof(plan.info().v));
   if (plan.empty()) {
     std::memset(vis, 0, n * 2 * sizeof(T));
@@ -185,8 +291,25 @@ void host_dirty2vis(const WgridderOptions* o, size_t nrow, size_t nchan, const d
   }
   DevBuf img = upload(dirty, npix * sizeof(T), s);
   DevBuf out(n * 2 * sizeof(T), s);
-  plan.degrid(img.as<T>(), u.in, out.as<T>(), s);
-  check_cuda(cudaMemcpyAsync(vis, out.get(), n * 2 * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
+  if (plan.chunks() == 1) {
+    plan.degrid(img.as<T>(), u.in, out.as<T>(), s);
+    check_cuda(cudaMemcpyAsync(vis, out.get(), n * 2 * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
+    finish(plan, s);
+    return;
+  }
+  // Each row chunk's visibilities go back while the next chunk is degridded.
+  cudaStream_t sc = copy_stream();
+  Events done(plan.chunks());
+  plan.degrid(img.as<T>(), u.in, out.as<T>(), s, done.e.data());
+  const size_t rowb = nchan * 2 * sizeof(T);
+  for (int c = 0; c < plan.chunks(); c++) {
+    const size_t r0 = plan.row_begin(c), r1 = plan.row_begin(c + 1);
+    check_cuda(cudaStreamWaitEvent(sc, done.e[c], 0), "wait");
+    check_cuda(cudaMemcpyAsync(reinterpret_cast<unsigned char*>(vis) + r0 * rowb, out.as<unsigned char>() + r0 * rowb,
+                               (r1 - r0) * rowb, cudaMemcpyDeviceToHost, sc),
+               "copy to host");
+  }
+  check_cuda(cudaStreamSynchronize(sc), "copy to host");
   finish(plan, s);
 }
 

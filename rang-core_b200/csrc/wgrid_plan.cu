@@ -184,10 +184,11 @@ __device__ __forceinline__ uint32_t warp_aggregated_add(uint32_t* counters, uint
   return res;
 }
 
+// With rows_per_chunk > 0 the key is chunk * nbins + bin, chunk = row / rows_per_chunk.
 template <class T>
 __global__ void k_bin_count(const __grid_constant__ Geom<T> g, const double* __restrict__ uvw,
                             const double* __restrict__ foc, Inputs in, int with_vis, uint32_t* __restrict__ key,
-                            uint32_t* __restrict__ counts) {
+                            uint32_t* __restrict__ counts, uint32_t rows_per_chunk = 0, uint32_t nbins = 0) {
   uint64_t n = g.nrow * g.nchan;
   uint64_t nround = (n + 31) & ~31ull;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -197,7 +198,10 @@ __global__ void k_bin_count(const __grid_constant__ Geom<T> g, const double* __r
     uint32_t k = INACTIVE;
     if (i < n) {
       act = is_active<T>(in, with_vis != 0, i);
-      if (act) k = bin_of_rc(g, uvw, foc, rc.row, rc.ch);
+      if (act) {
+        k = bin_of_rc(g, uvw, foc, rc.row, rc.ch);
+        if (rows_per_chunk) k += (rc.row / rows_per_chunk) * nbins;
+      }
       key[i] = k;
     }
     warp_aggregated_add(counts, k, act);
@@ -317,8 +321,10 @@ __device__ __forceinline__ uint32_t plane_at(const uint32_t* starts, uint64_t b0
   return lo / nsub;
 }
 
+// `ntiles` counts the (row chunk, tile) pairs; the task keeps the tile.
 __global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t stride, uint32_t nsub, uint32_t ntiles,
-                            const uint32_t* __restrict__ off, Task* __restrict__ tasks, uint32_t* __restrict__ ntotal) {
+                            uint32_t tiles_per_chunk, const uint32_t* __restrict__ off, Task* __restrict__ tasks,
+                            uint32_t* __restrict__ ntotal) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntiles) return;
   uint64_t b0 = (uint64_t)t * stride;
@@ -327,7 +333,7 @@ __global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t stride
   for (uint32_t k0 = s, q = q0; k0 < e; k0 += TASK_CHUNK, q++) {
     uint32_t k1 = min(k0 + TASK_CHUNK, e);
     Task tk;
-    tk.tile = t;
+    tk.tile = t % tiles_per_chunk;
     tk.k0 = k0;
     tk.k1 = k1;
     tk.plo = (uint16_t)plane_at(starts, b0, stride, nsub, k0);
@@ -684,7 +690,7 @@ __device__ __forceinline__ void tc_flush(const Geom<float>& g, cplx<float>* __re
 template <int S>
 __global__ void __launch_bounds__(TC_BATCH)
     k_grid_tc(const __grid_constant__ Geom<float> g, Inputs in, int mode, const double* __restrict__ uvw,
-              const double* __restrict__ foc, const uint32_t* __restrict__ sorted, uint64_t nsorted,
+              const double* __restrict__ foc, const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend,
               cplx<float>* __restrict__ grids, int pg0, int npg) {
   static_assert(S <= 8, "windows hold 8 + S - 1 <= 16 rows");
   extern __shared__ __align__(16) unsigned char smem[];
@@ -694,8 +700,8 @@ __global__ void __launch_bounds__(TC_BATCH)
   for (int c = lane; c < (int)(TcSlots::bytes() / 16); c += TC_BATCH)
     reinterpret_cast<float4*>(smem)[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   __syncwarp();
-  const uint64_t k0 = (uint64_t)blockIdx.x * TC_CHUNK;
-  const uint64_t k1 = min(nsorted, k0 + TC_CHUNK);
+  const uint64_t k0 = kbase + (uint64_t)blockIdx.x * TC_CHUNK;
+  const uint64_t k1 = min(kend, k0 + TC_CHUNK);
   const uint32_t nchan = (uint32_t)g.nchan;
   const int np = g.do_wgridding ? S : 1;
   const uint32_t tmask = (1u << g.log2tile) - 1u;
@@ -1200,6 +1206,7 @@ template <class T, int S>
 void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, const Inputs& in, int mode,
                  const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
                  const uint32_t* ntasks, cplx<T>* grids, int pg0, int npg, int gmax, int* err) {
+  if (nblocks == 0) return;
   const int batch = staging_batch<T, S>();
   const int total = smem + batch * (int)GridStaging<T, S>::bytes_per_vis();
   check_cuda(cudaFuncSetAttribute(k_grid<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, total), "smem");
@@ -1213,13 +1220,15 @@ void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, c
 
 template <int S>
 void launch_grid_tc(cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode, const double* uvw,
-                    const double* foc, const uint32_t* sorted, uint64_t nsorted, cplx<float>* grids, int pg0, int npg) {
+                    const double* foc, const uint32_t* sorted, uint64_t kbase, uint64_t kend, cplx<float>* grids,
+                    int pg0, int npg) {
+  if (kend <= kbase) return;
   const int smem = (int)TcSlots::bytes();
-  const unsigned nblocks = (unsigned)((nsorted + TC_CHUNK - 1) / TC_CHUNK);
+  const unsigned nblocks = (unsigned)((kend - kbase + TC_CHUNK - 1) / TC_CHUNK);
   check_cuda(cudaFuncSetAttribute(k_grid_tc<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
   {
     StageTimer timer_(ST_GRID, s);
-    k_grid_tc<S><<<nblocks, TC_BATCH, smem, s>>>(g, in, mode, uvw, foc, sorted, nsorted, grids, pg0, npg);
+    k_grid_tc<S><<<nblocks, TC_BATCH, smem, s>>>(g, in, mode, uvw, foc, sorted, kbase, kend, grids, pg0, npg);
   }
   check_cuda(cudaGetLastError(), "grid kernel (tensor cores)");
 }
@@ -1229,6 +1238,7 @@ void launch_degrid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g,
                    const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
                    const uint32_t* ntasks, const cplx<T>* grids, int pg0, int npg, int gmax, cplx<T>* vis,
                    int first, int last, int* err) {
+  if (nblocks == 0) return;
   check_cuda(cudaFuncSetAttribute(k_degrid<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
   {
     StageTimer timer_(ST_DEGRID, s);
@@ -1387,8 +1397,10 @@ int max_window_planes(int L, size_t cell_bytes) {
 
 template <class T>
 Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw_dev, const double* freq_host,
-              const Inputs& act, bool with_vis, cudaStream_t s)
+              const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks)
     : o_(o), nrow_(nrow), nchan_(nchan), n_(nrow * nchan) {
+  rows_per_chunk_ = chunk_rows(nrow, row_chunks);
+  nchunk_ = (int)((std::max<size_t>(nrow, 1) + rows_per_chunk_ - 1) / rows_per_chunk_);
   check_common(o, nrow, nchan);
   if (n_ >= 0xffffffffull) throw InvalidArgument("too many visibilities for one call (at most 2^32 - 2)");
   recentring(o, r_l_, r_m_);
@@ -1418,6 +1430,10 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   check_cuda(cudaMemcpyAsync(&r, so.get(), sizeof(r), cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaStreamSynchronize(s), "scan");
   nvis_ = r.count;
+  scan_[0] = r.count;
+  scan_[1] = r.finite;
+  scan_[2] = r.lo_bits;
+  scan_[3] = r.hi_bits;
   double wmin_d = 1e300, wmax_d = -1e300;
   if (r.finite) {
     std::memcpy(&wmin_d, &r.lo_bits, sizeof(double));
@@ -1436,19 +1452,25 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
   ntiles_ = (size_t)g_.ntu * g_.ntv;
   nbins_ = ntiles_ * (size_t)g_.nbuckets * (size_t)g_.nsub;
   if (nbins_ >= 0xffffffffull) throw InvalidArgument("too many uv tiles and w-planes for one call");
+  if ((size_t)nchunk_ * nbins_ >= 0xffffffffull) {  // row chunks are an optimisation: drop them
+    nchunk_ = 1;
+    rows_per_chunk_ = std::max<size_t>(nrow_, 1);
+  }
+  const size_t K = (size_t)nchunk_, nkeys = K * nbins_, nvt = K * ntiles_;
   key_.alloc(n_ * 4, s);
-  starts_.alloc((nbins_ + 1) * 4, s);
-  check_cuda(cudaMemsetAsync(starts_.get(), 0, (nbins_ + 1) * 4, s), "memset");
+  starts_.alloc((nkeys + 1) * 4, s);
+  check_cuda(cudaMemsetAsync(starts_.get(), 0, (nkeys + 1) * 4, s), "memset");
   {
     StageTimer timer_(ST_BIN_COUNT, s);
     k_bin_count<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act,
-                                                        with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>());
+                                                        with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>(),
+                                                        K > 1 ? (uint32_t)rows_per_chunk_ : 0u, (uint32_t)nbins_);
   }
   check_cuda(cudaGetLastError(), "bin count");
-  exclusive_scan(starts_.as<uint32_t>(), starts_.as<uint32_t>(), nbins_ + 1, s);
+  exclusive_scan(starts_.as<uint32_t>(), starts_.as<uint32_t>(), nkeys + 1, s);
   {
-    DevBuf cursor((nbins_ + 1) * 4, s);
-    check_cuda(cudaMemcpyAsync(cursor.get(), starts_.get(), (nbins_ + 1) * 4, cudaMemcpyDeviceToDevice, s), "copy");
+    DevBuf cursor((nkeys + 1) * 4, s);
+    check_cuda(cudaMemcpyAsync(cursor.get(), starts_.get(), (nkeys + 1) * 4, cudaMemcpyDeviceToDevice, s), "copy");
     sorted_.alloc(nvis_ * 4, s);
     {
       StageTimer timer_(ST_BIN_SCATTER, s);
@@ -1457,28 +1479,60 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
     }
     check_cuda(cudaGetLastError(), "bin scatter");
   }
-  // Tasks.
-  max_tasks_ = nvis_ / TASK_CHUNK + ntiles_ + 1;
-  DevBuf ntask((ntiles_ + 1) * 4, s);
+  // Tasks, over (row chunk, tile) pairs.
+  max_tasks_ = nvis_ / TASK_CHUNK + nvt + 1;
+  DevBuf ntask((nvt + 1) * 4, s);
   {
     StageTimer timer_(ST_TASKS, s);
-    k_task_count<<<(unsigned)((ntiles_ + 1 + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(),
-                                                                       (uint32_t)(g_.nbuckets * g_.nsub),
-                                                                       (uint32_t)ntiles_, ntask.as<uint32_t>());
+    k_task_count<<<(unsigned)((nvt + 1 + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(),
+                                                                   (uint32_t)(g_.nbuckets * g_.nsub), (uint32_t)nvt,
+                                                                   ntask.as<uint32_t>());
   }
   check_cuda(cudaGetLastError(), "tasks");
-  exclusive_scan(ntask.as<uint32_t>(), ntask.as<uint32_t>(), ntiles_ + 1, s);
+  exclusive_scan(ntask.as<uint32_t>(), ntask.as<uint32_t>(), nvt + 1, s);
   tasks_.alloc(max_tasks_ * sizeof(Task), s);
   ntasks_.alloc(4, s);
   {
     StageTimer timer_(ST_TASKS, s);
-    k_task_emit<<<(unsigned)((ntiles_ + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(),
-                                                                  (uint32_t)(g_.nbuckets * g_.nsub), (uint32_t)g_.nsub,
-                                                                  (uint32_t)ntiles_, ntask.as<uint32_t>(),
-                                                                  tasks_.as<Task>(), ntasks_.as<uint32_t>());
+    k_task_emit<<<(unsigned)((nvt + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(),
+                                                              (uint32_t)(g_.nbuckets * g_.nsub), (uint32_t)g_.nsub,
+                                                              (uint32_t)nvt, (uint32_t)ntiles_, ntask.as<uint32_t>(),
+                                                              tasks_.as<Task>(), ntasks_.as<uint32_t>());
   }
   check_cuda(cudaGetLastError(), "tasks");
+  // Where each row chunk starts in the sorted order and in the task list.
+  std::vector<uint32_t> so(K + 1), to(K + 1);
+  for (size_t c = 0; c <= K; c++) {
+    check_cuda(cudaMemcpyAsync(&so[c], starts_.as<uint32_t>() + c * nbins_, 4, cudaMemcpyDeviceToHost, s), "copy");
+    check_cuda(cudaMemcpyAsync(&to[c], ntask.as<uint32_t>() + c * ntiles_, 4, cudaMemcpyDeviceToHost, s), "copy");
+  }
+  check_cuda(cudaStreamSynchronize(s), "layout");
+  chunk_sorted_.assign(so.begin(), so.end());
+  chunk_tasks_.assign(to.begin(), to.end());
   corrections(s);
+}
+
+template <class T>
+bool Plan<T>::same_scan(const Inputs& act, bool with_vis, cudaStream_t s) const {
+  DevBuf so(sizeof(ScanOut), s);
+  ScanOut init{0, 0, 0, 0};
+  const double big = 1e300;
+  std::memcpy(&init.lo_bits, &big, sizeof(big));
+  check_cuda(cudaMemcpyAsync(so.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s), "copy");
+  if (n_) {
+    {
+      StageTimer timer_(ST_SCAN, s);
+      k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow_, (uint32_t)nchan_, uvw_.as<double>(),
+                                                    foc_.as<double>(), o_.flip_w ? 1.0 : -1.0, act, with_vis ? 1 : 0,
+                                                    so.as<ScanOut>());
+    }
+    check_cuda(cudaGetLastError(), "scan kernel");
+  }
+  ScanOut r;
+  check_cuda(cudaMemcpyAsync(&r, so.get(), sizeof(r), cudaMemcpyDeviceToHost, s), "copy");
+  check_cuda(cudaStreamSynchronize(s), "scan");
+  if (r.count != scan_[0] || r.finite != scan_[1]) return false;
+  return r.finite == 0 || (r.lo_bits == scan_[2] && r.hi_bits == scan_[3]);
 }
 
 template <class T>
@@ -1522,7 +1576,7 @@ size_t Plan<T>::plane_group(size_t cell_bytes) const {
 }
 
 template <class T>
-void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s) {
+void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready) {
   size_t npix = (size_t)o_.nx * o_.ny;
   if (nvis_ == 0) {
     check_cuda(cudaMemsetAsync(image, 0, npix * sizeof(T), s), "memset");
@@ -1544,16 +1598,19 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s)
     check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
     auto run = [&](auto S) {
       constexpr int SV = decltype(S)::value;
-      if constexpr (sizeof(T) == 4) {
-        if (grid_method() == GRID_TF32X3) {
-          launch_grid_tc<SV>(s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(), sorted_.as<uint32_t>(),
-                             nvis_, grids.as<cplx<T>>(), (int)pg0, n);
-          return;
+      for (int c = 0; c < nchunk_; c++) {  // row chunk c once its rows are on the device
+        if (ready && pg0 == 0) check_cuda(cudaStreamWaitEvent(s, ready[c], 0), "wait");
+        if constexpr (sizeof(T) == 4) {
+          if (grid_method() == GRID_TF32X3) {
+            launch_grid_tc<SV>(s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(), sorted_.as<uint32_t>(),
+                               chunk_sorted_[c], chunk_sorted_[c + 1], grids.as<cplx<T>>(), (int)pg0, n);
+            continue;
+          }
         }
+        launch_grid<T, SV>(smem, chunk_tasks_[c + 1] - chunk_tasks_[c], s, g_, data, (int)mode, uvw_.as<double>(),
+                           foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>() + chunk_tasks_[c],
+                           ntasks_.as<uint32_t>(), grids.as<cplx<T>>(), (int)pg0, n, gmax, err_.as<int>());
       }
-      launch_grid<T, SV>(smem, (unsigned)max_tasks_, s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(),
-                         sorted_.as<uint32_t>(), tasks_.as<Task>(), ntasks_.as<uint32_t>(), grids.as<cplx<T>>(),
-                         (int)pg0, n, gmax, err_.as<int>());
     };
     if constexpr (sizeof(T) == 4)
       with_supp_float(g_.supp, run);
@@ -1577,9 +1634,13 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s)
 }
 
 template <class T>
-void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s) {
+void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, cudaEvent_t* done) {
   check_cuda(cudaMemsetAsync(vis, 0, n_ * 2 * sizeof(T), s), "memset");
-  if (nvis_ == 0) return;
+  if (nvis_ == 0) {
+    if (done)
+      for (int c = 0; c < nchunk_; c++) check_cuda(cudaEventRecord(done[c], s), "record");
+    return;
+  }
   const size_t npix = (size_t)o_.nx * o_.ny;
   const size_t cell = sizeof(cplx<T>);
   const size_t nplanes = (size_t)std::max(g_.nplanes, 1);
@@ -1619,10 +1680,14 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s) 
     }
     bool first = pg0 == 0, last = pg0 + n >= nplanes;
     auto run = [&](auto S) {
-      launch_degrid<T, decltype(S)::value>(smem, (unsigned)max_tasks_, s, g_, wts, uvw_.as<double>(),
-                                           foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>(),
-                                           ntasks_.as<uint32_t>(), grids.as<cplx<T>>(), (int)pg0, n, gmax,
-                                           reinterpret_cast<cplx<T>*>(vis), first, last, err_.as<int>());
+      for (int c = 0; c < nchunk_; c++) {  // row chunk c, final after the last plane group
+        launch_degrid<T, decltype(S)::value>(smem, chunk_tasks_[c + 1] - chunk_tasks_[c], s, g_, wts,
+                                             uvw_.as<double>(), foc_.as<double>(), sorted_.as<uint32_t>(),
+                                             tasks_.as<Task>() + chunk_tasks_[c], ntasks_.as<uint32_t>(),
+                                             grids.as<cplx<T>>(), (int)pg0, n, gmax,
+                                             reinterpret_cast<cplx<T>*>(vis), first, last, err_.as<int>());
+        if (done && last) check_cuda(cudaEventRecord(done[c], s), "record");
+      }
     };
     if constexpr (sizeof(T) == 4)
       with_supp_float(g_.supp, run);
@@ -1643,6 +1708,7 @@ int Plan<T>::kernel_errors(cudaStream_t s) const {
 template <class T>
 void Plan<T>::export_binning(uint32_t* key_host, uint32_t* sorted_host, cudaStream_t s) const {
   if (nvis_ == 0) return;
+  if (nchunk_ != 1) throw DeviceError("binning export of a plan with row chunks");
   check_cuda(cudaMemcpyAsync(key_host, key_.get(), n_ * 4, cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaMemcpyAsync(sorted_host, sorted_.get(), nvis_ * 4, cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaStreamSynchronize(s), "copy");

@@ -7,6 +7,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -63,8 +64,12 @@ class Plan {
   // Scan the active set (`with_vis`: |vis|^2 wgt mask != 0, else wgt mask
   // != 0), choose kernel and grid, and bin the active visibilities. `uvw`
   // and the arrays of `act` are device pointers; `freq` is on the host.
+  // With `row_chunks` > 1 the rows are split into that many equal ranges and
+  // the sorted order is chunk-major (each range's visibilities contiguous,
+  // binned among themselves), so that gridding can start on the rows that
+  // have arrived and degridding can hand out finished rows early.
   Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw_dev, const double* freq_host,
-       const Inputs& act, bool with_vis, cudaStream_t s);
+       const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks = 1);
 
   bool empty() const { return nvis_ == 0; }
   const PlanInfo& info() const { return info_; }
@@ -72,12 +77,26 @@ class Plan {
   const Geom<T>& geom() const { return g_; }
 
   // vis2dirty into `image` (nx * ny, device): `data` gives the data and the
-  // weights; VALUE_UNIT grids unit visibilities (the PSF).
-  void grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s);
+  // weights; VALUE_UNIT grids unit visibilities (the PSF). With `ready`
+  // (one event per row chunk), chunk c is gridded after ready[c].
+  void grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready = nullptr);
   // dirty2vis of `image` into `vis` (nrow * nchan interleaved complex,
   // device, overwritten; inactive visibilities zero), times the weights of
-  // `wts`.
-  void degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s);
+  // `wts`. With `done` (one event per row chunk), done[c] is recorded once
+  // the rows of chunk c are final.
+  void degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, cudaEvent_t* done = nullptr);
+
+  // Rows per chunk when `nrow` rows are asked to be split `row_chunks` ways.
+  static size_t chunk_rows(size_t nrow, int row_chunks) {
+    const size_t k = std::max<size_t>(1, std::min<size_t>((size_t)std::max(row_chunks, 1), std::max<size_t>(nrow, 1)));
+    return std::max<size_t>(1, (nrow + k - 1) / k);
+  }
+  // Row chunks of the sorted order: chunk c holds rows [row_begin(c), row_begin(c + 1)).
+  int chunks() const { return nchunk_; }
+  size_t row_begin(int c) const { return std::min(nrow_, (size_t)c * rows_per_chunk_); }
+  // Scans another active set and tells whether its count and |w| range equal
+  // this plan's (then the kernel, grid and planes would be the same).
+  bool same_scan(const Inputs& act, bool with_vis, cudaStream_t s) const;
 
   // Waits for `s` and returns the inconsistencies the kernels flagged (0: none).
   int kernel_errors(cudaStream_t s) const;
@@ -109,6 +128,11 @@ class Plan {
   DevBuf corr_;     // double per pixel: the global correction
   DevBuf err_;      // int: kernel-detected inconsistencies
   size_t nbins_ = 0, ntiles_ = 0, max_tasks_ = 0;
+  int nchunk_ = 1;
+  size_t rows_per_chunk_ = 0;
+  std::vector<uint64_t> chunk_sorted_;  // nchunk_ + 1 offsets into the sorted order
+  std::vector<uint32_t> chunk_tasks_;   // nchunk_ + 1 offsets into the task list
+  unsigned long long scan_[4] = {0, 0, 0, 0};  // count, finite count, |w| min and max bits
 };
 
 // How single-precision gridding accumulates footprints: split-precision
