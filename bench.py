@@ -48,7 +48,7 @@ from rang import synth  # noqa: E402
 
 WORKLOAD = "ms2dirty+dirty2ms 1.06G vis 4096^2"
 # DRAM bytes (read + written) of one launch of the dominant kernels, measured
-# with ncu on a B200 (profiles/dram_grid_degrid_1.06G_4096.md).
+# with ncu on a B200 (profiles/launches_dram_ms2dirty_dirty2ms_1.06G_4096.md).
 DRAM_TRAFFIC = {
     (WORKLOAD, 1e-5, "k_grid_tc"): 19.83e9 + 0.571e9,
     (WORKLOAD, 1e-5, "k_degrid"): 9.61e9 + 9.51e9,
@@ -405,7 +405,8 @@ def run_b200(args):
                                             info)
             assert st == 0, ext.wgridder_last_error()
 
-        e2e_step()
+        for _ in range(args.warmup):
+            e2e_step()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
