@@ -47,8 +47,9 @@ sys.path.insert(0, str(REPO / "rang-core_b200"))
 from rang import synth  # noqa: E402
 
 WORKLOAD = "ms2dirty+dirty2ms 1.06G vis 4096^2"
-# DRAM bytes (read + written) of one launch of the dominant kernels, measured
-# with ncu on a B200 (profiles/launches_dram_ms2dirty_dirty2ms_1.06G_4096.md).
+# DRAM bytes (read + written) of one launch of the dominant kernels on this
+# workload, measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+# on a B200: a profiler figure, not something this script can time.
 DRAM_TRAFFIC = {
     (WORKLOAD, 1e-5, "k_grid_tc"): 19.83e9 + 0.571e9,
     (WORKLOAD, 1e-5, "k_degrid"): 9.61e9 + 9.51e9,
