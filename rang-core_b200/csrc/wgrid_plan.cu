@@ -643,6 +643,14 @@ __device__ __forceinline__ void split_fast(float x, uint32_t& hi, uint32_t& lo) 
   hi = (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
   lo = __float_as_uint(x - __uint_as_float(hi));
 }
+// d = a * b from zero: the first product of a block.
+__device__ __forceinline__ void mma_tf32_zero(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%10,%10,%10,%10};\n"
+      : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(0.0f));
+}
 __device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
   asm(
       "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -813,7 +821,7 @@ __global__ void __launch_bounds__(TC_BATCH)
           const bool two = j + 1 < S;
           if (!((pact >> j) & (two ? 3u : 1u))) continue;
           uint32_t ah[2][4], al[2][4];
-          float d[2][2][4];
+          float d[2][2][4];  // each block's products start from zero
 #pragma unroll
           for (int h = 0; h < 2; h++) {
             if (h == 1 && !two) break;
@@ -822,16 +830,12 @@ __global__ void __launch_bounds__(TC_BATCH)
             split_fast(w0 * ku01, ah[h][1], al[h][1]);  // A[gq + 8][tq]
             split_fast(w1 * ku10, ah[h][2], al[h][2]);  // A[gq][tq + 4]
             split_fast(w1 * ku11, ah[h][3], al[h][3]);  // A[gq + 8][tq + 4]
-#pragma unroll
-            for (int c = 0; c < 2; c++)
-#pragma unroll
-              for (int r = 0; r < 4; r++) d[h][c][r] = 0.0f;
           }
 #pragma unroll
           for (int h = 0; h < 2; h++)
             if (h == 0 || two) {
-              mma_tf32(d[h][0], ah[h], brh0, brh1);
-              mma_tf32(d[h][1], ah[h], bih0, bih1);
+              mma_tf32_zero(d[h][0], ah[h], brh0, brh1);
+              mma_tf32_zero(d[h][1], ah[h], bih0, bih1);
             }
 #pragma unroll
           for (int h = 0; h < 2; h++)
