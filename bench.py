@@ -442,7 +442,57 @@ def run_b200(args):
             "vis_rel_linf": float(dv.abs().max() / vpeak),
             "vis_rel_rms": float(dv.abs().pow(2).mean().sqrt() / vpeak),
         }
-        del d64, v64, dd, dv
+        del v64, dd, dv
+
+        # The tensor-core (3 x TF32) and CUDA-core (FP32) gridders at epsilon
+        # 1e-5 (support 6) and 1e-6 (support 8; the single-precision kernels
+        # stop at 8.1e-7, so 1e-7 needs double precision, timed last): one
+        # plan + grid and one plan + degrid each (after a warm-up), errors
+        # against float64 at epsilon 1e-7 on the same inputs: the dirty image
+        # of the data, and the visibilities of one fixed image (the float64
+        # dirty image in float32). Degridding has one kernel for both methods.
+        img = d64.float()
+        q64 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=1e-7, single=False, **common)
+        v64 = q64.degrid(img.double())
+        q64.close()
+        vpeak = v64.abs().max()
+        methods = []
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        cases = [(1e-5, "tf32x3", 1, True), (1e-5, "fp32", 0, True), (1e-6, "tf32x3", 1, True),
+                 (1e-6, "fp32", 0, True), (1e-7, "fp64", 1, False)]
+        for eps_m, name, code, single in cases:
+            ext.wgridder_set_method(code)
+            vin = vis if single else vis.to(torch.complex128)
+            iin = img if single else img.double()
+            for _ in range(2):
+                torch.cuda.synchronize()
+                ev[0].record()
+                pa = wgrid_torch.DevicePlan(uvw, freq, vis=vin, mask=mask, epsilon=eps_m, single=single, **common)
+                dm = pa.grid(vin)
+                ev[1].record()
+                pb = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=eps_m, single=single, **common)
+                vm = pb.degrid(iin)
+                ev[2].record()
+                torch.cuda.synchronize()
+                supp = pa.info["supp"]
+                pa.close()
+                pb.close()
+            entry = {"method": name, "epsilon": eps_m, "supp": int(supp),
+                     "vis2dirty_ms": ev[0].elapsed_time(ev[1]), "dirty2vis_ms": ev[1].elapsed_time(ev[2])}
+            if single:
+                dd = dm.double() - d64
+                dv = vm.to(torch.complex128) - v64
+                entry.update({"dirty_rel_linf": float(dd.abs().max() / peak),
+                              "dirty_rel_rms": float(dd.pow(2).mean().sqrt() / peak),
+                              "vis_rel_linf": float(dv.abs().max() / vpeak),
+                              "vis_rel_rms": float(dv.abs().pow(2).mean().sqrt() / vpeak)})
+                del dd, dv
+            methods.append(entry)
+            del dm, vm, vin, iin
+        ext.wgridder_set_method(1)
+        accuracy["methods"] = methods
+        accuracy["methods_reference"] = "float64 GPU run at epsilon 1e-7; errors near 1e-7 are at that reference's level"
+        del d64, v64, img
 
     fst = None
     if rank == 0 and not args.no_fista:
