@@ -46,8 +46,8 @@ class Options(ctypes.Structure):
 
 def build():
     """Compile liboracle.so with the committed Makefile (idempotent)."""
-    src = HERE / "wgridder_oracle.cpp"
-    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+    srcs = [HERE / "wgridder_oracle.cpp", HERE / "weights_oracle.cpp"]
+    if not LIB.exists() or any(LIB.stat().st_mtime < src.stat().st_mtime for src in srcs):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
 
@@ -78,6 +78,13 @@ def lib():
         _lib.oracle_last_error.argtypes = [P, S]
         _lib.oracle_last_error.restype = S
         _lib.oracle_set_threads.argtypes = [I]
+        _lib.oracle_padded_size.argtypes = [S, ctypes.c_double]
+        _lib.oracle_padded_size.restype = S
+        _lib.oracle_weight_grid_shape.argtypes = [S, S, ctypes.c_double, P]
+        _lib.oracle_stokes_i.argtypes = [S, P, P, P, P, P]
+        D = ctypes.c_double
+        _lib.oracle_imaging_weights.argtypes = [S, S, P, P, P, P, ctypes.c_uint32, D, S, S, D, D, D, D, S, P, P, P]
+        _lib.oracle_imaging_weights.restype = I
     return _lib
 
 
@@ -346,3 +353,55 @@ def dft_vis(uvw, freq, image, dx, dy):
 
 if os.environ.get("RANG_ORACLE_THREADS"):
     set_threads(int(os.environ["RANG_ORACLE_THREADS"]))
+
+
+# ------------------------------------------------------------------ imaging weights (core/src/weights.rs)
+
+WEIGHT_CLASSES = {"natural": 0, "uniform": 1, "briggs": 2}
+
+
+def padded_size(trimmed, padding=1.2):
+    return int(lib().oracle_padded_size(int(trimmed), float(padding)))
+
+
+def weight_grid_shape(width, height, super_weight=1.0):
+    out = np.zeros(2, np.uint64)
+    lib().oracle_weight_grid_shape(int(width), int(height), float(super_weight), out.ctypes.data)
+    return int(out[0]), int(out[1])
+
+
+def stokes_i(data, weights, flags):
+    """`data` complex64 (..., 4), `weights` float32 and `flags` bool alike:
+    Stokes I complex64 values and float32 weights."""
+    data = np.ascontiguousarray(data, np.complex64)
+    weights = np.ascontiguousarray(weights, np.float32)
+    flags = np.ascontiguousarray(flags, np.uint8)
+    shape = data.shape[:-1]
+    n = int(np.prod(shape, dtype=np.int64))
+    vis = np.zeros(shape, np.complex64)
+    w = np.zeros(shape, np.float32)
+    lib().oracle_stokes_i(n, data.ctypes.data, weights.ctypes.data, flags.ctypes.data, vis.ctypes.data, w.ctypes.data)
+    return vis, w
+
+
+def imaging_weights(uvw, wavelength, weights, row_selected, mode="briggs", robust=0.5, width=616, height=616,
+                    pixel_scale=8.0 * np.pi / (180.0 * 3600.0), super_weight=1.0, rank_filter=(3.0, 16)):
+    """The reference's imaging_weights (weights.rs:465-520) on host arrays:
+    {"weights", "grid" (height // 2, width), "sums" (four values)}."""
+    uvw = np.ascontiguousarray(uvw, np.float64)
+    wavelength = np.ascontiguousarray(wavelength, np.float64)
+    weights = np.ascontiguousarray(weights, np.float32)
+    sel = np.ascontiguousarray(row_selected, np.uint8)
+    nrow, nchan = weights.shape
+    level, size = rank_filter if rank_filter is not None else (0.0, 0)
+    gw, gh = weight_grid_shape(width, height, super_weight)
+    out = np.zeros((nrow, nchan), np.float32)
+    grid = np.zeros((gh // 2, gw), np.float64)
+    sums = np.zeros(4, np.float64)
+    st = lib().oracle_imaging_weights(nrow, nchan, uvw.ctypes.data, wavelength.ctypes.data, weights.ctypes.data,
+                                      sel.ctypes.data, WEIGHT_CLASSES[mode], float(robust), int(width), int(height),
+                                      float(pixel_scale), float(pixel_scale), float(super_weight), float(level),
+                                      int(size), out.ctypes.data, grid.ctypes.data, sums.ctypes.data)
+    if st:
+        raise ValueError("invalid imaging-weight arguments")
+    return {"weights": out, "grid": grid, "sums": sums}
