@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "rang_weights.h"
 #include "rang_wgridder.h"
 
 namespace py = pybind11;
@@ -236,6 +237,74 @@ PYBIND11_MODULE(_core, m) {
     return (int)rang_core_wgridder_kernel_row(index, p);
   });
   m.def("wgridder_last_error", &last_error);
+
+  // Imaging weights and Stokes I (lib.rs:792-904): the reference's bindings of ffi_weights.rs.
+  m.def("weight_grid_shape", [](size_t width, size_t height, double super_weight) {
+    size_t shape[2] = {0, 0};
+    int st = (int)rang_core_weight_grid_shape(width, height, super_weight, shape);
+    return py::make_tuple(st, shape[0], shape[1]);
+  });
+  m.def("padded_size", [](size_t trimmed, double padding) { return rang_core_padded_size(trimmed, padding); });
+  m.def("stokes_i", [](size_t ncell, py::object data, py::object weights, py::object flags, py::object vis,
+                       py::object weight) {
+    size_t nd, nw, nf, nv, no;
+    StokesIInputs in{ncell, ro<float>(data, "data", &nd), ro<float>(weights, "weights", &nw),
+                     ro<uint8_t>(flags, "flags", &nf)};
+    StokesIOutputs out{rw<float>(vis, "vis", &nv), rw<float>(weight, "weight", &no)};
+    if (nd != 8 * ncell) throw py::value_error("data must hold 8 * ncell floats");
+    if (nw != 4 * ncell || nf != 4 * ncell) throw py::value_error("weights and flags must hold 4 * ncell values");
+    if (nv != 2 * ncell || no != ncell) throw py::value_error("vis must hold 2 * ncell and weight ncell values");
+    py::gil_scoped_release release;
+    return (int)rang_core_stokes_i(&in, &out);
+  });
+  m.def("imaging_weights",
+        [](size_t nrow, size_t nchan, py::object uvw, py::object wavelength, py::object weights,
+           py::object row_selected, uint32_t cls, double robust, size_t width, size_t height, double psx, double psy,
+           double super_weight, double level, size_t rank_size, py::object out_weights, py::object grid,
+           py::object sums) {
+          size_t nu, nl, nw, ns, no, ng = 0, nsum = 0;
+          ImagingWeightInputs in{};
+          in.nrow = nrow;
+          in.nchan = nchan;
+          in.uvw = ro<double>(uvw, "uvw", &nu);
+          in.wavelength = ro<double>(wavelength, "wavelength", &nl);
+          in.weights = ro<float>(weights, "weights", &nw);
+          in.row_selected = ro<uint8_t>(row_selected, "row_selected", &ns);
+          in.class_ = cls;
+          in.robust = robust;
+          in.width = width;
+          in.height = height;
+          in.pixel_scale_x = psx;
+          in.pixel_scale_y = psy;
+          in.super_weight = super_weight;
+          in.rank_filter_level = level;
+          in.rank_filter_size = rank_size;
+          if (nu != 3 * nrow) throw py::value_error("uvw must hold 3 * nrow values");
+          if (nl != nchan) throw py::value_error("wavelength must hold nchan values");
+          if (nw != nrow * nchan) throw py::value_error("weights must hold nrow * nchan values");
+          if (ns != nrow) throw py::value_error("row_selected must hold nrow values");
+          ImagingWeightOutputs out{};
+          out.weights = rw<float>(out_weights, "out_weights", &no);
+          if (no != nrow * nchan) throw py::value_error("out_weights must hold nrow * nchan values");
+          if (!grid.is_none()) {
+            out.grid = rw<double>(grid, "grid", &ng);
+            if (super_weight > 0.0) {
+              size_t shape[2];
+              rang_core_weight_grid_shape(width, height, super_weight, shape);
+              if (ng != shape[0] * shape[1] / 2) throw py::value_error("grid must hold width * height / 2 values");
+            }
+          }
+          if (!sums.is_none()) {
+            out.sums = rw<double>(sums, "sums", &nsum);
+            if (nsum != 4) throw py::value_error("sums must hold 4 values");
+          }
+          py::gil_scoped_release release;
+          return (int)rang_core_imaging_weights(&in, &out);
+        },
+        py::arg("nrow"), py::arg("nchan"), py::arg("uvw"), py::arg("wavelength"), py::arg("weights"),
+        py::arg("row_selected"), py::arg("class_"), py::arg("robust"), py::arg("width"), py::arg("height"),
+        py::arg("pixel_scale_x"), py::arg("pixel_scale_y"), py::arg("super_weight"), py::arg("rank_filter_level"),
+        py::arg("rank_filter_size"), py::arg("out_weights"), py::arg("grid"), py::arg("sums"));
 
   // Device-pointer plans (pointers as integers, e.g. torch.Tensor.data_ptr()).
   m.def(

@@ -14,7 +14,16 @@
 #include <mutex>
 #include <string>
 
+#include "rang_weights.h"
 #include "wgrid_plan.h"
+
+// The imaging-weight pipeline (wgrid_weights.cu).
+namespace wg {
+void weight_grid_shape(size_t width, size_t height, double super_weight, size_t* w, size_t* h);
+size_t padded_size(size_t trimmed, double padding);
+void stokes_i(const StokesIInputs& in, StokesIOutputs& out, cudaStream_t s);
+void imaging_weights(const ImagingWeightInputs& in, ImagingWeightOutputs& out, cudaStream_t s);
+}  // namespace wg
 
 using namespace wg;
 
@@ -425,6 +434,31 @@ int32_t rang_core_wgridder_kernel_row(size_t index, double* out) {
   double v[7] = {(double)r->w, r->ofactor, r->epsilon, r->beta, r->e0, (double)r->ndim, (double)r->single};
   std::memcpy(out, v, sizeof(v));
   return 0;
+}
+
+// ------------------------------------------------------------------ imaging weights (ffi_weights.rs)
+
+int32_t rang_core_weight_grid_shape(size_t width, size_t height, double super_weight, size_t* shape) {
+  if (!shape || !(super_weight > 0.0)) return 1;
+  return guarded([&] { wg::weight_grid_shape(width, height, super_weight, &shape[0], &shape[1]); });
+}
+
+size_t rang_core_padded_size(size_t trimmed, double padding) {
+  try {
+    return wg::padded_size(trimmed, padding);
+  } catch (...) {
+    return 0;
+  }
+}
+
+int32_t rang_core_stokes_i(const StokesIInputs* inputs, StokesIOutputs* outputs) {
+  if (!inputs || !outputs) return 1;
+  return guarded([&] { wg::stokes_i(*inputs, *outputs, call_stream()); });
+}
+
+int32_t rang_core_imaging_weights(const ImagingWeightInputs* inputs, ImagingWeightOutputs* outputs) {
+  if (!inputs || !outputs) return 1;
+  return guarded([&] { wg::imaging_weights(*inputs, *outputs, call_stream()); });
 }
 
 size_t rang_core_wgridder_last_error(uint8_t* buf, size_t len) {

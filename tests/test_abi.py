@@ -42,6 +42,28 @@ def test_library_exports_every_declared_symbol(built):
         assert hasattr(lib, name), name
 
 
+def test_library_exports_every_weights_symbol(built):
+    text = (REPO / "include" / "rang_weights.h").read_text()
+    names = sorted(set(re.findall(r"^\w+\s+(rang_core_\w+)\s*\(", text, re.M)))
+    assert names == ["rang_core_imaging_weights", "rang_core_padded_size", "rang_core_stokes_i",
+                     "rang_core_weight_grid_shape"]
+    lib = ctypes.CDLL(str(built.LIB))
+    for name in names:
+        assert hasattr(lib, name), name
+
+
+def test_weight_geometry_without_a_gpu(built):
+    # Host-side functions of the weights ABI against the oracle (weights.rs:38-42, :102-112).
+    from rang import core_weights
+
+    for trimmed in (512, 1024, 2, 4096, 1000):
+        assert core_weights.padded_size(trimmed) == oracle.padded_size(trimmed)
+    for args in [(616, 616, 1.0), (616, 616, 3.0), (610, 610, 4.0), (614, 614, 4.0), (1232, 900, 2.5)]:
+        assert core_weights.grid_shape(*args) == oracle.weight_grid_shape(*args)
+    with pytest.raises(ValueError):
+        core_weights.grid_shape(616, 616, 0.0)
+
+
 def test_kernel_table_through_the_extension(built):
     from rang import core_wgridder
 
