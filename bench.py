@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fista", action="store_true")
+    ap.add_argument("--no-weights", action="store_true")
     return ap.parse_args()
 
 
@@ -260,6 +261,61 @@ def run_fista(dev, max_iterations=200, sigma=0.05):
             "fista_s": t_iter, "ms_per_iteration": 1e3 * t_iter / (max_iterations + 1),
             "model_rel_error": err,
             "learned": None, "learned_note": "the learned U-Net preconditioner is not built"}
+
+
+# ------------------------------------------------------------------ imaging weights
+
+
+def run_imaging_weights(wl, uvw_np, freq, mask, args):
+    """WSClean Briggs weights (robust 0.5, rank filter 3 over 16 cells) of
+    every sample of the workload, the image's padded size and pixel scale,
+    with the flags as zero weights: through the C ABI binding with pinned,
+    caller-owned host arrays (copies included, as for the gridder's e2e),
+    against the oracle on the CPU sample's integrations."""
+    import torch
+
+    from rang import core, core_weights
+
+    nrow, nchan = uvw_np.shape[0], freq.size
+    wave = core_weights.wsclean_wavelengths(freq)
+    size = core_weights.padded_size(wl["npix"])
+    scale = wl["cell_arcsec"] * synth.ARCSEC
+    w_h = torch.empty((nrow, nchan), dtype=torch.float32, pin_memory=True)
+    w_h.copy_(mask.to(torch.float32))
+    w_np = w_h.numpy()
+    sel = np.ones(nrow, np.uint8)
+    kw = dict(mode="briggs", robust=0.5, width=size, height=size, pixel_scale=scale, rank_filter=(3.0, 16))
+    out_h = torch.empty((nrow, nchan), dtype=torch.float32, pin_memory=True)
+    out_np, sums = out_h.numpy(), np.zeros(4)
+    ext = core.extension()
+
+    def call():
+        st = ext.imaging_weights(nrow, nchan, uvw_np, wave, w_np, sel, 2, 0.5, size, size, scale, scale, 1.0, 3.0, 16,
+                                 out_np, None, sums)
+        assert st == 0, ext.wgridder_last_error()
+
+    for _ in range(2):
+        call()
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        call()
+        times.append(time.perf_counter() - t0)
+    t = min(times)
+    out = {"samples": nrow * nchan, "gpu_e2e_ms": 1e3 * t, "gpu_e2e_msamples_per_s": nrow * nchan / t / 1e6,
+           "h2d_bytes": int(w_np.nbytes + uvw_np.nbytes), "d2h_bytes": int(w_np.nbytes)}
+    if not args.no_cpu:
+        sys.path.insert(0, str(REPO / "oracle"))
+        import oracle
+
+        nt = max(1, int(round(wl["ntime"] * args.cpu_fraction)))
+        rows = nt * 2016
+        t0 = time.perf_counter()
+        oracle.imaging_weights(uvw_np[:rows], wave, w_np[:rows], sel[:rows], **kw)
+        tc = time.perf_counter() - t0
+        out["cpu_oracle"] = {"samples": rows * nchan, "ms": 1e3 * tc, "msamples_per_s": rows * nchan / tc / 1e6,
+                             "cores": 1, "kind": "port"}
+    return out
 
 
 # ------------------------------------------------------------------ GPU
@@ -507,6 +563,10 @@ def run_b200(args):
                "sample": f"first {nt} of {wl['ntime']} integrations ({svis.size} visibilities), one round trip, "
                          f"full {npix}^2 image and grid, {threads} threads"}
 
+    weights_leg = None
+    if rank == 0 and world == 1 and not args.no_weights:
+        weights_leg = run_imaging_weights(wl, uvw_np, freq, mask, args)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -518,7 +578,7 @@ def run_b200(args):
                        "l2": f"inputs larger than L2 ({nvis * 8 / 1e9:.2f} GB of visibilities)",
                        "plan": {k: plan_info[k] for k in ("kernel_index", "supp", "nu", "nv", "nplanes")}},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk, "accuracy": accuracy, "fista": fst,
+            "clocks": clk, "accuracy": accuracy, "fista": fst, "imaging_weights": weights_leg,
             "stages_ms": {k: round(v[1], 3) for k, v in prof.items() if v[0]},
         }
         print(json.dumps(line, default=_plain), flush=True)
