@@ -405,3 +405,99 @@ def imaging_weights(uvw, wavelength, weights, row_selected, mode="briggs", robus
     if st:
         raise ValueError("invalid imaging-weight arguments")
     return {"weights": out, "grid": grid, "sums": sums}
+
+
+# ------------------------------------------------------------------ Gram operator (core/src/gridder_gram.rs)
+
+
+def w_expansion(stencil, theta, ridge):
+    """WExpansion::new (gridder_gram.rs:88-163) in NumPy: the (8193, stencil)
+    coefficient table, the sampled sup error and the Lebesgue constant."""
+    s = int(stencil)
+    t = np.arange(s) - (s - 1) / 2.0
+    m = 64 * s
+    xi = np.cos(np.pi * (np.arange(m) + 0.5) / m)
+
+    def kern(d):
+        return np.cos(theta * np.multiply.outer(np.asarray(d, float), xi)).sum(-1) / m
+
+    normal = kern(t[:, None] - t[None, :])
+    normal[np.diag_indices(s)] *= 1.0 + ridge
+    bins = 8192
+    sv = -0.5 + np.arange(bins + 1) / bins
+    rhs = kern(sv[:, None] - t[None, :])
+    table = np.linalg.solve(normal, rhs.T).T
+    lebesgue = float(np.abs(table).sum(1).max())
+
+    def coeff(sval):
+        f = (sval + 0.5) * bins
+        b = min(int(f), bins - 1)
+        a = f - b
+        return table[b] + a * (table[b + 1] - table[b])
+
+    sup = 0.0
+    xs = np.arange(513) / 512.0
+    for sb in range(257):
+        sval = -0.5 + sb / 256.0 + (0.5 / 8192.0 if sb < 256 else 0.0)
+        c = coeff(sval)
+        re = np.cos(theta * xs * sval) - (c[None, :] * np.cos(theta * xs[:, None] * t[None, :])).sum(1)
+        im = np.sin(theta * xs * sval) - (c[None, :] * np.sin(theta * xs[:, None] * t[None, :])).sum(1)
+        sup = max(sup, float(np.hypot(re, im).max()))
+    return table, sup, lebesgue
+
+
+def gram_direct(uvw, freq, wgt, m, cell, flip_v=False, flip_w=False):
+    """The direct sum of the Gram matrix in the gridder's conventions
+    (the reference's test oracle, gridder_gram.rs:765-803): for an n x n
+    model m, sum_p W_p sum_l' m(l') cos 2 pi (u (l - l') + v (m - m') + w (x - x'))."""
+    n = m.shape[0]
+    half = n / 2
+    fv = -1.0 if flip_v else 1.0
+    fw = -1.0 if flip_w else 1.0
+    idx = np.arange(n)
+    L = (idx[:, None] - half) * cell * np.ones((1, n))
+    M = (idx[None, :] - half) * cell * np.ones((n, 1))
+    r2 = L * L + M * M
+    X = -r2 / (np.sqrt(np.maximum(1.0 - r2, 0.0)) + 1.0)
+    nz = np.nonzero(m)
+    lp, mp, xp, vals = L[nz], M[nz], X[nz], m[nz]
+    out = np.zeros((n, n))
+    foc = np.asarray(freq) / 299792458.0
+    for row in range(uvw.shape[0]):
+        for ch in range(len(freq)):
+            u, v, w = uvw[row, 0] * foc[ch], fv * uvw[row, 1] * foc[ch], fw * uvw[row, 2] * foc[ch]
+            wt = wgt[row, ch]
+            ph = 2.0 * np.pi * (u * (L[..., None] - lp) + v * (M[..., None] - mp) + w * (X[..., None] - xp))
+            out += wt * (np.cos(ph) * vals).sum(-1)
+    return out
+
+
+def gram_case(n, nrow, wmax, flip):
+    """The reference's test case (gridder_gram.rs:727-763): xorshift uvw,
+    two channels at c and 1.05 c, weights normalised to sum 1, cell 8e-3."""
+    state = 77
+    mask = (1 << 64) - 1
+
+    def nxt():
+        nonlocal state
+        state ^= (state << 13) & mask
+        state ^= state >> 7
+        state ^= (state << 17) & mask
+        return (state >> 11) / float(1 << 53) - 0.5
+
+    freq = np.array([299792458.0, 1.05 * 299792458.0])
+    cell = 8e-3
+    umax = 0.45 / cell
+    uvw = np.array([nxt() * 2.0 * (wmax if i % 3 == 2 else umax / 1.05) for i in range(3 * nrow)]).reshape(nrow, 3)
+    raw = np.array([0.2 + abs(nxt()) for _ in range(2 * nrow)])
+    wgt = (raw / raw.sum()).reshape(nrow, 2)
+    return uvw, freq, wgt, cell
+
+
+def gram_test_model(n):
+    m = np.zeros((n, n))
+    m.flat[0] = 1.0
+    m.flat[n * n - 1] = -0.5
+    m.flat[(n // 2) * n + n // 2] = 0.75
+    m.flat[5 * n + (n - 3)] = 0.25
+    return m

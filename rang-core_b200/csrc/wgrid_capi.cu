@@ -6,6 +6,7 @@
 // gridded or degridded there, and the outputs copied back. Part 2 exposes the
 // device-resident plan.
 #include <cstring>
+#include <functional>
 #include <map>
 #include <algorithm>
 #include <vector>
@@ -23,6 +24,8 @@ void weight_grid_shape(size_t width, size_t height, double super_weight, size_t*
 size_t padded_size(size_t trimmed, double padding);
 void stokes_i(const StokesIInputs& in, StokesIOutputs& out, cudaStream_t s);
 void imaging_weights(const ImagingWeightInputs& in, ImagingWeightOutputs& out, cudaStream_t s);
+int32_t gram_guarded(const std::function<void()>& f);
+cudaStream_t gram_stream(void* stream);
 }  // namespace wg
 
 using namespace wg;
@@ -325,6 +328,16 @@ void host_dirty2vis(const WgridderOptions* o, size_t nrow, size_t nchan, const d
 }  // namespace
 
 std::string* wg::last_error_slot() { return &g_last_error; }
+
+// The Gram operator's entry points (wgrid_gram.cu) share the status mapping,
+// the per-thread message and the per-thread stream.
+int32_t wg::gram_guarded(const std::function<void()>& f) { return guarded(f); }
+cudaStream_t wg::gram_stream(void* stream) {
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "no CUDA device");
+  configure_pool(dev);
+  return (cudaStream_t)stream;  // the caller's stream; null is the legacy default stream
+}
 
 struct RangWgridPlan {
   int single = 0;

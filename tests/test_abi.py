@@ -52,6 +52,15 @@ def test_library_exports_every_weights_symbol(built):
         assert hasattr(lib, name), name
 
 
+def test_library_exports_every_gram_symbol(built):
+    text = (REPO / "include" / "rang_gram.h").read_text()
+    names = sorted(set(re.findall(r"^\w+\s+(rang_b200_gram_\w+)\s*\(", text, re.M)))
+    assert len(names) == 7
+    lib = ctypes.CDLL(str(built.LIB))
+    for name in names:
+        assert hasattr(lib, name), name
+
+
 def test_weight_geometry_without_a_gpu(built):
     # Host-side functions of the weights ABI against the oracle (weights.rs:38-42, :102-112).
     from rang import core_weights
