@@ -41,10 +41,11 @@ def soft_threshold(z, tau, signed):
 
 
 def solve(gram, dirty, lam, step, max_iterations, q0=0.0, x0=None, momentum=True, restart=True, signed=False,
-          observer=None, stop=None):
+          observer=None, stop=None, gx0=None):
     """FISTA with gradient restart from `x0` (zero by default). `observer(k, x,
     gx, misfit)` sees every iterate; `stop(k, misfit)` returning True ends the
-    run early. Returns (x, G x, iterations, restarts)."""
+    run early; `gx0`, when given, is G x0 (it saves the first apply of G).
+    Returns (x, G x, iterations, restarts)."""
     x = torch.zeros_like(dirty) if x0 is None else x0.clone()
     x_prev = x.clone()
     y = x.clone()
@@ -53,7 +54,7 @@ def solve(gram, dirty, lam, step, max_iterations, q0=0.0, x0=None, momentum=True
     beta = 0.0
     restarts = 0
     for k in range(max_iterations + 1):
-        g_y = gram(y)
+        g_y = gx0 if (k == 0 and gx0 is not None) else gram(y)
         g_x = g_y if beta == 0.0 else (g_y + beta * g_x_prev) / (1.0 + beta)
         misfit = q0 - float(torch.dot(dirty.double().ravel(), x.double().ravel())) + 0.5 * float(
             torch.dot(x.double().ravel(), g_x.double().ravel()))

@@ -1,0 +1,587 @@
+"""Learned-preconditioned FISTA on the B200: a U-Net proposes model updates
+from the residual image and the PSF, trained and run by this library's own
+bfloat16 kernels (the C ABI of include/rang_nn.h), and every proposal is
+accepted only if the exact gridder's residual decreases.
+
+The reference has no learned solver on its imaging path. Its solver is
+`prox_solver::solve` (core/src/prox_solver.rs:302-445, `rang.fista` here);
+its nearest learned relatives are the learned-stage interpreter
+(core/src/learned_interp.rs:1-22) and the learned deconvolution trial
+(examples/dl4b_train.py:51-72). The network and the acceptance rule here are
+new:
+
+* `UNet`: 4 levels of 32/64/128/256 channels, two 3x3 convolutions with
+  ReLU per level, 2x2 average pooling down, nearest 2x upsampling up, skip
+  connections by concatenation ([upsampled | encoder] channels), a 1x1 head
+  to one float32 channel. Input: a 256 x 256 residual patch in units of the
+  PSF peak and the PSF patch (peak 1) as two of 32 input channels. Output: a
+  model update in sky units. Weights bfloat16 with float32 masters; Adam.
+* `make_training_set`: patches of (residual, sky - model) pairs from seeded
+  random skies (300 point sources and 40 Gaussians on 2048^2, the FISTA
+  measurement's distribution) predicted onto random antenna subsets by the
+  GPU gridder, with models from plain FISTA snapshots.
+* `solve`: FISTA whose cycles begin with a proposal: the network's update d,
+  projected onto the positive orthant, scaled by the exact minimiser of the
+  quadratic misfit along it (one apply of G = A^H A by the exact gridder),
+  and kept only when the misfit decreases; `cycle` plain FISTA iterations
+  follow from the accepted point.
+"""
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import core, fista, synth
+
+LEVELS = (32, 64, 128, 256)
+IN_CHANNELS = 32
+PATCH = 256
+
+
+def layers(levels=LEVELS):
+    """The 3x3 convolutions in order: (name, cin, cout)."""
+    c1, c2, c3, c4 = levels
+    return [("enc1a", IN_CHANNELS, c1), ("enc1b", c1, c1), ("enc2a", c1, c2), ("enc2b", c2, c2),
+            ("enc3a", c2, c3), ("enc3b", c3, c3), ("mid_a", c3, c4), ("mid_b", c4, c4),
+            ("dec3a", c4 + c3, c3), ("dec3b", c3, c3), ("dec2a", c3 + c2, c2), ("dec2b", c2, c2),
+            ("dec1a", c2 + c1, c1), ("dec1b", c1, c1)]
+
+
+def initial_parameters(levels=LEVELS, seed=0, live_inputs=2):
+    """He-normal convolution weights (fan-in 9 cin; the first layer counts
+    its `live_inputs` live channels), zero biases, a head of variance 1/32."""
+    rng = np.random.default_rng(seed)
+    p = {}
+    for i, (name, cin, cout) in enumerate(layers(levels)):
+        fan = 9 * (live_inputs if i == 0 else cin)
+        p[name + ".w"] = rng.standard_normal((cout, 9, cin)) * np.sqrt(2.0 / fan)
+        p[name + ".b"] = np.zeros(cout)
+    p["head.w"] = rng.standard_normal(levels[0]) * np.sqrt(1.0 / levels[0])
+    p["head.b"] = np.zeros(1)
+    return p
+
+
+_lib = None
+_SIGNATURES = {
+    "conv3": "PLPPPLPLLIIIIIIP",
+    "conv3_weight_grad": "PLPLPPLIIIIP",
+    "conv3_flip": "PPIIP",
+    "pool": "PLPLLIIIP",
+    "pool_backward": "PLPLPLLIIIP",
+    "upsample": "PLPLLIIIP",
+    "upsample_backward": "PLPLLIIIP",
+    "pack": "PPLPLFFPLIIP",
+    "head": "PLPPPLP",
+    "head_backward": "PLPPPLPPLP",
+    "mse": "PPPLPPLIIP",
+    "unpack": "PPPLFPLIIP",
+    "adam": "PPPPPLFFFFIP",
+    "to_bf16": "PPLP",
+}
+
+
+def _library():
+    global _lib
+    if _lib is None:
+        lib = ctypes.CDLL(core.library_path())
+        kinds = {"P": ctypes.c_void_p, "L": ctypes.c_int64, "I": ctypes.c_int32, "F": ctypes.c_float}
+        for name, sig in _SIGNATURES.items():
+            f = getattr(lib, "rang_b200_nn_" + name)
+            f.argtypes = [kinds[k] for k in sig]
+            f.restype = ctypes.c_int32
+        _lib = lib
+    return _lib
+
+
+def _call(name, *args):
+    status = getattr(_library(), "rang_b200_nn_" + name)(*args)
+    if status != 0:
+        kind = ValueError if status == 1 else RuntimeError
+        raise kind(f"rang_b200_nn_{name} failed with status {status}")
+
+
+def _p(t, c0=0):
+    """Device pointer of channel c0 of an (pixels, channels) tensor."""
+    return t.data_ptr() + c0 * t.element_size()
+
+
+def _stream(device):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+class Workspace:
+    """The activations (and, for training, the gradients) of `batch`
+    height x width inputs: (pixels, channels) bfloat16 tensors, the
+    concatenation buffers `catN` holding [upsampled | encoder] channels."""
+
+    def __init__(self, net, batch, height, width, training=False):
+        if height % 8 or width % 8:
+            raise ValueError("height and width must be multiples of 8")
+        self.batch, self.height, self.width, self.training = int(batch), int(height), int(width), training
+        c1, c2, c3, c4 = net.levels
+        dev = net.device
+        P = [self.batch * (self.height >> k) * (self.width >> k) for k in range(4)]
+
+        def bf(n, c):
+            return torch.empty((n, c), dtype=torch.bfloat16, device=dev)
+
+        self.x, self.c1a, self.cat1, self.p1 = bf(P[0], IN_CHANNELS), bf(P[0], c1), bf(P[0], c2 + c1), bf(P[1], c1)
+        self.c2a, self.cat2, self.p2 = bf(P[1], c2), bf(P[1], c3 + c2), bf(P[2], c2)
+        self.c3a, self.cat3, self.p3 = bf(P[2], c3), bf(P[2], c4 + c3), bf(P[3], c3)
+        self.ma, self.mb = bf(P[3], c4), bf(P[3], c4)
+        self.d3a, self.d3b, self.d2a, self.d2b = bf(P[2], c3), bf(P[2], c3), bf(P[1], c2), bf(P[1], c2)
+        self.d1a, self.d1b = bf(P[0], c1), bf(P[0], c1)
+        self.y = torch.empty(P[0], dtype=torch.float32, device=dev)
+        self.offsets = torch.zeros(self.batch, dtype=torch.int64, device=dev)
+        if training:
+            self.dy = torch.empty(P[0], dtype=torch.float32, device=dev)
+            self.loss = torch.zeros(1, dtype=torch.float32, device=dev)
+            self.g_d1b, self.g_d1a, self.g_cat1 = bf(P[0], c1), bf(P[0], c1), bf(P[0], c2 + c1)
+            self.g_d2b, self.g_d2a, self.g_cat2 = bf(P[1], c2), bf(P[1], c2), bf(P[1], c3 + c2)
+            self.g_d3b, self.g_d3a, self.g_cat3 = bf(P[2], c3), bf(P[2], c3), bf(P[2], c4 + c3)
+            self.g_mb, self.g_ma, self.g_p3 = bf(P[3], c4), bf(P[3], c4), bf(P[3], c3)
+            self.g_c3a, self.g_p2, self.g_c2a = bf(P[2], c3), bf(P[2], c2), bf(P[1], c2)
+            self.g_p1, self.g_c1a = bf(P[1], c1), bf(P[0], c1)
+
+    def launches(self):
+        """Kernel launches of one use: a training step (pack, forward, loss,
+        backward, Adam, weight flips) or a proposal (pack, forward, unpack)."""
+        forward = 14 + 3 + 3 + 1  # convolutions, pools, upsamplings, head
+        if not self.training:
+            return 1 + forward + 1
+        backward = 1 + 14 * 2 + 13 + 3 + 3  # head, weight+bias gradients, input gradients, upsample, pool
+        return 1 + forward + 1 + backward + 1 + 14
+
+
+class UNet:
+    """The proposal network on `device`: float32 master parameters, their
+    bfloat16 copy, gradients and Adam moments in flat buffers (every tensor
+    at a multiple of 8 elements), and the flipped weights of the
+    input-gradient convolutions."""
+
+    def __init__(self, device="cuda", seed=0, levels=LEVELS, params=None):
+        self.device = torch.device(device)
+        self.levels = tuple(int(c) for c in levels)
+        if any(c % 32 for c in self.levels):
+            raise ValueError("channel counts must be multiples of 32")
+        self.table = layers(self.levels)
+        self.dims = {name: (cin, cout) for name, cin, cout in self.table}
+        self.slots = {}
+        off = 0
+        shapes = [s for name, cin, cout in self.table for s in ((name + ".w", (cout, 9, cin)), (name + ".b", (cout,)))]
+        shapes += [("head.w", (self.levels[0],)), ("head.b", (1,))]
+        for key, shape in shapes:
+            self.slots[key] = (off, shape)
+            off += (int(np.prod(shape)) + 7) // 8 * 8
+        self.size = off
+        f32 = dict(dtype=torch.float32, device=self.device)
+        self.master = torch.zeros(off, **f32)
+        self.grad = torch.zeros(off, **f32)
+        self.m = torch.zeros(off, **f32)
+        self.v = torch.zeros(off, **f32)
+        self.wb = torch.zeros(off, dtype=torch.bfloat16, device=self.device)
+        self.flipped = {name: torch.empty(cin * 9 * cout, dtype=torch.bfloat16, device=self.device)
+                        for name, cin, cout in self.table}
+        self.step = 0
+        self.load(initial_parameters(self.levels, seed) if params is None else params)
+
+    def _ptr(self, key, buf):
+        return buf.data_ptr() + self.slots[key][0] * buf.element_size()
+
+    def parameters(self):
+        """The float32 master parameters as float64 NumPy arrays."""
+        host = self.master.double().cpu().numpy()
+        return {k: host[o:o + int(np.prod(s))].reshape(s).copy() for k, (o, s) in self.slots.items()}
+
+    def gradients(self):
+        """The accumulated parameter gradients as float64 NumPy arrays."""
+        host = self.grad.double().cpu().numpy()
+        return {k: host[o:o + int(np.prod(s))].reshape(s).copy() for k, (o, s) in self.slots.items()}
+
+    def zero_grad(self):
+        self.grad.zero_()
+
+    def load(self, params):
+        host = np.zeros(self.size, np.float32)
+        for k, (o, s) in self.slots.items():
+            a = np.asarray(params[k], np.float64)
+            if a.shape != s:
+                raise ValueError(f"{k}: shape {a.shape}, expected {s}")
+            host[o:o + a.size] = a.ravel()
+        self.master.copy_(torch.from_numpy(host))
+        self.refresh()
+
+    def refresh(self):
+        """The bfloat16 copy and the flipped weights from the masters."""
+        s = _stream(self.device)
+        _call("to_bf16", self.master.data_ptr(), self.wb.data_ptr(), self.size, s)
+        self._flip()
+
+    def _flip(self):
+        s = _stream(self.device)
+        for name, cin, cout in self.table:
+            _call("conv3_flip", self._ptr(name + ".w", self.wb), self.flipped[name].data_ptr(), cin, cout, s)
+
+    # ---------------------------------------------------------------- layers
+
+    def _conv(self, ws, name, src, s0, dst, d0, level):
+        cin, cout = self.dims[name]
+        _call("conv3", _p(src, s0), src.shape[1], self._ptr(name + ".w", self.wb), self._ptr(name + ".b", self.master),
+              _p(dst, d0), dst.shape[1], None, 0, ws.batch, ws.height >> level, ws.width >> level, cin, cout, 1, 0,
+              _stream(self.device))
+
+    def _wgrad(self, ws, name, src, s0, dz, z0, level):
+        cin, cout = self.dims[name]
+        _call("conv3_weight_grad", _p(src, s0), src.shape[1], _p(dz, z0), dz.shape[1], self._ptr(name + ".w", self.grad),
+              self._ptr(name + ".b", self.grad), ws.batch, ws.height >> level, ws.width >> level, cin, cout,
+              _stream(self.device))
+
+    def _dgrad(self, ws, name, dz, z0, dst, mask, level):
+        cin, cout = self.dims[name]
+        _call("conv3", _p(dz, z0), dz.shape[1], self.flipped[name].data_ptr(), None, dst.data_ptr(), dst.shape[1],
+              None if mask is None else mask.data_ptr(), 0 if mask is None else mask.shape[1], ws.batch,
+              ws.height >> level, ws.width >> level, cout, cin, 0, 0, _stream(self.device))
+
+    def _pool(self, ws, src, s0, dst, level, c):
+        _call("pool", _p(src, s0), src.shape[1], dst.data_ptr(), dst.shape[1], ws.batch, ws.height >> level,
+              ws.width >> level, c, _stream(self.device))
+
+    def _up(self, ws, src, dst, level, c):
+        _call("upsample", src.data_ptr(), src.shape[1], dst.data_ptr(), dst.shape[1], ws.batch, ws.height >> level,
+              ws.width >> level, c, _stream(self.device))
+
+    def forward(self, ws):
+        """ws.y = the network applied to ws.x."""
+        c1, c2, c3, c4 = self.levels
+        self._conv(ws, "enc1a", ws.x, 0, ws.c1a, 0, 0)
+        self._conv(ws, "enc1b", ws.c1a, 0, ws.cat1, c2, 0)
+        self._pool(ws, ws.cat1, c2, ws.p1, 0, c1)
+        self._conv(ws, "enc2a", ws.p1, 0, ws.c2a, 0, 1)
+        self._conv(ws, "enc2b", ws.c2a, 0, ws.cat2, c3, 1)
+        self._pool(ws, ws.cat2, c3, ws.p2, 1, c2)
+        self._conv(ws, "enc3a", ws.p2, 0, ws.c3a, 0, 2)
+        self._conv(ws, "enc3b", ws.c3a, 0, ws.cat3, c4, 2)
+        self._pool(ws, ws.cat3, c4, ws.p3, 2, c3)
+        self._conv(ws, "mid_a", ws.p3, 0, ws.ma, 0, 3)
+        self._conv(ws, "mid_b", ws.ma, 0, ws.mb, 0, 3)
+        self._up(ws, ws.mb, ws.cat3, 2, c4)
+        self._conv(ws, "dec3a", ws.cat3, 0, ws.d3a, 0, 2)
+        self._conv(ws, "dec3b", ws.d3a, 0, ws.d3b, 0, 2)
+        self._up(ws, ws.d3b, ws.cat2, 1, c3)
+        self._conv(ws, "dec2a", ws.cat2, 0, ws.d2a, 0, 1)
+        self._conv(ws, "dec2b", ws.d2a, 0, ws.d2b, 0, 1)
+        self._up(ws, ws.d2b, ws.cat1, 0, c2)
+        self._conv(ws, "dec1a", ws.cat1, 0, ws.d1a, 0, 0)
+        self._conv(ws, "dec1b", ws.d1a, 0, ws.d1b, 0, 0)
+        _call("head", ws.d1b.data_ptr(), ws.d1b.shape[1], self._ptr("head.w", self.master),
+              self._ptr("head.b", self.master), ws.y.data_ptr(), ws.y.numel(), _stream(self.device))
+        return ws.y
+
+    def backward(self, ws):
+        """Adds the gradients of sum(ws.dy * ws.y) to self.grad (after `forward`)."""
+        c1, c2, c3, c4 = self.levels
+        s = _stream(self.device)
+        B = ws.batch
+        _call("head_backward", ws.d1b.data_ptr(), ws.d1b.shape[1], self._ptr("head.w", self.master), ws.dy.data_ptr(),
+              ws.g_d1b.data_ptr(), ws.g_d1b.shape[1], self._ptr("head.w", self.grad), self._ptr("head.b", self.grad),
+              ws.y.numel(), s)
+        self._wgrad(ws, "dec1b", ws.d1a, 0, ws.g_d1b, 0, 0)
+        self._dgrad(ws, "dec1b", ws.g_d1b, 0, ws.g_d1a, ws.d1a, 0)
+        self._wgrad(ws, "dec1a", ws.cat1, 0, ws.g_d1a, 0, 0)
+        self._dgrad(ws, "dec1a", ws.g_d1a, 0, ws.g_cat1, ws.cat1, 0)
+        _call("upsample_backward", ws.g_cat1.data_ptr(), ws.g_cat1.shape[1], ws.g_d2b.data_ptr(), c2, B,
+              ws.height >> 1, ws.width >> 1, c2, s)
+        self._wgrad(ws, "dec2b", ws.d2a, 0, ws.g_d2b, 0, 1)
+        self._dgrad(ws, "dec2b", ws.g_d2b, 0, ws.g_d2a, ws.d2a, 1)
+        self._wgrad(ws, "dec2a", ws.cat2, 0, ws.g_d2a, 0, 1)
+        self._dgrad(ws, "dec2a", ws.g_d2a, 0, ws.g_cat2, ws.cat2, 1)
+        _call("upsample_backward", ws.g_cat2.data_ptr(), ws.g_cat2.shape[1], ws.g_d3b.data_ptr(), c3, B,
+              ws.height >> 2, ws.width >> 2, c3, s)
+        self._wgrad(ws, "dec3b", ws.d3a, 0, ws.g_d3b, 0, 2)
+        self._dgrad(ws, "dec3b", ws.g_d3b, 0, ws.g_d3a, ws.d3a, 2)
+        self._wgrad(ws, "dec3a", ws.cat3, 0, ws.g_d3a, 0, 2)
+        self._dgrad(ws, "dec3a", ws.g_d3a, 0, ws.g_cat3, ws.cat3, 2)
+        _call("upsample_backward", ws.g_cat3.data_ptr(), ws.g_cat3.shape[1], ws.g_mb.data_ptr(), c4, B,
+              ws.height >> 3, ws.width >> 3, c4, s)
+        self._wgrad(ws, "mid_b", ws.ma, 0, ws.g_mb, 0, 3)
+        self._dgrad(ws, "mid_b", ws.g_mb, 0, ws.g_ma, ws.ma, 3)
+        self._wgrad(ws, "mid_a", ws.p3, 0, ws.g_ma, 0, 3)
+        self._dgrad(ws, "mid_a", ws.g_ma, 0, ws.g_p3, None, 3)
+        for level, cat, gcat, prev, gprev, first, up_c, c, src, gsrc in (
+                (2, ws.cat3, ws.g_cat3, ws.c3a, ws.g_c3a, "enc3", c4, c3, ws.p2, ws.g_p2),
+                (1, ws.cat2, ws.g_cat2, ws.c2a, ws.g_c2a, "enc2", c3, c2, ws.p1, ws.g_p1),
+                (0, ws.cat1, ws.g_cat1, ws.c1a, ws.g_c1a, "enc1", c2, c1, ws.x, None)):
+            dpool = {2: ws.g_p3, 1: ws.g_p2, 0: ws.g_p1}[level]
+            _call("pool_backward", _p(gcat, up_c), gcat.shape[1], dpool.data_ptr(), dpool.shape[1], _p(cat, up_c),
+                  cat.shape[1], B, ws.height >> level, ws.width >> level, c, s)
+            self._wgrad(ws, first + "b", prev, 0, gcat, up_c, level)
+            self._dgrad(ws, first + "b", gcat, up_c, gprev, prev, level)
+            self._wgrad(ws, first + "a", src, 0, gprev, 0, level)
+            if gsrc is not None:
+                self._dgrad(ws, first + "a", gprev, 0, gsrc, None, level)
+
+    # ---------------------------------------------------------------- training
+
+    def pack(self, ws, resid, offsets, ld_resid, psf, ld_psf, scale_resid=1.0, scale_psf=1.0):
+        """ws.x from residual patches at `offsets` (device int64) of `resid`
+        and the PSF patch `psf` (float32 device tensors)."""
+        _call("pack", resid.data_ptr(), offsets.data_ptr(), ld_resid, psf.data_ptr(), ld_psf, float(scale_resid),
+              float(scale_psf), ws.x.data_ptr(), ws.batch, ws.height, ws.width, _stream(self.device))
+
+    def loss_and_grad(self, ws, target, offsets, ld_target):
+        """ws.loss += the mean squared error of ws.y, ws.dy its gradient."""
+        _call("mse", ws.y.data_ptr(), target.data_ptr(), offsets.data_ptr(), ld_target, ws.dy.data_ptr(),
+              ws.loss.data_ptr(), ws.batch, ws.height, ws.width, _stream(self.device))
+
+    def adam(self, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+        """One Adam step on all parameters; clears the gradients."""
+        self.step += 1
+        s = _stream(self.device)
+        _call("adam", self.master.data_ptr(), self.wb.data_ptr(), self.grad.data_ptr(), self.m.data_ptr(),
+              self.v.data_ptr(), self.size, float(lr), float(beta1), float(beta2), float(eps), self.step, s)
+        self._flip()
+
+    def train_step(self, ws, resid, target, psf, offsets, lr):
+        """One step on the patches at `offsets` of the (N, PATCH, PATCH)
+        residual and target tensors with the PSF patch `psf`."""
+        ws.loss.zero_()
+        self.pack(ws, resid, offsets, ws.width, psf, ws.width)
+        self.forward(ws)
+        self.loss_and_grad(ws, target, offsets, ws.width)
+        self.backward(ws)
+        self.adam(lr)
+
+
+# -------------------------------------------------------------------- data
+
+
+class TrainingSet:
+    """Patches on the GPU: residuals in units of the PSF peak and targets
+    (true sky minus model) in sky units, (N, PATCH, PATCH) float32; the PSF
+    patch (peak 1) of each coverage and the coverage of every patch."""
+
+    def __init__(self, resid, target, psf, coverage, info):
+        self.resid, self.target, self.psf, self.coverage, self.info = resid, target, psf, coverage, info
+
+    def __len__(self):
+        return int(self.resid.shape[0])
+
+
+def psf_patch(psf, patch=PATCH):
+    """The central patch of a PSF image, divided by its peak, and the peak."""
+    n0, n1 = psf.shape
+    peak = psf[n0 // 2, n1 // 2]
+    crop = psf[n0 // 2 - patch // 2:n0 // 2 + patch // 2, n1 // 2 - patch // 2:n1 // 2 + patch // 2]
+    return (crop / peak).contiguous().float(), float(peak)
+
+
+def _patches(img, patch=PATCH):
+    n0, n1 = img.shape
+    return img.reshape(n0 // patch, patch, n1 // patch, patch).permute(0, 2, 1, 3).reshape(-1, patch, patch)
+
+
+def make_training_set(device, n_patches=20000, n_coverages=8, nant=(32, 64), npix=2048, cell_arcsec=1.5, ntime=128,
+                      nchan=64, snapshots=(0, 4, 12, 30), sigma=0.05, seed=1000, epsilon=1e-5):
+    """`n_patches` training patches from seeded random skies (the FISTA
+    measurement's distribution: 300 point sources and 40 Gaussians on
+    npix^2) over `n_coverages` random subsets of 32-64 antennas of the
+    64-antenna array, each sky predicted by the GPU degridder with noise
+    `sigma` and imaged by the gridder; the models are plain FISTA iterates at
+    the `snapshots` iteration counts (0: the dirty image)."""
+    from . import wgrid_torch
+
+    dev = torch.device(device)
+    cell = cell_arcsec * synth.ARCSEC
+    per_sky = len(snapshots) * (npix // PATCH) ** 2
+    skies = max(1, math.ceil(n_patches / (per_sky * n_coverages)))
+    resid = torch.empty((n_patches, PATCH, PATCH), dtype=torch.float32, device=dev)
+    target = torch.empty_like(resid)
+    psfs = []
+    coverage = np.zeros(n_patches, np.int64)
+    filled = 0
+    info = {"coverages": [], "skies": 0}
+    for c in range(n_coverages):
+        rng = np.random.default_rng(seed + c)
+        na = int(rng.integers(nant[0], nant[1] + 1))
+        subset = rng.choice(64, na, replace=False)
+        uvw = torch.from_numpy(synth.uvw_tracks(nant=64, ntime=ntime, subset=subset)).to(dev)
+        freq = synth.channels(nchan)
+        plan = wgrid_torch.DevicePlan(uvw, freq, npix_x=npix, npix_y=npix, pixsize_x=cell, pixsize_y=cell,
+                                      epsilon=epsilon, single=True)
+        pp, peak = psf_patch(plan.grid(None))
+        psfs.append(pp)
+        lmax, _ = fista.power_iteration(plan.gram, plan.shape, dev, max_iterations=30)
+        info["coverages"].append({"antennas": na, "visibilities": int(uvw.shape[0]) * nchan, "psf_peak": peak,
+                                  "lmax": lmax})
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed + 7919 * (c + 1))
+        for k in range(skies):
+            if filled >= n_patches:
+                break
+            sky = torch.from_numpy(synth.extended_sky(npix, seed=seed + 100 * c + k + 1)).to(dev)
+            vis = plan.degrid(sky)
+            vis += sigma * math.sqrt(2.0) * torch.randn(vis.shape, dtype=vis.dtype, device=dev, generator=g)
+            dirty, q = plan.residual(vis, None)
+            del vis
+            snaps = {}
+
+            def keep(it, x, gx, misfit):
+                if it in snapshots:
+                    snaps[it] = (x.clone(), gx.clone())
+
+            fista.solve(plan.gram, dirty, 1e-4 * float(dirty.max()), 1.0 / lmax, max(snapshots), q0=0.5 * q,
+                        observer=keep)
+            for it in snapshots:
+                x, gx = snaps[it]
+                r = _patches((dirty - gx) / peak)
+                e = _patches(sky - x)
+                n = min(r.shape[0], n_patches - filled)
+                resid[filled:filled + n] = r[:n]
+                target[filled:filled + n] = e[:n]
+                coverage[filled:filled + n] = c
+                filled += n
+            info["skies"] += 1
+        plan.close()
+    if filled < n_patches:
+        resid, target, coverage = resid[:filled], target[:filled], coverage[:filled]
+    return TrainingSet(resid, target, torch.stack(psfs), coverage, info)
+
+
+def train(net, data, steps, batch=16, lr=1e-3, lr_final=1e-5, warmup=50, seed=0, log_every=25):
+    """`steps` Adam steps on random batches of one coverage at a time
+    (cosine learning-rate decay after a linear warm-up). Returns the loss
+    every `log_every` steps."""
+    rng = np.random.default_rng(seed)
+    ws = Workspace(net, batch, PATCH, PATCH, training=True)
+    groups = [np.flatnonzero(data.coverage == c) for c in range(data.psf.shape[0])]
+    sizes = np.array([len(gr) for gr in groups], np.float64)
+    cov = rng.choice(len(groups), size=steps, p=sizes / sizes.sum())
+    idx = np.stack([rng.choice(groups[c], batch, replace=len(groups[c]) < batch) for c in cov])
+    offsets = torch.from_numpy(idx * PATCH * PATCH).to(net.device)
+    losses = []
+    for t in range(steps):
+        if t < warmup:
+            rate = lr * (t + 1) / warmup
+        else:
+            rate = lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * (t - warmup) / max(1, steps - warmup)))
+        net.train_step(ws, data.resid, data.target, data.psf[cov[t]], offsets[t], rate)
+        if t % log_every == 0 or t == steps - 1:
+            losses.append((t, float(ws.loss)))
+    return losses
+
+
+# -------------------------------------------------------------------- inference
+
+
+def tiles(npix, patch=PATCH, margin=16):
+    """Patch corners along one axis and the window of each patch (patch
+    coordinates) such that the windows tile [0, npix) once: neighbouring
+    patches overlap by at least 2 margin and split the overlap in half."""
+    if npix < patch:
+        raise ValueError("the image is smaller than a patch")
+    step = patch - 2 * margin
+    pos = list(range(0, npix - patch, step)) + [npix - patch]
+    pos = sorted(set(pos))
+    cuts = [0] + [(a + b + patch) // 2 for a, b in zip(pos[:-1], pos[1:])] + [npix]
+    return [(p, cuts[i] - p, cuts[i + 1] - p) for i, p in enumerate(pos)]
+
+
+class Proposer:
+    """The network over an npix x npix residual image in overlapping
+    patches (one batch): update = U(residual * scale, PSF patch)."""
+
+    def __init__(self, net, npix, margin=16):
+        self.net, self.npix = net, int(npix)
+        ax = tiles(self.npix, PATCH, margin)
+        corners = [(a, b) for a in ax for b in ax]
+        self.batch = len(corners)
+        self.ws = Workspace(net, self.batch, PATCH, PATCH, training=False)
+        offs = np.array([a[0] * self.npix + b[0] for a, b in corners], np.int64)
+        win = np.array([[a[1], a[2], b[1], b[2]] for a, b in corners], np.int32).ravel()
+        self.ws.offsets.copy_(torch.from_numpy(offs))
+        self.windows = torch.from_numpy(win).to(net.device)
+
+    def __call__(self, resid, psf, scale, out=None):
+        resid = resid.float().contiguous()
+        if tuple(resid.shape) != (self.npix, self.npix):
+            raise ValueError("residual image size")
+        if out is None:
+            out = torch.empty_like(resid)
+        self.net.pack(self.ws, resid, self.ws.offsets, self.npix, psf, PATCH, scale, 1.0)
+        self.net.forward(self.ws)
+        _call("unpack", self.ws.y.data_ptr(), self.ws.offsets.data_ptr(), self.windows.data_ptr(), self.npix, 1.0,
+              out.data_ptr(), self.batch, PATCH, PATCH, _stream(self.net.device))
+        return out
+
+
+def solve(gram, dirty, lam, step, proposer, psf, peak, max_iterations, q0=0.0, cycle=10, stop=None, observer=None):
+    """Learned-preconditioned FISTA: repeat { proposal; `cycle` FISTA
+    iterations } until `max_iterations` applies of `gram` (the exact
+    gridder's A^H A) are spent. A proposal d = max(x + U(r / peak, psf), 0)
+    - x is scaled by alpha = <d, r> / <d, G d> (the exact minimiser of the
+    misfit along d; capped where positivity would break) and kept only when
+    the misfit Q(0) - <dirty, x> + <x, G x> / 2 decreases. `stop(k, misfit)`
+    and `observer(k, x, gx, misfit)` see every iterate, k counting applies
+    of G. Returns (x, G x, applies, proposal statistics)."""
+    x = torch.zeros_like(dirty)
+    gx = torch.zeros_like(dirty)
+    k = 0
+    stats = {"proposals": 0, "accepted": 0, "alphas": [], "misfit_drops": []}
+
+    def misfit_of(x, gx):
+        return q0 - float(torch.dot(dirty.double().ravel(), x.double().ravel())) + 0.5 * float(
+            torch.dot(x.double().ravel(), gx.double().ravel()))
+
+    misfit = misfit_of(x, gx)
+    while k < max_iterations:
+        r = dirty - gx
+        d = torch.clamp(x + proposer(r, psf, 1.0 / peak), min=0.0) - x
+        gd = gram(d)
+        k += 1
+        stats["proposals"] += 1
+        num = float(torch.dot(d.double().ravel(), r.double().ravel()))
+        den = float(torch.dot(d.double().ravel(), gd.double().ravel()))
+        if num > 0.0 and den > 0.0:
+            alpha = num / den
+            neg = d < 0
+            if bool(neg.any()):
+                alpha = min(alpha, float((x[neg] / -d[neg]).min()))
+            x_try = x + alpha * d
+            gx_try = gx + alpha * gd
+            m_try = misfit_of(x_try, gx_try)
+            if m_try < misfit:
+                stats["accepted"] += 1
+                stats["alphas"].append(alpha)
+                stats["misfit_drops"].append(misfit - m_try)
+                x, gx, misfit = x_try, gx_try, m_try
+        if observer is not None:
+            observer(k, x, gx, misfit)
+        if stop is not None and stop(k, misfit):
+            return x, gx, k, stats
+        n = min(cycle, max_iterations - k)
+        if n <= 0:
+            break
+        base = k
+        ended = {}
+
+        def inner_stop(i, m):
+            if i == 0:
+                return False
+            if stop is not None and stop(base + i, m):
+                ended["k"] = base + i
+                return True
+            return False
+
+        def inner_observer(i, xi, gi, m):
+            if observer is not None and i > 0:
+                observer(base + i, xi, gi, m)
+
+        x, gx, used, _ = fista.solve(gram, dirty, lam, step, n, q0=q0, x0=x, gx0=gx, stop=inner_stop,
+                                     observer=inner_observer)
+        k = base + used
+        misfit = misfit_of(x, gx)
+        if "k" in ended:
+            return x, gx, k, stats
+    return x, gx, k, stats

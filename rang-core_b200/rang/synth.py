@@ -26,9 +26,12 @@ def antennas(nant=64, seed=7, core_frac=0.75, core_sigma=500.0, disk_radius=4000
     return np.concatenate([core, outer])
 
 
-def uvw_tracks(nant=64, ntime=128, tint=8.0, dec_deg=-30.0, lat_deg=-30.7, seed=7):
-    """(ntime * nbaselines, 3) uvw in metres, time-major."""
+def uvw_tracks(nant=64, ntime=128, tint=8.0, dec_deg=-30.0, lat_deg=-30.7, seed=7, subset=None):
+    """(ntime * nbaselines, 3) uvw in metres, time-major; `subset` (antenna
+    indices) keeps those antennas of the array only."""
     en = antennas(nant, seed)
+    if subset is not None:
+        en = en[np.sort(np.asarray(subset))]
     lat = np.deg2rad(lat_deg)
     east, north, up = en[:, 0], en[:, 1], np.zeros(len(en))
     x = -np.sin(lat) * north + np.cos(lat) * up
