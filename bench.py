@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fista", action="store_true")
     ap.add_argument("--no-weights", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned-patches", type=int, default=20000)
+    ap.add_argument("--learned-steps", type=int, default=2500)
     return ap.parse_args()
 
 
@@ -195,7 +198,7 @@ def run_reference(args):
 # ------------------------------------------------------------------ FISTA
 
 
-def run_fista(dev, max_iterations=200, sigma=0.05):
+def run_fista(dev, max_iterations=200, sigma=0.05, learn=None):
     """Plain FISTA (L1 with positivity, step 1 / ||A^H A|| from 30 power
     iterations) on 2048^2 at 1.5 arcsec: 300 point sources and 40 elliptical
     Gaussians predicted by the degridder onto the 64-antenna coverage of 128
@@ -203,7 +206,8 @@ def run_fista(dev, max_iterations=200, sigma=0.05):
     component. Reports the GPU time until the visibility residual RMS (per
     real component) first reaches 1.2 sigma (null if it does not within the
     iterations), plan and power iteration included, and the RMS every 20
-    iterations."""
+    iterations; with `learn`, learned-preconditioned FISTA on the same
+    measurement (`run_learned`)."""
     import torch
 
     from rang import fista, wgrid_torch
@@ -232,11 +236,16 @@ def run_fista(dev, max_iterations=200, sigma=0.05):
     trajectory, reached = [], {}
     t_first = {}
 
+    marks = []
+
     def stop(k, misfit):
         rms = float(np.sqrt(max(2.0 * misfit, 0.0) / (2 * nvis)))
         if k % 20 == 0 or k == max_iterations:
             trajectory.append([k, rms])
         reached["rms"], reached["k"] = rms, k
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        marks.append((rms, e))
         if rms <= target and "event" not in t_first:
             t_first["event"] = torch.cuda.Event(enable_timing=True)
             t_first["event"].record()
@@ -252,6 +261,12 @@ def run_fista(dev, max_iterations=200, sigma=0.05):
     t_iter = ev[2].elapsed_time(ev[3]) / 1e3
     t_target = ev[0].elapsed_time(t_first["event"]) / 1e3 if "event" in t_first else None
     err = float((x - sky).norm() / sky.norm())
+    final_rms = reached.get("rms")
+    t_final = t_setup + t_power + ev[2].elapsed_time(next(e for r, e in marks if r <= final_rms)) / 1e3
+    learned_report = None
+    if learn is not None:
+        learned_report = run_learned(dev, plan, dirty, q, lmax, lam, sky, nvis, target, final_rms, t_final,
+                                     t_setup + t_power, max_iterations, learn)
     # The visibility-free Gram operator on the same measurement: setup, one
     # apply, and its distance from the exact A^H A on the dirty image.
     from rang import gram
@@ -295,8 +310,87 @@ def run_fista(dev, max_iterations=200, sigma=0.05):
             "iterations": max_iterations, "final_rms": reached.get("rms"), "rms_trajectory": trajectory,
             "restarts": int(restarts), "plan_and_dirty_s": t_setup, "power_iteration_s": t_power,
             "fista_s": t_iter, "ms_per_iteration": 1e3 * t_iter / (max_iterations + 1),
-            "model_rel_error": err, "gram_operator": gram_report,
-            "learned": None, "learned_note": "the learned U-Net preconditioner is not built"}
+            "model_rel_error": err, "time_to_final_rms_s": t_final, "gram_operator": gram_report,
+            "learned": learned_report}
+
+
+def run_learned(dev, plan, dirty, q, lmax, lam, sky, nvis, target, plain_rms, plain_time, t_shared, max_iterations,
+                learn):
+    """Learned-preconditioned FISTA (rang.learned) on the FISTA measurement.
+    The U-Net is first trained by the library's own kernels on patches the
+    gridder generates from other seeds (random skies of the same
+    distribution over 8 random subsets of 32-64 antennas at 64 channels);
+    that one-off cost is reported apart. The solve shares the plain run's
+    plan, dirty image and power iteration (their time is added to its own)
+    and adds the PSF and the network; it reports the GPU time until the
+    residual RMS first reaches plain FISTA's final RMS and 1.2 sigma."""
+    import torch
+
+    from rang import learned
+
+    npix = dirty.shape[0]
+    t0 = time.perf_counter()
+    data = learned.make_training_set(dev, n_patches=learn["patches"])
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    net = learned.UNet(dev, seed=0)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e[0].record()
+    losses = learned.train(net, data, steps=learn["steps"], batch=learn["batch"], lr=1e-3, warmup=100,
+                           log_every=max(1, learn["steps"] // 10))
+    e[1].record()
+    torch.cuda.synchronize()
+    t_train = e[0].elapsed_time(e[1]) / 1e3
+    training = {"patches": len(data), "coverages": data.info["coverages"], "skies": data.info["skies"],
+                "data_s": t_data, "steps": learn["steps"], "batch": learn["batch"], "train_s": t_train,
+                "train_tflops": learn["steps"] * learn["batch"] * learned.flops(training=True) / t_train / 1e12,
+                "loss": losses}
+    del data
+    torch.cuda.empty_cache()
+    first = {}
+    trajectory = []
+
+    def stop(k, misfit):
+        rms = float(np.sqrt(max(2.0 * misfit, 0.0) / (2 * nvis)))
+        if k % 20 == 0:
+            trajectory.append([k, rms])
+        for name, level in (("plain", plain_rms), ("target", target)):
+            if rms <= level and name not in first:
+                first[name] = (k, torch.cuda.Event(enable_timing=True))
+                first[name][1].record()
+        return False
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    psf, peak = learned.psf_patch(plan.grid(None))
+    prop = learned.Proposer(net, npix)
+    x, gx, applies, st = learned.solve(plan.gram, dirty, lam, 1.0 / lmax, prop, psf, peak, max_iterations + 1,
+                                       q0=0.5 * q, stop=stop)
+    ev[1].record()
+    torch.cuda.synchronize()
+    rms = float(np.sqrt(max(2.0 * (0.5 * q - float(torch.dot(dirty.double().ravel(), x.double().ravel())) + 0.5 * float(
+        torch.dot(x.double().ravel(), gx.double().ravel()))), 0.0) / (2 * nvis)))
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    prop(dirty, psf, 1.0 / peak)
+    p1.record()
+    torch.cuda.synchronize()
+    t_plain = t_shared + ev[0].elapsed_time(first["plain"][1]) / 1e3 if "plain" in first else None
+    t_target = t_shared + ev[0].elapsed_time(first["target"][1]) / 1e3 if "target" in first else None
+    return {"network": "U-Net 32/64/128/256 channels, bf16 weights, f32 accumulation, 256^2 residual + PSF patches",
+            "training": training, "proposal_ms": p0.elapsed_time(p1), "proposal_patches": prop.batch,
+            "proposal_tflops": prop.batch * learned.flops() / p0.elapsed_time(p1) / 1e9,
+            "solve": "FISTA with a proposal every 40 iterations from the first, split into a 4-pixel Gaussian "
+                     "low-pass part and the rest, each scaled by the exact minimiser of the misfit (exact gridder)",
+            "time_to_plain_final_rms_s": t_plain, "iterations_to_plain_final_rms": first.get("plain", (None,))[0],
+            "plain_time_to_final_rms_s": plain_time,
+            "speedup_vs_plain": plain_time / t_plain if t_plain else None,
+            "time_to_target_s": t_target, "iterations_to_target": first.get("target", (None,))[0],
+            "applies": applies, "final_rms": rms, "rms_trajectory": trajectory,
+            "model_rel_error": float((x - sky).norm() / sky.norm()), "proposals": st["proposals"],
+            "accepted": st["accepted"], "first_step": st["steps"][0] if st["steps"] else None,
+            "solve_s": ev[0].elapsed_time(ev[1]) / 1e3}
 
 
 # ------------------------------------------------------------------ imaging weights
@@ -588,7 +682,8 @@ def run_b200(args):
 
     fst = None
     if rank == 0 and not args.no_fista:
-        fst = run_fista(dev)
+        learn = None if args.no_learned else {"patches": args.learned_patches, "steps": args.learned_steps, "batch": 16}
+        fst = run_fista(dev, learn=learn)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -63,6 +63,19 @@ def initial_parameters(levels=LEVELS, seed=0, live_inputs=2):
     return p
 
 
+def flops(height=PATCH, width=PATCH, levels=LEVELS, training=False):
+    """Floating-point operations of the convolutions for one height x width
+    input: the forward pass, or a training step (forward, input gradients
+    except the first layer's, weight gradients)."""
+    f = 0
+    for name, cin, cout in layers(levels):
+        level = {"enc1": 0, "enc2": 1, "enc3": 2, "mid_": 3, "dec3": 2, "dec2": 1, "dec1": 0}[name[:4]]
+        f += 2 * 9 * cin * cout * (height >> level) * (width >> level)
+    if not training:
+        return f
+    return 3 * f - 2 * 9 * IN_CHANNELS * levels[0] * height * width
+
+
 _lib = None
 _SIGNATURES = {
     "conv3": "PLPPPLPLLIIIIIIP",
@@ -383,16 +396,18 @@ def _patches(img, patch=PATCH):
 
 
 def make_training_set(device, n_patches=20000, n_coverages=8, nant=(32, 64), npix=2048, cell_arcsec=1.5, ntime=128,
-                      nchan=64, snapshots=(0, 4, 12, 30), sigma=0.05, seed=1000, epsilon=1e-5):
-    """`n_patches` training patches from seeded random skies (the FISTA
-    measurement's distribution: 300 point sources and 40 Gaussians on
-    npix^2) over `n_coverages` random subsets of 32-64 antennas of the
-    64-antenna array, each sky predicted by the GPU degridder with noise
-    `sigma` and imaged by the gridder; the models are plain FISTA iterates at
-    the `snapshots` iteration counts (0: the dirty image)."""
+                      nchan=64, snapshots=(0, 4, 12, 30), sigma=0.05, seed=1000, epsilon=1e-5, sky=None):
+    """`n_patches` training patches from seeded random skies (by default the
+    FISTA measurement's distribution: 300 point sources and 40 Gaussians on
+    npix^2; `sky` overrides `synth.extended_sky`'s keywords) over
+    `n_coverages` random subsets of 32-64 antennas of the 64-antenna array,
+    each sky predicted by the GPU degridder with noise `sigma` and imaged by
+    the gridder; the models are plain FISTA iterates at the `snapshots`
+    iteration counts (0: the dirty image)."""
     from . import wgrid_torch
 
     dev = torch.device(device)
+    sky_kw = dict(sky or {})
     cell = cell_arcsec * synth.ARCSEC
     per_sky = len(snapshots) * (npix // PATCH) ** 2
     skies = max(1, math.ceil(n_patches / (per_sky * n_coverages)))
@@ -420,8 +435,8 @@ def make_training_set(device, n_patches=20000, n_coverages=8, nant=(32, 64), npi
         for k in range(skies):
             if filled >= n_patches:
                 break
-            sky = torch.from_numpy(synth.extended_sky(npix, seed=seed + 100 * c + k + 1)).to(dev)
-            vis = plan.degrid(sky)
+            truth = torch.from_numpy(synth.extended_sky(npix, seed=seed + 100 * c + k + 1, **sky_kw)).to(dev)
+            vis = plan.degrid(truth)
             vis += sigma * math.sqrt(2.0) * torch.randn(vis.shape, dtype=vis.dtype, device=dev, generator=g)
             dirty, q = plan.residual(vis, None)
             del vis
@@ -436,7 +451,7 @@ def make_training_set(device, n_patches=20000, n_coverages=8, nant=(32, 64), npi
             for it in snapshots:
                 x, gx = snaps[it]
                 r = _patches((dirty - gx) / peak)
-                e = _patches(sky - x)
+                e = _patches(truth - x)
                 n = min(r.shape[0], n_patches - filled)
                 resid[filled:filled + n] = r[:n]
                 target[filled:filled + n] = e[:n]
@@ -516,72 +531,96 @@ class Proposer:
         return out
 
 
-def solve(gram, dirty, lam, step, proposer, psf, peak, max_iterations, q0=0.0, cycle=10, stop=None, observer=None):
-    """Learned-preconditioned FISTA: repeat { proposal; `cycle` FISTA
-    iterations } until `max_iterations` applies of `gram` (the exact
-    gridder's A^H A) are spent. A proposal d = max(x + U(r / peak, psf), 0)
-    - x is scaled by alpha = <d, r> / <d, G d> (the exact minimiser of the
-    misfit along d; capped where positivity would break) and kept only when
-    the misfit Q(0) - <dirty, x> + <x, G x> / 2 decreases. `stop(k, misfit)`
-    and `observer(k, x, gx, misfit)` see every iterate, k counting applies
-    of G. Returns (x, G x, applies, proposal statistics)."""
-    x = torch.zeros_like(dirty)
-    gx = torch.zeros_like(dirty)
-    k = 0
-    stats = {"proposals": 0, "accepted": 0, "alphas": [], "misfit_drops": []}
+def _blur(img, sigma):
+    """A periodic Gaussian blur of standard deviation `sigma` pixels (FFT)."""
+    n0, n1 = img.shape
+    f0 = torch.fft.fftfreq(n0, device=img.device, dtype=torch.float64)
+    f1 = torch.fft.rfftfreq(n1, device=img.device, dtype=torch.float64)
+    k = torch.exp(-2.0 * math.pi**2 * sigma**2 * (f0[:, None] ** 2 + f1[None, :] ** 2)).to(torch.float32)
+    return torch.fft.irfft2(torch.fft.rfft2(img) * k, s=(n0, n1))
+
+
+def solve(gram, dirty, lam, step, proposer, psf, peak, max_iterations, q0=0.0, cycle=40, bands=2, sigma=4.0,
+          first=0, stop=None, observer=None):
+    """Learned-preconditioned FISTA on the misfit Q(x) = Q(0) - <dirty, x> +
+    <x, G x> / 2 with the L1 prior and positivity (the FISTA of `rang.fista`,
+    with gradient restart), where at iteration `first` and every `cycle`
+    iterations after it the network proposes an update from the residual:
+    d = max(x + U(r / peak, psf), 0) - x. With `bands` 1 the step is alpha d,
+    alpha = <d, r> / <d, G d> the exact minimiser of Q along d (one apply of
+    the exact gridder's G); with `bands` 2, d is split into its Gaussian
+    low-pass part (`sigma` pixels) and the rest, each scaled by the exact
+    minimiser of Q over the pair (two applies). The step is kept only when
+    Q decreases, and then shifts the iterate, the previous iterate and the
+    extrapolated point alike, so that FISTA's momentum carries on.
+    `stop(k, misfit)` and `observer(k, x, gx, misfit)` see every iterate, k
+    counting applies of G. Returns (x, G x, applies, proposal statistics)."""
+    dd = dirty.double().ravel()
 
     def misfit_of(x, gx):
-        return q0 - float(torch.dot(dirty.double().ravel(), x.double().ravel())) + 0.5 * float(
-            torch.dot(x.double().ravel(), gx.double().ravel()))
+        xd = x.double().ravel()
+        return q0 - float(torch.dot(dd, xd)) + 0.5 * float(torch.dot(xd, gx.double().ravel()))
 
-    misfit = misfit_of(x, gx)
-    while k < max_iterations:
-        r = dirty - gx
-        d = torch.clamp(x + proposer(r, psf, 1.0 / peak), min=0.0) - x
-        gd = gram(d)
-        k += 1
-        stats["proposals"] += 1
-        num = float(torch.dot(d.double().ravel(), r.double().ravel()))
-        den = float(torch.dot(d.double().ravel(), gd.double().ravel()))
-        if num > 0.0 and den > 0.0:
-            alpha = num / den
-            neg = d < 0
-            if bool(neg.any()):
-                alpha = min(alpha, float((x[neg] / -d[neg]).min()))
-            x_try = x + alpha * d
-            gx_try = gx + alpha * gd
-            m_try = misfit_of(x_try, gx_try)
-            if m_try < misfit:
-                stats["accepted"] += 1
-                stats["alphas"].append(alpha)
-                stats["misfit_drops"].append(misfit - m_try)
-                x, gx, misfit = x_try, gx_try, m_try
+    def dot(a, b):
+        return float(torch.dot(a.double().ravel(), b.double().ravel()))
+
+    x = torch.zeros_like(dirty)
+    x_prev = x.clone()
+    y = x.clone()
+    g_x_prev = torch.zeros_like(dirty)
+    t, beta = 1.0, 0.0
+    applies = 0
+    stats = {"proposals": 0, "accepted": 0, "steps": [], "misfit_drops": []}
+    k = 0
+    while True:
+        g_y = gram(y)
+        applies += 1
+        g_x = g_y if beta == 0.0 else (g_y + beta * g_x_prev) / (1.0 + beta)
+        misfit = misfit_of(x, g_x)
+        if k >= first and (k - first) % cycle == 0 and applies + bands <= max_iterations:
+            r = dirty - g_x
+            d = torch.clamp(x + proposer(r, psf, 1.0 / peak), min=0.0) - x
+            parts = [d] if bands == 1 else [_blur(d, sigma), None]
+            if bands != 1:
+                parts[1] = d - parts[0]
+            gparts = [gram(p) for p in parts]
+            applies += len(parts)
+            stats["proposals"] += 1
+            b = np.array([dot(p, r) for p in parts])
+            m = np.array([[dot(p, q) for q in gparts] for p in parts])
+            try:
+                coef = np.linalg.solve(m, b)
+            except np.linalg.LinAlgError:
+                coef = np.zeros(len(parts))
+            drop = float(coef @ b - 0.5 * coef @ m @ coef)
+            if np.all(np.isfinite(coef)) and drop > 0.0:
+                shift = sum(c * p for c, p in zip(coef, parts))
+                gshift = sum(c * g for c, g in zip(coef, gparts))
+                x_try, g_try = x + shift, g_x + gshift
+                m_try = misfit_of(x_try, g_try)
+                if m_try < misfit:
+                    stats["accepted"] += 1
+                    stats["steps"].append([round(float(c), 4) for c in coef])
+                    stats["misfit_drops"].append(misfit - m_try)
+                    x, g_x, misfit = x_try, g_try, m_try
+                    x_prev, g_x_prev = x_prev + shift, g_x_prev + gshift
+                    y, g_y = y + shift, g_y + gshift
         if observer is not None:
-            observer(k, x, gx, misfit)
-        if stop is not None and stop(k, misfit):
-            return x, gx, k, stats
-        n = min(cycle, max_iterations - k)
-        if n <= 0:
-            break
-        base = k
-        ended = {}
-
-        def inner_stop(i, m):
-            if i == 0:
-                return False
-            if stop is not None and stop(base + i, m):
-                ended["k"] = base + i
-                return True
-            return False
-
-        def inner_observer(i, xi, gi, m):
-            if observer is not None and i > 0:
-                observer(base + i, xi, gi, m)
-
-        x, gx, used, _ = fista.solve(gram, dirty, lam, step, n, q0=q0, x0=x, gx0=gx, stop=inner_stop,
-                                     observer=inner_observer)
-        k = base + used
-        misfit = misfit_of(x, gx)
-        if "k" in ended:
-            return x, gx, k, stats
-    return x, gx, k, stats
+            observer(applies, x, g_x, misfit)
+        if applies >= max_iterations or (stop is not None and stop(applies, misfit)):
+            return x, g_x, applies, stats
+        z = y + step * (dirty - g_y)
+        x_next = fista.soft_threshold(z, step * lam, False)
+        next_beta = 0.0
+        inner = float(torch.sum((y - x_next) * (x_next - x)))
+        if inner > 0.0:
+            t = 1.0
+        else:
+            t_next = 0.5 * (1.0 + math.sqrt(1.0 + 4.0 * t * t))
+            next_beta = (t - 1.0) / t_next
+            t = t_next
+        g_x_prev = g_x
+        x_prev, x = x, x_next
+        y = x + next_beta * (x - x_prev)
+        beta = next_beta
+        k += 1
