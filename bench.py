@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--no-fista", action="store_true")
     ap.add_argument("--no-weights", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-msv4", action="store_true")
     ap.add_argument("--learned-patches", type=int, default=20000)
     ap.add_argument("--learned-steps", type=int, default=2500)
     return ap.parse_args()
@@ -393,6 +394,69 @@ def run_learned(dev, plan, dirty, q, lmax, lam, sky, nvis, target, plain_rms, pl
             "solve_s": ev[0].elapsed_time(ev[1]) / 1e3}
 
 
+# ------------------------------------------------------------------ MSv4 ingest
+
+
+def run_msv4(threads=None):
+    """The MSv4 reader feeding the gridder (rang.msv4): a processing set of
+    the 16.5 M-visibility workload's shape (64 antennas, 128 integrations,
+    64 channels, 4 linear correlations; noise visibilities, 5 % flags,
+    random weights) written to local disk as xradio stores it (Blosc/LZ4
+    byte-shuffled data in chunks of 8 integrations and 1 MiB blocks, zstd
+    coordinates), then read back: the chunks decoded on all host threads,
+    the rows in the reference's layout, Stokes I on the GPU and vis2dirty
+    (1024^2 at 1.5 arcsec, epsilon 1e-5) through the C ABI, each timed."""
+    from rang import core_wgridder, msv4
+
+    wl = synth.WORKLOADS["ms2dirty 16.5M vis 1024^2"]
+    ntime, nchan, nant = wl["ntime"], wl["nchan"], 64
+    a1, a2 = np.triu_indices(nant, 1)
+    nbl = len(a1)
+    rng = np.random.default_rng(5)
+    shape = (ntime, nbl, nchan, 4)
+    vis = np.empty(shape, np.complex64)
+    vis.real = rng.standard_normal(shape, np.float32)
+    vis.imag = rng.standard_normal(shape, np.float32)
+    part = {"time": 1.6e9 + 8.0 * np.arange(ntime), "frequency": synth.channels(nchan),
+            "polarization": ["XX", "XY", "YX", "YY"], "antenna_name": [f"m{i:03d}" for i in range(nant)],
+            "antenna1": a1, "antenna2": a2, "VISIBILITY": vis, "FLAG": rng.random(shape, np.float32) < 0.05,
+            "WEIGHT": rng.uniform(0.5, 1.5, shape).astype(np.float32),
+            "UVW": synth.uvw_tracks(nant=nant, ntime=ntime).reshape(ntime, nbl, 3)}
+    raw = sum(part[k].nbytes for k in ("VISIBILITY", "FLAG", "WEIGHT", "UVW"))
+    with tempfile.TemporaryDirectory() as tmp:
+        t0 = time.perf_counter()
+        root = msv4.write_processing_set(Path(tmp) / "ps.zarr", {"obs_0": part}, time_chunk=8, blocksize=1 << 20)
+        t_write = time.perf_counter() - t0
+        stored = sum(f.stat().st_size for f in root.rglob("*") if f.is_file())
+        del part, vis
+        t0 = time.perf_counter()
+        p = msv4.open_processing_set(root).partition("obs_0")
+        for var in ("VISIBILITY", "FLAG", "WEIGHT", "UVW"):
+            p._read(var)
+        t_decode = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rows = p.rows()
+        t_rows = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        g = msv4.gridder_inputs(p, rows)
+        t_stokes = time.perf_counter() - t0
+        cell = wl["cell_arcsec"] * synth.ARCSEC
+        t0 = time.perf_counter()
+        dirty = core_wgridder.vis2dirty(uvw=g["uvw"], freq=g["freq"], vis=g["vis"], wgt=g["wgt"], mask=g["mask"],
+                                        npix_x=wl["npix"], npix_y=wl["npix"], pixsize_x=cell, pixsize_y=cell,
+                                        epsilon=1e-5)
+        t_grid = time.perf_counter() - t0
+    nvis = g["vis"].size
+    total = t_decode + t_rows + t_stokes + t_grid
+    return {"store": f"{ntime} integrations x {nbl} baselines x {nchan} channels x 4 correlations, "
+                     "Blosc/LZ4 byte shuffle, chunks of 8 integrations, 1 MiB blocks",
+            "raw_bytes": int(raw), "stored_bytes": int(stored), "write_s": t_write,
+            "decode_s": t_decode, "decode_gb_per_s": raw / t_decode / 1e9, "threads": os.cpu_count(),
+            "rows_s": t_rows, "stokes_i_s": t_stokes, "vis2dirty_s": t_grid, "stokes_i_visibilities": int(nvis),
+            "store_to_dirty_s": total, "store_to_dirty_mvis_per_s": nvis / total / 1e6,
+            "dirty_finite": bool(np.isfinite(dirty).all())}
+
+
 # ------------------------------------------------------------------ imaging weights
 
 
@@ -698,6 +762,10 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_weights:
         weights_leg = run_imaging_weights(wl, uvw_np, freq, mask, args)
 
+    msv4_leg = None
+    if rank == 0 and world == 1 and not args.no_msv4:
+        msv4_leg = run_msv4()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -709,7 +777,7 @@ def run_b200(args):
                        "l2": f"inputs larger than L2 ({nvis * 8 / 1e9:.2f} GB of visibilities)",
                        "plan": {k: plan_info[k] for k in ("kernel_index", "supp", "nu", "nv", "nplanes")}},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk, "accuracy": accuracy, "fista": fst, "imaging_weights": weights_leg,
+            "clocks": clk, "accuracy": accuracy, "fista": fst, "imaging_weights": weights_leg, "msv4_ingest": msv4_leg,
             "stages_ms": {k: round(v[1], 3) for k, v in prof.items() if v[0]},
         }
         print(json.dumps(line, default=_plain), flush=True)

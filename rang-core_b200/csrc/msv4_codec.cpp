@@ -177,10 +177,25 @@ int parse(const uint8_t* src, size_t n, Header& h) {
   return 0;
 }
 
+// Element i gathers its bytes from the ts byte planes; the writes run
+// contiguously (the planes are read as ts sequential streams).
+template <size_t TS>
+void unshuffle_fixed(const uint8_t* src, uint8_t* dst, size_t ne) {
+  for (size_t i = 0; i < ne; i++)
+    for (size_t j = 0; j < TS; j++) dst[i * TS + j] = src[j * ne + i];
+}
+
 void unshuffle(const uint8_t* src, uint8_t* dst, size_t bytes, size_t ts) {
   const size_t ne = bytes / ts;
-  for (size_t j = 0; j < ts; j++)
-    for (size_t i = 0; i < ne; i++) dst[i * ts + j] = src[j * ne + i];
+  switch (ts) {
+    case 2: unshuffle_fixed<2>(src, dst, ne); break;
+    case 4: unshuffle_fixed<4>(src, dst, ne); break;
+    case 8: unshuffle_fixed<8>(src, dst, ne); break;
+    case 16: unshuffle_fixed<16>(src, dst, ne); break;
+    default:
+      for (size_t i = 0; i < ne; i++)
+        for (size_t j = 0; j < ts; j++) dst[i * ts + j] = src[j * ne + i];
+  }
   std::memcpy(dst + ne * ts, src + ne * ts, bytes - ne * ts);
 }
 
@@ -196,6 +211,36 @@ size_t nsplits_for(const Header& h, size_t bsize, bool last) {
   return split ? h.typesize : 1;
 }
 
+// Block j of a parsed, non-memcpyed chunk into dst + j * blocksize.
+int decode_block(const Header& h, const uint8_t* src, size_t j, uint8_t* dst, std::vector<uint8_t>& scratch) {
+  const size_t nb = h.nblocks();
+  const size_t leftover = h.nbytes % h.blocksize;
+  const bool last = j + 1 == nb && leftover > 0;
+  const size_t bsize = last ? leftover : h.blocksize;
+  const bool shuffled = (h.flags & kShuffle) && h.typesize > 1;
+  size_t at = le32(src + kHeader + 4 * j);
+  if (at < kHeader + 4 * nb || at > h.cbytes) return 1;
+  const size_t ns = nsplits_for(h, bsize, last);
+  const size_t neblock = bsize / ns;
+  if (ns * neblock != bsize) return 1;
+  if (shuffled && scratch.size() < bsize) scratch.resize(h.blocksize);
+  uint8_t* out = shuffled ? scratch.data() : dst + j * h.blocksize;
+  for (size_t k = 0; k < ns; k++) {
+    if (h.cbytes - at < 4) return 1;
+    const size_t cb = le32(src + at);
+    at += 4;
+    if (cb > h.cbytes - at) return 1;
+    if (cb == neblock) {
+      std::memcpy(out + k * neblock, src + at, neblock);
+    } else if (lz4_decode(src + at, cb, out + k * neblock, neblock) != neblock) {
+      return 1;
+    }
+    at += cb;
+  }
+  if (shuffled) unshuffle(scratch.data(), dst + j * h.blocksize, bsize, h.typesize);
+  return 0;
+}
+
 int decode(const uint8_t* src, size_t n, uint8_t* dst, size_t cap) {
   Header h;
   int st = parse(src, n, h);
@@ -205,33 +250,9 @@ int decode(const uint8_t* src, size_t n, uint8_t* dst, size_t cap) {
     std::memcpy(dst, src + kHeader, h.nbytes);
     return 0;
   }
-  const size_t nb = h.nblocks();
-  const size_t leftover = h.nbytes % h.blocksize;
-  const bool shuffled = (h.flags & kShuffle) && h.typesize > 1;
-  std::vector<uint8_t> scratch(shuffled ? h.blocksize : 0);
-  for (size_t j = 0; j < nb; j++) {
-    const bool last = j + 1 == nb && leftover > 0;
-    const size_t bsize = last ? leftover : h.blocksize;
-    size_t at = le32(src + kHeader + 4 * j);
-    if (at < kHeader + 4 * nb || at > h.cbytes) return 1;
-    const size_t ns = nsplits_for(h, bsize, last);
-    const size_t neblock = bsize / ns;
-    uint8_t* out = shuffled ? scratch.data() : dst + j * h.blocksize;
-    for (size_t k = 0; k < ns; k++) {
-      if (h.cbytes - at < 4) return 1;
-      const size_t cb = le32(src + at);
-      at += 4;
-      if (cb > h.cbytes - at) return 1;
-      if (cb == neblock) {
-        std::memcpy(out + k * neblock, src + at, neblock);
-      } else if (lz4_decode(src + at, cb, out + k * neblock, neblock) != neblock) {
-        return 1;
-      }
-      at += cb;
-    }
-    if (ns * neblock != bsize) return 1;
-    if (shuffled) unshuffle(scratch.data(), dst + j * h.blocksize, bsize, h.typesize);
-  }
+  std::vector<uint8_t> scratch;
+  for (size_t j = 0; j < h.nblocks(); j++)
+    if ((st = decode_block(h, src, j, dst, scratch))) return st;
   return 0;
 }
 
@@ -333,17 +354,43 @@ int32_t rang_b200_blosc_encode(const uint8_t* src, size_t nbytes, int32_t typesi
 int32_t rang_b200_blosc_decode_many(size_t n, const uint8_t* const* srcs, const size_t* srclens, uint8_t* const* dsts,
                                     const size_t* dstcaps, int32_t threads, int32_t* status) {
   if (n && (!srcs || !srclens || !dsts || !dstcaps || !status)) return 1;
+  // Tasks are (chunk, block) pairs, so that a few large chunks still use
+  // every thread; a memcpyed chunk is one task.
+  std::vector<Header> heads(n);
+  std::vector<std::pair<size_t, size_t>> tasks;
+  for (size_t i = 0; i < n; i++) {
+    status[i] = parse(srcs[i], srclens[i], heads[i]);
+    if (!status[i] && heads[i].nbytes > dstcaps[i]) status[i] = 1;
+    if (status[i]) continue;
+    const size_t nb = (heads[i].flags & kMemcpyed) ? 1 : heads[i].nblocks();
+    for (size_t j = 0; j < nb; j++) tasks.emplace_back(i, j);
+  }
+  std::vector<std::atomic<int32_t>> fail(n);
+  for (auto& f : fail) f = 0;
   std::atomic<size_t> next{0};
   auto work = [&] {
-    for (size_t i; (i = next.fetch_add(1)) < n;) status[i] = decode(srcs[i], srclens[i], dsts[i], dstcaps[i]);
+    std::vector<uint8_t> scratch;
+    for (size_t t; (t = next.fetch_add(1)) < tasks.size();) {
+      const size_t i = tasks[t].first, j = tasks[t].second;
+      const Header& h = heads[i];
+      int st = 0;
+      if (h.flags & kMemcpyed)
+        std::memcpy(dsts[i], srcs[i] + kHeader, h.nbytes);
+      else
+        st = decode_block(h, srcs[i], j, dsts[i], scratch);
+      if (st) fail[i] = st;
+    }
   };
-  const size_t nt = std::max<size_t>(1, std::min<size_t>(threads > 0 ? (size_t)threads : 1, n));
+  const size_t nt = std::max<size_t>(1, std::min<size_t>(threads > 0 ? (size_t)threads : 1, tasks.size()));
   std::vector<std::thread> pool;
   for (size_t t = 1; t < nt; t++) pool.emplace_back(work);
   work();
   for (auto& t : pool) t.join();
   int32_t worst = 0;
-  for (size_t i = 0; i < n; i++) worst = std::max(worst, status[i]);
+  for (size_t i = 0; i < n; i++) {
+    if (!status[i]) status[i] = fail[i];
+    worst = std::max(worst, status[i]);
+  }
   return worst;
 }
 

@@ -103,10 +103,12 @@ def blosc_decode(chunk, nbytes=None):
     return out
 
 
-def blosc_decode_many(chunks, sizes, threads=None):
-    """Chunks decoded on `threads` host threads (default: all cores)."""
+def blosc_decode_many(chunks, sizes, threads=None, outs=None):
+    """Chunks decoded on `threads` host threads (default: all cores), into
+    new arrays or into `outs` (contiguous uint8 arrays of `sizes` bytes)."""
     n = len(chunks)
-    outs = [np.empty(s, np.uint8) for s in sizes]
+    if outs is None:
+        outs = [np.empty(s, np.uint8) for s in sizes]
     if n == 0:
         return outs
     srcs = [np.frombuffer(c, np.uint8) for c in chunks]
@@ -236,29 +238,42 @@ class Array:
         return self.path + "/c" + "".join(self._sep + str(i) for i in idx) if idx else self.path + "/c"
 
     def read(self, threads=None):
-        """The whole array as a numpy array."""
-        out = np.full(self.shape, self.fill_value, dtype=self.dtype)
+        """The whole array as a numpy array. Chunks that span every axis but
+        the first are decoded straight into the result."""
         if 0 in self.shape:
-            return out
-        grid = [range(-(-s // c)) for s, c in zip(self.shape, self.chunks)]
-        idxs = list(np.ndindex(*[len(g) for g in grid])) if self.shape else [()]
+            return np.full(self.shape, self.fill_value, dtype=self.dtype)
+        grid = [-(-s // c) for s, c in zip(self.shape, self.chunks)]
+        idxs = list(np.ndindex(*grid)) if self.shape else [()]
         raw, where = [], []
         for idx in idxs:
             data = self.store.get(self._key(idx))
             if data is not None:
                 raw.append(data)
                 where.append(idx)
+        if len(raw) < len(idxs):
+            out = np.full(self.shape, self.fill_value, dtype=self.dtype)
+        else:
+            out = np.empty(self.shape, dtype=self.dtype)
         nbytes = int(np.prod(self.chunks, dtype=np.int64)) * self.dtype.itemsize
+        slab = len(self.shape) > 0 and tuple(self.chunks[1:]) == tuple(self.shape[1:])
+        dsts, inplace = [], []
+        for idx in where:
+            lo = idx[0] * self.chunks[0] if self.shape else 0
+            direct = self.compressor == "blosc" and slab and lo + self.chunks[0] <= self.shape[0]
+            dsts.append(out[lo:lo + self.chunks[0]].reshape(-1).view(np.uint8) if direct else np.empty(nbytes, np.uint8))
+            inplace.append(direct)
         if self.compressor == "blosc":
-            decoded = blosc_decode_many(raw, [nbytes] * len(raw), threads)
+            decoded = blosc_decode_many(raw, [nbytes] * len(raw), threads, dsts)
         elif self.compressor == "zstd":
             z = _zstd()
             decoded = [np.frombuffer(z.decompress(r, decompressed_size=nbytes), np.uint8) for r in raw]
         else:
             decoded = [np.frombuffer(r, np.uint8) for r in raw]
-        for idx, buf in zip(where, decoded):
+        for idx, buf, direct in zip(where, decoded, inplace):
             if buf.size != nbytes:
                 raise ValueError(f"{self.path}: chunk {idx} holds {buf.size} bytes, expected {nbytes}")
+            if direct:
+                continue
             block = buf.view(self.dtype).reshape(self.chunks)
             sl = tuple(slice(i * c, min((i + 1) * c, s)) for i, c, s in zip(idx, self.chunks, self.shape))
             out[sl] = block[tuple(slice(0, s.stop - s.start) for s in sl)]
