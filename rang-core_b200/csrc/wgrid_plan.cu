@@ -95,6 +95,15 @@ struct RowCh {
   }
 };
 
+// The scan's reduction target before the scan: no visibilities, min |w| =
+// 1e300, max |w| = 0 (a kernel, so that no host buffer is copied).
+__global__ void k_scan_init(ScanOut* so) {
+  so->count = 0;
+  so->finite = 0;
+  so->lo_bits = (unsigned long long)__double_as_longlong(1e300);
+  so->hi_bits = 0;
+}
+
 // scan (wgridder.rs:1051-1077): the count is exact and min/max are order
 // independent, so the result is the reference's bit for bit.
 template <class T>
@@ -1417,10 +1426,7 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   check_cuda(cudaMemsetAsync(err_.get(), 0, sizeof(int), s), "memset");
   // Scan.
   DevBuf so(sizeof(ScanOut), s);
-  ScanOut init{0, 0, 0, 0};
-  const double big = 1e300;
-  std::memcpy(&init.lo_bits, &big, sizeof(big));
-  check_cuda(cudaMemcpyAsync(so.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s), "copy");
+  k_scan_init<<<1, 1, 0, s>>>(so.as<ScanOut>());
   double fw = o.flip_w ? 1.0 : -1.0;
   if (n_) {
     {
@@ -1505,24 +1511,29 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
   }
   check_cuda(cudaGetLastError(), "tasks");
   // Where each row chunk starts in the sorted order and in the task list.
-  std::vector<uint32_t> so(K + 1), to(K + 1);
-  for (size_t c = 0; c <= K; c++) {
-    check_cuda(cudaMemcpyAsync(&so[c], starts_.as<uint32_t>() + c * nbins_, 4, cudaMemcpyDeviceToHost, s), "copy");
-    check_cuda(cudaMemcpyAsync(&to[c], ntask.as<uint32_t>() + c * ntiles_, 4, cudaMemcpyDeviceToHost, s), "copy");
+  // One chunk needs no read-back (and no wait for the device): it spans
+  // the whole sorted order, and its launches take the task bound, the
+  // kernels stopping at the device-side task count.
+  if (K == 1) {
+    chunk_sorted_.assign({0u, (uint32_t)nvis_});
+    chunk_tasks_.assign({0u, (uint32_t)max_tasks_});
+  } else {
+    std::vector<uint32_t> so(K + 1), to(K + 1);
+    for (size_t c = 0; c <= K; c++) {
+      check_cuda(cudaMemcpyAsync(&so[c], starts_.as<uint32_t>() + c * nbins_, 4, cudaMemcpyDeviceToHost, s), "copy");
+      check_cuda(cudaMemcpyAsync(&to[c], ntask.as<uint32_t>() + c * ntiles_, 4, cudaMemcpyDeviceToHost, s), "copy");
+    }
+    check_cuda(cudaStreamSynchronize(s), "layout");
+    chunk_sorted_.assign(so.begin(), so.end());
+    chunk_tasks_.assign(to.begin(), to.end());
   }
-  check_cuda(cudaStreamSynchronize(s), "layout");
-  chunk_sorted_.assign(so.begin(), so.end());
-  chunk_tasks_.assign(to.begin(), to.end());
   corrections(s);
 }
 
 template <class T>
 bool Plan<T>::same_scan(const Inputs& act, bool with_vis, cudaStream_t s) const {
   DevBuf so(sizeof(ScanOut), s);
-  ScanOut init{0, 0, 0, 0};
-  const double big = 1e300;
-  std::memcpy(&init.lo_bits, &big, sizeof(big));
-  check_cuda(cudaMemcpyAsync(so.get(), &init, sizeof(init), cudaMemcpyHostToDevice, s), "copy");
+  k_scan_init<<<1, 1, 0, s>>>(so.as<ScanOut>());
   if (n_) {
     {
       StageTimer timer_(ST_SCAN, s);
@@ -1539,18 +1550,39 @@ bool Plan<T>::same_scan(const Inputs& act, bool with_vis, cudaStream_t s) const 
   return r.finite == 0 || (r.lo_bits == scan_[2] && r.hi_bits == scan_[3]);
 }
 
+// The kernel's correction function at the image's pixel frequencies, cfu =
+// corfunc(i / nu) for i <= nx / 2 then cfv = corfunc(j / nv) for j <= ny / 2,
+// on the current device: computed on the host once per (kernel, grid,
+// image) and kept for the life of the process, so that a plan copies it on
+// its stream without waiting for the device.
+const double* correction_table(const EsKernel* k, size_t nu, size_t nv, size_t nx, size_t ny) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const EsKernel*, size_t, size_t, size_t, size_t>, double*> cache;
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "device");
+  std::lock_guard<std::mutex> lock(mu);
+  double*& slot = cache[std::make_tuple(dev, k, nu, nv, nx, ny)];
+  if (!slot) {
+    const size_t nu2 = nx / 2 + 1, nv2 = ny / 2 + 1;
+    std::vector<double> tab(nu2 + nv2);
+    for (size_t i = 0; i < nu2; i++) tab[i] = k->corfunc((double)i * (1.0 / (double)nu));
+    for (size_t j = 0; j < nv2; j++) tab[nu2 + j] = k->corfunc((double)j * (1.0 / (double)nv));
+    double* d = nullptr;
+    check_cuda(cudaMalloc(&d, tab.size() * sizeof(double)), "device memory");
+    check_cuda(cudaMemcpy(d, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice), "copy");
+    slot = d;
+  }
+  return slot;
+}
+
 template <class T>
 void Plan<T>::corrections(cudaStream_t s) {
   // cfu, cfv tables on the host (corfunc_table, wgridder.rs:353-355).
   size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
-  std::vector<double> tab(nu2 + nv2);
-  for (size_t i = 0; i < nu2; i++) tab[i] = kernel_->corfunc((double)i * (1.0 / (double)g_.nu));
-  for (size_t j = 0; j < nv2; j++) tab[nu2 + j] = kernel_->corfunc((double)j * (1.0 / (double)g_.nv));
+  const double* tab = correction_table(kernel_, g_.nu, g_.nv, g_.nx, g_.ny);
   size_t npix = (size_t)g_.nx * g_.ny;
   corr_.alloc((nu2 + nv2 + (g_.do_wgridding ? npix : 0)) * sizeof(double), s);
-  check_cuda(cudaMemcpyAsync(corr_.get(), tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, s), "copy");
-  // The stream must not outlive `tab`.
-  check_cuda(cudaStreamSynchronize(s), "corrections");
+  check_cuda(cudaMemcpyAsync(corr_.get(), tab, (nu2 + nv2) * sizeof(double), cudaMemcpyDeviceToDevice, s), "copy");
   if (g_.do_wgridding) {
     CorrNodes cn{};
     cn.n = (int)kernel_->corr_x.size();
@@ -1813,10 +1845,7 @@ void bin_noalloc(const WgridderOptions& o, size_t nrow, size_t nchan, const doub
                           std::to_string(NOALLOC_SCRATCH_BYTES) + " bytes)");
   ScanOut* so = reinterpret_cast<ScanOut*>(base);
   double* dfoc = reinterpret_cast<double*>(base + foc_off);
-  ScanOut init{0, 0, 0, 0};
-  const double big = 1e300;
-  std::memcpy(&init.lo_bits, &big, sizeof(big));
-  check_cuda(cudaMemcpyAsync(so, &init, sizeof(init), cudaMemcpyHostToDevice, s), "copy");
+  k_scan_init<<<1, 1, 0, s>>>(so);
   check_cuda(cudaMemcpyAsync(dfoc, foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, s), "copy");
   const double fw = o.flip_w ? 1.0 : -1.0;
   if (n) {

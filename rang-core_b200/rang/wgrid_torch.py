@@ -78,13 +78,18 @@ class DevicePlan:
             int(vis is not None), int(self.single), _stream(self.device))
         _check(status)
         self._handle = handle
+        self._stream = torch.cuda.current_stream(self.device)
         from .core_wgridder import info_dict
 
         self.info = info_dict(info)
 
     def close(self):
+        """Releases the plan. Its device memory is freed in order on the
+        stream it was made on, so no wait is needed while the current stream
+        is that one; otherwise the device is synchronised first."""
         if getattr(self, "_handle", 0):
-            torch.cuda.current_stream(self.device).synchronize()
+            if torch.cuda.current_stream(self.device) != getattr(self, "_stream", None):
+                torch.cuda.synchronize(self.device)
             core.extension().wgridder_plan_destroy(self._handle)
             self._handle = 0
 
