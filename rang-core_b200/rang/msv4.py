@@ -449,20 +449,25 @@ class Partition:
         ntime, nbl, nchan, ncorr = vis.shape
         uvw = uvw.reshape(ntime * nbl, 3)
         vis = vis.reshape(ntime * nbl, nchan, ncorr)
-        pad = np.isnan(uvw).all(axis=1) & np.isnan(vis).reshape(ntime * nbl, -1).all(axis=1)
-        keep = ~pad
+        # A pad has all-NaN UVW; only those cells' visibilities are checked.
+        pad = np.isnan(uvw).all(axis=1)
+        if pad.any():
+            cand = np.flatnonzero(pad)
+            pad[cand] = np.isnan(vis[cand].reshape(len(cand), -1)).all(axis=1)
+        npad = int(pad.sum())
+        keep = slice(None) if npad == 0 else ~pad  # no pads: views, no copies
         return {
             "ANTENNA1": np.tile(self.antenna1, ntime)[keep],
             "ANTENNA2": np.tile(self.antenna2, ntime)[keep],
             "TIME": np.repeat(self.time[sl], nbl)[keep],
-            "FLAG_ROW": np.zeros(int(keep.sum()), bool),
+            "FLAG_ROW": np.zeros(ntime * nbl - npad, bool),
             "DATA": vis[keep],
             "FLAG": flag.reshape(ntime * nbl, nchan, ncorr)[keep],
             "WEIGHT_SPECTRUM": weight.reshape(ntime * nbl, nchan, ncorr)[keep],
             "UVW": uvw[keep],
             "FIELD_NAME": np.repeat(self.field_name[sl], nbl)[keep],
             "SCAN_NAME": np.repeat(self.scan_name[sl], nbl)[keep],
-            "PADS": int(pad.sum()),
+            "PADS": npad,
         }
 
     def chunks(self, time_rows=None):
