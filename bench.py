@@ -171,10 +171,35 @@ def cpu_sample(wl, fraction, seed=0):
     return oracle, uvw, freq, vis, mask, nt
 
 
+def replica_env():
+    """(world size, rank, local rank) of this process under torchrun; one
+    process per GPU, each an independent replica of the workload."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(value, dist, device):
+    """The largest of every rank's `value` (a time): the job is as slow as its
+    slowest replica. `dist` None means one process."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank, steps, seconds):
+    """Whole-job throughput in millions of units per second: every replica
+    processes `units_per_rank` per step, timed as the slowest rank."""
+    return world * units_per_rank * steps / seconds / 1e6
+
+
 def run_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
+    _, rank, _ = replica_env()
     if rank != 0:
-        return
+        return  # the CPU reference runs once, on rank 0; the other ranks exit without work
     wl = synth.WORKLOADS[args.workload]
     oracle, uvw, freq, vis, mask, nt = cpu_sample(wl, args.cpu_fraction)
     threads = oracle.set_threads(os.cpu_count() or 1)
@@ -520,9 +545,7 @@ def run_b200(args):
 
     from rang import core, wgrid_torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = replica_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     dist = None
@@ -598,12 +621,8 @@ def run_b200(args):
     last[0].status()
     last[1].status()
     last = None
-    ms = start.elapsed_time(end)
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * nvis * args.steps / (ms / 1e3) / 1e6
+    ms = max_over_ranks(start.elapsed_time(end), dist, dev)
+    value = job_rate(world, nvis, args.steps, ms / 1e3)
 
     # Dominant kernel and its roofline (algorithmic bytes per launch).
     hbm, peak_kind = peaks()
@@ -662,14 +681,10 @@ def run_b200(args):
         t0 = time.perf_counter()
         for _ in range(args.steps):
             e2e_step()
-        te = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([te], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(time.perf_counter() - t0, dist, dev)
         h2d = 2 * (uvw_np.nbytes + freq.nbytes + mask_np.nbytes) + vis_np.nbytes + dirty_np.nbytes
         d2h = dirty_np.nbytes + out_np.nbytes
-        e2e = {"value": world * nvis * args.steps / te / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": job_rate(world, nvis, args.steps, te), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te / args.steps}
         del vis_h, mask_h, out_h, dirty_h
 
