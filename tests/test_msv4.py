@@ -182,7 +182,7 @@ def test_decoded_values_are_the_msv2_bytes():
     from rang import msv4
 
     z = zipfile.ZipFile(FIXTURE)
-    ms = {n.split("/")[-1]: z.read(n) for n in z.namelist() if n.startswith("m05.ms/")}
+    ms = {n.split("/")[-1]: z.read(n) for n in z.namelist() if n.startswith("m05.ms/table.")}  # main table
     ps = msv4.open_processing_set(FIXTURE)
     for name, cube in zip(ps.names(), ("TSM1", "TSM2")):
         r = ps.partition(name).rows()
