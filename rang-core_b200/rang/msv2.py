@@ -15,9 +15,10 @@ reference's writer and casacore use for them.
   order, the columns in descending pixel size. A column is read here by
   mapping a hypercube's tiles into NumPy and reordering them with one
   reshape and transpose.
-* Refused with a `ValueError` naming the cause: IncrementalStMan, string
-  columns, and the row count of `table.lock` (tables are read with the row
-  count of `table.dat`).
+* IncrementalStMan (ms.rs:1049-1320): runs of rows sharing one value, for
+  numeric and boolean scalars, fixed-shape arrays and indirect arrays.
+* Refused with a `ValueError` naming the cause: string columns and the row
+  count of `table.lock` (tables are read with the row count of `table.dat`).
 
 Cells come back in NumPy order: a casacore array of shape (ncorr, nchan)
 per row reads as (nrow, nchan, ncorr). `rows(path, data_desc_id)` gives the
@@ -215,6 +216,8 @@ class Table:
                 self.managers[seq] = _Ssm(self, seq, blob, mine)
             elif kind in ("TiledShapeStMan", "TiledColumnStMan", "TiledCellStMan"):
                 self.managers[seq] = _Tsm(self, seq, kind, mine)
+            elif kind == "IncrementalStMan":
+                self.managers[seq] = _Ism(self, seq, blob, mine)
             else:
                 self.managers[seq] = kind
 
@@ -371,6 +374,98 @@ def _indirect(path, big, col, offsets):
     if not out:
         return np.zeros((0,), NUMPY[col.code])
     return np.stack(out)
+
+
+class _Ism:
+    """IncrementalStMan (core/src/ms.rs:1049-1320): a value is stored once
+    for a run of rows. Buckets follow the 512-byte header; each starts with
+    the offset of its interval table (low 28 bits; a high bit marks 64-bit
+    row numbers), which holds per column the first row of each run and the
+    offset of its value; the index of buckets follows the initial buckets."""
+
+    def __init__(self, table, seq, blob, cols):
+        c = Cursor(blob, True)
+        c.magic()
+        obj = c.start("ISM")
+        c.string()
+        c.end(obj)
+        self.path = table.file(seq)
+        raw = self.path.read_bytes()
+        h = Cursor(raw[:BUCKET_START], not table.little)
+        h.magic()
+        obj = h.start("IncrementalStMan")
+        self.big = h.bool() if obj[2] >= 5 else True
+        if self.big == table.little:
+            raise ValueError("IncrementalStMan byte order differs from the table's")
+        self.bucket_size = h.u32()
+        ninit = h.u32()
+        ic = Cursor(raw[BUCKET_START + ninit * self.bucket_size:], self.big)
+        ic.magic()
+        obj = ic.start("ISMIndex")
+        used = ic.u32()
+        self.starts = np.asarray(ic.block(wide=obj[2] > 1)[:used + 1], np.int64)
+        self.buckets = ic.block()[:used]
+        self.raw = raw
+        self.slot = {col.name: i for i, col in enumerate(cols)}
+        self.ncol = len(cols)
+
+    def _intervals(self, bucket, k):
+        order = "big" if self.big else "little"
+        word = int.from_bytes(bucket[:4], order)
+        wide = bool(word & 0xF0000000)
+        at = word & 0x0FFFFFFF
+        for col in range(self.ncol):
+            n = int.from_bytes(bucket[at:at + 4], order)
+            at += 4
+            rsize = 8 if wide else 4
+            rows = [int.from_bytes(bucket[at + rsize * i:at + rsize * (i + 1)], order) for i in range(n)]
+            at += rsize * n
+            offs = [int.from_bytes(bucket[at + 4 * i:at + 4 * (i + 1)], order) for i in range(n)]
+            at += 4 * n
+            if col == k:
+                return rows, offs
+        raise ValueError("IncrementalStMan bucket without the column")
+
+    def _value(self, col, bucket, at):
+        """One row's value at byte `at` of a bucket."""
+        if col.is_array and not col.direct:
+            off = int.from_bytes(bucket[at:at + 8], "big" if self.big else "little")
+            if off == 0:
+                raise ValueError(f"a row of {col.name} has no array")
+            return _indirect(Path(str(self.path) + "i"), self.big, col, [off])[0]
+        nelem = int(np.prod(col.shape)) if col.is_array else 1
+        if col.is_array and not col.fixed_shape:
+            raise ValueError(f"{col.name}: IncrementalStMan direct arrays without a fixed shape are not read")
+        if col.code == 0:
+            vals = _bits(bucket[at:at + (nelem + 7) // 8], 0, nelem)
+        else:
+            vals = np.frombuffer(bucket, _dtype(col.code, self.big), nelem, at).astype(np.dtype(NUMPY[col.code]))
+        return vals.reshape(tuple(reversed(col.shape))) if col.is_array else vals[0]
+
+    def read(self, col, start, count):
+        if col.code == STRING:
+            raise ValueError(f"{col.name}: string columns are not read")
+        k = self.slot[col.name]
+        out = []
+        row, end = start, start + count
+        while row < end:
+            i = int(np.searchsorted(self.starts, row, side="right")) - 1
+            if i < 0 or i + 1 >= len(self.starts):
+                raise ValueError(f"row {row} beyond the IncrementalStMan index")
+            b0, b1 = int(self.starts[i]), int(self.starts[i + 1])
+            at = BUCKET_START + self.buckets[i] * self.bucket_size
+            bucket = self.raw[at:at + self.bucket_size]
+            rows, offs = self._intervals(bucket, k)
+            last = min(b1, end) - 1
+            while row <= last:
+                local = row - b0
+                j = max(0, int(np.searchsorted(rows, local, side="right")) - 1)
+                until = rows[j + 1] if j + 1 < len(rows) else b1 - b0
+                n = min(until, last - b0 + 1) - local
+                value = self._value(col, bucket, 4 + offs[j])
+                out.extend([value] * n)
+                row += n
+        return np.stack([np.asarray(v) for v in out]) if out else np.zeros(0, NUMPY[col.code])
 
 
 class _Tsm:

@@ -6,8 +6,8 @@ fixtures (tests/golden/make_ms_fixtures.py):
   the converted store, bit for bit (the reference's own check of its two
   readers, its tests/test_msv4.py:1-13);
 * the reference's MSv2 edge-case tables against its oracle.json: cells of
-  four shapes in a TiledCellStMan; IncrementalStMan and string columns
-  refused with the cause named;
+  four shapes in a TiledCellStMan, IncrementalStMan scalars and arrays;
+  string columns refused with the cause named;
 * on the GPU, a data description's rows through Stokes I into the gridder,
   equal to the MSv4 path's dirty image.
 """
@@ -74,8 +74,16 @@ def test_edge_tables_against_the_reference_oracle(tables):
         got = t.read("F32", row, 1)[0]
         assert got.dtype == np.float32 and list(got.shape) == want["shape"]
         assert np.array_equal(got, np.asarray(want["values"], np.float32).reshape(want["shape"]))
-    with pytest.raises(ValueError, match="IncrementalStMan"):
-        msv2.Table(tables / "edge" / "t06-ism").read("I32")
+    # IncrementalStMan: runs of rows sharing a value, scalars and an array.
+    ism = oracle["t06-ism"]
+    t = msv2.Table(tables / "edge" / "t06-ism")
+    for name in ("I32", "F64", "B", "ARR"):
+        whole = t.read(name)
+        for row, want in enumerate(ism["columns"][name]):
+            w = np.asarray(want["values"], want["dtype"]).reshape(want["shape"])
+            assert np.array_equal(t.read(name, row, 1)[0], w) and np.array_equal(whole[row], w), (name, row)
+    with pytest.raises(ValueError, match="string"):
+        t.read("S")
     with pytest.raises(ValueError, match="string"):
         msv2.Table(tables / "edge" / "t07-strings").read("FIXED")
 
