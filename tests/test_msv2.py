@@ -8,8 +8,9 @@ fixtures (tests/golden/make_ms_fixtures.py):
 * the reference's MSv2 edge-case tables against its oracle.json: cells of
   four shapes in a TiledCellStMan, IncrementalStMan scalars and arrays;
   string columns refused with the cause named;
-* on the GPU, a data description's rows through Stokes I into the gridder,
-  equal to the MSv4 path's dirty image.
+* on the GPU, a data description's rows through Stokes I into the gridder:
+  the same gridder inputs as the MSv4 path, bit for bit, and the same dirty
+  image to float32 rounding.
 """
 
 import json
@@ -106,12 +107,18 @@ def test_bad_tables_are_refused(tables, tmp_path):
 def test_msv2_rows_feed_the_gridder_like_msv4(tables):
     from rang import core_wgridder, msv2, msv4
 
+    # The gridder's inputs are equal bit for bit; its float atomics make two
+    # runs agree to rounding, not bit for bit.
     ps = msv4.open_processing_set(GOLDEN / "msv4_m05.zip")
-    images = []
+    inputs, images = [], []
     for source in (msv2.DataDescription(tables / "m05.ms", 1), ps.partition(ps.names()[1])):
         r = _sorted(source.rows())
         g = msv4.gridder_inputs(source, r)
+        inputs.append(g)
         images.append(core_wgridder.vis2dirty(uvw=g["uvw"], freq=g["freq"], vis=g["vis"], wgt=g["wgt"],
                                               mask=g["mask"], npix_x=64, npix_y=64, pixsize_x=2e-4,
                                               pixsize_y=2e-4, epsilon=1e-5))
-    assert np.array_equal(images[0], images[1]) and np.abs(images[0]).max() > 0
+    for key in ("uvw", "freq", "vis", "wgt", "mask"):
+        assert np.array_equal(inputs[0][key], inputs[1][key]), key
+    assert np.abs(images[0]).max() > 0
+    assert np.abs(images[0] - images[1]).max() <= 1e-6 * np.abs(images[1]).max()
