@@ -605,34 +605,37 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
 // from one block to the next.
 //
 // Staging (one visibility per lane) stores, per slot, the u taps at [8, 8+S)
-// of a zero-padded 24-entry column, the pre-split B entries at [3, 3+S) of an
-// 11-entry column, and the S w-taps; the zero padding makes every operand
-// fetch a plain load (at row - du + 8, column - dv + 3). Slot TC_BATCH is all
-// zero and stands in for the missing visibilities of a short block.
+// of a zero-padded 24-entry column, the B entries (value * v tap, complex) at
+// [3, 3+S) of an 11-entry column, and the S w-taps; the zero padding makes
+// every operand fetch a plain load (at row - du + 8, column - dv + 3). Slot
+// TC_BATCH is all zero and stands in for the missing visibilities of a short
+// block. B is split into TF32 hi and lo where a block loads it, which keeps a
+// slot at 256 bytes and lets more warps share an SM.
 constexpr int TC_BATCH = 32;
 constexpr uint32_t TC_CHUNK = 8192;  // sorted visibilities per warp
 // u-tap columns: 24 entries, taps at [8, 8 + S), read at row - du + 8; the
 // slot stride (25) is odd so that the lanes' stores fall in distinct banks.
 constexpr int TC_USTRIDE = 25;
-// B columns: 11 float4 entries, taps at [3, 3 + S), read at column - dv + 3
-// (dv < 4); a slot stride of 6 mod 8 float4s puts the 8 lanes of one 128-bit
-// load phase (two columns, four slots) in distinct bank groups.
-constexpr int TC_VSTRIDE = 14;
+// B columns: 11 float2 entries, taps at [3, 3 + S), read at column - dv + 3
+// (dv < 4); a slot stride of 96 bytes puts the four slots a half-warp reads
+// (eight bytes per lane, four consecutive columns each) 32 bytes apart mod
+// 128, in distinct banks.
+constexpr int TC_VSTRIDE = 12;
 constexpr int TC_WSTRIDE = 9;  // w taps, odd stride as the u taps
 
 struct TcSlots {
-  float4* kb;     // [TC_BATCH + 1][TC_VSTRIDE]: (re hi, re lo, im hi, im lo) of value * kv
+  float2* kb;     // [TC_BATCH + 1][TC_VSTRIDE]: value * kv (re, im)
   float* ku;      // [TC_BATCH + 1][TC_USTRIDE]
   float* kw;      // [TC_BATCH + 1][TC_WSTRIDE]
   uint32_t* key;  // [TC_BATCH + 1]
   uint32_t* duv;  // [TC_BATCH + 1]: du | dv << 8
   // Rounded up to whole float4s, all of which the kernel zeroes.
   __host__ __device__ static constexpr size_t bytes() {
-    return ((size_t)(TC_BATCH + 1) * (TC_VSTRIDE * sizeof(float4) + (TC_USTRIDE + TC_WSTRIDE) * sizeof(float) + 8) +
+    return ((size_t)(TC_BATCH + 1) * (TC_VSTRIDE * sizeof(float2) + (TC_USTRIDE + TC_WSTRIDE) * sizeof(float) + 8) +
             15) / 16 * 16;
   }
   __device__ void carve(unsigned char* base) {
-    kb = reinterpret_cast<float4*>(base);
+    kb = reinterpret_cast<float2*>(base);
     ku = reinterpret_cast<float*>(kb + (TC_BATCH + 1) * TC_VSTRIDE);
     kw = ku + (TC_BATCH + 1) * TC_USTRIDE;
     key = reinterpret_cast<uint32_t*>(kw + (TC_BATCH + 1) * TC_WSTRIDE);
@@ -704,8 +707,9 @@ __device__ __forceinline__ void tc_flush(const Geom<float>& g, cplx<float>* __re
   }
 }
 
+// Supports up to 6 fit 96 registers (20 warps per SM); wider ones are not capped.
 template <int S>
-__global__ void __launch_bounds__(TC_BATCH)
+__global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
     k_grid_tc(const __grid_constant__ Geom<float> g, Inputs in, int mode, const double* __restrict__ uvw,
               const double* __restrict__ foc, const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend,
               cplx<float>* __restrict__ grids, int pg0, int npg) {
@@ -763,14 +767,12 @@ __global__ void __launch_bounds__(TC_BATCH)
         cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
         if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
         float* cu = st.ku + lane * TC_USTRIDE + 8;
-        float4* cb = st.kb + lane * TC_VSTRIDE + 3;
+        float2* cb = st.kb + lane * TC_VSTRIDE + 3;
         float* cw = st.kw + lane * TC_WSTRIDE;
 #pragma unroll
         for (int i = 0; i < S; i++) {
           cu[i] = ku[i];
-          const float re = val.re * kv[i], im = val.im * kv[i];
-          const float rh = __uint_as_float(to_tf32(re)), ih = __uint_as_float(to_tf32(im));
-          cb[i] = make_float4(rh, re - rh, ih, im - ih);
+          cb[i] = make_float2(val.re * kv[i], val.im * kv[i]);
         }
         if (g.do_wgridding) {
 #pragma unroll
@@ -816,12 +818,13 @@ __global__ void __launch_bounds__(TC_BATCH)
         const float* u0 = st.ku + e0 * TC_USTRIDE + gq - du0 + 8;
         const float* u1 = st.ku + e1 * TC_USTRIDE + gq - du1 + 8;
         const float ku00 = u0[0], ku01 = u0[8], ku10 = u1[0], ku11 = u1[8];
-        const float4 b0 = st.kb[e0 * TC_VSTRIDE + gq - dv0 + 3];
-        const float4 b1 = st.kb[e1 * TC_VSTRIDE + gq - dv1 + 3];
-        const uint32_t brh0 = __float_as_uint(b0.x), brl0 = __float_as_uint(b0.y);
-        const uint32_t bih0 = __float_as_uint(b0.z), bil0 = __float_as_uint(b0.w);
-        const uint32_t brh1 = __float_as_uint(b1.x), brl1 = __float_as_uint(b1.y);
-        const uint32_t bih1 = __float_as_uint(b1.z), bil1 = __float_as_uint(b1.w);
+        const float2 b0 = st.kb[e0 * TC_VSTRIDE + gq - dv0 + 3];
+        const float2 b1 = st.kb[e1 * TC_VSTRIDE + gq - dv1 + 3];
+        uint32_t brh0, brl0, bih0, bil0, brh1, brl1, bih1, bil1;
+        split_fast(b0.x, brh0, brl0);
+        split_fast(b0.y, bih0, bil0);
+        split_fast(b1.x, brh1, brl1);
+        split_fast(b1.y, bih1, bil1);
         const float* w0p = st.kw + e0 * TC_WSTRIDE;
         const float* w1p = st.kw + e1 * TC_WSTRIDE;
         // Planes in pairs: four independent accumulator chains in flight.
