@@ -51,7 +51,7 @@ WORKLOAD = "ms2dirty+dirty2ms 1.06G vis 4096^2"
 # workload, measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum)
 # on a B200: a profiler figure, not something this script can time.
 DRAM_TRAFFIC = {
-    (WORKLOAD, 1e-5, "k_grid_tc"): 19.83e9 + 0.571e9,
+    (WORKLOAD, 1e-5, "k_grid_tc"): 20.79e9 + 0.70e9,
     (WORKLOAD, 1e-5, "k_degrid"): 9.61e9 + 9.51e9,
 }
 METRIC = "Mvis/s ms2dirty+dirty2ms @eps=1e-5 vs FP64"
