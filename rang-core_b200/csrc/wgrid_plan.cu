@@ -217,14 +217,26 @@ __global__ void k_bin_count(const __grid_constant__ Geom<T> g, const double* __r
   }
 }
 
+// Each thread takes four indices a grid-stride apart per round, so that four
+// independent atomics (each returning its run's base) are in flight at once:
+// the kernel is bound by their latency. The order within a bin is free.
 __global__ void k_bin_scatter(uint64_t n, const uint32_t* __restrict__ key, uint32_t* __restrict__ cursor,
                               uint32_t* __restrict__ sorted) {
-  uint64_t nround = (n + 31) & ~31ull;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nround; i += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t k = i < n ? key[i] : INACTIVE;
-    bool act = k != INACTIVE;
-    uint32_t pos = warp_aggregated_add(cursor, k, act);
-    if (act) sorted[pos] = (uint32_t)i;
+  constexpr int U = 4;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32: warps stay aligned
+  const uint64_t nround = (n + 31) & ~31ull;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nround; i += U * stride) {
+    uint32_t k[U], pos[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint64_t j = i + u * stride;
+      k[u] = j < n ? key[j] : INACTIVE;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) pos[u] = warp_aggregated_add(cursor, k[u], k[u] != INACTIVE);
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (k[u] != INACTIVE) sorted[pos[u]] = (uint32_t)(i + u * stride);
   }
 }
 
