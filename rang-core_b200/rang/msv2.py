@@ -17,8 +17,12 @@ reference's writer and casacore use for them.
   reshape and transpose.
 * IncrementalStMan (ms.rs:1049-1320): runs of rows sharing one value, for
   numeric and boolean scalars, fixed-shape arrays and indirect arrays.
-* Refused with a `ValueError` naming the cause: string columns and the row
-  count of `table.lock` (tables are read with the row count of `table.dat`).
+* Strings (ms.rs:847-964, :1296-1318): fixed-length and indirect scalars in
+  StandardStMan buckets, string arrays in its chained string buckets,
+  IncrementalStMan strings and indirect string arrays in `table.fNi`; they
+  come back as NumPy object arrays of `str`.
+* The row count: that of `table.lock`'s sync record where it has one (rows
+  added after `table.dat` was written), else `table.dat`'s.
 
 Cells come back in NumPy order: a casacore array of shape (ncorr, nchan)
 per row reads as (nrow, nchan, ncorr). `rows(path, data_desc_id)` gives the
@@ -126,6 +130,27 @@ class Cursor:
         return out
 
 
+def _lock_rows(path):
+    """The row count of the sync record of `table.lock` (ms.rs:2254-2280):
+    after the lock requests ((1 + 2 * 32) big-endian ints), the record's
+    length and an AipsIO `sync` object whose first field is the row count;
+    None when there is none."""
+    lock = path / "table.lock"
+    if not lock.is_file():
+        return None
+    raw = lock.read_bytes()
+    at = (1 + 2 * 32) * 4
+    if len(raw) < at + 4:
+        return None
+    n = int.from_bytes(raw[at:at + 4], "big")
+    if n == 0:
+        return None
+    c = Cursor(raw[at + 4:at + 4 + n], True)
+    c.magic()
+    obj = c.start("sync")
+    return c.u32() if obj[2] == 1 else c.u64()
+
+
 class Column:
     def __init__(self, name, code, is_array, option, shape, max_length, manager):
         self.name, self.code, self.is_array, self.option = name, code, is_array, option
@@ -149,6 +174,9 @@ class Table:
         if table[2] > 3:
             raise ValueError(f"table.dat version {table[2]} is not read")
         self.nrows = c.u64() if table[2] > 2 else c.u32()
+        synced = _lock_rows(self.path)
+        if synced:  # rows added after table.dat was written (ms.rs:1925-1933)
+            self.nrows = synced
         self.little = c.u32() != 0
         kind = c.string()
         if kind != "PlainTable":
@@ -230,8 +258,6 @@ class Table:
             raise KeyError(f"{self.path.name}: no column {name}")
         col = self.columns[name]
         count = self.nrows - start if count is None else count
-        if col.code == STRING:
-            raise ValueError(f"{name}: string columns are not read")
         mgr = self.managers[col.manager]
         if isinstance(mgr, str):
             raise ValueError(f"{name}: storage manager {mgr} is not read")
@@ -314,9 +340,91 @@ class _Ssm:
                 yield f.read(self.bucket_size), off, row - first, stop - row
                 row = stop
 
+    def _bucket(self, f, n):
+        if n < 0 or n >= self.nbuckets:
+            raise ValueError("string bucket chain leaves the file")
+        f.seek(BUCKET_START + n * self.bucket_size)
+        return f.read(self.bucket_size)
+
+    def _chars(self, f, bucket, offset, length, cursor=None):
+        """`length` characters from (bucket, offset) of the string buckets
+        (16 big-endian bookkeeping bytes: the bucket number, the bytes used,
+        deleted bytes, the next bucket; then characters), following the chain;
+        returns them and the position after them."""
+        out = bytearray()
+        b, at = bucket, offset
+        data = self._bucket(f, b)
+        guard = 0
+        while len(out) < length:
+            used = max(0, int.from_bytes(data[4:8], "big", signed=True))
+            take = min(length - len(out), max(0, used - at))
+            out += data[16 + at:16 + at + take]
+            at += take
+            if len(out) < length:
+                guard += 1
+                if guard > self.nbuckets:
+                    raise ValueError("string bucket chain loops")
+                b, at = int.from_bytes(data[12:16], "big", signed=True), 0
+                data = self._bucket(f, b)
+        return bytes(out), (b, at)
+
+    def _strings_at(self, f, pos, n):
+        """`n` strings from a position of the string buckets, each a
+        big-endian length and its characters; returns them and the end."""
+        out = []
+        for _ in range(n):
+            raw, pos = self._chars(f, pos[0], pos[1], 4)
+            text, pos = self._chars(f, pos[0], pos[1], max(0, int.from_bytes(raw, "big", signed=True)))
+            out.append(text.decode("utf-8", "replace"))
+        return out, pos
+
+    def _read_strings(self, col, start, count):
+        fixed_scalar = not col.is_array and col.max_length > 0
+        width = col.max_length if fixed_scalar else 12
+        order = "big" if self.big else "little"
+        slots = []
+        for b, off, first, n in self._runs(col, start, count):
+            for r in range(n):
+                slots.append(b[off + (first + r) * width:off + (first + r + 1) * width])
+        out = []
+        with open(self.path, "rb") as f:
+            for row, slot in enumerate(slots, start):
+                if fixed_scalar:
+                    out.append(slot.split(b"\0", 1)[0].decode("utf-8", "replace"))
+                    continue
+                bk, o, ln = (int.from_bytes(slot[4 * i:4 * i + 4], order, signed=True) for i in range(3))
+                if not col.is_array:  # up to 8 characters sit in the slot itself
+                    text = slot[:max(ln, 0)] if ln <= 8 else self._chars(f, bk, o, ln)[0]
+                    out.append(text.decode("utf-8", "replace"))
+                    continue
+                if col.fixed_shape:
+                    shape = list(col.shape)
+                    n = int(np.prod(shape))
+                    vals = self._strings_at(f, (bk, o), n)[0] if ln > 0 else [""] * n
+                else:
+                    if ln <= 0:
+                        raise ValueError(f"row {row} of {col.name} has no array")
+                    raw, pos = self._chars(f, bk, o, 4)
+                    ndim = int.from_bytes(raw, "big", signed=True)
+                    if not 0 <= ndim <= 64:
+                        raise ValueError(f"row {row} of {col.name}: string array of {ndim} axes")
+                    shape = []
+                    for _ in range(ndim):
+                        raw, pos = self._chars(f, pos[0], pos[1], 4)
+                        shape.append(int.from_bytes(raw, "big", signed=True))
+                    raw, pos = self._chars(f, pos[0], pos[1], 4)
+                    n = int(np.prod(shape)) if shape else 1
+                    vals = self._strings_at(f, pos, n)[0] if int.from_bytes(raw, "big") else [""] * n
+                out.append(np.array(vals, dtype=object).reshape(tuple(reversed(shape))))
+        if not col.is_array:
+            return np.array(out, dtype=object)
+        if any(a.shape != out[0].shape for a in out):
+            raise ValueError(f"rows of {col.name} differ in shape; read fewer rows at once")
+        return np.stack(out) if out else np.zeros(0, dtype=object)
+
     def read(self, col, start, count):
         if col.code == STRING:
-            raise ValueError(f"{col.name}: string columns are not read")
+            return self._read_strings(col, start, count)
         if not col.is_array:
             parts = []
             for b, off, first, n in self._runs(col, start, count):
@@ -368,6 +476,13 @@ def _indirect(path, big, col, offsets):
             raise ValueError(f"rows of {col.name} differ in shape; read fewer rows at once")
         if col.code == 0:
             vals = _bits(raw[p:p + (n + 7) // 8], 0, n)
+        elif col.code == STRING:  # per element an offset to (length, characters); 0 for ""
+            vals = []
+            for e in range(n):
+                at_e = int.from_bytes(raw[p + 4 * e:p + 4 * e + 4], order)
+                ln = int.from_bytes(raw[at_e:at_e + 4], order) if at_e else 0
+                vals.append(raw[at_e + 4:at_e + 4 + ln].decode("utf-8", "replace") if at_e else "")
+            vals = np.array(vals, dtype=object)
         else:
             vals = np.frombuffer(raw, _dtype(col.code, big), n, p).astype(np.dtype(NUMPY[col.code]))
         out.append(vals.reshape(tuple(reversed(shape))))
@@ -436,6 +551,20 @@ class _Ism:
         nelem = int(np.prod(col.shape)) if col.is_array else 1
         if col.is_array and not col.fixed_shape:
             raise ValueError(f"{col.name}: IncrementalStMan direct arrays without a fixed shape are not read")
+        if col.code == STRING:
+            # The total length (itself included), then one string's characters,
+            # or for several strings each one's length and characters.
+            order = "big" if self.big else "little"
+            total = int.from_bytes(bucket[at:at + 4], order)
+            body = bucket[at + 4:at + max(total, 4)]
+            if nelem == 1 and not col.is_array:
+                return body.decode("utf-8", "replace")
+            vals, p = [], 0
+            for _ in range(nelem):
+                ln = int.from_bytes(body[p:p + 4], order)
+                vals.append(body[p + 4:p + 4 + ln].decode("utf-8", "replace"))
+                p += 4 + ln
+            return np.array(vals, dtype=object).reshape(tuple(reversed(col.shape)))
         if col.code == 0:
             vals = _bits(bucket[at:at + (nelem + 7) // 8], 0, nelem)
         else:
@@ -443,8 +572,6 @@ class _Ism:
         return vals.reshape(tuple(reversed(col.shape))) if col.is_array else vals[0]
 
     def read(self, col, start, count):
-        if col.code == STRING:
-            raise ValueError(f"{col.name}: string columns are not read")
         k = self.slot[col.name]
         out = []
         row, end = start, start + count
@@ -465,7 +592,11 @@ class _Ism:
                 value = self._value(col, bucket, 4 + offs[j])
                 out.extend([value] * n)
                 row += n
-        return np.stack([np.asarray(v) for v in out]) if out else np.zeros(0, NUMPY[col.code])
+        if col.code == STRING and not col.is_array:
+            return np.array(out, dtype=object)
+        if not out:
+            return np.zeros(0, dtype=object if col.code == STRING else NUMPY[col.code])
+        return np.stack([np.asarray(v) for v in out])
 
 
 class _Tsm:
@@ -601,8 +732,9 @@ class _Tsm:
 def rows(path, data_desc_id=0):
     """The main-table rows of one data description, in the layout of
     `rang.msv4.Partition.rows` (DATA, FLAG, WEIGHT_SPECTRUM (else WEIGHT per
-    correlation), UVW, TIME (MJD s), ANTENNA1, ANTENNA2, FLAG_ROW), plus
-    the channel frequencies and the correlation names."""
+    correlation), UVW, TIME (MJD s), ANTENNA1, ANTENNA2, FLAG_ROW,
+    FIELD_NAME from the FIELD table, SCAN_NAME the scan number), plus the
+    channel frequencies and the correlation names."""
     path = Path(path)
     main = Table(path)
     ddid = main.read("DATA_DESC_ID")
@@ -621,12 +753,18 @@ def rows(path, data_desc_id=0):
     pol = int(dd.read("POLARIZATION_ID", data_desc_id, 1)[0])
     freq = Table(path / "SPECTRAL_WINDOW").read("CHAN_FREQ", spw, 1)[0].astype(np.float64)
     corr = Table(path / "POLARIZATION").read("CORR_TYPE", pol, 1)[0]
+    field = Table(path / "FIELD")
+    names = field.read("NAME") if field.nrows else np.zeros(0, dtype=object)
+    fid = col("FIELD_ID")
+    field_name = np.array([str(names[i]) if 0 <= i < len(names) else "" for i in fid], dtype=object)
+    scan_name = np.array([str(int(v)) for v in col("SCAN_NUMBER")], dtype=object)
     data = col("DATA")
     weight = col("WEIGHT_SPECTRUM") if "WEIGHT_SPECTRUM" in main.columns else \
         np.broadcast_to(col("WEIGHT")[:, None, :], data.shape).astype(np.float32)
     return {"ANTENNA1": col("ANTENNA1"), "ANTENNA2": col("ANTENNA2"), "TIME": col("TIME"),
             "FLAG_ROW": col("FLAG_ROW"), "DATA": data, "FLAG": col("FLAG"), "WEIGHT_SPECTRUM": weight,
-            "UVW": col("UVW"), "frequency": freq, "polarization": tuple(CORR_NAMES.get(int(c), str(c)) for c in corr)}
+            "UVW": col("UVW"), "FIELD_NAME": field_name, "SCAN_NAME": scan_name, "frequency": freq,
+            "polarization": tuple(CORR_NAMES.get(int(c), str(c)) for c in corr)}
 
 
 class DataDescription:

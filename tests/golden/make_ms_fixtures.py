@@ -3,7 +3,7 @@
 * `msv4_m05.zip`: the reference's `tests/data/msv4/m05.zip` (an xradio 1.3.1
   processing set `m05.ps.zarr/` and the MSv2 `m05.ms/` it was converted
   from, the reference's edge-case set's two-window MS,
-  `tests/test_msv4.py:1-13`), less the MSv2 lock files.
+  `tests/test_msv4.py:1-13`); the MSv2 lock files carry row counts.
 * `msv2_edge.zip`: the reference's `tests/data/msv2-edge/` casacore tables
   (TiledCellStMan cells of four shapes, IncrementalStMan, string columns)
   with its `oracle.json` of their values.
@@ -22,14 +22,13 @@ def main(reference):
     out = HERE / "msv4_m05.zip"
     with zipfile.ZipFile(out, "w", zipfile.ZIP_DEFLATED) as dst:
         for name in src.namelist():
-            if not name.endswith("table.lock"):
-                dst.writestr(name, src.read(name))
+            dst.writestr(name, src.read(name))
     print(out, out.stat().st_size)
     edge = ref / "msv2-edge"
     out = HERE / "msv2_edge.zip"
     with zipfile.ZipFile(out, "w", zipfile.ZIP_DEFLATED) as dst:
         for f in sorted(edge.rglob("*")):
-            if f.is_file() and f.name != "table.lock":
+            if f.is_file():
                 dst.write(f, f.relative_to(edge).as_posix())
     print(out, out.stat().st_size)
 

@@ -6,8 +6,8 @@ fixtures (tests/golden/make_ms_fixtures.py):
   the converted store, bit for bit (the reference's own check of its two
   readers, its tests/test_msv4.py:1-13);
 * the reference's MSv2 edge-case tables against its oracle.json: cells of
-  four shapes in a TiledCellStMan, IncrementalStMan scalars and arrays;
-  string columns refused with the cause named;
+  four shapes in a TiledCellStMan, IncrementalStMan scalars and arrays,
+  string scalars and arrays of every storage form;
 * on the GPU, a data description's rows through Stokes I into the gridder:
   the same gridder inputs as the MSv4 path, bit for bit, and the same dirty
   image to float32 rounding.
@@ -62,6 +62,17 @@ def test_msv2_equals_the_converted_msv4_store(tables, ddid):
         assert np.array_equal(a[key], b[key]), key
     assert np.array_equal(a["frequency"], part.frequency)
     assert a["polarization"] == part.polarization
+    assert list(a["SCAN_NAME"]) == list(b["SCAN_NAME"])
+    # xradio names a field by its MSv2 name and id ("F0" of FIELD row 0 -> "F0_0")
+    fid = msv2.Table(tables / "m05.ms").read("FIELD_ID")
+    assert all(f"{x}_{i}" == y for x, i, y in zip(a["FIELD_NAME"], fid, b["FIELD_NAME"]))
+
+
+def test_row_counts_come_from_the_lock_record(tables):
+    from rang import msv2
+
+    field = msv2.Table(tables / "m05.ms" / "FIELD")
+    assert field.nrows == 1 and list(field.read("NAME")) == ["F0"]
 
 
 def test_edge_tables_against_the_reference_oracle(tables):
@@ -83,10 +94,20 @@ def test_edge_tables_against_the_reference_oracle(tables):
         for row, want in enumerate(ism["columns"][name]):
             w = np.asarray(want["values"], want["dtype"]).reshape(want["shape"])
             assert np.array_equal(t.read(name, row, 1)[0], w) and np.array_equal(whole[row], w), (name, row)
-    with pytest.raises(ValueError, match="string"):
-        t.read("S")
-    with pytest.raises(ValueError, match="string"):
-        msv2.Table(tables / "edge" / "t07-strings").read("FIXED")
+    assert list(t.read("S")) == [c["values"][0] for c in ism["columns"]["S"]]
+    # Strings: a variable-shape array (cells undefined in some rows), a
+    # fixed-shape indirect array, a direct array (StandardStMan) and an
+    # IncrementalStMan array.
+    strings = oracle["t07-strings"]
+    t = msv2.Table(tables / "edge" / "t07-strings")
+    for name in ("VAR", "FIXED", "DIRECT", "ISM"):
+        for row, want in enumerate(strings["columns"][name]):
+            if want is None:
+                with pytest.raises(ValueError, match="no array"):
+                    t.read(name, row, 1)
+                continue
+            got = t.read(name, row, 1)[0]
+            assert list(got.shape) == want["shape"] and list(got.reshape(-1)) == want["values"], (name, row)
 
 
 def test_bad_tables_are_refused(tables, tmp_path):
