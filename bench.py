@@ -150,6 +150,19 @@ def cpu_round_trip(oracle, uvw, freq, vis, mask, npix, cell, eps):
     return time.perf_counter() - t0
 
 
+def cpu_model():
+    """The host CPU's model name and logical core count."""
+    name = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                name = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{name}, {os.cpu_count()} logical cores"
+
+
 def cpu_sample(wl, fraction, seed=0):
     """Host data of the first `fraction` of the integrations: visibilities
     predicted from the point sky by the oracle's own degridder (float64,
@@ -215,7 +228,8 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "epsilon": args.epsilon},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                         "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line, default=_plain), flush=True)
@@ -771,7 +785,17 @@ def run_b200(args):
         t = cpu_round_trip(oracle, suvw, sfreq, svis, smask, npix, cell, eps)
         cpu = {"value": svis.size / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"first {nt} of {wl['ntime']} integrations ({svis.size} visibilities), one round trip, "
-                         f"full {npix}^2 image and grid, {threads} threads"}
+                         f"full {npix}^2 image and grid, {threads} threads",
+               "cpu_model": cpu_model()}
+        # One core, on the first 4 integrations (a bounded sample of the same workload).
+        rows1 = 4 * 2016
+        oracle.set_threads(1)
+        t1 = cpu_round_trip(oracle, suvw[:rows1], sfreq, svis[:rows1], smask[:rows1], npix, cell, eps)
+        oracle.set_threads(threads)
+        cpu["single_core"] = {"value": svis[:rows1].size / t1 / 1e6, "unit": UNIT, "cores": 1,
+                              "sample": f"first 4 of {wl['ntime']} integrations ({svis[:rows1].size} visibilities), "
+                                        f"one round trip, full {npix}^2 image and grid (at this size the FFTs "
+                                        f"of the full grid take most of the time)"}
 
     weights_leg = None
     if rank == 0 and world == 1 and not args.no_weights:
