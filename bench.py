@@ -723,13 +723,13 @@ def run_b200(args):
         }
         del v64, dd, dv
 
-        # The tensor-core (3 x TF32) and CUDA-core (FP32) gridders at epsilon
+        # The tensor-core (3 x TF32, 3 x BF16) and CUDA-core (FP32) gridders at epsilon
         # 1e-5 (support 6) and 1e-6 (support 8; the single-precision kernels
         # stop at 8.1e-7, so 1e-7 needs double precision, timed last): one
         # plan + grid and one plan + degrid each (after a warm-up), errors
         # against float64 at epsilon 1e-7 on the same inputs: the dirty image
         # of the data, and the visibilities of one fixed image (the float64
-        # dirty image in float32). Degridding has one kernel for both methods.
+        # dirty image in float32). Degridding has one kernel for all three methods.
         img = d64.float()
         q64 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=1e-7, single=False, **common)
         v64 = q64.degrid(img.double())
@@ -737,13 +737,15 @@ def run_b200(args):
         vpeak = v64.abs().max()
         methods = []
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        cases = [(1e-5, "tf32x3", 1, True), (1e-5, "fp32", 0, True), (1e-6, "tf32x3", 1, True),
-                 (1e-6, "fp32", 0, True), (1e-7, "fp64", 1, False)]
+        cases = [(1e-5, "tf32x3", 1, True), (1e-5, "bf16x3", 2, True), (1e-5, "fp32", 0, True),
+                 (1e-6, "tf32x3", 1, True), (1e-6, "bf16x3", 2, True), (1e-6, "fp32", 0, True),
+                 (1e-7, "fp64", 1, False)]
         for eps_m, name, code, single in cases:
             ext.wgridder_set_method(code)
             vin = vis if single else vis.to(torch.complex128)
             iin = img if single else img.double()
-            for _ in range(2):
+            best = [float("inf"), float("inf")]
+            for rep in range(3):  # the first is a warm-up; the best of the other two is kept
                 torch.cuda.synchronize()
                 ev[0].record()
                 pa = wgrid_torch.DevicePlan(uvw, freq, vis=vin, mask=mask, epsilon=eps_m, single=single, **common)
@@ -756,8 +758,12 @@ def run_b200(args):
                 supp = pa.info["supp"]
                 pa.close()
                 pb.close()
+                if rep > 0:
+                    best = [min(best[0], ev[0].elapsed_time(ev[1])), min(best[1], ev[1].elapsed_time(ev[2]))]
+                if rep < 2:
+                    del dm, vm
             entry = {"method": name, "epsilon": eps_m, "supp": int(supp),
-                     "vis2dirty_ms": ev[0].elapsed_time(ev[1]), "dirty2vis_ms": ev[1].elapsed_time(ev[2])}
+                     "vis2dirty_ms": best[0], "dirty2vis_ms": best[1]}
             if single:
                 dd = dm.double() - d64
                 dv = vm.to(torch.complex128) - v64
@@ -772,6 +778,29 @@ def run_b200(args):
         accuracy["methods"] = methods
         accuracy["methods_reference"] = "float64 GPU run at epsilon 1e-7; errors near 1e-7 are at that reference's level"
         del d64, v64, img
+        # The same methods on sparse data, where the split error of a single
+        # footprint does not average away: the dirty image of one and of
+        # eight visibilities (seeded baselines up to 2 km, 1 GHz, 256^2 at
+        # 4 arcsec), relative L-inf error against float64 at epsilon 1e-12.
+        from rang import core_wgridder
+
+        srng = np.random.default_rng(11)
+        sparse = []
+        for nvis in (1, 8):
+            suvw = srng.uniform(-2000.0, 2000.0, size=(nvis, 3)) * np.array([1.0, 1.0, 0.2])
+            svis = srng.standard_normal((nvis, 1)) + 1j * srng.standard_normal((nvis, 1))
+            skw = dict(uvw=suvw, freq=np.array([1.0e9]), npix_x=256, npix_y=256,
+                       pixsize_x=4.0 * np.pi / 648000.0, pixsize_y=4.0 * np.pi / 648000.0)
+            ref = core_wgridder.vis2dirty(vis=svis, epsilon=1e-12, **skw)
+            for eps_m in (1e-5, 1e-6):
+                entry = {"visibilities": nvis, "epsilon": eps_m}
+                for name, code in (("fp32", 0), ("tf32x3", 1), ("bf16x3", 2)):
+                    ext.wgridder_set_method(code)
+                    dm = core_wgridder.vis2dirty(vis=svis.astype(np.complex64), epsilon=eps_m, **skw)
+                    entry[name + "_dirty_rel_linf"] = float(np.abs(dm - ref).max() / np.abs(ref).max())
+                sparse.append(entry)
+        ext.wgridder_set_method(1)
+        accuracy["methods_sparse"] = sparse
 
     fst = None
     if rank == 0 and not args.no_fista:

@@ -198,8 +198,11 @@ int64_t rang_b200_wgridder_launch_count(void);
 /* How single-precision gridding forms its sums (no counterpart in the
  * reference, whose RANG_WGRIDDER_SIMD selects CPU instruction sets,
  * wgridder.rs:1593-1627): 1 split-precision 3 x TF32 tensor-core products
- * with FP32 accumulation (the default), 0 plain FP32 FMAs on the CUDA cores.
- * Process-wide; RANG_WGRIDDER_GPU_METHOD=fp32|tf32x3 sets the initial value.
+ * with FP32 accumulation (the default), 0 plain FP32 FMAs on the CUDA cores,
+ * 2 split-precision 3 x BF16 tensor-core products (about 16 bits of each
+ * factor; a comparison point, not more accurate or faster than 1).
+ * Process-wide; RANG_WGRIDDER_GPU_METHOD=fp32|tf32x3|bf16x3 sets the initial
+ * value. Other values select 1.
  * Returns the previous method. */
 int32_t rang_b200_wgridder_set_method(int32_t method);
 void rang_b200_wgridder_profile(int32_t on);

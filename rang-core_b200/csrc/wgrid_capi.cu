@@ -589,7 +589,7 @@ int64_t rang_b200_wgridder_launch_count(void) { return launch_count(); }
 
 int32_t rang_b200_wgridder_set_method(int32_t method) {
   int old = grid_method();
-  set_grid_method(method == GRID_FP32 ? GRID_FP32 : GRID_TF32X3);
+  set_grid_method(method == GRID_FP32 ? GRID_FP32 : method == GRID_BF16X3 ? GRID_BF16X3 : GRID_TF32X3);
   return old;
 }
 

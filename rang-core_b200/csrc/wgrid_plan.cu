@@ -890,6 +890,224 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
   if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
 }
 
+// ------------------------------------------------------------------ tensor-core gridding (3 x BF16)
+
+// The same rank-K window updates as k_grid_tc, with mma.sync m16n8k16 on BF16
+// operands: a block holds up to 16 visibilities of one bin, and each operand
+// is split as x = hi + lo with both halves rounded to BF16 (8 significant
+// bits each, about 16 bits of x), the product formed as hi*hi + hi*lo + lo*hi.
+// Each dropped term is below 2^-16 of the product, so a visibility's footprint
+// carries a relative error of a few 1e-6; k_grid_tc's 3 x TF32 keeps about 21
+// bits. Staging, bins and the flush are k_grid_tc's.
+
+// x0 in the low half, x1 in the high half (the lower column or k index).
+__device__ __forceinline__ uint32_t pack_bf16(float x0, float x1) {
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(x1), "f"(x0));
+  return r;
+}
+// (x0, x1) = hi + lo, both packed as BF16 pairs; x - hi is exact in FP32.
+__device__ __forceinline__ void split_bf16(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  hi = pack_bf16(x0, x1);
+  lo = pack_bf16(x0 - __uint_as_float(hi << 16), x1 - __uint_as_float(hi & 0xffff0000u));
+}
+__device__ __forceinline__ void mma_bf16_zero(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%10,%10,%10,%10};\n"
+      : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(0.0f));
+}
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Supports up to 5 fit 96 registers (20 warps per SM), 6 fits 128 (16 warps)
+// without spilling; wider ones are not capped.
+template <int S>
+__global__ void __launch_bounds__(TC_BATCH, S <= 5 ? 20 : S == 6 ? 16 : 12)
+    k_grid_bf16(const __grid_constant__ Geom<float> g, Inputs in, int mode, const double* __restrict__ uvw,
+                const double* __restrict__ foc, const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend,
+                cplx<float>* __restrict__ grids, int pg0, int npg) {
+  static_assert(S <= 8, "windows hold 8 + S - 1 <= 16 rows");
+  extern __shared__ __align__(16) unsigned char smem[];
+  TcSlots st;
+  st.carve(smem);
+  const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
+  for (int c = lane; c < (int)(TcSlots::bytes() / 16); c += TC_BATCH)
+    reinterpret_cast<float4*>(smem)[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  __syncwarp();
+  const uint64_t k0 = kbase + (uint64_t)blockIdx.x * TC_CHUNK;
+  const uint64_t k1 = min(kend, k0 + TC_CHUNK);
+  const uint32_t nchan = (uint32_t)g.nchan;
+  const int np = g.do_wgridding ? S : 1;
+  const uint32_t tmask = (1u << g.log2tile) - 1u;
+  const uint32_t vmask = (1u << g.log2subv) - 1u;
+
+  float acc[S][2][4];
+#pragma unroll
+  for (int j = 0; j < S; j++)
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+      for (int r = 0; r < 4; r++) acc[j][c][r] = 0.0f;
+  uint32_t gcur = INACTIVE;
+  int su0 = 0, sv0 = 0, mpc = 0;
+  unsigned pact = 0;
+
+  for (uint64_t kb = k0; kb < k1; kb += TC_BATCH) {
+    const int nb = (int)min((uint64_t)TC_BATCH, k1 - kb);
+    __syncwarp();
+    if (lane < nb) {  // staging: one visibility per lane, as in k_grid_tc
+      uint32_t key = INACTIVE, duv = 0;
+      const uint32_t idx = sorted[kb + lane];
+      const uint32_t row = idx / nchan, ch = idx - row * nchan;
+      double b[3];
+      const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+      const double f = foc[ch];
+      const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
+      const int mp = minplane(g, w);
+      if (!g.do_wgridding || (mp <= pg0 + npg - 1 && mp + S - 1 >= pg0)) {
+        double uf, vf;
+        int64_t iu0, iv0;
+        getpix(g, u, v, uf, vf, iu0, iv0);
+        const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
+        const uint32_t sub = ((su & tmask) >> 3) * (uint32_t)g.nsub_v + ((sv & tmask) >> g.log2subv);
+        key = (((su >> g.log2tile) * (uint32_t)g.ntv + (sv >> g.log2tile)) * (uint32_t)g.nbuckets + (uint32_t)mp) *
+                  (uint32_t)g.nsub + sub;
+        duv = (su & 7u) | ((sv & vmask) << 8);
+        float ku[S], kv[S];
+        const float x0 = (float)(-uf * 2.0 + ((double)S - 1.0));
+        const float y0 = (float)(-vf * 2.0 + ((double)S - 1.0));
+        eval_taps2<float, S>(g.coeff, g.ne, x0, y0, ku, kv);
+        cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
+        if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
+        float* cu = st.ku + lane * TC_USTRIDE + 8;
+        float2* cb = st.kb + lane * TC_VSTRIDE + 3;
+        float* cw = st.kw + lane * TC_WSTRIDE;
+#pragma unroll
+        for (int i = 0; i < S; i++) {
+          cu[i] = ku[i];
+          cb[i] = make_float2(val.re * kv[i], val.im * kv[i]);
+        }
+        if (g.do_wgridding) {
+#pragma unroll
+          for (int j = 0; j < S; j++) {
+            const int p = mp + j;
+            cw[j] = (p >= pg0 && p < pg0 + npg) ? w_factor<float, S>(g, j, p, w) : 0.0f;
+          }
+        } else {
+          cw[0] = 1.0f;
+        }
+      }
+      st.key[lane] = key;
+      st.duv[lane] = duv;
+    }
+    __syncwarp();
+    int q = 0;
+    while (q < nb) {
+      const uint32_t gk = st.key[q];
+      if (gk != gcur) {
+        if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
+#pragma unroll
+        for (int j = 0; j < S; j++)
+#pragma unroll
+          for (int c = 0; c < 2; c++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) acc[j][c][r] = 0.0f;
+        gcur = gk;
+        pact = 0;
+        if (gk != INACTIVE) {
+          tc_decode(g, gk, su0, sv0, mpc);
+          for (int j = 0; j < np; j++)
+            if (mpc + j >= pg0 && mpc + j < pg0 + npg) pact |= 1u << j;
+        }
+      }
+      // The block: the leading visibilities (at most 16) of the current bin.
+      const bool same = lane < 16 && q + lane < nb && st.key[q + lane] == gk;
+      const unsigned m = __ballot_sync(0xffffffffu, same);
+      const int kbk = __ffs(~m) - 1;
+      if (gk != INACTIVE) {
+        // This lane's k indices: 2 tq, 2 tq + 1, 2 tq + 8, 2 tq + 9.
+        int e[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int k = 2 * tq + (i & 1) + (i >> 1) * 8;
+          e[i] = k < kbk ? q + k : TC_BATCH;
+        }
+        float ku0[4], ku1[4];  // u taps at rows gq and gq + 8
+        float2 bv[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const uint32_t d = st.duv[e[i]];
+          const int du = (int)(d & 255u), dv = (int)(d >> 8);
+          const float* u = st.ku + e[i] * TC_USTRIDE + gq - du + 8;
+          ku0[i] = u[0];
+          ku1[i] = u[8];
+          bv[i] = st.kb[e[i] * TC_VSTRIDE + gq - dv + 3];
+        }
+        uint32_t brh0, brl0, bih0, bil0, brh1, brl1, bih1, bil1;
+        split_bf16(bv[0].x, bv[1].x, brh0, brl0);
+        split_bf16(bv[0].y, bv[1].y, bih0, bil0);
+        split_bf16(bv[2].x, bv[3].x, brh1, brl1);
+        split_bf16(bv[2].y, bv[3].y, bih1, bil1);
+        // Planes in pairs: four independent accumulator chains in flight.
+#pragma unroll
+        for (int j = 0; j < S; j += 2) {
+          const bool two = j + 1 < S;
+          if (!((pact >> j) & (two ? 3u : 1u))) continue;
+          uint32_t ah[2][4], al[2][4];
+          float d[2][2][4];  // each block's products start from zero
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            if (h == 1 && !two) break;
+            float w[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) w[i] = st.kw[e[i] * TC_WSTRIDE + j + h];
+            split_bf16(w[0] * ku0[0], w[1] * ku0[1], ah[h][0], al[h][0]);  // A[gq][2tq, 2tq+1]
+            split_bf16(w[0] * ku1[0], w[1] * ku1[1], ah[h][1], al[h][1]);  // A[gq+8][2tq, 2tq+1]
+            split_bf16(w[2] * ku0[2], w[3] * ku0[3], ah[h][2], al[h][2]);  // A[gq][2tq+8, 2tq+9]
+            split_bf16(w[2] * ku1[2], w[3] * ku1[3], ah[h][3], al[h][3]);  // A[gq+8][2tq+8, 2tq+9]
+          }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (h == 0 || two) {
+              mma_bf16_zero(d[h][0], ah[h], brh0, brh1);
+              mma_bf16_zero(d[h][1], ah[h], bih0, bih1);
+            }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (h == 0 || two) {
+              mma_bf16(d[h][0], ah[h], brl0, brl1);
+              mma_bf16(d[h][1], ah[h], bil0, bil1);
+            }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (h == 0 || two) {
+              mma_bf16(d[h][0], al[h], brh0, brh1);
+              mma_bf16(d[h][1], al[h], bih0, bih1);
+            }
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (h == 0 || two) {
+#pragma unroll
+              for (int r = 0; r < 4; r++) {
+                acc[j + h][0][r] += d[h][0][r];
+                acc[j + h][1][r] += d[h][1][r];
+              }
+            }
+        }
+      }
+      q += kbk;
+    }
+  }
+  if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
+}
+
 // ------------------------------------------------------------------ degridding
 
 // Row stride of the degridder's shared-memory window: the smallest stride of
@@ -1261,6 +1479,21 @@ void launch_grid_tc(cudaStream_t s, const Geom<float>& g, const Inputs& in, int 
   check_cuda(cudaGetLastError(), "grid kernel (tensor cores)");
 }
 
+template <int S>
+void launch_grid_bf16(cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode, const double* uvw,
+                      const double* foc, const uint32_t* sorted, uint64_t kbase, uint64_t kend, cplx<float>* grids,
+                      int pg0, int npg) {
+  if (kend <= kbase) return;
+  const int smem = (int)TcSlots::bytes();
+  const unsigned nblocks = (unsigned)((kend - kbase + TC_CHUNK - 1) / TC_CHUNK);
+  check_cuda(cudaFuncSetAttribute(k_grid_bf16<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
+  {
+    StageTimer timer_(ST_GRID, s);
+    k_grid_bf16<S><<<nblocks, TC_BATCH, smem, s>>>(g, in, mode, uvw, foc, sorted, kbase, kend, grids, pg0, npg);
+  }
+  check_cuda(cudaGetLastError(), "grid kernel (tensor cores, 3 x BF16)");
+}
+
 template <class T, int S>
 void launch_degrid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, const Inputs& wts,
                    const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
@@ -1410,7 +1643,8 @@ int grid_method() {
   int m = g_method.load();
   if (m < 0) {
     const char* e = std::getenv("RANG_WGRIDDER_GPU_METHOD");
-    m = (e && std::string(e) == "fp32") ? GRID_FP32 : GRID_TF32X3;
+    const std::string v = e ? e : "";
+    m = v == "fp32" ? GRID_FP32 : v == "bf16x3" ? GRID_BF16X3 : GRID_TF32X3;
     g_method = m;
   }
   return m;
@@ -1655,6 +1889,12 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
           if (grid_method() == GRID_TF32X3) {
             launch_grid_tc<SV>(s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(), sorted_.as<uint32_t>(),
                                chunk_sorted_[c], chunk_sorted_[c + 1], grids.as<cplx<T>>(), (int)pg0, n);
+            continue;
+          }
+          if (grid_method() == GRID_BF16X3) {
+            launch_grid_bf16<SV>(s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(),
+                                 sorted_.as<uint32_t>(), chunk_sorted_[c], chunk_sorted_[c + 1],
+                                 grids.as<cplx<T>>(), (int)pg0, n);
             continue;
           }
         }

@@ -136,10 +136,12 @@ class Plan {
 };
 
 // How single-precision gridding accumulates footprints: split-precision
-// 3 x TF32 tensor-core products (default) or plain FP32 CUDA-core FMAs.
-// Double precision always uses FP64 CUDA-core FMAs. The environment
-// variable RANG_WGRIDDER_GPU_METHOD (fp32 | tf32x3) sets the default.
-enum GridMethod : int { GRID_FP32 = 0, GRID_TF32X3 = 1 };
+// 3 x TF32 tensor-core products (default), split-precision 3 x BF16
+// tensor-core products (about 16 bits of each factor, for comparison), or
+// plain FP32 CUDA-core FMAs. Double precision always uses FP64 CUDA-core FMAs.
+// The environment variable RANG_WGRIDDER_GPU_METHOD (fp32 | tf32x3 | bf16x3)
+// sets the default.
+enum GridMethod : int { GRID_FP32 = 0, GRID_TF32X3 = 1, GRID_BF16X3 = 2 };
 int grid_method();
 void set_grid_method(int method);
 
