@@ -219,6 +219,7 @@ def run_reference(args):
     cell = wl["cell_arcsec"] * synth.ARCSEC
     for _ in range(args.warmup):
         cpu_round_trip(oracle, uvw, freq, vis, mask, wl["npix"], cell, args.epsilon)
+    load = os.getloadavg()
     times = [cpu_round_trip(oracle, uvw, freq, vis, mask, wl["npix"], cell, args.epsilon) for _ in range(args.steps)]
     t = sum(times)
     value = vis.size * args.steps / t / 1e6
@@ -229,7 +230,8 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "epsilon": args.epsilon},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
-                         "cpu_model": cpu_model()},
+                         "cpu_model": cpu_model(), "median_step_s": statistics.median(times),
+                         "step_s": [round(x, 4) for x in times], "load_avg_before": list(load)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line, default=_plain), flush=True)
@@ -811,11 +813,13 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         oracle, suvw, sfreq, svis, smask, nt = cpu_sample(wl, args.cpu_fraction)
         threads = oracle.set_threads(os.cpu_count() or 1)
+        load = os.getloadavg()
         t = cpu_round_trip(oracle, suvw, sfreq, svis, smask, npix, cell, eps)
         cpu = {"value": svis.size / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"first {nt} of {wl['ntime']} integrations ({svis.size} visibilities), one round trip, "
                          f"full {npix}^2 image and grid, {threads} threads",
-               "cpu_model": cpu_model()}
+               "cpu_model": cpu_model(), "load_avg_before": list(load),
+               "ns_per_vis": 1e9 * t / svis.size}
         # One core, on the first 4 integrations (a bounded sample of the same workload).
         rows1 = 4 * 2016
         oracle.set_threads(1)
