@@ -33,7 +33,8 @@ extern "C" {
 /* out[p, co] = bias[co] + sum_{tap, ci} w[co, tap, ci] in[p + (ky - 1, kx - 1), ci]
  * with zeros outside each height x width image, then (in this order) plus
  * the old out (accumulate), max(., 0) (relu), and zero where mask <= 0
- * (mask non-null). cin and cout are multiples of 32. Tensor cores. */
+ * (mask non-null). cin and cout are multiples of 32. Tensor cores: tcgen05
+ * where the shapes allow it (rang_b200_nn_set_conv_path). */
 int32_t rang_b200_nn_conv3(const void* in, int64_t ld_in, const void* w, const float* bias, void* out, int64_t ld_out,
                            const void* mask, int64_t ld_mask, int64_t batch, int32_t height, int32_t width,
                            int32_t cin, int32_t cout, int32_t relu, int32_t accumulate, void* stream);
@@ -43,6 +44,17 @@ int32_t rang_b200_nn_conv3(const void* in, int64_t ld_in, const void* w, const f
 int32_t rang_b200_nn_conv3_weight_grad(const void* in, int64_t ld_in, const void* dz, int64_t ld_dz, float* dw,
                                        float* dbias, int64_t batch, int32_t height, int32_t width, int32_t cin,
                                        int32_t cout, void* stream);
+
+/* Which kernel conv3 runs: 0 (the default) the tcgen05 kernel (TMA operands,
+ * TMEM accumulator) wherever width is a multiple of 16, height of 8 and the
+ * tensors are 16-byte aligned, else the mma.sync kernel; 1 always the
+ * mma.sync kernel. Process-wide; returns the previous value. */
+int32_t rang_b200_nn_set_conv_path(int32_t path);
+
+/* Waits for the stream and reports whether a tcgen05 convolution gave up on
+ * a wait (a stalled pipeline, which then leaves its output unspecified):
+ * 0 none, 3 one did (the flag is cleared), 2 a CUDA error. */
+int32_t rang_b200_nn_device_status(void* stream);
 
 /* wt[ci, tap, co] = w[co, 8 - tap, ci]: the weights with which conv3 computes
  * the gradient with respect to its input. */

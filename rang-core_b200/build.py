@@ -30,9 +30,9 @@ NVCC = str(CUDA / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = PKG / "librang_wgrid_b200.so"
 
-CU_SOURCES = ["wgrid_plan.cu", "wgrid_capi.cu", "wgrid_weights.cu", "wgrid_gram.cu", "nn_kernels.cu"]
+CU_SOURCES = ["wgrid_plan.cu", "wgrid_capi.cu", "wgrid_weights.cu", "wgrid_gram.cu", "nn_kernels.cu", "nn_conv_tc.cu"]
 CXX_SOURCES = ["wgrid_setup.cpp", "msv4_codec.cpp"]
-HEADERS = ["wgrid_common.h", "wgrid_device.cuh", "wgrid_plan.h", "wgrid_setup.h", "kernel_db.inc"]
+HEADERS = ["wgrid_common.h", "wgrid_device.cuh", "wgrid_plan.h", "wgrid_setup.h", "kernel_db.inc", "nn_conv_tc.h"]
 
 
 def ext_path():

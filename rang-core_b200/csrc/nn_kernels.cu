@@ -9,8 +9,11 @@
 // copy). Every sum is accumulated in float32; master weights, gradients of
 // the weights and the optimiser state are float32.
 //
-// The 3x3 convolution is an implicit GEMM on the tensor cores
-// (mma.sync m16n8k16 bf16 -> f32): M = pixels (128 per block), N = output
+// The 3x3 convolution runs on the fifth-generation tensor cores (tcgen05.mma
+// with TMA operands and a TMEM accumulator, nn_conv_tc.cu) wherever the image
+// tiles into 16 x 8 patches; otherwise, and on request
+// (rang_b200_nn_set_conv_path), it is an implicit GEMM on the legacy tensor
+// core path (mma.sync m16n8k16 bf16 -> f32): M = pixels (128 per block), N = output
 // channels (32 or 64 per block), K = 9 taps x input channels in chunks of 32,
 // with the A (pixel x channel, zero-filled outside the image) and B (weight)
 // tiles staged in shared memory by cp.async in a 3-stage pipeline and read
@@ -21,8 +24,10 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
+#include "nn_conv_tc.h"
 #include "rang_nn.h"
 
 namespace {
@@ -621,6 +626,10 @@ bool aligned4(const void* p) { return ((uintptr_t)p & 3u) == 0; }
 
 int32_t launched() { return cudaGetLastError() == cudaSuccess ? 0 : 2; }
 
+// Which kernel rang_b200_nn_conv3 runs: 0 the tcgen05 / TMA kernel where the
+// shapes allow it, else the mma.sync kernel; 1 always the mma.sync kernel.
+std::atomic<int> g_conv_path{0};
+
 }  // namespace
 
 extern "C" {
@@ -632,6 +641,11 @@ int32_t rang_b200_nn_conv3(const void* in, int64_t ld_in, const void* w, const f
   if (cin % 32 || cout % 32 || ld_in < cin || ld_out < cout || ld_in % 8 || ld_out % 8) return 1;
   if (!aligned16(in) || !aligned16(w) || !aligned4(out) || (mask && (ld_mask % 8 || !aligned4(mask)))) return 1;
   if (ld_in > INT32_MAX || ld_out > INT32_MAX || ld_mask > INT32_MAX) return 1;
+  if (g_conv_path.load() == 0) {
+    const TcConvArgs t{(const bf16*)in, (const bf16*)w, bias, (bf16*)out, (const bf16*)mask, batch, height, width,
+                       (int)ld_in, (int)ld_out, (int)ld_mask, cin, cout, relu, accumulate};
+    if (conv3_tc_supported(t)) return conv3_tc(t, (cudaStream_t)stream);
+  }
   ConvArgs a{(const bf16*)in, (const bf16*)w, bias, (bf16*)out, (const bf16*)mask,
              batch * height * width, height, width, (int)ld_in, (int)ld_out, (int)ld_mask, cin, cout, relu, accumulate};
   const unsigned gx = (unsigned)((a.P + CONV_BM - 1) / CONV_BM);
@@ -676,6 +690,10 @@ int32_t rang_b200_nn_conv3_weight_grad(const void* in, int64_t ld_in, const void
   }
   return launched();
 }
+
+int32_t rang_b200_nn_set_conv_path(int32_t path) { return g_conv_path.exchange(path == 1 ? 1 : 0); }
+
+int32_t rang_b200_nn_device_status(void* stream) { return conv3_tc_status((cudaStream_t)stream); }
 
 int32_t rang_b200_nn_conv3_flip(const void* w, void* wt, int32_t cin, int32_t cout, void* stream) {
   if (!w || !wt || cin <= 0 || cout <= 0) return 1;

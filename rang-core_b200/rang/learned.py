@@ -92,6 +92,8 @@ _SIGNATURES = {
     "unpack": "PPPLFPLIIP",
     "adam": "PPPPPLFFFFIP",
     "to_bf16": "PPLP",
+    "set_conv_path": "I",
+    "device_status": "P",
 }
 
 

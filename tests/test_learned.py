@@ -62,7 +62,7 @@ def test_library_exports_every_nn_symbol():
 
     text = (REPO / "include" / "rang_nn.h").read_text()
     names = sorted(set(re.findall(r"^\w+\s+(rang_b200_nn_\w+)\s*\(", text, re.M)))
-    assert len(names) == 14
+    assert len(names) == 16
     lib = ctypes.CDLL(core.library_path())
     for name in names:
         assert hasattr(lib, name), name
@@ -154,6 +154,52 @@ def test_conv3_matches_the_oracle(cin, cout, relu, offset):
     assert np.abs(got - nno.bf16(ref)).max() <= 2.0**-7 * np.abs(ref).max()
     assert np.abs(got - ref).max() <= 2.0**-8 * np.abs(ref).max() + 2.0**-8 * np.abs(ref).max()
     assert (_np(out)[:, cout:] == 0).all()
+
+
+@pytest.fixture
+def conv_path():
+    """The process-wide convolution kernel choice, restored afterwards."""
+    from rang import learned
+
+    lib = learned._library()
+    old = lib.rang_b200_nn_set_conv_path(0)
+    yield lib
+    lib.rang_b200_nn_set_conv_path(old)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cin,cout,B,H,W", [(64, 64, 1, 8, 16), (32, 32, 1, 8, 16), (64, 128, 2, 16, 32),
+                                            (96, 32, 2, 16, 16), (384, 128, 1, 16, 16), (128, 384, 1, 8, 16),
+                                            (256, 256, 2, 32, 32), (32, 64, 1, 64, 64)],
+                         ids=lambda v: str(v))
+def test_conv3_tcgen05_matches_the_oracle_and_mma_sync(conv_path, cin, cout, B, H, W):
+    """The tcgen05 kernel (TMA boxes with zero fill for the padding, TMEM
+    accumulator) on shapes it takes: within one bfloat16 unit of the FP64
+    oracle like the mma.sync kernel, within one unit of the mma.sync kernel's
+    output, with no wait given up (device status 0)."""
+    import torch
+
+    from rang import learned
+
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(cin * 3 + cout + H)
+    x = nno.bf16(rng.standard_normal((B, H, W, cin)))
+    w = nno.bf16(rng.standard_normal((cout, 9, cin)) / np.sqrt(9 * cin))
+    b = rng.standard_normal(cout).astype(np.float32)
+    xt, wt, bt = _bf16_tensor(x.reshape(-1, cin), dev), _bf16_tensor(w, dev), torch.from_numpy(b).to(dev)
+    outs = []
+    for path in (0, 1):
+        conv_path.rang_b200_nn_set_conv_path(path)
+        out = torch.zeros((B * H * W, cout), dtype=torch.bfloat16, device=dev)
+        learned._call("conv3", xt.data_ptr(), cin, wt.data_ptr(), bt.data_ptr(), out.data_ptr(), cout, None, 0, B, H,
+                      W, cin, cout, 1, 0, s)
+        assert conv_path.rang_b200_nn_device_status(s) == 0
+        outs.append(_np(out).reshape(B, H, W, cout))
+    ref = np.maximum(nno.conv3(x, w, b.astype(np.float64)), 0.0)
+    scale = np.abs(ref).max()
+    assert np.abs(outs[0] - ref).max() <= 2.0**-7 * scale
+    assert np.abs(outs[0] - outs[1]).max() <= 2.0**-7 * scale
 
 
 @pytest.mark.gpu
