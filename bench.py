@@ -356,6 +356,49 @@ def run_fista(dev, max_iterations=200, sigma=0.05, learn=None):
             "learned": learned_report}
 
 
+def conv3_kernels(dev, batch=16):
+    """The U-Net's 3x3 convolutions at the training batch on both kernels
+    (rang_b200_nn_set_conv_path: 0 tcgen05 with TMA operands and a TMEM
+    accumulator, 1 mma.sync), forward with bias and ReLU, CUDA events over 20
+    launches after 3; seeded random bf16 inputs and weights."""
+    import torch
+
+    from rang import learned
+
+    lib = learned._library()
+    s = torch.cuda.current_stream(dev).cuda_stream
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    rows = []
+    for name, hw, cin, cout in (("enc1b", 256, 32, 32), ("enc2a", 128, 32, 64), ("enc2b", 128, 64, 64),
+                                ("enc3b", 64, 128, 128), ("enc4b", 32, 256, 256), ("dec3a", 64, 384, 128),
+                                ("dec3a input gradient", 64, 128, 384), ("dec1a", 256, 96, 32)):
+        x = torch.randn(batch * hw * hw, cin, device=dev, generator=g).to(torch.bfloat16)
+        w = (torch.randn(cout * 9 * cin, device=dev, generator=g) / np.sqrt(9 * cin)).to(torch.bfloat16)
+        b = torch.randn(cout, device=dev, generator=g)
+        o = torch.empty(batch * hw * hw, cout, device=dev, dtype=torch.bfloat16)
+        flops = 2.0 * 9 * cin * cout * batch * hw * hw
+        row = {"layer": name, "size": hw, "cin": cin, "cout": cout}
+        for path, key in ((0, "tcgen05"), (1, "mma_sync")):
+            old = lib.rang_b200_nn_set_conv_path(path)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            for i in range(23):
+                if i == 3:
+                    ev[0].record()
+                learned._call("conv3", x.data_ptr(), cin, w.data_ptr(), b.data_ptr(), o.data_ptr(), cout, None, 0,
+                              batch, hw, hw, cin, cout, 1, 0, s)
+            ev[1].record()
+            torch.cuda.synchronize()
+            lib.rang_b200_nn_set_conv_path(old)
+            assert lib.rang_b200_nn_device_status(s) == 0
+            ms = ev[0].elapsed_time(ev[1]) / 20
+            row[key + "_ms"] = ms
+            row[key + "_tflops"] = flops / ms / 1e9
+        rows.append(row)
+        del x, w, b, o
+    return rows
+
+
 def run_learned(dev, plan, dirty, q, lmax, lam, sky, nvis, target, plain_rms, plain_time, t_shared, max_iterations,
                 learn):
     """Learned-preconditioned FISTA (rang.learned) on the FISTA measurement.
@@ -432,7 +475,7 @@ def run_learned(dev, plan, dirty, q, lmax, lam, sky, nvis, target, plain_rms, pl
             "applies": applies, "final_rms": rms, "rms_trajectory": trajectory,
             "model_rel_error": float((x - sky).norm() / sky.norm()), "proposals": st["proposals"],
             "accepted": st["accepted"], "first_step": st["steps"][0] if st["steps"] else None,
-            "solve_s": ev[0].elapsed_time(ev[1]) / 1e3}
+            "solve_s": ev[0].elapsed_time(ev[1]) / 1e3, "conv3_kernels": conv3_kernels(dev)}
 
 
 # ------------------------------------------------------------------ MSv4 ingest
