@@ -40,15 +40,17 @@ int32_t rang_b200_nn_conv3(const void* in, int64_t ld_in, const void* w, const f
                            int32_t cin, int32_t cout, int32_t relu, int32_t accumulate, void* stream);
 
 /* dw[co, tap, ci] += sum_p dz[p, co] in[p + (ky - 1, kx - 1), ci] and, when
- * dbias is non-null, dbias[co] += sum_p dz[p, co]. Tensor cores. */
+ * dbias is non-null, dbias[co] += sum_p dz[p, co]. Tensor cores: tcgen05
+ * where width is a multiple of 16, height of 8 and cin and cout of 64
+ * (rang_b200_nn_set_conv_path). */
 int32_t rang_b200_nn_conv3_weight_grad(const void* in, int64_t ld_in, const void* dz, int64_t ld_dz, float* dw,
                                        float* dbias, int64_t batch, int32_t height, int32_t width, int32_t cin,
                                        int32_t cout, void* stream);
 
-/* Which kernel conv3 runs: 0 (the default) the tcgen05 kernel (TMA operands,
- * TMEM accumulator) wherever width is a multiple of 16, height of 8 and the
- * tensors are 16-byte aligned, else the mma.sync kernel; 1 always the
- * mma.sync kernel. Process-wide; returns the previous value. */
+/* Which kernels conv3 and conv3_weight_grad run: 0 (the default) the tcgen05
+ * kernels (TMA operands, TMEM accumulator) wherever the shapes and alignments
+ * allow them, else the mma.sync kernels; 1 always the mma.sync kernels.
+ * Process-wide; returns the previous value. */
 int32_t rang_b200_nn_set_conv_path(int32_t path);
 
 /* Waits for the stream and reports whether a tcgen05 convolution gave up on

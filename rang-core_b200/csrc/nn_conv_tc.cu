@@ -281,6 +281,156 @@ __global__ void __launch_bounds__(128, 1)
   if (threadIdx.x == 0 && (*bad || !ok)) atomicExch(&g_conv_tc_error, 1);
 }
 
+// ------------------------------------------------------------------ weight gradient
+
+// dw[co][tap][ci] += sum_p dz[p][co] in[p + off(tap)][ci] on the tcgen05 path,
+// one GEMM per tap: M = 128 output channels, N = BN input channels, K = the
+// pixels of a range of 8 x 16 patches (one patch, 128 pixels, per K block).
+// Both operands are channel-contiguous (MN-major): the A tile is two TMA boxes
+// of dz, 64 channels x 16 x 8 pixels each at the patch (output channels past
+// cout come back as zeros), the B tile BN / 64 boxes of the input at the
+// patch shifted by the tap (zeros outside the image). Each box is 128 rows
+// (pixels, the K index) of 128 bytes in the 128-byte swizzle; 8-row groups
+// are 1024 bytes apart and the 64-channel groups one box (16 KB) apart. The
+// block's 128 x BN sum, accumulated in TMEM over its patches, is added to dw
+// with vector atomics.
+constexpr int DW_STAGES = 3;
+constexpr int DW_BOX = TC_M * 64 * 2;  // one 64-channel box of one patch
+
+template <int BN>
+struct TcDwLayout {
+  static constexpr int A_BYTES = 2 * DW_BOX;
+  static constexpr int B_BYTES = (BN / 64) * DW_BOX;
+  static constexpr int STAGE = A_BYTES + B_BYTES;
+  static constexpr int BYTES = DW_STAGES * STAGE + (2 * DW_STAGES + 1) * 8 + 8 + 1024;
+};
+
+// MN-major operand, 128-byte swizzle: K groups of 8 rows 1024 bytes apart
+// (stride byte offset), 64-element MN groups `group_bytes` apart (leading
+// byte offset).
+__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr, uint32_t group_bytes) {
+  uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((group_bytes >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+// f32 accumulator, bf16 A and B, both MN-major, M = 128, N.
+__host__ __device__ constexpr uint32_t instr_desc_mn(int n) {
+  return instr_desc(n) | (1u << 15) | (1u << 16);
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128, 1)
+    k_conv3_dw_tc(const __grid_constant__ CUtensorMap tdz, const __grid_constant__ CUtensorMap tin,
+                  const TcDwArgs a) {
+  using L = TcDwLayout<BN>;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + DW_STAGES * L::STAGE);
+  uint64_t* empty = full + DW_STAGES;
+  uint64_t* done = empty + DW_STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* bad = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tap = blockIdx.z, dx = tap % 3 - 1, dy = tap / 3 - 1;
+  const int ci_tiles = a.Cin / BN;
+  const int co0 = (blockIdx.y / ci_tiles) * 128, ci0 = (blockIdx.y % ci_tiles) * BN;
+  const int tiles_x = a.W / TC_TW, tiles_y = a.H / TC_TH;
+  const int64_t q0 = (int64_t)blockIdx.x * a.patches_per_block;
+  const int64_t q1 = q0 + a.patches_per_block < a.patches ? q0 + a.patches_per_block : a.patches;
+  const int nk = (int)(q1 - q0);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < DW_STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *bad = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tmem_slot)),
+                 "r"((uint32_t)BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {  // loader
+    int issued = 0;
+    for (int kb = 0; kb < nk; kb++) {
+      const int s = kb % DW_STAGES;
+      if (kb >= DW_STAGES && !mbar_wait(&empty[s], ((kb / DW_STAGES) - 1) & 1)) {
+        *bad = 1;
+        break;
+      }
+      int64_t q = q0 + kb;
+      const int tx = (int)(q % tiles_x);
+      q /= tiles_x;
+      const int ty = (int)(q % tiles_y);
+      const int img = (int)(q / tiles_y);
+      const int x0 = tx * TC_TW, y0 = ty * TC_TH;
+      unsigned char* st = smem + s * L::STAGE;
+      mbar_expect_tx(&full[s], (uint32_t)L::STAGE);
+      tma_load_4d(st, &tdz, &full[s], co0, x0, y0, img);
+      tma_load_4d(st + DW_BOX, &tdz, &full[s], co0 + 64, x0, y0, img);
+#pragma unroll
+      for (int h = 0; h < BN / 64; h++)
+        tma_load_4d(st + L::A_BYTES + h * DW_BOX, &tin, &full[s], ci0 + 64 * h, x0 + dx, y0 + dy, img);
+      issued = kb + 1;
+    }
+    for (int kb = issued > DW_STAGES ? issued - DW_STAGES : 0; kb < issued; kb++)
+      if (!mbar_wait(&full[kb % DW_STAGES], (kb / DW_STAGES) & 1)) *bad = 1;
+  } else if (warp == 1 && lane == 0) {  // MMA issuer
+    const uint32_t idesc = instr_desc_mn(BN);
+    for (int kb = 0; kb < nk; kb++) {
+      const int s = kb % DW_STAGES;
+      if (!mbar_wait(&full[s], (kb / DW_STAGES) & 1)) {
+        *bad = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t sa = saddr(smem + s * L::STAGE), sb = sa + L::A_BYTES;
+#pragma unroll
+      for (int k = 0; k < TC_M / 16; k++)  // 16 pixels (two 8-row groups) per MMA
+        umma(tmem, smem_desc_mn(sa + 2048u * k, DW_BOX), smem_desc_mn(sb + 2048u * k, DW_BOX), idesc,
+             (kb | k) != 0);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);
+  }
+  __syncwarp();
+  const bool ok = mbar_wait(done, 0);
+  tc_fence_after();
+
+  // Epilogue: thread (warp, lane) owns TMEM lane 32 warp + lane, output channel co.
+  const int co = co0 + warp * 32 + lane;
+#pragma unroll 1
+  for (int c = 0; c < BN; c += 16) {
+    float v[16];
+    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    if (!ok || nk == 0 || co >= a.Cout) continue;
+    float* row = a.dw + ((int64_t)co * 9 + tap) * a.Cin + ci0 + c;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (ci0 + c + 4 * j < a.Cin)
+        atomicAdd(reinterpret_cast<float4*>(row + 4 * j), make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]));
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
+  }
+  if (threadIdx.x == 0 && (*bad || !ok)) atomicExch(&g_conv_tc_error, 1);
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -334,7 +484,55 @@ int launch_kc(const TcConvArgs& a, cudaStream_t s) {
   return launch<KC, 32>(a, s);
 }
 
+// A 4-D map of an NHWC bf16 tensor, box (64 channels, 16, 8, 1), 128-byte swizzle.
+bool nhwc_map(CUtensorMap* m, const bf16* base, int channels, int ld, int W, int H, int64_t batch) {
+  const cuuint64_t px = (cuuint64_t)ld * 2;
+  cuuint64_t dims[4] = {(cuuint64_t)channels, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)batch};
+  cuuint64_t strides[3] = {px, px * (cuuint64_t)W, px * (cuuint64_t)W * (cuuint64_t)H};
+  cuuint32_t box[4] = {64, (cuuint32_t)TC_TW, (cuuint32_t)TC_TH, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  return encoder()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN>
+int launch_dw(TcDwArgs a, cudaStream_t s, int sms) {
+  using L = TcDwLayout<BN>;
+  if (!encoder()) return 2;
+  CUtensorMap tdz, tin;
+  if (!nhwc_map(&tdz, a.dz, a.Cout, a.ld_dz, a.W, a.H, a.batch) || !nhwc_map(&tin, a.in, a.Cin, a.ld_in, a.W, a.H, a.batch))
+    return 1;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(k_conv3_dw_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
+  });
+  a.patches = a.batch * (a.W / TC_TW) * (a.H / TC_TH);
+  const int tiles = ((a.Cout + 127) / 128) * (a.Cin / BN);
+  // about two blocks per SM over all taps and tiles, at least 8 patches each
+  int64_t splits = (2 * sms + 9 * tiles - 1) / (9 * tiles);
+  const int64_t max_splits = (a.patches + 7) / 8;
+  if (splits > max_splits) splits = max_splits;
+  if (splits < 1) splits = 1;
+  a.patches_per_block = (a.patches + splits - 1) / splits;
+  splits = (a.patches + a.patches_per_block - 1) / a.patches_per_block;
+  k_conv3_dw_tc<BN><<<dim3((unsigned)splits, tiles, 9), 128, L::BYTES, s>>>(tdz, tin, a);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
 }  // namespace
+
+bool conv3_dw_tc_supported(const TcDwArgs& a) {
+  const auto a16 = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+  return a.W % TC_TW == 0 && a.H % TC_TH == 0 && a.Cin % 64 == 0 && a.Cout % 64 == 0 && a.ld_in % 8 == 0 &&
+         a.ld_dz % 8 == 0 && a16(a.in) && a16(a.dz) && a16(a.dw) && encoder() != nullptr;
+}
+
+int conv3_dw_tc(const TcDwArgs& a, cudaStream_t s) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return a.Cin % 128 == 0 ? launch_dw<128>(a, s, sms) : launch_dw<64>(a, s, sms);
+}
 
 bool conv3_tc_supported(const TcConvArgs& a) {
   const auto a16 = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };

@@ -668,6 +668,21 @@ int32_t rang_b200_nn_conv3_weight_grad(const void* in, int64_t ld_in, const void
     cudaFuncSetAttribute(k_conv3_dw<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, dw_smem_bytes<32>());
     configured = true;
   }
+  if (g_conv_path.load() == 0) {
+    const TcDwArgs t{(const bf16*)in, (const bf16*)dz, dw, batch, 0, 0, height, width, (int)ld_in, (int)ld_dz,
+                     cin, cout};
+    if (conv3_dw_tc_supported(t)) {
+      const int st = conv3_dw_tc(t, (cudaStream_t)stream);
+      if (st != 0) return st;
+      if (dbias) {
+        const int64_t rows = 4096, P = batch * height * width;
+        k_bias_grad<<<(unsigned)((P + rows - 1) / rows), 256, 0, (cudaStream_t)stream>>>((const bf16*)dz,
+                                                                                        (int)ld_dz, P, cout, dbias,
+                                                                                        rows);
+      }
+      return launched();
+    }
+  }
   DwArgs a{(const bf16*)in, (const bf16*)dz, dw, batch * height * width, 0, height, width, (int)ld_in, (int)ld_dz,
            cin, cout};
   const int tm = cout % 64 == 0 ? 64 : 32;

@@ -203,6 +203,39 @@ def test_conv3_tcgen05_matches_the_oracle_and_mma_sync(conv_path, cin, cout, B, 
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cin,cout,B,H,W", [(64, 64, 1, 8, 16), (64, 128, 2, 16, 32), (192, 64, 1, 16, 16),
+                                            (128, 384, 1, 8, 16), (256, 256, 2, 32, 32), (384, 128, 2, 64, 64)],
+                         ids=lambda v: str(v))
+def test_conv3_weight_grad_tcgen05_matches_the_oracle_and_mma_sync(conv_path, cin, cout, B, H, W):
+    """The tcgen05 weight gradient (MN-major TMA operands, K = pixels, TMEM
+    accumulator, vector atomics into dw): within 1e-5 of the FP64 oracle and
+    of the mma.sync kernel, accumulating, with no wait given up."""
+    import torch
+
+    from rang import learned
+
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(cin + 5 * cout + W)
+    x = nno.bf16(np.maximum(rng.standard_normal((B, H, W, cin)), 0.0))
+    dz = nno.bf16(rng.standard_normal((B, H, W, cout)))
+    xt, dzt = _bf16_tensor(x.reshape(-1, cin), dev), _bf16_tensor(dz.reshape(-1, cout), dev)
+    got = []
+    for path in (0, 1):
+        conv_path.rang_b200_nn_set_conv_path(path)
+        dw = torch.zeros(cout * 9 * cin, dtype=torch.float32, device=dev)
+        for _ in range(2):  # accumulates
+            learned._call("conv3_weight_grad", xt.data_ptr(), cin, dzt.data_ptr(), cout, dw.data_ptr(), None, B, H,
+                          W, cin, cout, s)
+        assert conv_path.rang_b200_nn_device_status(s) == 0
+        got.append(_np(dw).reshape(cout, 9, cin))
+    ref = 2 * nno.conv3_weight_grad(x, dz)
+    scale = np.abs(ref).max()
+    assert np.abs(got[0] - ref).max() <= 1e-5 * scale
+    assert np.abs(got[0] - got[1]).max() <= 1e-5 * scale
+
+
+@pytest.mark.gpu
 def test_conv3_epilogue_accumulate_and_mask():
     import torch
 
