@@ -359,8 +359,9 @@ def run_fista(dev, max_iterations=200, sigma=0.05, learn=None):
 def conv3_kernels(dev, batch=16):
     """The U-Net's 3x3 convolutions at the training batch on both kernels
     (rang_b200_nn_set_conv_path: 0 tcgen05 with TMA operands and a TMEM
-    accumulator, 1 mma.sync), forward with bias and ReLU, CUDA events over 20
-    launches after 3; seeded random bf16 inputs and weights."""
+    accumulator, 1 mma.sync): forward with bias and ReLU, then weight
+    gradients with the bias gradient; CUDA events over 20 launches after 3;
+    seeded random bf16 inputs and weights."""
     import torch
 
     from rang import learned
@@ -396,6 +397,32 @@ def conv3_kernels(dev, batch=16):
             row[key + "_tflops"] = flops / ms / 1e9
         rows.append(row)
         del x, w, b, o
+    # weight gradients (dw and the bias gradient) where both kernels apply: 64-channel multiples
+    for name, hw, cin, cout in (("enc2b weight gradient", 128, 64, 64), ("enc3b weight gradient", 64, 128, 128),
+                                ("enc4b weight gradient", 32, 256, 256), ("dec3a weight gradient", 64, 384, 128)):
+        x = torch.randn(batch * hw * hw, cin, device=dev, generator=g).to(torch.bfloat16)
+        dz = torch.randn(batch * hw * hw, cout, device=dev, generator=g).to(torch.bfloat16)
+        dw = torch.zeros(cout * 9 * cin, device=dev)
+        db = torch.zeros(cout, device=dev)
+        flops = 2.0 * 9 * cin * cout * batch * hw * hw
+        row = {"layer": name, "size": hw, "cin": cin, "cout": cout}
+        for path, key in ((0, "tcgen05"), (1, "mma_sync")):
+            old = lib.rang_b200_nn_set_conv_path(path)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            for i in range(23):
+                if i == 3:
+                    ev[0].record()
+                learned._call("conv3_weight_grad", x.data_ptr(), cin, dz.data_ptr(), cout, dw.data_ptr(),
+                              db.data_ptr(), batch, hw, hw, cin, cout, s)
+            ev[1].record()
+            torch.cuda.synchronize()
+            lib.rang_b200_nn_set_conv_path(old)
+            assert lib.rang_b200_nn_device_status(s) == 0
+            ms = ev[0].elapsed_time(ev[1]) / 20
+            row[key + "_ms"] = ms
+            row[key + "_tflops"] = flops / ms / 1e9
+        rows.append(row)
+        del x, dz, dw, db
     return rows
 
 

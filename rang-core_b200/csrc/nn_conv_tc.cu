@@ -20,6 +20,9 @@
 // 32w .. 32w + 31, one pixel per thread) and apply the epilogue of the
 // mma.sync kernel: bias, accumulate, ReLU, mask, bf16.
 //
+// The weight gradient (k_conv3_dw_tc, further down) is the same machinery with
+// K = pixels and both operands read channel-contiguous (MN-major).
+//
 // Every wait on an mbarrier gives up after about two seconds of device time;
 // the block then records the failure in a device flag
 // (rang_b200_nn_device_status) and returns after its own copies have landed

@@ -19,8 +19,9 @@
 // tiles staged in shared memory by cp.async in a 3-stage pipeline and read
 // with ldmatrix. The gradient with respect to the input is the same
 // convolution with the weights flipped and transposed; the gradient with
-// respect to the weights is a second tensor-core kernel whose K dimension is
-// the pixels.
+// respect to the weights is a second GEMM whose K dimension is the pixels,
+// on tcgen05 (nn_conv_tc.cu) where the channel counts are multiples of 64 and
+// otherwise the mma.sync kernel below.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
