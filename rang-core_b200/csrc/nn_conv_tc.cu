@@ -289,34 +289,34 @@ __global__ void __launch_bounds__(128, 1)
 // dw[co][tap][ci] += sum_p dz[p][co] in[p + off(tap)][ci] on the tcgen05 path,
 // one GEMM per tap: M = 128 output channels, N = BN input channels, K = the
 // pixels of a range of 8 x 16 patches (one patch, 128 pixels, per K block).
-// Both operands are channel-contiguous (MN-major): the A tile is two TMA boxes
-// of dz, 64 channels x 16 x 8 pixels each at the patch (output channels past
-// cout come back as zeros), the B tile BN / 64 boxes of the input at the
-// patch shifted by the tap (zeros outside the image). Each box is 128 rows
-// (pixels, the K index) of 128 bytes in the 128-byte swizzle; 8-row groups
-// are 1024 bytes apart and the 64-channel groups one box (16 KB) apart. The
-// block's 128 x BN sum, accumulated in TMEM over its patches, is added to dw
-// with vector atomics.
+// Both operands are channel-contiguous (MN-major): the A tile is 128 / CA TMA
+// boxes of dz, CA channels x 16 x 8 pixels each at the patch (channels past
+// cout come back as zeros, so narrow layers fill M = 128 with zeros), the B
+// tile BN / CB boxes of the input at the patch shifted by the tap (zeros
+// outside the image). A box of C channels is 128 rows (pixels, the K index)
+// of 2C bytes in the 2C-byte swizzle: 8-row groups are 16C bytes apart and
+// the channel groups one box apart. The block's 128 x BN sum, accumulated in
+// TMEM over its patches, is added to dw with vector atomics.
 constexpr int DW_STAGES = 3;
-constexpr int DW_BOX = TC_M * 64 * 2;  // one 64-channel box of one patch
 
-template <int BN>
+template <int CA, int CB, int BN>
 struct TcDwLayout {
-  static constexpr int A_BYTES = 2 * DW_BOX;
-  static constexpr int B_BYTES = (BN / 64) * DW_BOX;
+  static constexpr int A_BOX = TC_M * CA * 2, B_BOX = TC_M * CB * 2;
+  static constexpr int A_BYTES = (128 / CA) * A_BOX;
+  static constexpr int B_BYTES = (BN / CB) * B_BOX;
   static constexpr int STAGE = A_BYTES + B_BYTES;
   static constexpr int BYTES = DW_STAGES * STAGE + (2 * DW_STAGES + 1) * 8 + 8 + 1024;
 };
 
-// MN-major operand, 128-byte swizzle: K groups of 8 rows 1024 bytes apart
-// (stride byte offset), 64-element MN groups `group_bytes` apart (leading
-// byte offset).
-__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr, uint32_t group_bytes) {
+// MN-major operand whose channel groups of C (64 or 32) elements are
+// swizzled rows of 2C bytes: 8-row K groups 16C bytes apart (stride byte
+// offset), channel groups `group_bytes` apart (leading byte offset).
+__device__ __forceinline__ uint64_t smem_desc_mn(uint32_t addr, uint32_t row_bytes, uint32_t group_bytes) {
   uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
   d |= (uint64_t)((group_bytes >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)(((8u * row_bytes) >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;
-  d |= (uint64_t)2 << 61;
+  d |= (uint64_t)(row_bytes == 128 ? 2 : 4) << 61;
   return d;
 }
 // f32 accumulator, bf16 A and B, both MN-major, M = 128, N.
@@ -324,11 +324,11 @@ __host__ __device__ constexpr uint32_t instr_desc_mn(int n) {
   return instr_desc(n) | (1u << 15) | (1u << 16);
 }
 
-template <int BN>
+template <int CA, int CB, int BN>
 __global__ void __launch_bounds__(128, 1)
     k_conv3_dw_tc(const __grid_constant__ CUtensorMap tdz, const __grid_constant__ CUtensorMap tin,
                   const TcDwArgs a) {
-  using L = TcDwLayout<BN>;
+  using L = TcDwLayout<CA, CB, BN>;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + DW_STAGES * L::STAGE);
@@ -381,11 +381,11 @@ __global__ void __launch_bounds__(128, 1)
       const int x0 = tx * TC_TW, y0 = ty * TC_TH;
       unsigned char* st = smem + s * L::STAGE;
       mbar_expect_tx(&full[s], (uint32_t)L::STAGE);
-      tma_load_4d(st, &tdz, &full[s], co0, x0, y0, img);
-      tma_load_4d(st + DW_BOX, &tdz, &full[s], co0 + 64, x0, y0, img);
 #pragma unroll
-      for (int h = 0; h < BN / 64; h++)
-        tma_load_4d(st + L::A_BYTES + h * DW_BOX, &tin, &full[s], ci0 + 64 * h, x0 + dx, y0 + dy, img);
+      for (int h = 0; h < 128 / CA; h++) tma_load_4d(st + h * L::A_BOX, &tdz, &full[s], co0 + CA * h, x0, y0, img);
+#pragma unroll
+      for (int h = 0; h < BN / CB; h++)
+        tma_load_4d(st + L::A_BYTES + h * L::B_BOX, &tin, &full[s], ci0 + CB * h, x0 + dx, y0 + dy, img);
       issued = kb + 1;
     }
     for (int kb = issued > DW_STAGES ? issued - DW_STAGES : 0; kb < issued; kb++)
@@ -402,8 +402,8 @@ __global__ void __launch_bounds__(128, 1)
       const uint32_t sa = saddr(smem + s * L::STAGE), sb = sa + L::A_BYTES;
 #pragma unroll
       for (int k = 0; k < TC_M / 16; k++)  // 16 pixels (two 8-row groups) per MMA
-        umma(tmem, smem_desc_mn(sa + 2048u * k, DW_BOX), smem_desc_mn(sb + 2048u * k, DW_BOX), idesc,
-             (kb | k) != 0);
+        umma(tmem, smem_desc_mn(sa + 32u * CA * k, 2 * CA, L::A_BOX),
+             smem_desc_mn(sb + 32u * CB * k, 2 * CB, L::B_BOX), idesc, (kb | k) != 0);
       umma_commit(&empty[s]);
     }
     umma_commit(done);
@@ -422,8 +422,7 @@ __global__ void __launch_bounds__(128, 1)
     float* row = a.dw + ((int64_t)co * 9 + tap) * a.Cin + ci0 + c;
 #pragma unroll
     for (int j = 0; j < 4; j++)
-      if (ci0 + c + 4 * j < a.Cin)
-        atomicAdd(reinterpret_cast<float4*>(row + 4 * j), make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]));
+      atomicAdd(reinterpret_cast<float4*>(row + 4 * j), make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]));
   }
   tc_fence_before();
   __syncthreads();
@@ -487,28 +486,29 @@ int launch_kc(const TcConvArgs& a, cudaStream_t s) {
   return launch<KC, 32>(a, s);
 }
 
-// A 4-D map of an NHWC bf16 tensor, box (64 channels, 16, 8, 1), 128-byte swizzle.
-bool nhwc_map(CUtensorMap* m, const bf16* base, int channels, int ld, int W, int H, int64_t batch) {
+// A 4-D map of an NHWC bf16 tensor, box (C channels, 16, 8, 1), 2C-byte swizzle.
+bool nhwc_map(CUtensorMap* m, const bf16* base, int channels, int ld, int W, int H, int64_t batch, int C) {
   const cuuint64_t px = (cuuint64_t)ld * 2;
   cuuint64_t dims[4] = {(cuuint64_t)channels, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)batch};
   cuuint64_t strides[3] = {px, px * (cuuint64_t)W, px * (cuuint64_t)W * (cuuint64_t)H};
-  cuuint32_t box[4] = {64, (cuuint32_t)TC_TW, (cuuint32_t)TC_TH, 1};
+  cuuint32_t box[4] = {(cuuint32_t)C, (cuuint32_t)TC_TW, (cuuint32_t)TC_TH, 1};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   return encoder()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(base), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, C == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int BN>
+template <int CA, int CB, int BN>
 int launch_dw(TcDwArgs a, cudaStream_t s, int sms) {
-  using L = TcDwLayout<BN>;
+  using L = TcDwLayout<CA, CB, BN>;
   if (!encoder()) return 2;
   CUtensorMap tdz, tin;
-  if (!nhwc_map(&tdz, a.dz, a.Cout, a.ld_dz, a.W, a.H, a.batch) || !nhwc_map(&tin, a.in, a.Cin, a.ld_in, a.W, a.H, a.batch))
+  if (!nhwc_map(&tdz, a.dz, a.Cout, a.ld_dz, a.W, a.H, a.batch, CA) ||
+      !nhwc_map(&tin, a.in, a.Cin, a.ld_in, a.W, a.H, a.batch, CB))
     return 1;
   static std::once_flag once;
   std::call_once(once, [] {
-    cudaFuncSetAttribute(k_conv3_dw_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
+    cudaFuncSetAttribute(k_conv3_dw_tc<CA, CB, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
   });
   a.patches = a.batch * (a.W / TC_TW) * (a.H / TC_TH);
   const int tiles = ((a.Cout + 127) / 128) * (a.Cin / BN);
@@ -519,22 +519,29 @@ int launch_dw(TcDwArgs a, cudaStream_t s, int sms) {
   if (splits < 1) splits = 1;
   a.patches_per_block = (a.patches + splits - 1) / splits;
   splits = (a.patches + a.patches_per_block - 1) / a.patches_per_block;
-  k_conv3_dw_tc<BN><<<dim3((unsigned)splits, tiles, 9), 128, L::BYTES, s>>>(tdz, tin, a);
+  k_conv3_dw_tc<CA, CB, BN><<<dim3((unsigned)splits, tiles, 9), 128, L::BYTES, s>>>(tdz, tin, a);
   return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+template <int CA>
+int launch_dw_ca(const TcDwArgs& a, cudaStream_t s, int sms) {
+  if (a.Cin % 128 == 0) return launch_dw<CA, 64, 128>(a, s, sms);
+  if (a.Cin % 64 == 0) return launch_dw<CA, 64, 64>(a, s, sms);
+  return launch_dw<CA, 32, 32>(a, s, sms);
 }
 
 }  // namespace
 
 bool conv3_dw_tc_supported(const TcDwArgs& a) {
   const auto a16 = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
-  return a.W % TC_TW == 0 && a.H % TC_TH == 0 && a.Cin % 64 == 0 && a.Cout % 64 == 0 && a.ld_in % 8 == 0 &&
+  return a.W % TC_TW == 0 && a.H % TC_TH == 0 && a.Cin % 32 == 0 && a.Cout % 32 == 0 && a.ld_in % 8 == 0 &&
          a.ld_dz % 8 == 0 && a16(a.in) && a16(a.dz) && a16(a.dw) && encoder() != nullptr;
 }
 
 int conv3_dw_tc(const TcDwArgs& a, cudaStream_t s) {
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return a.Cin % 128 == 0 ? launch_dw<128>(a, s, sms) : launch_dw<64>(a, s, sms);
+  return a.Cout % 64 == 0 ? launch_dw_ca<64>(a, s, sms) : launch_dw_ca<32>(a, s, sms);
 }
 
 bool conv3_tc_supported(const TcConvArgs& a) {

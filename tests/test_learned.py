@@ -203,8 +203,10 @@ def test_conv3_tcgen05_matches_the_oracle_and_mma_sync(conv_path, cin, cout, B, 
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cin,cout,B,H,W", [(64, 64, 1, 8, 16), (64, 128, 2, 16, 32), (192, 64, 1, 16, 16),
-                                            (128, 384, 1, 8, 16), (256, 256, 2, 32, 32), (384, 128, 2, 64, 64)],
+@pytest.mark.parametrize("cin,cout,B,H,W", [(64, 64, 1, 8, 16), (32, 32, 1, 8, 16), (64, 128, 2, 16, 32),
+                                            (192, 64, 1, 16, 16), (96, 32, 1, 16, 16), (32, 64, 2, 16, 32),
+                                            (64, 32, 1, 8, 16), (128, 384, 1, 8, 16), (256, 256, 2, 32, 32),
+                                            (384, 128, 2, 64, 64)],
                          ids=lambda v: str(v))
 def test_conv3_weight_grad_tcgen05_matches_the_oracle_and_mma_sync(conv_path, cin, cout, B, H, W):
     """The tcgen05 weight gradient (MN-major TMA operands, K = pixels, TMEM
