@@ -41,7 +41,8 @@ int32_t rang_b200_nn_conv3(const void* in, int64_t ld_in, const void* w, const f
 
 /* dw[co, tap, ci] += sum_p dz[p, co] in[p + (ky - 1, kx - 1), ci] and, when
  * dbias is non-null, dbias[co] += sum_p dz[p, co]. Tensor cores: tcgen05
- * where width is a multiple of 16 and height of 8 (rang_b200_nn_set_conv_path). */
+ * where width is a multiple of 16, height of 8 and cout of 64
+ * (rang_b200_nn_set_conv_path). */
 int32_t rang_b200_nn_conv3_weight_grad(const void* in, int64_t ld_in, const void* dz, int64_t ld_dz, float* dw,
                                        float* dbias, int64_t batch, int32_t height, int32_t width, int32_t cin,
                                        int32_t cout, void* stream);

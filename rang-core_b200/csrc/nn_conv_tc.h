@@ -34,7 +34,8 @@ struct TcDwArgs {
 };
 
 // Whether the weight gradient's shapes fit the tcgen05 kernel: W a multiple
-// of 16, H of 8, channels of 32, pixel strides of 8, 16-byte aligned tensors.
+// of 16, H of 8, input channels of 32, output channels of 64, pixel strides
+// of 8, 16-byte aligned tensors.
 bool conv3_dw_tc_supported(const TcDwArgs& a);
 // dw += the weight gradient on s; 0, 1 (the tensor maps were refused) or 2.
 int conv3_dw_tc(const TcDwArgs& a, cudaStream_t s);

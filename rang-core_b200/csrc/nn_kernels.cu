@@ -663,12 +663,6 @@ int32_t rang_b200_nn_conv3_weight_grad(const void* in, int64_t ld_in, const void
   if (!in || !dz || !dw || batch <= 0 || height <= 0 || width <= 0 || cin <= 0 || cout <= 0) return 1;
   if (cin % 32 || cout % 32 || ld_in < cin || ld_dz < cout || ld_in % 8 || ld_dz % 8 || cout > 512) return 1;
   if (!aligned16(in) || !aligned16(dz) || ld_in > INT32_MAX || ld_dz > INT32_MAX) return 1;
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(k_conv3_dw<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dw_smem_bytes<64>());
-    cudaFuncSetAttribute(k_conv3_dw<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, dw_smem_bytes<32>());
-    configured = true;
-  }
   if (g_conv_path.load() == 0) {
     const TcDwArgs t{(const bf16*)in, (const bf16*)dz, dw, batch, 0, 0, height, width, (int)ld_in, (int)ld_dz,
                      cin, cout};
@@ -684,6 +678,9 @@ int32_t rang_b200_nn_conv3_weight_grad(const void* in, int64_t ld_in, const void
       return launched();
     }
   }
+  // per call: the attribute belongs to the current device's context
+  cudaFuncSetAttribute(k_conv3_dw<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dw_smem_bytes<64>());
+  cudaFuncSetAttribute(k_conv3_dw<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, dw_smem_bytes<32>());
   DwArgs a{(const bf16*)in, (const bf16*)dz, dw, batch * height * width, 0, height, width, (int)ld_in, (int)ld_dz,
            cin, cout};
   const int tm = cout % 64 == 0 ? 64 : 32;

@@ -210,8 +210,9 @@ def test_conv3_tcgen05_matches_the_oracle_and_mma_sync(conv_path, cin, cout, B, 
                          ids=lambda v: str(v))
 def test_conv3_weight_grad_tcgen05_matches_the_oracle_and_mma_sync(conv_path, cin, cout, B, H, W):
     """The tcgen05 weight gradient (MN-major TMA operands, K = pixels, TMEM
-    accumulator, vector atomics into dw): within 1e-5 of the FP64 oracle and
-    of the mma.sync kernel, accumulating, with no wait given up."""
+    accumulator, vector atomics into dw) where cout is a multiple of 64, the
+    mma.sync kernel for the 32-output-channel cases: within 1e-5 of the FP64
+    oracle and of the mma.sync kernel, accumulating, with no wait given up."""
     import torch
 
     from rang import learned
