@@ -203,6 +203,17 @@ def max_over_ranks(value, dist, device):
     return float(t.item())
 
 
+def all_ranks(flag, dist, device):
+    """Whether `flag` holds on every rank (a collective: every rank calls it)."""
+    if dist is None:
+        return bool(flag)
+    import torch
+
+    t = torch.tensor([1 if flag else 0], device=device, dtype=torch.int32)
+    dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    return bool(t.item())
+
+
 def job_rate(world, units_per_rank, steps, seconds):
     """Whole-job throughput in millions of units per second: every replica
     processes `units_per_rank` per step, timed as the slowest rank."""
@@ -741,15 +752,29 @@ def run_b200(args):
 
     # End to end through the C ABI with pinned host arrays.
     e2e = None
+    pinned = None
+    reason = "pinned host memory refused on another rank"
     if not args.no_e2e:
+        # Each rank pins about 18 GB of host memory; if any rank cannot, every
+        # rank skips this leg together (its timing is a collective).
+        try:
+            pinned = [torch.empty((nrow, nchan), dtype=torch.complex64, pin_memory=True),
+                      torch.empty((nrow, nchan), dtype=torch.uint8, pin_memory=True),
+                      torch.empty((nrow, nchan), dtype=torch.complex64, pin_memory=True),
+                      torch.empty((npix, npix), dtype=torch.float32, pin_memory=True)]
+        except RuntimeError as exc:
+            pinned = None
+            reason = f"pinned host memory: {exc}".splitlines()[0][:200]
+        if not all_ranks(pinned is not None, dist, dev):
+            pinned = None
+            e2e = {"unavailable": reason}
+    if pinned is not None:
         from rang.core_wgridder import options_list
 
-        vis_h = torch.empty((nrow, nchan), dtype=torch.complex64, pin_memory=True)
+        vis_h, mask_h, out_h, dirty_h = pinned
+        pinned = None
         vis_h.copy_(vis)
-        mask_h = torch.empty((nrow, nchan), dtype=torch.uint8, pin_memory=True)
         mask_h.copy_(mask)
-        out_h = torch.empty((nrow, nchan), dtype=torch.complex64, pin_memory=True)
-        dirty_h = torch.empty((npix, npix), dtype=torch.float32, pin_memory=True)
         vis_np, mask_np, out_np, dirty_np = vis_h.numpy(), mask_h.numpy(), out_h.numpy(), dirty_h.numpy()
         opts = options_list(npix, npix, cell, cell, eps, {})
         info = np.empty(14)

@@ -43,7 +43,10 @@ def _rank(rank, world, port, out):
         ms = 100.0 + 25.0 * r  # the slower replica sets the job's time
         slowest = bench.max_over_ranks(ms, dist, torch.device("cpu"))
         rate = bench.job_rate(w, 1_000_000, 3, slowest / 1e3)
-        out.put((r, w, l, slowest, rate))
+        # a leg that needs every rank (pinned host memory): one refusal skips it everywhere
+        both = bench.all_ranks(True, dist, torch.device("cpu"))
+        one_refused = bench.all_ranks(r != 1, dist, torch.device("cpu"))
+        out.put((r, w, l, slowest, rate, both, one_refused))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -66,11 +69,13 @@ def test_two_gloo_replicas_report_the_slowest_rank():
     assert all(r[3] == 125.0 for r in results)
     # 2 replicas x 1 M units x 3 steps in 0.125 s
     assert all(r[4] == pytest.approx(48.0) for r in results)
+    assert all(r[5] is True and r[6] is False for r in results)
 
 
 def test_one_process_needs_no_collective():
     bench = _bench()
     assert bench.max_over_ranks(7.5, None, None) == 7.5
+    assert bench.all_ranks(True, None, None) and not bench.all_ranks(False, None, None)
     assert bench.job_rate(1, 2_000_000, 2, 0.5) == pytest.approx(8.0)
 
 
