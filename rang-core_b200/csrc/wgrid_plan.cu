@@ -60,7 +60,22 @@ struct ScanOut {
   unsigned long long finite;   // of which with a non-NaN |w|
   unsigned long long lo_bits;  // min |w| as the bits of a non-negative double
   unsigned long long hi_bits;  // max |w|
+  unsigned long long u_bits;   // max |u| in metres over all rows (k_umax); +inf if any is not finite
 };
+
+// The largest |u| (metres) over all rows, +inf when one is not finite: times
+// the largest f / c it bounds every visibility's |u| in wavelengths, which
+// is what the touched-row pruning needs (rows, not visibilities: cheaper
+// than the scan, and flagged rows only widen the bound).
+__global__ void k_umax(uint32_t nrow, const double* __restrict__ uvw, ScanOut* out) {
+  double m = 0.0;
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nrow; r += (uint64_t)gridDim.x * blockDim.x) {
+    const double a = fabs(uvw[3 * r]);
+    m = isfinite(a) ? fmax(m, a) : __longlong_as_double(0x7ff0000000000000ll);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&out->u_bits, (unsigned long long)__double_as_longlong(m));
+}
 
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -102,6 +117,7 @@ __global__ void k_scan_init(ScanOut* so) {
   so->finite = 0;
   so->lo_bits = (unsigned long long)__double_as_longlong(1e300);
   so->hi_bits = 0;
+  so->u_bits = 0;
 }
 
 // The scan gives each warp runs of 32 x SCAN_ROUNDS consecutive visibilities,
@@ -130,7 +146,7 @@ struct RoundStep {
 // scan (wgridder.rs:1051-1077): the count is exact and min/max are order
 // independent, so the result is the reference's bit for bit.
 template <class T>
-__global__ void k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__ uvw,
+__global__ void __launch_bounds__(256, 8) k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__ uvw,
                        const double* __restrict__ foc, double fw, Inputs in, int with_vis, ScanOut* out) {
   const uint64_t n = (uint64_t)nrow * nchan;
   const uint64_t run = 32ull * SCAN_ROUNDS;
@@ -1488,6 +1504,44 @@ void fft_rows(FftPair& f, cplx<T>* plane, int dir, cudaStream_t s) {
   check_fft(FftTraits<T>::exec(f.rows, plane, dir), "rows");
 }
 
+// Row transforms (length nv) of `batch` consecutive rows, per device, kept
+// for the life of the process; batches are rounded up to 64 rows so that few
+// plans exist.
+template <class T>
+FftPair& fft_row_plan(int nv, int batch) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int>, std::unique_ptr<FftPair>> cache;
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "device");
+  std::lock_guard<std::mutex> lock(mu);
+  auto& slot = cache[std::make_tuple(dev, nv, batch)];
+  if (!slot) {
+    auto p = std::make_unique<FftPair>();
+    int n_row[1] = {nv};
+    check_fft(cufftPlanMany(&p->rows, 1, n_row, nullptr, 1, nv, nullptr, 1, nv, FftTraits<T>::type, batch),
+              "row plan");
+    slot = std::move(p);
+  }
+  return *slot;
+}
+
+// The v transforms of the rows footprints can touch: storage rows
+// [0, urows) and [nu - urows, nu) (urows rounded up to 64), or every row
+// when urows is 0.
+template <class T>
+void fft_touched_rows(FftPair& all, cplx<T>* plane, int nu, int nv, int urows, int dir, cudaStream_t s) {
+  const int b = urows > 0 ? (urows + 63) / 64 * 64 : 0;
+  if (b == 0 || 2 * b >= nu) {
+    fft_rows<T>(all, plane, dir, s);
+    return;
+  }
+  FftPair& f = fft_row_plan<T>(nv, b);
+  std::lock_guard<std::mutex> lock(f.mu);
+  check_fft(cufftSetStream(f.rows, s), "stream");
+  check_fft(FftTraits<T>::exec(f.rows, plane, dir), "rows");
+  check_fft(FftTraits<T>::exec(f.rows, plane + (size_t)(nu - b) * nv, dir), "rows");
+}
+
 template <class T, int S>
 void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, const Inputs& in, int mode,
                  const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
@@ -1722,6 +1776,7 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
       StageTimer timer_(ST_SCAN, s);
       k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw_.as<double>(),
                                                     foc_.as<double>(), fw, act, with_vis ? 1 : 0, so.as<ScanOut>());
+      k_umax<<<blocks_for(nrow, 256, 148u * 8u), 256, 0, s>>>((uint32_t)nrow, uvw_.as<double>(), so.as<ScanOut>());
     }
     check_cuda(cudaGetLastError(), "scan kernel");
   }
@@ -1743,7 +1798,27 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
     return;
   }
   make_geom<T>(o, nrow, nchan, nvis_, wmin_d, wmax_d, r_l_, r_m_, g_, info_, kernel_);
+  double umax_d = 0.0;  // metres; times the largest f / c
+  std::memcpy(&umax_d, &r.u_bits, sizeof(double));
+  urows_ = touched_rows(umax_d * *std::max_element(foc.begin(), foc.end()), wmax_d);
   build_layout(act, with_vis, s);
+}
+
+// The grid rows footprints can reach, from the scan's largest |u| and |w|
+// (wavelengths): the recentred coordinate is u + r_l w, at most
+// |u|max + |r_l| |w|max; its cell offset from the centre is that times
+// pixsize_x * nu, and a footprint spans the support around it. Rows beyond
+// a margin of a tile plus the support are left untransformed along v (they
+// are zero when gridding, and nothing reads them when degridding): the
+// reference's touched-row pruning (grid_to_image, wgridder.rs:2320-2399).
+template <class T>
+int Plan<T>::touched_rows(double umax, double wmax) const {
+  if (!(umax >= 0.0) || !std::isfinite(umax) || !(wmax >= 0.0) || !std::isfinite(wmax)) return 0;
+  const double ext = (umax + std::fabs(r_l_) * wmax) * g_.pixsize_x;  // in cycles of the grid
+  if (!(ext < 0.4)) return 0;  // near the aliasing limit: transform every row
+  const double rows = std::ceil(ext * g_.nu) + 2.0 * g_.supp + 64.0;
+  if (2.0 * rows >= 0.9 * g_.nu) return 0;
+  return (int)rows;
 }
 
 template <class T>
@@ -1950,7 +2025,7 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
     for (int p = 0; p < n; p++) {
       cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
       StageTimer timer_(ST_FFT, s, 3);
-      fft_rows<T>(fft, pl, CUFFT_INVERSE, s);
+      fft_touched_rows<T>(fft, pl, g_.nu, g_.nv, urows_, CUFFT_INVERSE, s);
       fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_INVERSE, s);
     }
     bool first = pg0 == 0, last = pg0 + n >= nplanes;
@@ -2006,7 +2081,7 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
       {
         StageTimer timer_(ST_FFT, s, 3);
         fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_FORWARD, s);
-        fft_rows<T>(fft, pl, CUFFT_FORWARD, s);
+        fft_touched_rows<T>(fft, pl, g_.nu, g_.nv, urows_, CUFFT_FORWARD, s);
       }
     }
     bool first = pg0 == 0, last = pg0 + n >= nplanes;

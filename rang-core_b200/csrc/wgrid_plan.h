@@ -110,6 +110,7 @@ class Plan {
  private:
   void build_layout(const Inputs& act, bool with_vis, cudaStream_t s);
   void corrections(cudaStream_t s);
+  int touched_rows(double umax, double wmax) const;
   size_t plane_group(size_t cell_bytes) const;
 
   WgridderOptions o_;
@@ -133,6 +134,9 @@ class Plan {
   std::vector<uint64_t> chunk_sorted_;  // nchunk_ + 1 offsets into the sorted order
   std::vector<uint32_t> chunk_tasks_;   // nchunk_ + 1 offsets into the task list
   unsigned long long scan_[4] = {0, 0, 0, 0};  // count, finite count, |w| min and max bits
+  // Grid rows (u) that footprints can touch: storage rows [0, urows_) and
+  // [nu - urows_, nu); 0 means all rows (the v transforms run on these only).
+  int urows_ = 0;
 };
 
 // How single-precision gridding accumulates footprints: split-precision

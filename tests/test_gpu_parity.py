@@ -155,6 +155,34 @@ def test_options_match_oracle(cw, opts, single):
 
 
 @pytest.mark.parametrize("single", [True, False])
+@pytest.mark.parametrize("opts", [{}, {"center_x": 0.01, "center_y": -0.02}, {"flip_u": True, "center_x": -0.005}],
+                         ids=["centred", "shifted", "flipped-shifted"])
+def test_touched_row_pruning_matches_oracle(cw, opts, single):
+    """Small pixels (0.5 arcsec, 256^2) against baselines up to 41 k
+    wavelengths: the footprints reach a tenth of the grid's width on either
+    side of the centre, so the v transforms run on about two thirds of the
+    rows (with the recentring term |r_l| |w| in the bound). Both directions
+    equal the oracle, which transforms every row."""
+    uvw, freq = meerkat_like(nant=32, ntime=16, nchan=16, seed=4)
+    rng = np.random.default_rng(21)
+    shape = (uvw.shape[0], freq.size)
+    vis = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    mask = (rng.uniform(size=shape) > 0.1).astype(np.uint8)
+    if single:
+        vis = vis.astype(np.complex64)
+    nx = ny = 256
+    dx = 0.5 * np.pi / 648000.0
+    eps = 1e-5 if single else 1e-10
+    kw = dict(uvw=uvw, freq=freq, mask=mask, pixsize_x=dx, pixsize_y=dx, epsilon=eps, **opts)
+    d, info = cw.vis2dirty(vis=vis, npix_x=nx, npix_y=ny, return_info=True, **kw)
+    od, oinfo = oracle.vis2dirty(vis=vis, npix_x=nx, npix_y=ny, return_info=True, **kw)
+    _info_equal(info, oinfo)
+    assert rel_linf(d, od) < TOL[single]
+    x = rng.standard_normal((nx, ny)).astype(np.float32 if single else np.float64)
+    assert rel_linf(cw.dirty2vis(dirty=x, **kw), oracle.dirty2vis(dirty=x, **kw)) < TOL[single]
+
+
+@pytest.mark.parametrize("single", [True, False])
 def test_binning_is_bit_exact(cw, single):
     """iu0, iv0, tile and first plane of every visibility equal the oracle's
     (the reference's index arithmetic), and the GPU's order is the oracle's
