@@ -1383,6 +1383,42 @@ __global__ void k_project(const __grid_constant__ Geom<T> g, const cplx<T>* __re
   }
 }
 
+// k_project on the transposed columns: plane p's column of image column j is
+// t[(p - pg0) * ny + j][.]. Consecutive threads take consecutive image rows i,
+// so the reads of t are contiguous.
+template <class T>
+__global__ void k_project_t(const __grid_constant__ Geom<T> g, const cplx<T>* __restrict__ t, int pg0, int npg,
+                            T* __restrict__ acc, int first, int last, const double* __restrict__ corr,
+                            const double* __restrict__ cfu, const double* __restrict__ cfv, T* __restrict__ out) {
+  uint64_t npix = (uint64_t)g.nx * g.ny;
+  for (uint64_t qq = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; qq < npix; qq += (uint64_t)gridDim.x * blockDim.x) {
+    int j = (int)(qq / g.nx), i = (int)(qq - (uint64_t)j * g.nx);
+    uint64_t q = (uint64_t)i * g.ny + j;
+    int ix = (g.nu - g.nx / 2 + i) % g.nu;
+    T a = first ? (T)0 : acc[q];
+    double s = g.do_wgridding ? screen_arg(g, i, j) : 0.0;
+    for (int p = pg0; p < pg0 + npg; p++) {
+      cplx<T> gv = t[((size_t)(p - pg0) * g.ny + j) * g.nu + ix];
+      T term;
+      if (g.do_wgridding) {
+        cplx<T> ph = screen<T>(g, s, p, true);
+        term = gv.re * ph.re - gv.im * ph.im;
+      } else {
+        term = gv.re;
+      }
+      a = a + term;
+    }
+    if (!last) {
+      acc[q] = a;
+    } else if (g.do_wgridding) {
+      out[q] = a * (T)corr[q];
+    } else {
+      int iu = g.nx / 2 - min(i, g.nx - i), iv = g.ny / 2 - min(j, g.ny - j);
+      out[q] = (T)((double)a * cfu[iu] * cfv[iv]);
+    }
+  }
+}
+
 // The corrected image of a degridding call (wgridder.rs:3064-3091).
 template <class T>
 __global__ void k_correct_input(const __grid_constant__ Geom<T> g, const T* __restrict__ dirty,
@@ -1418,6 +1454,70 @@ __global__ void k_place(const __grid_constant__ Geom<T> g, const T* __restrict__
       v = {d, (T)0};
     }
     grid[(size_t)ix * g.nv + jx] = v;
+  }
+}
+
+// The u transforms run on the image columns transposed: t[j][u] holds column
+// jx(j) = (nv - ny/2 + j) mod nv of a plane, so that each is one contiguous
+// length-nu transform (a single cuFFT pass, where the strided columns took
+// four). `rows` is the touched-row count of fft_touched_rows (0: all rows):
+// the other rows are zero after gridding and are written as zeros unread.
+template <class T>
+__global__ void k_cols_to_t(const __grid_constant__ Geom<T> g, const cplx<T>* __restrict__ plane, int rows,
+                            cplx<T>* __restrict__ t) {
+  __shared__ cplx<T> tile[32][33];
+  const int u0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {  // plane rows: consecutive j
+    const int u = u0 + k, j = j0 + threadIdx.x;
+    cplx<T> v = {(T)0, (T)0};
+    if (u < g.nu && j < g.ny && (rows == 0 || u < rows || u >= g.nu - rows))
+      v = plane[(size_t)u * g.nv + (g.nv - g.ny / 2 + j) % g.nv];
+    tile[k][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {  // t rows: consecutive u
+    const int j = j0 + k, u = u0 + threadIdx.x;
+    if (u < g.nu && j < g.ny) t[(size_t)j * g.nu + u] = tile[threadIdx.x][k];
+  }
+}
+
+// The inverse of k_cols_to_t for the rows the degridder reads (`rows` as
+// there): plane[u][jx(j)] = t[j][u].
+template <class T>
+__global__ void k_t_to_cols(const __grid_constant__ Geom<T> g, const cplx<T>* __restrict__ t, int rows,
+                            cplx<T>* __restrict__ plane) {
+  __shared__ cplx<T> tile[32][33];
+  const int u0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {  // t rows: consecutive u
+    const int j = j0 + k, u = u0 + threadIdx.x;
+    tile[k][threadIdx.x] = (u < g.nu && j < g.ny) ? t[(size_t)j * g.nu + u] : cplx<T>{(T)0, (T)0};
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {  // plane rows: consecutive j
+    const int u = u0 + k, j = j0 + threadIdx.x;
+    if (u < g.nu && j < g.ny && (rows == 0 || u < rows || u >= g.nu - rows))
+      plane[(size_t)u * g.nv + (g.nv - g.ny / 2 + j) % g.nv] = tile[threadIdx.x][k];
+  }
+}
+
+// k_place into the transposed columns: t[j][ix] (t zeroed first). Consecutive
+// threads take consecutive image rows i, so that the writes are contiguous.
+template <class T>
+__global__ void k_place_t(const __grid_constant__ Geom<T> g, const T* __restrict__ img, int p,
+                          cplx<T>* __restrict__ t) {
+  uint64_t npix = (uint64_t)g.nx * g.ny;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < npix; q += (uint64_t)gridDim.x * blockDim.x) {
+    int j = (int)(q / g.nx), i = (int)(q - (uint64_t)j * g.nx);
+    int ix = (g.nu - g.nx / 2 + i) % g.nu;
+    T d = img[(size_t)i * g.ny + j];
+    cplx<T> v;
+    if (g.do_wgridding) {
+      cplx<T> ph = screen<T>(g, screen_arg(g, i, j), p, false);
+      v = {d * ph.re, d * ph.im};
+    } else {
+      v = {d, (T)0};
+    }
+    t[(size_t)j * g.nu + ix] = v;
   }
 }
 
@@ -1525,13 +1625,18 @@ FftPair& fft_row_plan(int nv, int batch) {
   return *slot;
 }
 
-// The v transforms of the rows footprints can touch: storage rows
-// [0, urows) and [nu - urows, nu) (urows rounded up to 64), or every row
-// when urows is 0.
-template <class T>
-void fft_touched_rows(FftPair& all, cplx<T>* plane, int nu, int nv, int urows, int dir, cudaStream_t s) {
+// The touched rows as transformed: urows rounded up to 64, or 0 (every row)
+// when that would cover the plane.
+int touched_row_count(int urows, int nu) {
   const int b = urows > 0 ? (urows + 63) / 64 * 64 : 0;
-  if (b == 0 || 2 * b >= nu) {
+  return (b == 0 || 2 * b >= nu) ? 0 : b;
+}
+
+// The v transforms of the rows footprints can touch: storage rows [0, b)
+// and [nu - b, nu), b = touched_row_count (every row when b is 0).
+template <class T>
+void fft_touched_rows(FftPair& all, cplx<T>* plane, int nu, int nv, int b, int dir, cudaStream_t s) {
+  if (b == 0) {
     fft_rows<T>(all, plane, dir, s);
     return;
   }
@@ -1967,7 +2072,7 @@ void Plan<T>::corrections(cudaStream_t s) {
 template <class T>
 size_t Plan<T>::plane_group(size_t cell_bytes) const {
   size_t nplanes = (size_t)std::max(g_.nplanes, 1);
-  size_t plane = (size_t)g_.nu * g_.nv * cell_bytes;
+  size_t plane = ((size_t)g_.nu * g_.nv + (size_t)g_.ny * g_.nu) * cell_bytes;  // the plane and its columns, transposed
   size_t freeb = 0, total = 0;
   check_cuda(cudaMemGetInfo(&freeb, &total), "memory info");
   size_t budget = std::min<size_t>(freeb / 2, (size_t)64 << 30);
@@ -1987,6 +2092,8 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
   const size_t group = plane_group(cell);
   const size_t plane = (size_t)g_.nu * g_.nv;
   DevBuf grids(group * plane * cell, s);
+  const size_t tplane = (size_t)g_.ny * g_.nu;  // a plane's image columns, transposed
+  DevBuf cols(group * tplane * cell, s);
   DevBuf acc(group < nplanes ? npix * sizeof(T) : 0, s);
   FftPair& fft = fft_plans<T>(g_.nu, g_.nv, g_.ny);
   const int gmax = std::min<int>(max_window_planes(g_.L, sizeof(cplx<T>)), (int)std::min<size_t>(nplanes, 64));
@@ -2022,18 +2129,26 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
       with_supp_float(g_.supp, run);
     else
       with_supp_double(g_.supp, run);
+    const int rows = touched_row_count(urows_, g_.nu);
+    const dim3 tgrid((unsigned)((g_.nu + 31) / 32), (unsigned)((g_.ny + 31) / 32)), tblock(32, 8);
+    FftPair& tf = fft_row_plan<T>(g_.nu, g_.ny);  // the image columns, transposed: ny transforms of length nu
     for (int p = 0; p < n; p++) {
       cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
+      cplx<T>* tp = cols.as<cplx<T>>() + (size_t)p * tplane;
       StageTimer timer_(ST_FFT, s, 3);
-      fft_touched_rows<T>(fft, pl, g_.nu, g_.nv, urows_, CUFFT_INVERSE, s);
-      fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_INVERSE, s);
+      fft_touched_rows<T>(fft, pl, g_.nu, g_.nv, rows, CUFFT_INVERSE, s);
+      k_cols_to_t<T><<<tgrid, tblock, 0, s>>>(g_, pl, rows, tp);
+      check_cuda(cudaGetLastError(), "transpose");
+      std::lock_guard<std::mutex> lock(tf.mu);
+      check_fft(cufftSetStream(tf.rows, s), "stream");
+      check_fft(FftTraits<T>::exec(tf.rows, tp, CUFFT_INVERSE), "columns");
     }
     bool first = pg0 == 0, last = pg0 + n >= nplanes;
     {
       StageTimer timer_(ST_PROJECT, s);
-      k_project<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, grids.as<cplx<T>>(), (int)pg0, n, acc.as<T>(), first,
-                                                         last, g_.do_wgridding ? corr + nu2 + nv2 : nullptr, corr,
-                                                         corr + nu2, image);
+      k_project_t<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, cols.as<cplx<T>>(), (int)pg0, n, acc.as<T>(), first,
+                                                           last, g_.do_wgridding ? corr + nu2 + nv2 : nullptr, corr,
+                                                           corr + nu2, image);
     }
     check_cuda(cudaGetLastError(), "project");
   }
@@ -2068,20 +2183,32 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
       std::max<int>(1, (int)(SMEM_WINDOW_BYTES / ((size_t)g_.L * Lp * sizeof(cplx<T>)))),
       (int)std::min<size_t>(nplanes, 64));
   const int smem = gmax * g_.L * Lp * (int)sizeof(cplx<T>);
+  const int rows = touched_row_count(urows_, g_.nu);
+  const size_t tplane = (size_t)g_.ny * g_.nu;  // a plane's image columns, transposed
+  DevBuf cols(tplane * cell, s);
+  const dim3 tgrid((unsigned)((g_.nu + 31) / 32), (unsigned)((g_.ny + 31) / 32)), tblock(32, 8);
+  FftPair& tf = fft_row_plan<T>(g_.nu, g_.ny);
   for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
     int n = (int)std::min(group, nplanes - pg0);
     check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
     for (int p = 0; p < n; p++) {
       cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
+      check_cuda(cudaMemsetAsync(cols.get(), 0, tplane * cell, s), "memset");
       {
         StageTimer timer_(ST_PLACE, s);
-        k_place<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, img.as<T>(), (int)pg0 + p, pl);
+        k_place_t<T><<<blocks_for(npix, 256), 256, 0, s>>>(g_, img.as<T>(), (int)pg0 + p, cols.as<cplx<T>>());
       }
       check_cuda(cudaGetLastError(), "place");
       {
         StageTimer timer_(ST_FFT, s, 3);
-        fft_cols<T>(fft, pl, g_.nv, g_.ny, CUFFT_FORWARD, s);
-        fft_touched_rows<T>(fft, pl, g_.nu, g_.nv, urows_, CUFFT_FORWARD, s);
+        {
+          std::lock_guard<std::mutex> lock(tf.mu);
+          check_fft(cufftSetStream(tf.rows, s), "stream");
+          check_fft(FftTraits<T>::exec(tf.rows, cols.as<cplx<T>>(), CUFFT_FORWARD), "columns");
+        }
+        k_t_to_cols<T><<<tgrid, tblock, 0, s>>>(g_, cols.as<cplx<T>>(), rows, pl);
+        check_cuda(cudaGetLastError(), "transpose");
+        fft_touched_rows<T>(fft, pl, g_.nu, g_.nv, rows, CUFFT_FORWARD, s);
       }
     }
     bool first = pg0 == 0, last = pg0 + n >= nplanes;
