@@ -2080,6 +2080,23 @@ size_t Plan<T>::plane_group(size_t cell_bytes) const {
   return std::min(group, nplanes);
 }
 
+// Zeroes the rows of n planes that the gridder writes and the transforms
+// read: every row when `rows` is 0, else storage rows [0, rows) and
+// [nu - rows, nu) of each plane (the others are never read).
+template <class T>
+void zero_touched(cplx<T>* grids, int n, const Geom<T>& g, int rows, cudaStream_t s) {
+  const size_t plane = (size_t)g.nu * g.nv, row = (size_t)g.nv * sizeof(cplx<T>);
+  if (rows == 0) {
+    check_cuda(cudaMemsetAsync(grids, 0, (size_t)n * plane * sizeof(cplx<T>), s), "memset");
+    return;
+  }
+  for (int p = 0; p < n; p++) {
+    cplx<T>* pl = grids + (size_t)p * plane;
+    check_cuda(cudaMemsetAsync(pl, 0, (size_t)rows * row, s), "memset");
+    check_cuda(cudaMemsetAsync(pl + (size_t)(g.nu - rows) * g.nv, 0, (size_t)rows * row, s), "memset");
+  }
+}
+
 template <class T>
 void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready) {
   size_t npix = (size_t)o_.nx * o_.ny;
@@ -2102,7 +2119,7 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
   const size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
   for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
     int n = (int)std::min(group, nplanes - pg0);
-    check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
+    zero_touched<T>(grids.as<cplx<T>>(), n, g_, touched_row_count(urows_, g_.nu), s);
     auto run = [&](auto S) {
       constexpr int SV = decltype(S)::value;
       for (int c = 0; c < nchunk_; c++) {  // row chunk c once its rows are on the device
@@ -2190,7 +2207,7 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
   FftPair& tf = fft_row_plan<T>(g_.nu, g_.ny);
   for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
     int n = (int)std::min(group, nplanes - pg0);
-    check_cuda(cudaMemsetAsync(grids.get(), 0, (size_t)n * plane * cell, s), "memset");
+    zero_touched<T>(grids.as<cplx<T>>(), n, g_, rows, s);
     for (int p = 0; p < n; p++) {
       cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
       check_cuda(cudaMemsetAsync(cols.get(), 0, tplane * cell, s), "memset");
