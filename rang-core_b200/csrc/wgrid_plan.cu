@@ -402,22 +402,34 @@ __device__ __forceinline__ uint32_t plane_at(const uint32_t* starts, uint64_t b0
 __global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t stride, uint32_t nsub, uint32_t ntiles,
                             uint32_t tiles_per_chunk, const uint32_t* __restrict__ off, Task* __restrict__ tasks,
                             uint32_t* __restrict__ ntotal) {
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ntiles) return;
-  uint64_t b0 = (uint64_t)t * stride;
-  uint32_t s = starts[b0], e = starts[b0 + stride];
-  uint32_t q0 = off[t];
-  for (uint32_t k0 = s, q = q0; k0 < e; k0 += TASK_CHUNK, q++) {
-    uint32_t k1 = min(k0 + TASK_CHUNK, e);
-    Task tk;
-    tk.tile = t % tiles_per_chunk;
-    tk.k0 = k0;
-    tk.k1 = k1;
-    tk.plo = (uint16_t)plane_at(starts, b0, stride, nsub, k0);
-    tk.phi = (uint16_t)plane_at(starts, b0, stride, nsub, k1 - 1);
-    tasks[q] = tk;
+  // One thread per task: task q belongs to the last tile t with off[t] <= q
+  // (that tile has at least one task, as off[t + 1] > q), and is its
+  // (q - off[t])-th run of at most TASK_CHUNK visibilities. A dense tile's
+  // many tasks are thus emitted in parallel.
+  const uint32_t total = off[ntiles];
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q == 0) *ntotal = total;
+  if (q >= total) return;
+  uint32_t lo = 0, hi = ntiles - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= q)
+      lo = mid;
+    else
+      hi = mid - 1;
   }
-  if (t == ntiles - 1) *ntotal = off[ntiles];
+  const uint32_t t = lo;
+  const uint64_t b0 = (uint64_t)t * stride;
+  const uint32_t e = starts[b0 + stride];
+  const uint32_t k0 = starts[b0] + (q - off[t]) * TASK_CHUNK;
+  const uint32_t k1 = min(k0 + TASK_CHUNK, e);
+  Task tk;
+  tk.tile = t % tiles_per_chunk;
+  tk.k0 = k0;
+  tk.k1 = k1;
+  tk.plo = (uint16_t)plane_at(starts, b0, stride, nsub, k0);
+  tk.phi = (uint16_t)plane_at(starts, b0, stride, nsub, k1 - 1);
+  tasks[q] = tk;
 }
 
 // ------------------------------------------------------------------ gridding
@@ -1973,7 +1985,7 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
   ntasks_.alloc(4, s);
   {
     StageTimer timer_(ST_TASKS, s);
-    k_task_emit<<<(unsigned)((nvt + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(),
+    k_task_emit<<<(unsigned)((max_tasks_ + 255) / 256), 256, 0, s>>>(starts_.as<uint32_t>(),
                                                               (uint32_t)(g_.nbuckets * g_.nsub), (uint32_t)g_.nsub,
                                                               (uint32_t)nvt, (uint32_t)ntiles_, ntask.as<uint32_t>(),
                                                               tasks_.as<Task>(), ntasks_.as<uint32_t>());
