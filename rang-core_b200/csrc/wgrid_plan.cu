@@ -723,11 +723,6 @@ struct TcSlots {
   }
 };
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
 // x = hi + lo with hi rounded to TF32 (to nearest, ties away; a carry out of
 // the mantissa moves into the exponent as rounding requires); lo is exact in
 // FP32 and the tensor core reads its leading TF32 bits.
