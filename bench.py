@@ -528,7 +528,7 @@ def run_msv4(threads=None):
     coordinates), then read back: the chunks decoded on all host threads,
     the rows in the reference's layout, Stokes I on the GPU and vis2dirty
     (1024^2 at 1.5 arcsec, epsilon 1e-5) through the C ABI, each timed."""
-    from rang import core_wgridder, msv4
+    from rang import gridder, msv4
 
     wl = synth.WORKLOADS["ms2dirty 16.5M vis 1024^2"]
     ntime, nchan, nant = wl["ntime"], wl["nchan"], 64
@@ -564,7 +564,7 @@ def run_msv4(threads=None):
         t_stokes = time.perf_counter() - t0
         cell = wl["cell_arcsec"] * synth.ARCSEC
         t0 = time.perf_counter()
-        dirty = core_wgridder.vis2dirty(uvw=g["uvw"], freq=g["freq"], vis=g["vis"], wgt=g["wgt"], mask=g["mask"],
+        dirty = gridder.vis2dirty(uvw=g["uvw"], freq=g["freq"], vis=g["vis"], wgt=g["wgt"], mask=g["mask"],
                                         npix_x=wl["npix"], npix_y=wl["npix"], pixsize_x=cell, pixsize_y=cell,
                                         epsilon=1e-5)
         t_grid = time.perf_counter() - t0
@@ -590,11 +590,11 @@ def run_imaging_weights(wl, uvw_np, freq, mask, args):
     against the oracle on the CPU sample's integrations."""
     import torch
 
-    from rang import core, core_weights
+    from rang import core, weighting
 
     nrow, nchan = uvw_np.shape[0], freq.size
-    wave = core_weights.wsclean_wavelengths(freq)
-    size = core_weights.padded_size(wl["npix"])
+    wave = weighting.wavelengths(freq)
+    size = weighting.padded_size(wl["npix"])
     scale = wl["cell_arcsec"] * synth.ARCSEC
     w_h = torch.empty((nrow, nchan), dtype=torch.float32, pin_memory=True)
     w_h.copy_(mask.to(torch.float32))
@@ -769,7 +769,7 @@ def run_b200(args):
             pinned = None
             e2e = {"unavailable": reason}
     if pinned is not None:
-        from rang.core_wgridder import options_list
+        from rang.gridder import options_list
 
         vis_h, mask_h, out_h, dirty_h = pinned
         pinned = None
@@ -879,7 +879,7 @@ def run_b200(args):
         # footprint does not average away: the dirty image of one and of
         # eight visibilities (seeded baselines up to 2 km, 1 GHz, 256^2 at
         # 4 arcsec), relative L-inf error against float64 at epsilon 1e-12.
-        from rang import core_wgridder
+        from rang import gridder
 
         srng = np.random.default_rng(11)
         sparse = []
@@ -888,12 +888,12 @@ def run_b200(args):
             svis = srng.standard_normal((nvis, 1)) + 1j * srng.standard_normal((nvis, 1))
             skw = dict(uvw=suvw, freq=np.array([1.0e9]), npix_x=256, npix_y=256,
                        pixsize_x=4.0 * np.pi / 648000.0, pixsize_y=4.0 * np.pi / 648000.0)
-            ref = core_wgridder.vis2dirty(vis=svis, epsilon=1e-12, **skw)
+            ref = gridder.vis2dirty(vis=svis, epsilon=1e-12, **skw)
             for eps_m in (1e-5, 1e-6):
                 entry = {"visibilities": nvis, "epsilon": eps_m}
                 for name, code in (("fp32", 0), ("tf32x3", 1), ("bf16x3", 2)):
                     ext.wgridder_set_method(code)
-                    dm = core_wgridder.vis2dirty(vis=svis.astype(np.complex64), epsilon=eps_m, **skw)
+                    dm = gridder.vis2dirty(vis=svis.astype(np.complex64), epsilon=eps_m, **skw)
                     entry[name + "_dirty_rel_linf"] = float(np.abs(dm - ref).max() / np.abs(ref).max())
                 sparse.append(entry)
         ext.wgridder_set_method(1)

@@ -170,10 +170,11 @@ int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, siz
  * (NOALLOC_SCRATCH_BYTES); a call whose bin counters and scan do not fit in
  * it fails with status 1 and says how many bytes it needed. The first call on
  * a device looks up that array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture. All calls share the array, so
- * calls whose GPU work overlaps race: run them on one stream, or wait for one
- * before starting another. The call clears what must start at zero and
- * returns when its work on `stream` is done.
+ * that first call before any stream capture. Every call reads the scan's
+ * count back to the host and waits for `stream` before it returns. All calls
+ * share the array, so calls whose GPU work overlaps race: run them on one
+ * stream, or wait for one before starting another. The call clears what must
+ * start at zero.
  * Inputs: uvw_dev (nrow * 3 doubles) and the optional weights wgt_dev
  * (WGRIDDER_WGT_NONE, _F32 or _F64) and mask_dev (nrow * nchan) are device
  * arrays; freq is a host array; the active set is wgt * mask != 0 (as for

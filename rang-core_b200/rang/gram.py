@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import core
-from .core_wgridder import options_list
+from .gridder import options_list
 
 N_STATS = 14
 STAT_NAMES = ("planes", "stencil", "theta", "wmin", "wmax", "x_range", "sup_error", "lebesgue", "active_pairs",

@@ -485,14 +485,14 @@ def gridder_inputs(partition, rows=None):
     """The gridder's inputs from a partition's rows (linear XX, XY, YX, YY
     correlations): uvw (nrow, 3) float64, the channel frequencies, Stokes I
     visibilities complex64 and weights float32 (nrow, nchan), formed on the
-    GPU (`core_weights.stokes_i`), and the mask (nrow, nchan) uint8, 1 where
+    GPU (`weighting.stokes_i`), and the mask (nrow, nchan) uint8, 1 where
     the Stokes I sample is unflagged with a positive weight."""
-    from . import core_weights
+    from . import weighting
 
     if partition.polarization != ("XX", "XY", "YX", "YY"):
         raise ValueError(f"{partition.name}: Stokes I needs XX, XY, YX, YY, not {partition.polarization}")
     r = partition.rows() if rows is None else rows
-    vis, weight = core_weights.stokes_i(r["DATA"], r["WEIGHT_SPECTRUM"], r["FLAG"])
+    vis, weight = weighting.stokes_i(r["DATA"], r["WEIGHT_SPECTRUM"], r["FLAG"])
     mask = (weight > 0).astype(np.uint8)
     return {"uvw": np.ascontiguousarray(r["UVW"], np.float64), "freq": partition.frequency.copy(), "vis": vis,
             "wgt": weight, "mask": mask}

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import core
-from .core_wgridder import options_list
+from .gridder import options_list
 
 _VIS_KIND = {torch.complex64: 1, torch.complex128: 2}
 _WGT_KIND = {torch.float32: 1, torch.float64: 2}
@@ -79,7 +79,7 @@ class DevicePlan:
         _check(status)
         self._handle = handle
         self._stream = torch.cuda.current_stream(self.device)
-        from .core_wgridder import info_dict
+        from .gridder import info_dict
 
         self.info = info_dict(info)
 

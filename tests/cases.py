@@ -83,3 +83,41 @@ def meerkat_like(nant=64, ntime=16, nchan=16, dec_deg=-30.0, tint=8.0, f0=856e6,
 
 def rel_linf(a, b):
     return float(np.abs(np.asarray(a) - np.asarray(b)).max() / np.abs(np.asarray(b)).max())
+
+
+def df1_cases(golden):
+    """The four DF1 cases of `df1_cases.npz` (made by the reference's own
+    generator), as {name: {field: array}}."""
+    data = np.load(golden / "df1_cases.npz")
+    names = sorted({k.split("/")[0] for k in data.files})
+    return {n: {k.split("/")[1]: data[k] for k in data.files if k.startswith(n + "/")} for n in names}
+
+
+# Precisions and epsilons the reference's DF1 run recorded errors for.
+DF1_RECORDED = ((True, 1e-4), (True, 1e-5), (False, 1e-7), (False, 1e-9))
+
+
+def df1_record(golden, single, eps, direction):
+    """The reference gridder's worst error against the FP64 DFT for one
+    precision, epsilon and direction ("vis2dirty" or "dirty2vis"), as its DF1
+    run recorded it (research/results/df1-wgridder.json, "worst"): dirty2vis
+    over the four synthetic cases, vis2dirty over them and the LUNO slice."""
+    import json
+
+    rec = json.loads((golden / "df1_reference_errors.json").read_text())
+    return rec[f"{'f32' if single else 'f64'}_eps{eps:g} {direction} vs DFT"]
+
+
+def df1_worst(df1, single, eps, vis2dirty, dirty2vis):
+    """Worst L-inf error relative to the DFT's peak over the DF1 cases of the
+    gridder calls given (keyword APIs of rang.gridder or the oracle)."""
+    wd = wv = 0.0
+    for c in df1.values():
+        nx, ny, dx, dy = int(c["nx"]), int(c["ny"]), float(c["dx"]), float(c["dy"])
+        vis = c["vis"].astype(np.complex64) if single else c["vis"]
+        wgt = c["wgt"].astype(np.float32) if single else c["wgt"]
+        kw = dict(uvw=c["uvw"], freq=c["freq"], wgt=wgt, pixsize_x=dx, pixsize_y=dy, epsilon=eps)
+        wd = max(wd, rel_linf(vis2dirty(vis=vis, npix_x=nx, npix_y=ny, **kw), c["dft_dirty"]))
+        img = c["image"].astype(np.float32) if single else c["image"]
+        wv = max(wv, rel_linf(dirty2vis(dirty=img, **kw), c["dft_vis"]))
+    return wd, wv

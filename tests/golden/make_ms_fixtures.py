@@ -34,4 +34,6 @@ def main(reference):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit(f"usage: python {Path(__file__).name} REFERENCE_CHECKOUT")
+    main(sys.argv[1])

@@ -63,36 +63,37 @@ def test_library_exports_every_gram_symbol(built):
 
 def test_weight_geometry_without_a_gpu(built):
     # Host-side functions of the weights ABI against the oracle (weights.rs:38-42, :102-112).
-    from rang import core_weights
+    from rang import weighting
 
     for trimmed in (512, 1024, 2, 4096, 1000):
-        assert core_weights.padded_size(trimmed) == oracle.padded_size(trimmed)
+        assert weighting.padded_size(trimmed) == oracle.padded_size(trimmed)
     for args in [(616, 616, 1.0), (616, 616, 3.0), (610, 610, 4.0), (614, 614, 4.0), (1232, 900, 2.5)]:
-        assert core_weights.grid_shape(*args) == oracle.weight_grid_shape(*args)
+        geometry = weighting.ImagingWeights(args[0], args[1], 1.0, super_weight=args[2])
+        assert geometry.grid_shape() == oracle.weight_grid_shape(*args)
     with pytest.raises(ValueError):
-        core_weights.grid_shape(616, 616, 0.0)
+        weighting.ImagingWeights(616, 616, 1.0, super_weight=0.0).grid_shape()
 
 
 def test_kernel_table_through_the_extension(built):
-    from rang import core_wgridder
+    from rang import gridder
 
-    assert core_wgridder.kernel_table() == oracle.kernel_table()
-    assert core_wgridder.kernel_row(939) is None
+    assert gridder.kernel_table() == oracle.kernel_table()
+    assert gridder.kernel_row(939) is None
 
 
 def test_last_error_is_empty_then_set(built):
-    from rang import core_wgridder
+    from rang import gridder
 
     uvw, freq, vis, wgt, nx, ny, dx = small_case(nrow=6)
     common = dict(uvw=uvw, freq=freq, npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx)
     with pytest.raises(ValueError, match="ascending"):
-        core_wgridder.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-6, **{**common, "freq": freq[::-1]})
+        gridder.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-6, **{**common, "freq": freq[::-1]})
     with pytest.raises(ValueError, match="epsilon must be positive"):
-        core_wgridder.vis2dirty(vis=vis, wgt=wgt, epsilon=0.0, **common)
+        gridder.vis2dirty(vis=vis, wgt=wgt, epsilon=0.0, **common)
     with pytest.raises(ValueError, match="pixel sizes must be positive"):
-        core_wgridder.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-6, **{**common, "pixsize_x": -1.0})
+        gridder.vis2dirty(vis=vis, wgt=wgt, epsilon=1e-6, **{**common, "pixsize_x": -1.0})
     with pytest.raises(ValueError, match="positive"):
-        core_wgridder.dirty2vis(dirty=np.zeros((nx, ny)), uvw=uvw, freq=-freq, wgt=wgt, pixsize_x=dx,
+        gridder.dirty2vis(dirty=np.zeros((nx, ny)), uvw=uvw, freq=-freq, wgt=wgt, pixsize_x=dx,
                                 pixsize_y=dx, epsilon=1e-6)
 
 

@@ -51,7 +51,7 @@ def _case(single, seed=5, zeros=False):
 @pytest.mark.parametrize("single", [True, False])
 @pytest.mark.parametrize("k", [3, 7])
 def test_chunked_dirty2vis_is_bit_identical(chunks, single, k):
-    from rang import core_wgridder as cw
+    from rang import gridder as cw
 
     vis, wgt, mask, kw = _case(single)
     kw = {key: v for key, v in kw.items() if key not in ("npix_x", "npix_y")}
@@ -68,7 +68,7 @@ def test_chunked_dirty2vis_is_bit_identical(chunks, single, k):
 @pytest.mark.parametrize("single", [True, False])
 @pytest.mark.parametrize("k", [3, 7])
 def test_chunked_vis2dirty_matches(chunks, single, k):
-    from rang import core_wgridder as cw
+    from rang import gridder as cw
 
     vis, wgt, mask, kw = _case(single)
     chunks(1)
@@ -83,7 +83,7 @@ def test_chunked_vis2dirty_matches(chunks, single, k):
 
 @pytest.mark.parametrize("single", [True, False])
 def test_chunked_vis2dirty_with_zero_visibilities_falls_back(chunks, single):
-    from rang import core_wgridder as cw
+    from rang import gridder as cw
 
     vis, wgt, mask, kw = _case(single, seed=6, zeros=True)
     _, oinfo = oracle.vis2dirty(vis=vis, wgt=wgt, mask=mask, return_info=True, **kw)

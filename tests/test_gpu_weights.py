@@ -1,4 +1,4 @@
-"""Imaging weights and Stokes I on the GPU (rang.core_weights over the C ABI
+"""Imaging weights and Stokes I on the GPU (rang.weighting over the C ABI
 of include/rang_weights.h) against the CPU oracle's restatement of the
 reference's weights.rs.
 
@@ -27,80 +27,79 @@ def _case(seed, nant=40, ntime=20, nchan=32, flagged=0.1):
     w = rng.uniform(0.5, 2.0, shape).astype(np.float32)
     w[rng.uniform(size=shape) < flagged] = 0.0
     sel = (rng.uniform(size=uvw.shape[0]) > 0.05).astype(np.uint8)
-    from rang import core_weights
+    from rang import weighting
 
-    return uvw, core_weights.wsclean_wavelengths(freq), w, sel
+    return uvw, weighting.wavelengths(freq), w, sel
+
+
+def _gpu(uvw, wl, w, sel, width, height, pixel_scale, rank_filter=(3.0, 16), with_grid=True, **kw):
+    from rang import weighting
+
+    return weighting.ImagingWeights(width, height, pixel_scale, rank_filter=rank_filter, **kw)(
+        uvw, wl, w, sel, with_grid=with_grid)
 
 
 def _compare(got, ref):
-    assert np.array_equal(got["weights"].view(np.uint32), ref["weights"].view(np.uint32))
-    assert np.array_equal(got["grid"].view(np.uint64), ref["grid"].view(np.uint64))
-    s = got["sums"]
+    assert np.array_equal(got.weights.view(np.uint32), ref["weights"].view(np.uint32))
+    assert np.array_equal(got.grid.view(np.uint64), ref["grid"].view(np.uint64))
     r = ref["sums"]
-    assert s["count"] == int(r[3])
-    assert s["max_gridded_weight"] == r[2]
-    assert s["visibility_weight_sum"] == pytest.approx(r[0], rel=1e-12)
-    assert s["total_weight"] == pytest.approx(r[1], rel=1e-12)
+    assert got.count == int(r[3])
+    assert got.max_gridded_weight == r[2]
+    assert got.visibility_weight_sum == pytest.approx(r[0], rel=1e-12)
+    assert got.total_weight == pytest.approx(r[1], rel=1e-12)
 
 
 @pytest.mark.parametrize("mode,robust", [("briggs", 0.5), ("briggs", -1.0), ("briggs", 2.0), ("uniform", 0.0),
                                          ("natural", 0.0)])
 @pytest.mark.parametrize("rank", [(3.0, 16), None])
 def test_imaging_weights_match_the_oracle(mode, robust, rank):
-    from rang import core_weights
-
     uvw, wl, w, sel = _case(3)
     kw = dict(mode=mode, robust=robust, width=616, height=616, pixel_scale=SCALE * 4, rank_filter=rank)
-    _compare(core_weights.imaging_weights(uvw, wl, w, sel, **kw), oracle.imaging_weights(uvw, wl, w, sel, **kw))
+    _compare(_gpu(uvw, wl, w, sel, **kw), oracle.imaging_weights(uvw, wl, w, sel, **kw))
 
 
 def test_super_weight_and_odd_geometry():
-    from rang import core_weights
-
     uvw, wl, w, sel = _case(4, ntime=12, nchan=48)
     kw = dict(mode="briggs", robust=0.0, width=1000, height=904, pixel_scale=SCALE * 3, super_weight=2.5,
               rank_filter=(2.0, 7))
-    _compare(core_weights.imaging_weights(uvw, wl, w, sel, **kw), oracle.imaging_weights(uvw, wl, w, sel, **kw))
+    _compare(_gpu(uvw, wl, w, sel, **kw), oracle.imaging_weights(uvw, wl, w, sel, **kw))
 
 
 def test_reference_known_answers_on_the_gpu():
     # tests/test_core_weights.py:42-82 of the reference, through the GPU
-    from rang import core_weights
+    from rang import weighting
 
+    geom = dict(width=weighting.padded_size(512), height=weighting.padded_size(512), pixel_scale=SCALE)
     uvw = np.array([[100.0, 50.0, 0.0], [-100.0, -50.0, 0.0], [100.0, 50.0, 0.0]])
     wavelength = np.array([0.2, 0.25])
     weights = np.ones((3, 2), np.float32)
     weights[0, 1] = 3.0
-    r = core_weights.imaging_weights(uvw, wavelength, weights, [True, True, False], mode="briggs", robust=0.5)
-    out = r["weights"]
+    r = _gpu(uvw, wavelength, weights, [True, True, False], mode="briggs", robust=0.5, **geom)
+    out = r.weights
     assert np.all(out[2] == 0) and np.array_equal(out[0], out[1])
-    assert r["grid"].shape == (308, 616) and np.count_nonzero(r["grid"]) == 2
+    assert r.grid.shape == (308, 616) and np.count_nonzero(r.grid) == 2
     avg_w = (2.0**2 + 4.0**2) / 6.0
     f = 5.0 * 10.0**-0.5
     expected = 1.0 / (1.0 + np.array([2.0, 4.0]) * f * f / avg_w)
     np.testing.assert_array_equal(np.sort(out[0]), np.sort(expected.astype(np.float32)))
-    assert r["sums"]["count"] == 4 and r["sums"]["visibility_weight_sum"] == 6.0
-    numpy_sums = core_weights.weight_sums(weights, out)
-    assert numpy_sums["total_weight"] == pytest.approx(r["sums"]["total_weight"], rel=1e-12)
+    assert r.count == 4 and r.visibility_weight_sum == 6.0
+    total = float(np.sum((weights * out).astype(np.float64)))
+    assert total == pytest.approx(r.total_weight, rel=1e-12)
     uvw2 = np.array([[100.0, 50.0, 0.0], [100.0, 50.0, 0.0]])
     w2 = np.array([[2.0], [3.0]], np.float32)
-    assert np.all(core_weights.imaging_weights(uvw2, [0.2], w2, [1, 1], mode="uniform",
-                                               return_grid=False)["weights"] == np.float32(0.2))
-    assert np.all(core_weights.imaging_weights(uvw2, [0.2], w2, [1, 1], mode="natural",
-                                               rank_filter=None)["weights"] == 1.0)
+    assert np.all(_gpu(uvw2, [0.2], w2, [1, 1], mode="uniform", with_grid=False, **geom).weights == np.float32(0.2))
+    assert np.all(_gpu(uvw2, [0.2], w2, [1, 1], mode="natural", rank_filter=None, **geom).weights == 1.0)
 
 
 def test_invalid_arguments_give_status_1():
-    from rang import core_weights
-
     with pytest.raises(RuntimeError, match="code 1"):
-        core_weights.imaging_weights(np.zeros((1, 3)), [1.0], np.ones((1, 1)), [1], pixel_scale=-1.0)
+        _gpu(np.zeros((1, 3)), [1.0], np.ones((1, 1)), [1], width=616, height=616, pixel_scale=-1.0)
     with pytest.raises(ValueError):
-        core_weights.imaging_weights(np.zeros((1, 3)), [1.0], np.ones((1, 1)), [1], mode="robust")
+        _gpu(np.zeros((1, 3)), [1.0], np.ones((1, 1)), [1], width=616, height=616, pixel_scale=SCALE, mode="robust")
 
 
 def test_stokes_i_bit_identical():
-    from rang import core_weights
+    from rang import weighting
 
     rng = np.random.default_rng(8)
     shape = (37, 19, 4)
@@ -108,7 +107,7 @@ def test_stokes_i_bit_identical():
     data.ravel()[::97] = np.nan
     weights = rng.uniform(0, 3, shape).astype(np.float32)
     flags = rng.uniform(size=shape) < 0.2
-    vis, w = core_weights.stokes_i(data, weights, flags)
+    vis, w = weighting.stokes_i(data, weights, flags)
     ovis, ow = oracle.stokes_i(data, weights, flags)
     assert np.array_equal(vis.view(np.uint32), ovis.view(np.uint32))
     assert np.array_equal(w.view(np.uint32), ow.view(np.uint32))

@@ -114,7 +114,7 @@ def test_one_node_operator_is_the_psf_convolution():
     # GramOperator::no_w (gridder_gram.rs:415-486): G~ delta_c = the PSF about c.
     import torch
 
-    from rang import core_wgridder, gram
+    from rang import gridder, gram
 
     n = 48
     uvw, freq, wgt, cell = oracle.gram_case(n, 600, 300.0, False)
@@ -125,7 +125,7 @@ def test_one_node_operator_is_the_psf_convolution():
     delta = torch.zeros((n, n), dtype=torch.float64, device=dev)
     delta[n // 2, n // 2] = 1.0
     got = op.apply(delta).cpu().numpy()
-    _, psf = core_wgridder.dirty_psf(uvw=uvw, freq=freq, vis=np.ones((len(uvw), 2), np.complex128), wgt=wgt,
+    _, psf = gridder.dirty_psf(uvw=uvw, freq=freq, vis=np.ones((len(uvw), 2), np.complex128), wgt=wgt,
                                      npix_x=n, npix_y=n, pixsize_x=cell, pixsize_y=cell, epsilon=1e-10,
                                      do_wgridding=False)
     assert np.abs(got - psf).max() <= 1e-8 * np.abs(psf).max()

@@ -126,7 +126,7 @@ def test_bad_tables_are_refused(tables, tmp_path):
 
 @pytest.mark.gpu
 def test_msv2_rows_feed_the_gridder_like_msv4(tables):
-    from rang import core_wgridder, msv2, msv4
+    from rang import gridder, msv2, msv4
 
     # The gridder's inputs are equal bit for bit; its float atomics make two
     # runs agree to rounding, not bit for bit.
@@ -136,7 +136,7 @@ def test_msv2_rows_feed_the_gridder_like_msv4(tables):
         r = _sorted(source.rows())
         g = msv4.gridder_inputs(source, r)
         inputs.append(g)
-        images.append(core_wgridder.vis2dirty(uvw=g["uvw"], freq=g["freq"], vis=g["vis"], wgt=g["wgt"],
+        images.append(gridder.vis2dirty(uvw=g["uvw"], freq=g["freq"], vis=g["vis"], wgt=g["wgt"],
                                               mask=g["mask"], npix_x=64, npix_y=64, pixsize_x=2e-4,
                                               pixsize_y=2e-4, epsilon=1e-5))
     for key in ("uvw", "freq", "vis", "wgt", "mask"):

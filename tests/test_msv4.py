@@ -234,7 +234,7 @@ def test_written_store_reads_back(tmp_path):
 
 @pytest.mark.gpu
 def test_fixture_rows_feed_the_gridder():
-    from rang import core_wgridder, msv4
+    from rang import gridder, msv4
 
     part = msv4.open_processing_set(FIXTURE).partition("m05-var-spw-tssm_1")
     g = msv4.gridder_inputs(part)
@@ -243,7 +243,7 @@ def test_fixture_rows_feed_the_gridder():
     nx = ny = 64
     dx = 2.0e-4
     common = dict(uvw=g["uvw"], freq=g["freq"], npix_x=nx, npix_y=ny, pixsize_x=dx, pixsize_y=dx)
-    got = core_wgridder.vis2dirty(vis=g["vis"], wgt=g["wgt"], mask=g["mask"], epsilon=1e-5, **common)
+    got = gridder.vis2dirty(vis=g["vis"], wgt=g["wgt"], mask=g["mask"], epsilon=1e-5, **common)
     want = oracle.vis2dirty(vis=g["vis"], wgt=g["wgt"], mask=g["mask"], epsilon=1e-5, **common)
     assert rel_linf(got, want) < 2e-5
     dft = oracle.dft_dirty(g["uvw"], g["freq"], g["vis"].astype(np.complex128) * g["wgt"] * g["mask"], nx, ny, dx, dx)

@@ -9,8 +9,10 @@ ABI, twice in a row on different inputs (the second call must not see the
 first call's counters), and checks each result against the ordinary binning
 entry point: the per-visibility keys bit for bit, and the sorted order up to
 the order inside a (tile, plane) bin, which the GPU's counting sort leaves
-unspecified. It runs last (file name) so that a failure here does not stop
-the rest of the GPU suite.
+unspecified. It also checks the property the entry point exists for: once a
+first call has loaded the library's kernels and its array, a further call
+leaves the device's free memory unchanged. It runs last (file name) so that
+a failure here does not stop the rest of the GPU suite.
 """
 
 import ctypes
@@ -78,7 +80,7 @@ def _noalloc(lib, uvw, freq, wgt, mask, kw, single):
 
 @pytest.mark.parametrize("single", [True, False])
 def test_no_alloc_binning_matches_the_allocating_entry_point(single):
-    from rang import core_wgridder as cw
+    from rang import gridder as cw
 
     lib = _lib()
     cases = [_case(3, 32, 6, 24, 256, single), _case(4, 48, 4, 40, 384, single)]
@@ -92,3 +94,31 @@ def test_no_alloc_binning_matches_the_allocating_entry_point(single):
         k = key[srt].astype(np.int64)
         assert np.all(np.diff(k) >= 0)
         assert np.array_equal(srt[np.lexsort((srt, k))], rs[np.lexsort((rs, key[rs].astype(np.int64)))])
+
+
+def test_no_alloc_binning_takes_no_device_memory():
+    import torch
+
+    lib = _lib()
+    uvw, freq, wgt, mask, kw = _case(5, 40, 6, 32, 256, True)
+    _noalloc(lib, uvw, freq, wgt, mask, kw, True)  # loads the kernels and the array
+    n = uvw.shape[0] * freq.size
+    dev = torch.device("cuda", 0)
+    d_uvw = torch.from_numpy(uvw).to(dev)
+    d_wgt = torch.from_numpy(wgt).to(dev)
+    d_mask = torch.from_numpy(mask).to(dev)
+    key = torch.empty((n,), dtype=torch.int32, device=dev)
+    srt = torch.empty((n,), dtype=torch.int32, device=dev)
+    info = np.empty(14)
+    ns = ctypes.c_size_t(0)
+    o = oracle.options(kw["npix_x"], kw["npix_y"], kw["pixsize_x"], kw["pixsize_y"], kw["epsilon"])
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info(dev)
+    st = lib.rang_b200_wgridder_bin_noalloc(
+        ctypes.byref(o), uvw.shape[0], freq.size, d_uvw.data_ptr(), freq.ctypes.data, d_wgt.data_ptr(), 1,
+        d_mask.data_ptr(), 1, stream, key.data_ptr(), srt.data_ptr(), ctypes.byref(ns), info.ctypes.data)
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info(dev)
+    assert st == 0 and ns.value > 0
+    assert free_after == free_before
