@@ -150,7 +150,8 @@ void rang_b200_wgridder_plan_destroy(RangWgridPlan* plan);
 /* The visibility binning of a call on HOST arrays, for parity tests: per
  * visibility (row-major) iu0, iv0 (-1 when inactive) and the bin key
  * tile * max(nplanes, 1) + first plane (0xffffffff when inactive), and the
- * sorted order (`sorted`, nrow * nchan entries of room; `nsorted` receives
+ * active visibilities in the reference's layout order, (tile, first plane,
+ * row, channel) (`sorted`, nrow * nchan entries of room; `nsorted` receives
  * the active count). Arguments as rang_core_wgridder_vis2dirty_ex2_*;
  * with_vis selects the activity |vis|^2 wgt mask != 0. */
 int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, size_t nchan,
@@ -198,13 +199,16 @@ int32_t rang_b200_wgridder_bin_noalloc(const WgridderOptions* opts, size_t nrow,
 int64_t rang_b200_wgridder_launch_count(void);
 /* How single-precision gridding forms its sums (no counterpart in the
  * reference, whose RANG_WGRIDDER_SIMD selects CPU instruction sets,
- * wgridder.rs:1593-1627): 1 split-precision 3 x TF32 tensor-core products
- * with FP32 accumulation (the default), 0 plain FP32 FMAs on the CUDA cores,
- * 2 split-precision 3 x BF16 tensor-core products (about 16 bits of each
- * factor; a comparison point, not more accurate or faster than 1).
- * Process-wide; RANG_WGRIDDER_GPU_METHOD=fp32|tf32x3|bf16x3 sets the initial
- * value. Other values select 1.
- * Returns the previous method. */
+ * wgridder.rs:1593-1627): 3 (the default) exact integer products of 23-bit
+ * fixed-point factors on the integer tensor cores, summed in an int64
+ * fixed-point grid, so that results are bit-identical from call to call and
+ * do not depend on the visibilities' order; 1 split-precision 3 x TF32 and
+ * 2 split-precision 3 x BF16 tensor-core products with FP32 accumulation
+ * (their results depend on the order of the sorted visibilities, which the
+ * binning leaves free); 0 plain FP32 CUDA-core products, each rounded into
+ * the fixed-point grid (order-independent). Process-wide;
+ * RANG_WGRIDDER_GPU_METHOD=int8|fp32|tf32x3|bf16x3 sets the initial value.
+ * Other values select 3. Returns the previous method. */
 int32_t rang_b200_wgridder_set_method(int32_t method);
 void rang_b200_wgridder_profile(int32_t on);
 int32_t rang_b200_wgridder_profile_read(int64_t* launches, double* ms, int32_t n);

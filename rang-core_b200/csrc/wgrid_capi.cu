@@ -240,7 +240,7 @@ void host_vis2dirty_pipelined(const WgridderOptions* o, size_t nrow, size_t ncha
   Plan<T> exact(*o, nrow, nchan, u.uvw.as<double>(), freq, data, true, s);
   std::memcpy(info, exact.info().v, sizeof(exact.info().v));
   if (exact.empty()) return;
-  exact.grid(data, VALUE_DATA, img.as<T>(), s);
+  exact.grid(data, VALUE_DATA, img.as<T>(), s, nullptr, true);
   check_cuda(cudaMemcpyAsync(dirty, img.get(), npix * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
   finish(exact, s);
 }
@@ -273,11 +273,11 @@ void host_vis2dirty(const WgridderOptions* o, size_t nrow, size_t nchan, const d
   if (plan.empty()) return;
   DevBuf img(npix * sizeof(T), s);
   if (dirty) {
-    plan.grid(u.in, VALUE_DATA, img.as<T>(), s);
+    plan.grid(u.in, VALUE_DATA, img.as<T>(), s, nullptr, true);
     check_cuda(cudaMemcpyAsync(dirty, img.get(), npix * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
   }
   if (psf) {
-    plan.grid(u.in, VALUE_UNIT, img.as<T>(), s);
+    plan.grid(u.in, VALUE_UNIT, img.as<T>(), s, nullptr, true);
     check_cuda(cudaMemcpyAsync(psf, img.get(), npix * sizeof(T), cudaMemcpyDeviceToHost, s), "copy to host");
   }
   finish(plan, s);
@@ -589,7 +589,10 @@ int64_t rang_b200_wgridder_launch_count(void) { return launch_count(); }
 
 int32_t rang_b200_wgridder_set_method(int32_t method) {
   int old = grid_method();
-  set_grid_method(method == GRID_FP32 ? GRID_FP32 : method == GRID_BF16X3 ? GRID_BF16X3 : GRID_TF32X3);
+  set_grid_method(method == GRID_FP32     ? GRID_FP32
+                  : method == GRID_BF16X3 ? GRID_BF16X3
+                  : method == GRID_TF32X3 ? GRID_TF32X3
+                                          : GRID_INT8);
   return old;
 }
 

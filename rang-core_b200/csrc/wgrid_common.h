@@ -41,9 +41,9 @@ struct Geom {
   int32_t nx, ny, nu, nv;
   int32_t supp, nplanes, nbuckets;  // nbuckets = max(nplanes, 1)
   int32_t log2tile, ntu, ntv, L;    // L = tile + supp - 1
-  // Sub-tiles of a tile, 8 cells along u by 2^log2subv along v: nsub_side
-  // along u, nsub_v along v, nsub in all.
-  int32_t nsub_side, nsub_v, log2subv, nsub;
+  // Sub-tiles of a tile, sube cells square: nsub_side along each side, nsub
+  // in all (sub-tile (a, b) of a tile is a * nsub_side + b).
+  int32_t sube, nsub_side, nsub;
   int32_t ne;                       // rows of even (and of odd) coefficients
   int32_t do_wgridding, shifting, lmshift, divide_by_n;
   double fu, fv, fw;  // +-1: flips (w already negated as the reference does)

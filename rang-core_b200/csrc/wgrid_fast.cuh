@@ -1,0 +1,735 @@
+// The single-precision gridder and degridder on the tensor cores, and the
+// fixed-point grid that makes gridding exact and order-independent.
+//
+// Included by wgrid_plan.cu inside its anonymous namespace (it uses the scan,
+// binning and device helpers defined there).
+//
+// Records. The binning's count pass writes one 32-byte record per active
+// visibility at its own index: the tap arguments of u, v and w, the
+// visibility's index, its shift phase, its offset inside its sub-tile's
+// window, its first plane and its bin. The per-visibility FP64 arithmetic
+// (coordinates, getpix, minplane, the phase's argument reduction) is thus
+// done once per plan, and the gridder and degridder read records through
+// the sorted indices.
+//
+// Exact gridding. Every grid cell is an int64 fixed-point sum (a pair per
+// complex cell) of the footprint terms kw * ku * (value * kv). The gridder
+// forms both factors as 23-bit integers, A = rint(kw ku 2^22) and
+// B = rint(value kv 2^sb), splits each into three balanced 8-bit limbs
+// (x = x2 2^16 + x1 2^8 + x0, x0 and x1 in [-128, 127]) and contracts the
+// limbs on the integer tensor cores (mma.sync m16n8k32, s8 x s8 -> s32),
+// keeping the limb products of weight 2^32, 2^24 and 2^16: the kept sums are
+// exact integers and the dropped terms (weight 2^8 and 1, zero-mean) are
+// below 2^-21 of the largest term. Integer sums do not depend on the order
+// of their terms, so the result is bit for bit the same whatever the order
+// of the visibilities in the sorted layout, however they are split among
+// warps and blocks, and whatever the order of the atomic adds into the
+// grid: a call is reproducible and a one-pass PSF equals a separate call.
+// The grid is converted to floating point once, before the FFTs.
+
+namespace fast {
+
+// A grid cell in fixed point: value = (re + i im) * 2^-q.
+struct FixCell {
+  long long re, im;
+};
+
+// The fixed-point scales of one gridding pass (written on the device).
+struct FixScale {
+  int sb;         // B = rint(value * kv * 2^sb) in the integer gridder
+  int q;          // cell value = int64 * 2^-q
+  int nonfinite;  // an active value or tap was not finite: the planes are NaN
+  int pad;
+};
+
+// Largest |value| of a pass (device scalars, the scan's or k_value_max's).
+struct ValueBound {
+  unsigned long long vmax_bits;  // max |vis| |wgt| (as the bits of a non-negative double)
+  unsigned long long wmax_bits;  // max |wgt|
+};
+
+__device__ __forceinline__ void atomic_max_double(unsigned long long* a, double v) {
+  if (v > 0.0) atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+// max |vis| |wgt| and max |wgt| over the visibilities the plan keeps
+// (key != INACTIVE), for gridding data other than the plan's own.
+template <class T>
+__global__ void k_value_max(uint64_t n, Inputs in, const uint32_t* __restrict__ key, ValueBound* vb) {
+  double vm = 0.0, wm = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (key[i] == INACTIVE) continue;
+    const double w = fabs((double)wgt_get<T>(in, i));
+    const cplx<T> v = vis_get<T>(in, i);
+    const double a = sqrt((double)v.re * (double)v.re + (double)v.im * (double)v.im) * w;
+    // NaN compares false and is dropped here; the gridder flags it.
+    vm = a > vm ? a : vm;
+    wm = w > wm ? w : wm;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    vm = fmax(vm, __shfl_down_sync(0xffffffffu, vm, o));
+    wm = fmax(wm, __shfl_down_sync(0xffffffffu, wm, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_double(&vb->vmax_bits, vm);
+    atomic_max_double(&vb->wmax_bits, wm);
+  }
+}
+
+__global__ void k_bound_init(ValueBound* vb, unsigned long long vmax_bits, unsigned long long wmax_bits) {
+  vb->vmax_bits = vmax_bits;
+  vb->wmax_bits = wmax_bits;
+}
+
+// The scales of one pass from the value maxima of `values`. `unit`: unit
+// values (the PSF), bounded by max |wgt|; otherwise max |vis| |wgt|. The
+// integer gridder's terms are at most 2^28 grid units (q = sb + 6), so int64
+// holds 2^34 of them. For the floating-point gridders a cell sums at most
+// nvis terms, each at most max |value| (taps are at most 1 + eps), and q
+// leaves 2 bits of headroom over that bound. The scales depend on nothing
+// but the values and the active count, so a plan split into row chunks
+// grids to the same bits as one without.
+__global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long long nvis, int integer, FixScale* fs) {
+  double vmax = __longlong_as_double((long long)(unit ? values->wmax_bits : values->vmax_bits));
+  if (!(vmax > 0.0) || !isfinite(vmax)) vmax = 1.0;
+  const int ev = min(max(ilogb(vmax), -90), 90);  // vmax < 2^(ev + 1) (clamped: scales stay finite floats)
+  FixScale r;
+  r.nonfinite = 0;
+  r.pad = 0;
+  if (integer) {
+    r.sb = 21 - ev;  // |B| < 2^22
+    r.q = r.sb + 6;
+  } else {
+    r.sb = 0;
+    r.q = 60 - ev - ilogb((double)max(nvis, 1ull));  // nvis * vmax * 2^q < 2^62
+  }
+  *fs = r;
+}
+
+// One plane of the fixed-point grid to floating point: rows [0, rows) and
+// [nu - rows, nu) (every row when rows is 0), each cell rounded once.
+template <class T>
+__global__ void k_fix_to_plane(const FixCell* __restrict__ fix, int nu, int nv, int rows, const FixScale* fs,
+                               cplx<T>* __restrict__ out) {
+  const int q = fs->q;
+  const bool nan = fs->nonfinite != 0;
+  const int nr = rows == 0 ? nu : 2 * rows;
+  const uint64_t n = (uint64_t)nr * nv;
+  for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(c / nv);
+    const uint64_t cell = (uint64_t)(rows == 0 || r < rows ? r : nu - 2 * rows + r) * nv + (c - (uint64_t)r * nv);
+    const FixCell f = fix[cell];
+    cplx<T> v;
+    if (nan) {
+      v = {(T)__longlong_as_double(0x7ff8000000000000ll), (T)__longlong_as_double(0x7ff8000000000000ll)};
+    } else {
+      v = {(T)ldexp((double)f.re, -q), (T)ldexp((double)f.im, -q)};
+    }
+    out[cell] = v;
+  }
+}
+
+__device__ __forceinline__ void fix_add(FixCell* cell, long long re, long long im) {
+  if (re) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->re), (unsigned long long)re);
+  if (im) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->im), (unsigned long long)im);
+}
+
+// ------------------------------------------------------------------ records
+
+struct VisRecord {
+  float x0, y0, xw;  // tap arguments (taps_uv, w_factor's locz of the first plane)
+  uint32_t idx;      // visibility index, row * nchan + channel
+  float ph_re, ph_im;  // shift phase (shift_phase with sign +1), (1, 0) without shifts
+  uint32_t meta;     // du | dv << 4 | (w was flipped) << 8 | first plane << 16
+  uint32_t bin;      // the sorted key (chunk * nbins + bin)
+};
+static_assert(sizeof(VisRecord) == 32, "records are one 32-byte sector");
+
+// The count pass of the counting sort (k_bin_count) for single precision,
+// writing as well the record of each active visibility at its own index
+// (coalesced): its coordinates and taps' arguments are formed here once. The
+// scatter then moves only the 4-byte indices, and the gridder and degridder
+// read each record through the sorted index.
+__global__ void __launch_bounds__(256, 4)
+    k_bin_count_rec(const __grid_constant__ Geom<float> g, const double* __restrict__ uvw,
+                    const double* __restrict__ foc, Inputs in, int with_vis, uint32_t* __restrict__ key,
+                    uint32_t* __restrict__ counts, VisRecord* __restrict__ rec, uint32_t rows_per_chunk,
+                    uint32_t nbins) {
+  const uint64_t n = g.nrow * g.nchan;
+  const uint64_t nround = (n + 31) & ~31ull;
+  const uint32_t tmask = (1u << g.log2tile) - 1u;
+  const uint32_t se = (uint32_t)g.sube;
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  RowCh rc(i, (uint32_t)g.nchan, (uint64_t)gridDim.x * blockDim.x);
+  for (; i < nround; i += (uint64_t)gridDim.x * blockDim.x, rc.next((uint32_t)g.nchan)) {
+    bool act = false;
+    uint32_t k = INACTIVE;
+    if (i < n) {
+      act = is_active<float>(in, with_vis != 0, i);
+      if (act) {
+        double b[3];
+        const double imflip = row_coord(uvw, rc.row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+        const double f = foc[rc.ch];
+        const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
+        double uf, vf;
+        int64_t iu0, iv0;
+        getpix(g, u, v, uf, vf, iu0, iv0);
+        const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
+        const uint32_t sa = (su & tmask) / se, sb = (sv & tmask) / se;
+        const int mp = minplane(g, w);
+        // The key of bin_of_rc (Setup::locate refined by the sub-tile).
+        k = (((su >> g.log2tile) * (uint32_t)g.ntv + (sv >> g.log2tile)) * (uint32_t)g.nbuckets + (uint32_t)mp) *
+                (uint32_t)g.nsub + sa * (uint32_t)g.nsub_side + sb;
+        if (rows_per_chunk) k += (rc.row / rows_per_chunk) * nbins;
+        VisRecord r;
+        const double s1 = (double)g.supp - 1.0;
+        r.x0 = (float)(-uf * 2.0 + s1);
+        r.y0 = (float)(-vf * 2.0 + s1);
+        if (g.do_wgridding) {  // w_factor's argument for the first plane (nth 0)
+          const float z = (float)(g.xdw * ((g.wmin + (double)mp * g.dw) - w));
+          r.xw = z * 2.0f + (float)s1;
+        } else {
+          r.xw = 0.0f;
+        }
+        r.idx = (uint32_t)i;
+        if (g.shifting) {
+          const cplx<float> ph = shift_phase<float>(g, b, imflip, f, 1.0);
+          r.ph_re = ph.re;
+          r.ph_im = ph.im;
+        } else {
+          r.ph_re = 1.0f;
+          r.ph_im = 0.0f;
+        }
+        r.meta = ((su & tmask) - sa * se) | (((sv & tmask) - sb * se) << 4) | (imflip < 0.0 ? 256u : 0u) |
+                 ((uint32_t)mp << 16);
+        r.bin = k;
+        reinterpret_cast<uint4*>(rec + i)[0] = *reinterpret_cast<const uint4*>(&r.x0);
+        reinterpret_cast<uint4*>(rec + i)[1] = *reinterpret_cast<const uint4*>(&r.ph_re);
+      }
+      key[i] = k;
+    }
+    warp_aggregated_add(counts, k, act);
+  }
+}
+
+// The taps of one axis at x (the reference's eval_taps, one of the two axes
+// of eval_taps2).
+template <int S>
+__device__ __forceinline__ void eval_taps1(const float* __restrict__ c, float x, float* r) {
+  constexpr int ne = coeff_rows(S);
+  constexpr int H = (S + 1) / 2;
+  const float x2 = x * x;
+  float e[H], o[H];
+#pragma unroll
+  for (int i = 0; i < H; i++) {
+    e[i] = c[i];
+    o[i] = c[ne * S + i];
+  }
+#pragma unroll
+  for (int k = 1; k < ne; k++)
+#pragma unroll
+    for (int i = 0; i < H; i++) {
+      e[i] = fmaf(e[i], x2, c[k * S + i]);
+      o[i] = fmaf(o[i], x2, c[(ne + k) * S + i]);
+    }
+#pragma unroll
+  for (int i = 0; i < H; i++) r[i] = fmaf(o[i], x, e[i]);
+#pragma unroll
+  for (int i = 0; i < S - H; i++) r[S - 1 - i] = fmaf(o[i], -x, e[i]);
+}
+
+// The stored value of a record's visibility (unit_value, data_value,
+// wgridder.rs:1414-1435): value = vis * phase * wgt with the imaginary part
+// negated where w was flipped; the phase alone times wgt for unit values.
+__device__ __forceinline__ cplx<float> record_value(const VisRecord& r, const Inputs& in, int mode) {
+  const float flip = (r.meta & 256u) ? -1.0f : 1.0f;
+  float pr = r.ph_re, pi = r.ph_im;
+  if (in.wgt_kind != WGT_NONE) {
+    const float w = wgt_get<float>(in, r.idx);
+    pr *= w;
+    pi *= w;
+  }
+  if (mode == VALUE_DATA) {
+    const cplx<float> v = vis_get<float>(in, r.idx);
+    const float dr = v.re * pr - v.im * pi, di = v.re * pi + v.im * pr;
+    return {dr, di * flip};
+  }
+  return {pr, pi * flip};
+}
+
+// The window of a bin key: the grid row and column of its cell (0, 0) (the
+// sub-tile's first cell; windows are 8 x 8) and its first plane.
+__device__ __forceinline__ void window_of(const Geom<float>& g, uint32_t key, uint32_t nbins, int& su0, int& sv0,
+                                          int& mp) {
+  const uint32_t bin = key % nbins;
+  const uint32_t sub = bin % (uint32_t)g.nsub, t = bin / (uint32_t)g.nsub;
+  mp = (int)(t % (uint32_t)g.nbuckets);
+  const uint32_t tile = t / (uint32_t)g.nbuckets;
+  const uint32_t tu = tile / (uint32_t)g.ntv, tv = tile - tu * (uint32_t)g.ntv;
+  // Tiles are laid out on the shifted indices (i0 + n/2) mod n; the grid is
+  // stored unshifted.
+  su0 = (int)(((tu << g.log2tile) + (sub / (uint32_t)g.nsub_side) * (uint32_t)g.sube + (uint32_t)(g.nu - g.nu / 2)) %
+              (uint32_t)g.nu);
+  sv0 = (int)(((tv << g.log2tile) + (sub % (uint32_t)g.nsub_side) * (uint32_t)g.sube + (uint32_t)(g.nv - g.nv / 2)) %
+              (uint32_t)g.nv);
+}
+
+// ------------------------------------------------------------------ integer gridder
+
+constexpr int I8_BATCH = 32;         // records staged per round, one per lane
+constexpr uint32_t I8_CHUNK = 8192;  // sorted records per warp
+constexpr int I8_COL = 17;           // tap columns: taps at [8, 8 + S), read at 8 + row - offset (odd stride)
+constexpr float I8_ASCALE = 4194304.0f;  // 2^22
+
+// Staging of one round: per slot (record) the u taps and value * v taps
+// (scaled to integers' range) in zero-padded columns, the w taps times 2^22,
+// the window offsets and the key. Slot I8_BATCH stays zero.
+struct I8Slots {
+  float* ku;     // [I8_BATCH + 1][I8_COL]
+  float2* bv;    // [I8_BATCH + 1][I8_COL]: value * kv * 2^sb
+  float* kw;     // [I8_BATCH + 1][8]: kw * 2^22, zero outside the pass's planes
+  uint32_t* key; // [I8_BATCH + 1]
+  uint32_t* off; // [I8_BATCH + 1]: du | dv << 8
+  __host__ __device__ static constexpr size_t bytes() {
+    return ((size_t)(I8_BATCH + 1) * (I8_COL * 4 + I8_COL * 8 + 8 * 4 + 8) + 15) / 16 * 16;
+  }
+  __device__ void carve(unsigned char* base) {
+    bv = reinterpret_cast<float2*>(base);
+    ku = reinterpret_cast<float*>(bv + (I8_BATCH + 1) * I8_COL);
+    kw = ku + (I8_BATCH + 1) * I8_COL;
+    key = reinterpret_cast<uint32_t*>(kw + (I8_BATCH + 1) * 8);
+    off = key + (I8_BATCH + 1);
+  }
+};
+
+// Three balanced 8-bit limbs of four integers |x| < 2^22 + 2^15, packed
+// per limb (byte j of limb register L holds limb L of x[j]).
+__device__ __forceinline__ void limbs4(int x0, int x1, int x2, int x3, uint32_t& l0, uint32_t& l1, uint32_t& l2) {
+  // y = x + 0x8080: bytes 0 and 1 of y are the low limbs plus 128, y >> 16
+  // (byte 2 of y, as a signed byte) is the top limb.
+  const uint32_t y0 = (uint32_t)(x0 + 0x8080), y1 = (uint32_t)(x1 + 0x8080);
+  const uint32_t y2 = (uint32_t)(x2 + 0x8080), y3 = (uint32_t)(x3 + 0x8080);
+  const uint32_t a01 = __byte_perm(y0, y1, 0x5140), a23 = __byte_perm(y2, y3, 0x5140);  // b0 b0' b1 b1'
+  l0 = __byte_perm(a01, a23, 0x5410) ^ 0x80808080u;
+  l1 = __byte_perm(a01, a23, 0x7632) ^ 0x80808080u;
+  l2 = __byte_perm(__byte_perm(y0, y1, 0x0062), __byte_perm(y2, y3, 0x0062), 0x5410);
+}
+
+__device__ __forceinline__ void imma(int (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                     uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Adds a bin's exact window sums to the fixed-point grid. acc[h][c][g][r]:
+// plane pair h, component c (re, im), limb group g (weights 2^32, 2^24,
+// 2^16: the grid unit is 2^16 of the products), fragment element r (rows
+// gq / gq + 8 are planes 2h / 2h + 1 at window row gq; columns 2tq, 2tq + 1).
+template <int NP>
+__device__ __forceinline__ void i8_flush(const Geom<float>& g, FixCell* __restrict__ grids, int pg0, int npg,
+                                         int su0, int sv0, int mp, const int (&acc)[NP][2][3][4]) {
+  const int lane = threadIdx.x & 31, gq = lane >> 2, tq = lane & 3;
+  const size_t plane = (size_t)g.nu * g.nv;
+  int row = su0 + gq;
+  if (row >= g.nu) row -= g.nu;
+#pragma unroll
+  for (int h = 0; h < NP; h++)
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int p = mp + 2 * h + (r >> 1);
+      const long long re = ((long long)acc[h][0][0][r] << 16) + ((long long)acc[h][0][1][r] << 8) + acc[h][0][2][r];
+      const long long im = ((long long)acc[h][1][0][r] << 16) + ((long long)acc[h][1][1][r] << 8) + acc[h][1][2][r];
+      if ((re | im) == 0 || p < pg0 || p >= pg0 + npg) continue;
+      int col = sv0 + 2 * tq + (r & 1);
+      if (col >= g.nv) col -= g.nv;
+      fix_add(grids + (size_t)(p - pg0) * plane + (size_t)row * g.nv + col, re, im);
+    }
+}
+
+// Gridding of records [kbase, kend) (single precision): each warp takes
+// I8_CHUNK consecutive records, stages I8_BATCH at a time, and per run of
+// one bin forms the integer limbs of A (rows: w tap x placed u tap of planes
+// 2h and 2h + 1, columns: the run's records) and B (rows: records, columns:
+// value x placed v tap) and adds their limb products into int32 fragments
+// on the tensor cores; at the end of a bin the fragments are combined into
+// int64 and added to the grid. Records outside the run read the zero slot.
+template <int S>
+__global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
+    k_grid_i8(const __grid_constant__ Geom<float> g, Inputs in, int mode, const VisRecord* __restrict__ rec,
+              const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
+              FixCell* __restrict__ grids, int pg0, int npg, FixScale* __restrict__ fs) {
+  static_assert(S >= 1 && S <= 8, "8 x 8 windows");
+  constexpr int NP = (S + 1) / 2;  // plane pairs
+  extern __shared__ __align__(16) unsigned char smem[];
+  I8Slots st;
+  st.carve(smem);
+  const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
+  for (int c = lane; c < (int)(I8Slots::bytes() / 16); c += I8_BATCH)
+    reinterpret_cast<float4*>(smem)[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (lane == 0) st.key[I8_BATCH] = INACTIVE;
+  __syncwarp();
+  const uint64_t k0 = kbase + (uint64_t)blockIdx.x * I8_CHUNK;
+  const uint64_t k1 = min(kend, k0 + I8_CHUNK);
+  const float bscale = ldexpf(1.0f, fs->sb);
+  bool bad = false;
+
+  int acc[NP][2][3][4];
+#pragma unroll
+  for (int h = 0; h < NP; h++)
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+      for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int r = 0; r < 4; r++) acc[h][c][q][r] = 0;
+  uint32_t gcur = INACTIVE;
+  int su0 = 0, sv0 = 0, mpc = 0;
+
+  for (uint64_t kb = k0; kb < k1; kb += I8_BATCH) {
+    const int nb = (int)min((uint64_t)I8_BATCH, k1 - kb);
+    __syncwarp();
+    if (lane < nb) {  // staging, one record per lane
+      const VisRecord r = rec[sorted[kb + lane]];
+      float ku[S], kv[S], kw[S];
+      eval_taps2<float, S>(g.coeff, g.ne, r.x0, r.y0, ku, kv);
+      if (g.do_wgridding) eval_taps1<S>(g.coeff, r.xw, kw);
+      const cplx<float> val = record_value(r, in, mode);
+      const int mp = (int)(r.meta >> 16);
+      float* cu = st.ku + lane * I8_COL + 8;
+      float2* cb = st.bv + lane * I8_COL + 8;
+      float* cw = st.kw + lane * 8;
+#pragma unroll
+      for (int i = 0; i < S; i++) {
+        cu[i] = ku[i];
+        cb[i] = make_float2(val.re * bscale * kv[i], val.im * bscale * kv[i]);
+        bad |= !isfinite(cb[i].x) || !isfinite(cb[i].y) || !isfinite(ku[i]);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        float w = 0.0f;
+        if (g.do_wgridding) {
+          if (j < S && mp + j >= pg0 && mp + j < pg0 + npg) w = kw[j < S ? j : 0] * I8_ASCALE;
+        } else if (j == 0) {
+          w = I8_ASCALE;
+        }
+        bad |= !isfinite(w);
+        cw[j] = w;
+      }
+      st.key[lane] = r.bin;
+      st.off[lane] = (r.meta & 15u) | (((r.meta >> 4) & 15u) << 8);
+    }
+    __syncwarp();
+    int q = 0;
+    while (q < nb) {
+      const uint32_t gk = st.key[q];
+      if (gk != gcur) {
+        if (gcur != INACTIVE) i8_flush<NP>(g, grids, pg0, npg, su0, sv0, mpc, acc);
+#pragma unroll
+        for (int h = 0; h < NP; h++)
+#pragma unroll
+          for (int c = 0; c < 2; c++)
+#pragma unroll
+            for (int qq = 0; qq < 3; qq++)
+#pragma unroll
+              for (int r = 0; r < 4; r++) acc[h][c][qq][r] = 0;
+        gcur = gk;
+        window_of(g, gk, nbins, su0, sv0, mpc);
+      }
+      // The run: slots [q, q + len) of bin gk.
+      const unsigned m = __ballot_sync(0xffffffffu, lane >= q && lane < nb && st.key[lane] == gk);
+      const int len = __popc(m);
+      // This lane's eight records: k = 4tq + j and 16 + 4tq + j, j < 4.
+      int slot[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int k = (j < 4 ? 4 * tq : 16 + 4 * tq) + (j & 3);
+        slot[j] = (k >= q && k < q + len) ? k : I8_BATCH;
+      }
+      float kuv[8];
+      float2 bvv[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const uint32_t o = st.off[slot[j]];
+        kuv[j] = st.ku[slot[j] * I8_COL + 8 + gq - (int)(o & 255u)];
+        bvv[j] = st.bv[slot[j] * I8_COL + 8 + gq - (int)(o >> 8)];
+      }
+      // B limbs per component: registers for k 4tq.. and 16 + 4tq..
+      uint32_t b[2][3][2];
+#pragma unroll
+      for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int hf = 0; hf < 2; hf++) {
+          int x[4];
+#pragma unroll
+          for (int j = 0; j < 4; j++) x[j] = __float2int_rn(c ? bvv[4 * hf + j].y : bvv[4 * hf + j].x);
+          limbs4(x[0], x[1], x[2], x[3], b[c][0][hf], b[c][1][hf], b[c][2][hf]);
+        }
+#pragma unroll
+      for (int h = 0; h < NP; h++) {
+        uint32_t a[3][4];  // per limb: rows gq (plane 2h), gq + 8 (plane 2h + 1) x k halves
+#pragma unroll
+        for (int hf = 0; hf < 2; hf++)
+#pragma unroll
+          for (int pl = 0; pl < 2; pl++) {
+            int x[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const float w = (2 * h + pl < S) ? st.kw[slot[4 * hf + j] * 8 + 2 * h + pl] : 0.0f;
+              x[j] = __float2int_rn(w * kuv[4 * hf + j]);
+            }
+            limbs4(x[0], x[1], x[2], x[3], a[0][2 * hf + pl], a[1][2 * hf + pl], a[2][2 * hf + pl]);
+          }
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          // weight 2^32: a2 b2; 2^24: a2 b1 + a1 b2; 2^16: a2 b0 + a1 b1 + a0 b2
+          imma(acc[h][c][0], a[2][0], a[2][1], a[2][2], a[2][3], b[c][2][0], b[c][2][1]);
+          imma(acc[h][c][1], a[2][0], a[2][1], a[2][2], a[2][3], b[c][1][0], b[c][1][1]);
+          imma(acc[h][c][1], a[1][0], a[1][1], a[1][2], a[1][3], b[c][2][0], b[c][2][1]);
+          imma(acc[h][c][2], a[2][0], a[2][1], a[2][2], a[2][3], b[c][0][0], b[c][0][1]);
+          imma(acc[h][c][2], a[1][0], a[1][1], a[1][2], a[1][3], b[c][1][0], b[c][1][1]);
+          imma(acc[h][c][2], a[0][0], a[0][1], a[0][2], a[0][3], b[c][2][0], b[c][2][1]);
+        }
+      }
+      q += len;
+    }
+  }
+  if (gcur != INACTIVE) i8_flush<NP>(g, grids, pg0, npg, su0, sv0, mpc, acc);
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&fs->nonfinite, 1);
+}
+
+// ------------------------------------------------------------------ tensor-core degridder
+
+constexpr int H16_BATCH = 32;
+constexpr uint32_t H16_CHUNK = 8192;
+constexpr int H16_COL = 17;  // tap columns as I8_COL
+constexpr float H16_BSCALE = 16384.0f;  // 2^14: v taps stay clear of FP16 subnormals
+
+struct H16Slots {
+  float* ku;      // [H16_BATCH + 1][H16_COL]: u taps at [8, 8 + S)
+  float* kv;      // [H16_BATCH + 1][H16_COL]: v taps * 2^14
+  float* kw;      // [H16_BATCH + 1][8]: w taps (zero outside the pass's planes)
+  float4* out;    // [H16_BATCH + 1]: conj(phase) * wgt (re, im), imflip, index bits
+  uint32_t* key;  // [H16_BATCH + 1]
+  uint32_t* off;  // [H16_BATCH + 1]
+  __host__ __device__ static constexpr size_t bytes() {
+    return ((size_t)(H16_BATCH + 1) * (H16_COL * 8 + 8 * 4 + 16 + 8) + 15) / 16 * 16;
+  }
+  __device__ void carve(unsigned char* base) {
+    out = reinterpret_cast<float4*>(base);
+    ku = reinterpret_cast<float*>(out + (H16_BATCH + 1));
+    kv = ku + (H16_BATCH + 1) * H16_COL;
+    kw = kv + (H16_BATCH + 1) * H16_COL;
+    key = reinterpret_cast<uint32_t*>(kw + (H16_BATCH + 1) * 8);
+    off = key + (H16_BATCH + 1);
+  }
+};
+
+// (x0, x1) as FP16 hi + lo (x - hi is exact in FP32; lo rounds it to FP16).
+__device__ __forceinline__ void split_h2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  const __half2 h = __floats2half2_rn(x0, x1);
+  const float2 hf = __half22float2(h);
+  const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+__device__ __forceinline__ void hmma_zero(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%7,%7,%7,%7};\n"
+      : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+      : "r"(a0), "r"(a1), "r"(b0), "f"(0.0f));
+}
+__device__ __forceinline__ void hmma(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(b0));
+}
+
+// Degridding of records [kbase, kend) (single precision, degrid_task_body,
+// wgridder.rs:2793-2901): per bin the warp holds the bin's 8 x 8 window of
+// each plane as FP16 hi + lo fragments (scaled by a power of two to the
+// window's largest value); per block of eight records the v contraction
+// T[p][u][k] = sum_v G[p][u][v] kv_k[v - dv_k] runs on the tensor cores as
+// hi*hi + hi*lo + lo*hi (mma.sync m16n8k8, FP32 accumulation, each block
+// from zero); the w and u contractions and the final phase and weight
+// (wgridder.rs:3146-3159) run on the CUDA cores, reduced over the window
+// rows with shuffles. Each output depends only on its own record and the
+// window, so the result does not depend on the grouping. With plane groups
+// (first / last) the partial sums accumulate in `vis` and the final factor
+// is applied with the last group.
+template <int S>
+__global__ void __launch_bounds__(H16_BATCH, 16)
+    k_degrid_h(const __grid_constant__ Geom<float> g, Inputs wts, const VisRecord* __restrict__ rec,
+               const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
+               const cplx<float>* __restrict__ grids, int pg0, int npg, cplx<float>* __restrict__ vis, int first,
+               int last) {
+  static_assert(S >= 1 && S <= 8, "8 x 8 windows");
+  constexpr int NP = (S + 1) / 2;
+  extern __shared__ __align__(16) unsigned char smem[];
+  H16Slots st;
+  st.carve(smem);
+  const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
+  for (int c = lane; c < (int)(H16Slots::bytes() / 16); c += H16_BATCH)
+    reinterpret_cast<float4*>(smem)[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (lane == 0) st.key[H16_BATCH] = INACTIVE;
+  __syncwarp();
+  const uint64_t k0 = kbase + (uint64_t)blockIdx.x * H16_CHUNK;
+  const uint64_t k1 = min(kend, k0 + H16_CHUNK);
+  const size_t plane = (size_t)g.nu * g.nv;
+
+  uint32_t ahi[NP][2][2], alo[NP][2][2];  // [pair][re/im][rows gq, gq + 8]
+  float inv = 0.0f;                       // 1 / (window scale * 2^14)
+  uint32_t gcur = INACTIVE;
+
+  for (uint64_t kb = k0; kb < k1; kb += H16_BATCH) {
+    const int nb = (int)min((uint64_t)H16_BATCH, k1 - kb);
+    __syncwarp();
+    if (lane < nb) {
+      const VisRecord r = rec[sorted[kb + lane]];
+      float ku[S], kv[S], kw[S];
+      eval_taps2<float, S>(g.coeff, g.ne, r.x0, r.y0, ku, kv);
+      if (g.do_wgridding) eval_taps1<S>(g.coeff, r.xw, kw);
+      const int mp = (int)(r.meta >> 16);
+      float* cu = st.ku + lane * H16_COL + 8;
+      float* cv = st.kv + lane * H16_COL + 8;
+      float* cw = st.kw + lane * 8;
+#pragma unroll
+      for (int i = 0; i < S; i++) {
+        cu[i] = ku[i];
+        cv[i] = kv[i] * H16_BSCALE;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        float w = 0.0f;
+        if (g.do_wgridding) {
+          if (j < S && mp + j >= pg0 && mp + j < pg0 + npg) w = kw[j < S ? j : 0];
+        } else if (j == 0 && pg0 == 0) {
+          w = 1.0f;
+        }
+        cw[j] = w;
+      }
+      // The final factor conj(phase) * wgt (shift_phase with sign -1).
+      const float tw = wts.wgt_kind != WGT_NONE ? wgt_get<float>(wts, r.idx) : 1.0f;
+      st.out[lane] = make_float4(r.ph_re * tw, -r.ph_im * tw, (r.meta & 256u) ? -1.0f : 1.0f,
+                                 __uint_as_float(r.idx));
+      st.key[lane] = r.bin;
+      st.off[lane] = (r.meta & 15u) | (((r.meta >> 4) & 15u) << 8);
+    }
+    __syncwarp();
+    int q = 0;
+    while (q < nb) {
+      const uint32_t gk = st.key[q];
+      if (gk != gcur) {  // load the window of bin gk as FP16 fragments
+        gcur = gk;
+        int su0, sv0, mp;
+        window_of(g, gk, nbins, su0, sv0, mp);
+        int row = su0 + gq;
+        if (row >= g.nu) row -= g.nu;
+        int c0 = sv0 + 2 * tq, c1 = c0 + 1;
+        if (c0 >= g.nv) c0 -= g.nv;
+        if (c1 >= g.nv) c1 -= g.nv;
+        float2 v[NP][2][2];  // [pair][plane 2h + pl][column]
+        float m = 0.0f;
+#pragma unroll
+        for (int h = 0; h < NP; h++)
+#pragma unroll
+          for (int pl = 0; pl < 2; pl++) {
+            const int p = mp + 2 * h + pl;
+            const bool ok = (2 * h + pl < S) && p >= pg0 && p < pg0 + npg && (g.do_wgridding || p == 0);
+            const cplx<float>* src = grids + (size_t)(ok ? p - pg0 : 0) * plane + (size_t)row * g.nv;
+            const cplx<float> x0 = ok ? src[c0] : cplx<float>{0.0f, 0.0f};
+            const cplx<float> x1 = ok ? src[c1] : cplx<float>{0.0f, 0.0f};
+            v[h][pl][0] = make_float2(x0.re, x0.im);
+            v[h][pl][1] = make_float2(x1.re, x1.im);
+            m = fmaxf(m, fmaxf(fmaxf(fabsf(x0.re), fabsf(x0.im)), fmaxf(fabsf(x1.re), fabsf(x1.im))));
+          }
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        // Largest window value to about 2^14 (FP16 tops out at 65504).
+        const int e = (m > 0.0f && isfinite(m)) ? ilogbf(m) : 0;
+        const float sc = ldexpf(1.0f, 14 - e);
+        inv = ldexpf(1.0f, e - 14) / H16_BSCALE;
+#pragma unroll
+        for (int h = 0; h < NP; h++)
+#pragma unroll
+          for (int pl = 0; pl < 2; pl++) {
+            split_h2(v[h][pl][0].x * sc, v[h][pl][1].x * sc, ahi[h][0][pl], alo[h][0][pl]);
+            split_h2(v[h][pl][0].y * sc, v[h][pl][1].y * sc, ahi[h][1][pl], alo[h][1][pl]);
+          }
+      }
+      const unsigned mk = __ballot_sync(0xffffffffu, lane >= q && lane < nb && st.key[lane] == gk);
+      const int len = __popc(mk);
+      // Blocks of eight records of the run: this lane's B column is record gq.
+      for (int k8 = q; k8 < q + len; k8 += 8) {
+        const int sb = (k8 + gq < q + len) ? k8 + gq : H16_BATCH;
+        const uint32_t ob = st.off[sb];
+        const float* kvc = st.kv + sb * H16_COL + 8 - (int)(ob >> 8);
+        uint32_t bhi, blo;
+        split_h2(kvc[2 * tq], kvc[2 * tq + 1], bhi, blo);
+        // This lane's outputs: records k8 + 2tq and k8 + 2tq + 1.
+        int s2[2];
+        float kwv[2][8], kuv[2];
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          const int k = k8 + 2 * tq + c;
+          s2[c] = (k < q + len) ? k : H16_BATCH;
+          const uint32_t o = st.off[s2[c]];
+          kuv[c] = st.ku[s2[c] * H16_COL + 8 + gq - (int)(o & 255u)];
+#pragma unroll
+          for (int j = 0; j < 8; j++) kwv[c][j] = st.kw[s2[c] * 8 + j];
+        }
+        float tr[2] = {0.0f, 0.0f}, ti[2] = {0.0f, 0.0f};
+#pragma unroll
+        for (int h = 0; h < NP; h++) {
+          float dre[4], dim[4];
+          hmma_zero(dre, ahi[h][0][0], ahi[h][0][1], bhi);
+          hmma(dre, ahi[h][0][0], ahi[h][0][1], blo);
+          hmma(dre, alo[h][0][0], alo[h][0][1], bhi);
+          hmma_zero(dim, ahi[h][1][0], ahi[h][1][1], bhi);
+          hmma(dim, ahi[h][1][0], ahi[h][1][1], blo);
+          hmma(dim, alo[h][1][0], alo[h][1][1], bhi);
+          // d[0], d[1]: plane 2h, columns 2tq, 2tq + 1; d[2], d[3]: plane 2h + 1
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            tr[c] = fmaf(kwv[c][2 * h], dre[c], tr[c]);
+            ti[c] = fmaf(kwv[c][2 * h], dim[c], ti[c]);
+            if (2 * h + 1 < S) {
+              tr[c] = fmaf(kwv[c][2 * h + 1], dre[2 + c], tr[c]);
+              ti[c] = fmaf(kwv[c][2 * h + 1], dim[2 + c], ti[c]);
+            }
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          tr[c] *= kuv[c];
+          ti[c] *= kuv[c];
+#pragma unroll
+          for (int o = 4; o < 32; o <<= 1) {
+            tr[c] += __shfl_xor_sync(0xffffffffu, tr[c], o);
+            ti[c] += __shfl_xor_sync(0xffffffffu, ti[c], o);
+          }
+        }
+        if (gq == 0) {
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            if (s2[c] == H16_BATCH) continue;
+            const float4 f = st.out[s2[c]];
+            const uint32_t idx = __float_as_uint(f.w);
+            cplx<float> accv{tr[c] * inv, ti[c] * inv * f.z};
+            if (!first) {
+              const cplx<float> prev = vis[idx];
+              accv = {accv.re + prev.re, accv.im + prev.im};
+            }
+            if (last) accv = {accv.re * f.x - accv.im * f.y, accv.re * f.y + accv.im * f.x};
+            vis[idx] = accv;
+          }
+        }
+      }
+      q += len;
+    }
+  }
+}
+
+}  // namespace fast

@@ -21,6 +21,7 @@
 // All w-planes of a call stay resident in HBM when they fit (a 9450^2
 // complex64 plane is 714 MB), so every visibility is read once per
 // direction and the footprint on all of its planes is formed in one pass.
+#include <cuda_fp16.h>
 #include <cufft.h>
 
 #include <algorithm>
@@ -61,6 +62,8 @@ struct ScanOut {
   unsigned long long lo_bits;  // min |w| as the bits of a non-negative double
   unsigned long long hi_bits;  // max |w|
   unsigned long long u_bits;   // max |u| in metres over all rows (k_umax); +inf if any is not finite
+  unsigned long long vmax_bits;  // max |vis| |wgt| over the active set (a scan with the visibilities)
+  unsigned long long wmax_bits;  // max |wgt| over the active set
 };
 
 // The largest |u| (metres) over all rows, +inf when one is not finite: times
@@ -118,6 +121,8 @@ __global__ void k_scan_init(ScanOut* so) {
   so->lo_bits = (unsigned long long)__double_as_longlong(1e300);
   so->hi_bits = 0;
   so->u_bits = 0;
+  so->vmax_bits = 0;
+  so->wmax_bits = 0;
 }
 
 // The scan gives each warp runs of 32 x SCAN_ROUNDS consecutive visibilities,
@@ -146,14 +151,14 @@ struct RoundStep {
 // scan (wgridder.rs:1051-1077): the count is exact and min/max are order
 // independent, so the result is the reference's bit for bit.
 template <class T>
-__global__ void __launch_bounds__(256, 8) k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__ uvw,
+__global__ void __launch_bounds__(256, 6) k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__ uvw,
                        const double* __restrict__ foc, double fw, Inputs in, int with_vis, ScanOut* out) {
   const uint64_t n = (uint64_t)nrow * nchan;
   const uint64_t run = 32ull * SCAN_ROUNDS;
   const uint64_t wid = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t wstride = (((uint64_t)gridDim.x * blockDim.x) >> 5) * run;
   unsigned long long cnt = 0, fin = 0;
-  double lo = 1e300, hi = 0.0;
+  double lo = 1e300, hi = 0.0, vm = 0.0, wm = 0.0;
   uint64_t i0 = wid * run + (threadIdx.x & 31);
   RowCh rc(i0, nchan, wstride);
   const RoundStep step(nchan);
@@ -162,7 +167,23 @@ __global__ void __launch_bounds__(256, 8) k_scan(uint32_t nrow, uint32_t nchan, 
 #pragma unroll
     for (int u = 0; u < SCAN_ROUNDS; u++) {
       const uint64_t i = i0 + 32u * u;
-      act[u] = i < n && is_active<T>(in, with_vis != 0, i);
+      act[u] = false;
+      if (i < n) {  // is_active, keeping the magnitudes for the value bound
+        double tnorm = 1.0;
+        if (with_vis) {
+          const cplx<T> v = vis_get<T>(in, i);
+          tnorm = (double)(v.re * v.re + v.im * v.im);
+        }
+        const double twgt = in.wgt_kind != WGT_NONE ? (double)wgt_get<T>(in, i) : 1.0;
+        const double tmask = in.mask ? (double)in.mask[i] : 1.0;
+        act[u] = tnorm * twgt * tmask != 0.0;
+        if (act[u]) {
+          const double aw = fabs(twgt);
+          wm = aw > wm ? aw : wm;
+          const double av = sqrt(tnorm) * aw;
+          vm = av > vm ? av : vm;
+        }
+      }
     }
     uint32_t row = rc.row, ch = rc.ch;
 #pragma unroll
@@ -183,7 +204,11 @@ __global__ void __launch_bounds__(256, 8) k_scan(uint32_t nrow, uint32_t nchan, 
   fin = warp_sum(fin);
   lo = warp_min(lo);
   hi = warp_max(hi);
+  vm = warp_max(vm);
+  wm = warp_max(wm);
   if ((threadIdx.x & 31) == 0 && cnt) {
+    if (vm > 0.0) atomicMax(&out->vmax_bits, (unsigned long long)__double_as_longlong(vm));
+    if (wm > 0.0) atomicMax(&out->wmax_bits, (unsigned long long)__double_as_longlong(wm));
     atomicAdd(&out->count, cnt);
     if (fin) {
       atomicAdd(&out->finite, fin);
@@ -196,10 +221,10 @@ __global__ void __launch_bounds__(256, 8) k_scan(uint32_t nrow, uint32_t nchan, 
 // ------------------------------------------------------------------ binning
 
 // Setup::locate (wgridder.rs:1244-1255) as one key: the tile and first plane
-// of the reference's layout, refined by the 8 x 8 sub-tile of the first tap:
+// of the reference's layout, refined by the sub-tile of the first tap:
 // ((tile * nbuckets + plane) * nsub + sub-tile). Sorting by it keeps the
 // reference's (tile, plane) order and groups each plane's visibilities by
-// sub-tile, which the tensor-core gridder contracts block by block.
+// sub-tile, whose footprints the tensor-core kernels take as one window.
 template <class T>
 __device__ __forceinline__ uint32_t bin_of_rc(const Geom<T>& g, const double* __restrict__ uvw,
                                               const double* __restrict__ foc, uint32_t row, uint32_t ch,
@@ -214,7 +239,7 @@ __device__ __forceinline__ uint32_t bin_of_rc(const Geom<T>& g, const double* __
   const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
   const uint32_t tu = su >> g.log2tile, tv = sv >> g.log2tile;
   const uint32_t mask = (1u << g.log2tile) - 1u;
-  const uint32_t sub = ((su & mask) >> 3) * (uint32_t)g.nsub_v + ((sv & mask) >> g.log2subv);
+  const uint32_t sub = ((su & mask) / (uint32_t)g.sube) * (uint32_t)g.nsub_side + (sv & mask) / (uint32_t)g.sube;
   if (piu0) *piu0 = iu0;
   if (piv0) *piv0 = iv0;
   return ((tu * (uint32_t)g.ntv + tv) * (uint32_t)g.nbuckets + (uint32_t)minplane(g, w)) * (uint32_t)g.nsub + sub;
@@ -295,6 +320,8 @@ __global__ void k_bin_scatter(uint64_t n, const uint32_t* __restrict__ key, uint
       if (k[u] != INACTIVE) sorted[pos[u]] = (uint32_t)(i + u * stride);
   }
 }
+
+#include "wgrid_fast.cuh"
 
 // ------------------------------------------------------------------ exclusive scan (u32)
 
@@ -434,21 +461,18 @@ __global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t stride
 
 // ------------------------------------------------------------------ gridding
 
-// One grid cell += (re, im): a single 8-byte vector reduction in L2 for
-// complex float, two scalar ones for complex double.
-__device__ __forceinline__ void add_cell(cplx<float>* dst, float re, float im) {
-  atomicAdd(reinterpret_cast<float2*>(dst), make_float2(re, im));
-}
-__device__ __forceinline__ void add_cell(cplx<double>* dst, double re, double im) {
-  atomicAdd(&dst->re, re);
-  atomicAdd(&dst->im, im);
-}
+// One footprint term in the grid's fixed-point unit (`sc` = 2^q): the term
+// is rounded once in working precision, then scaled exactly and rounded to
+// an integer, so the sums below are exact and order-independent.
+__device__ __forceinline__ long long fix_term(float x, float sc) { return __float2ll_rn(x * sc); }
+__device__ __forceinline__ long long fix_term(double x, double sc) { return __double2ll_rn(x * sc); }
 
 // Thread layout of the gridding kernel. Thread (x, y, z) owns the window
 // cells whose u index is x mod S, v index y mod S and plane (z + k Z) mod S:
 // every footprint (S x S cells on each of S planes) holds exactly one cell of
 // each owner and plane residue, so the threads accumulate in shared memory
-// without atomics and in a fixed order (the visibilities' sorted order).
+// without atomics. Each term is added in the grid's fixed-point unit, so the
+// sums do not depend on the order of the visibilities.
 template <int S>
 struct GridLayout {
   static constexpr int S2 = S * S;
@@ -509,17 +533,20 @@ template <class T, int S>
 __global__ void __launch_bounds__(GridLayout<S>::THREADS)
     k_grid(const __grid_constant__ Geom<T> g, Inputs in, int mode, const double* __restrict__ uvw,
            const double* __restrict__ foc, const uint32_t* __restrict__ sorted, const Task* __restrict__ tasks,
-           const uint32_t* __restrict__ ntasks, cplx<T>* __restrict__ grids, int pg0, int npg, int gmax, int batch,
-           int* __restrict__ err) {
+           const uint32_t* __restrict__ ntasks, fast::FixCell* __restrict__ grids, int pg0, int npg, int gmax,
+           int batch, int* __restrict__ err, fast::FixScale* __restrict__ fs) {
   using Lay = GridLayout<S>;
   using St = GridStaging<T, S>;
+  using fast::FixCell;
   constexpr int S2 = S * S;
   if (blockIdx.x >= *ntasks) return;
   extern __shared__ __align__(16) unsigned char smem[];
   const int L = g.L, LL = L * L;
-  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem);
+  FixCell* buf = reinterpret_cast<FixCell*>(smem);
   St st;
-  st.carve(smem + (size_t)gmax * LL * sizeof(cplx<T>), batch);
+  st.carve(smem + (size_t)gmax * LL * sizeof(FixCell), batch);
+  const T sc = (T)ldexp(1.0, fs->q);
+  bool bad = false;
   const Task t = tasks[blockIdx.x];
   const int tu = (int)(t.tile / (uint32_t)g.ntv), tv = (int)(t.tile - (uint32_t)tu * (uint32_t)g.ntv);
   const int bu = tu << g.log2tile, bv = tv << g.log2tile;
@@ -535,14 +562,14 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
   const int oz = tid % Lay::Z, oxy = tid / Lay::Z;
   for (int w0 = lo; w0 <= hi; w0 += gmax) {
     const int gw = min(gmax, hi - w0 + 1);
-    for (int c = tid; c < gw * LL; c += blockDim.x) buf[c] = cplx<T>{(T)0, (T)0};
+    for (int c = tid; c < gw * LL; c += blockDim.x) buf[c] = FixCell{0, 0};
     // The owner's running sums: consecutive contributions to one cell are
     // added in registers and the sum added to the window when the cell changes.
-    cplx<T> acc[Lay::JPER];
+    FixCell acc[Lay::JPER];
     int cur[Lay::JPER];
 #pragma unroll
     for (int jj = 0; jj < Lay::JPER; jj++) {
-      acc[jj] = cplx<T>{(T)0, (T)0};
+      acc[jj] = FixCell{0, 0};
       cur[jj] = -1;
     }
     for (uint32_t kb = t.k0; kb < t.k1; kb += (uint32_t)batch) {
@@ -632,14 +659,16 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
             const int at = pv.pl * LL + c.off;
             if (at != cur[jj]) {
               if (cur[jj] >= 0) {
-                cplx<T> o = buf[cur[jj]];
-                buf[cur[jj]] = cplx<T>{o.re + acc[jj].re, o.im + acc[jj].im};
+                FixCell o = buf[cur[jj]];
+                buf[cur[jj]] = FixCell{o.re + acc[jj].re, o.im + acc[jj].im};
               }
               cur[jj] = at;
-              acc[jj] = cplx<T>{(T)0, (T)0};
+              acc[jj] = FixCell{0, 0};
             }
-            acc[jj].re = fma_t(pv.re, c.kk, acc[jj].re);
-            acc[jj].im = fma_t(pv.im, c.kk, acc[jj].im);
+            const T tr = pv.re * c.kk, ti = pv.im * c.kk;
+            bad |= !isfinite(tr) || !isfinite(ti);
+            acc[jj].re += fix_term(tr, sc);
+            acc[jj].im += fix_term(ti, sc);
           }
         }
       }
@@ -648,21 +677,21 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
 #pragma unroll
       for (int jj = 0; jj < Lay::JPER; jj++)
         if (cur[jj] >= 0) {
-          cplx<T> o = buf[cur[jj]];
-          buf[cur[jj]] = cplx<T>{o.re + acc[jj].re, o.im + acc[jj].im};
+          FixCell o = buf[cur[jj]];
+          buf[cur[jj]] = FixCell{o.re + acc[jj].re, o.im + acc[jj].im};
         }
     }
     __syncthreads();
     for (int c = tid; c < gw * LL; c += blockDim.x) {
-      const cplx<T> v = buf[c];
-      if (v.re == (T)0 && v.im == (T)0) continue;
+      const FixCell v = buf[c];
+      if (v.re == 0 && v.im == 0) continue;
       const int pl = c / LL, rem = c - pl * LL, i = rem / L, j = rem - i * L;
       const int row = (bu + i + g.nu / 2) % g.nu, col = (bv + j + g.nv / 2) % g.nv;
-      cplx<T>* dst = grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col;
-      add_cell(dst, v.re, v.im);
+      fast::fix_add(grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col, v.re, v.im);
     }
     __syncthreads();
   }
+  if (bad) atomicOr(&fs->nonfinite, 1);
 }
 
 // ------------------------------------------------------------------ tensor-core gridding (3 x TF32)
@@ -686,8 +715,8 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
 //
 // Staging (one visibility per lane) stores, per slot, the u taps at [8, 8+S)
 // of a zero-padded 24-entry column, the B entries (value * v tap, complex) at
-// [3, 3+S) of an 11-entry column, and the S w-taps; the zero padding makes
-// every operand fetch a plain load (at row - du + 8, column - dv + 3). Slot
+// [4, 4+S) of a 12-entry column, and the S w-taps; the zero padding makes
+// every operand fetch a plain load (at row - du + 8, column - dv + 4). Slot
 // TC_BATCH is all zero and stands in for the missing visibilities of a short
 // block. B is split into TF32 hi and lo where a block loads it, which keeps a
 // slot at 256 bytes and lets more warps share an SM.
@@ -696,8 +725,8 @@ constexpr uint32_t TC_CHUNK = 8192;  // sorted visibilities per warp
 // u-tap columns: 24 entries, taps at [8, 8 + S), read at row - du + 8; the
 // slot stride (25) is odd so that the lanes' stores fall in distinct banks.
 constexpr int TC_USTRIDE = 25;
-// B columns: 11 float2 entries, taps at [3, 3 + S), read at column - dv + 3
-// (dv < 4); a slot stride of 96 bytes puts the four slots a half-warp reads
+// B columns: 12 float2 entries, taps at [4, 4 + S), read at column - dv + 4
+// (dv < sube <= 5); a slot stride of 96 bytes puts the four slots a half-warp reads
 // (eight bytes per lane, four consecutive columns each) 32 bytes apart mod
 // 128, in distinct banks.
 constexpr int TC_VSTRIDE = 12;
@@ -754,22 +783,23 @@ __device__ __forceinline__ void tc_decode(const Geom<float>& g, uint32_t key, in
   const uint32_t tu = tile / (uint32_t)g.ntv, tv = tile - tu * (uint32_t)g.ntv;
   // Tiles are laid out on the shifted indices (i0 + n/2) mod n; the grid
   // itself is stored unshifted.
-  su0 = (int)(((tu << g.log2tile) + (sub / (uint32_t)g.nsub_v) * 8u + (uint32_t)(g.nu - g.nu / 2)) %
+  su0 = (int)(((tu << g.log2tile) + (sub / (uint32_t)g.nsub_side) * (uint32_t)g.sube + (uint32_t)(g.nu - g.nu / 2)) %
               (uint32_t)g.nu);
-  sv0 = (int)(((tv << g.log2tile) + ((sub % (uint32_t)g.nsub_v) << g.log2subv) + (uint32_t)(g.nv - g.nv / 2)) %
+  sv0 = (int)(((tv << g.log2tile) + (sub % (uint32_t)g.nsub_side) * (uint32_t)g.sube + (uint32_t)(g.nv - g.nv / 2)) %
               (uint32_t)g.nv);
 }
 
-// Adds a bin's windows to its planes of the grid.
+// Adds a bin's windows to its planes of the fixed-point grid (each sum
+// rounded once to the grid's unit, `sc` = 2^q).
 template <int S>
-__device__ __forceinline__ void tc_flush(const Geom<float>& g, cplx<float>* __restrict__ grids, int pg0, int su0,
-                                         int sv0, int mp, unsigned pact, const float (&acc)[S][2][4]) {
+__device__ __forceinline__ void tc_flush(const Geom<float>& g, fast::FixCell* __restrict__ grids, int pg0, int su0,
+                                         int sv0, int mp, unsigned pact, const float (&acc)[S][2][4], float sc) {
   const int lane = threadIdx.x & 31, gq = lane >> 2, tq = lane & 3;
   const size_t plane = (size_t)g.nu * g.nv;
 #pragma unroll
   for (int j = 0; j < S; j++) {
     if (!((pact >> j) & 1u)) continue;
-    cplx<float>* pl = grids + (size_t)(mp + j - pg0) * plane;
+    fast::FixCell* pl = grids + (size_t)(mp + j - pg0) * plane;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       const float re = acc[j][0][r], im = acc[j][1][r];
@@ -777,7 +807,7 @@ __device__ __forceinline__ void tc_flush(const Geom<float>& g, cplx<float>* __re
       int row = su0 + gq + (r >= 2 ? 8 : 0), col = sv0 + 2 * tq + (r & 1);
       while (row >= g.nu) row -= g.nu;
       while (col >= g.nv) col -= g.nv;
-      atomicAdd(reinterpret_cast<float2*>(pl + (size_t)row * g.nv + col), make_float2(re, im));
+      fast::fix_add(pl + (size_t)row * g.nv + col, __float2ll_rn(re * sc), __float2ll_rn(im * sc));
     }
   }
 }
@@ -787,8 +817,9 @@ template <int S>
 __global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
     k_grid_tc(const __grid_constant__ Geom<float> g, Inputs in, int mode, const double* __restrict__ uvw,
               const double* __restrict__ foc, const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend,
-              cplx<float>* __restrict__ grids, int pg0, int npg) {
+              fast::FixCell* __restrict__ grids, int pg0, int npg, const fast::FixScale* __restrict__ fs) {
   static_assert(S <= 8, "windows hold 8 + S - 1 <= 16 rows");
+  const float fsc = ldexpf(1.0f, fs->q);
   extern __shared__ __align__(16) unsigned char smem[];
   TcSlots st;
   st.carve(smem);
@@ -801,7 +832,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
   const uint32_t nchan = (uint32_t)g.nchan;
   const int np = g.do_wgridding ? S : 1;
   const uint32_t tmask = (1u << g.log2tile) - 1u;
-  const uint32_t vmask = (1u << g.log2subv) - 1u;
+  const uint32_t se = (uint32_t)g.sube;
 
   float acc[S][2][4];
 #pragma unroll
@@ -831,10 +862,10 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
         int64_t iu0, iv0;
         getpix(g, u, v, uf, vf, iu0, iv0);
         const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
-        const uint32_t sub = ((su & tmask) >> 3) * (uint32_t)g.nsub_v + ((sv & tmask) >> g.log2subv);
+        const uint32_t sa = (su & tmask) / se, sb = (sv & tmask) / se;
         key = (((su >> g.log2tile) * (uint32_t)g.ntv + (sv >> g.log2tile)) * (uint32_t)g.nbuckets + (uint32_t)mp) *
-                  (uint32_t)g.nsub + sub;
-        duv = (su & 7u) | ((sv & vmask) << 8);
+                  (uint32_t)g.nsub + sa * (uint32_t)g.nsub_side + sb;
+        duv = ((su & tmask) - sa * se) | (((sv & tmask) - sb * se) << 8);
         float ku[S], kv[S];
         const float x0 = (float)(-uf * 2.0 + ((double)S - 1.0));
         const float y0 = (float)(-vf * 2.0 + ((double)S - 1.0));
@@ -842,7 +873,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
         cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
         if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
         float* cu = st.ku + lane * TC_USTRIDE + 8;
-        float2* cb = st.kb + lane * TC_VSTRIDE + 3;
+        float2* cb = st.kb + lane * TC_VSTRIDE + 4;
         float* cw = st.kw + lane * TC_WSTRIDE;
 #pragma unroll
         for (int i = 0; i < S; i++) {
@@ -867,7 +898,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
     while (q < nb) {
       const uint32_t gk = st.key[q];
       if (gk != gcur) {
-        if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
+        if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc, fsc);
 #pragma unroll
         for (int j = 0; j < S; j++)
 #pragma unroll
@@ -893,8 +924,8 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
         const float* u0 = st.ku + e0 * TC_USTRIDE + gq - du0 + 8;
         const float* u1 = st.ku + e1 * TC_USTRIDE + gq - du1 + 8;
         const float ku00 = u0[0], ku01 = u0[8], ku10 = u1[0], ku11 = u1[8];
-        const float2 b0 = st.kb[e0 * TC_VSTRIDE + gq - dv0 + 3];
-        const float2 b1 = st.kb[e1 * TC_VSTRIDE + gq - dv1 + 3];
+        const float2 b0 = st.kb[e0 * TC_VSTRIDE + gq - dv0 + 4];
+        const float2 b1 = st.kb[e1 * TC_VSTRIDE + gq - dv1 + 4];
         uint32_t brh0, brl0, bih0, bil0, brh1, brl1, bih1, bil1;
         split_fast(b0.x, brh0, brl0);
         split_fast(b0.y, bih0, bil0);
@@ -950,7 +981,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 6 ? 20 : 12)
       q += kbk;
     }
   }
-  if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
+  if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc, fsc);
 }
 
 // ------------------------------------------------------------------ tensor-core gridding (3 x BF16)
@@ -995,8 +1026,9 @@ template <int S>
 __global__ void __launch_bounds__(TC_BATCH, S <= 5 ? 20 : S == 6 ? 16 : 12)
     k_grid_bf16(const __grid_constant__ Geom<float> g, Inputs in, int mode, const double* __restrict__ uvw,
                 const double* __restrict__ foc, const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend,
-                cplx<float>* __restrict__ grids, int pg0, int npg) {
+                fast::FixCell* __restrict__ grids, int pg0, int npg, const fast::FixScale* __restrict__ fs) {
   static_assert(S <= 8, "windows hold 8 + S - 1 <= 16 rows");
+  const float fsc = ldexpf(1.0f, fs->q);
   extern __shared__ __align__(16) unsigned char smem[];
   TcSlots st;
   st.carve(smem);
@@ -1009,7 +1041,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 5 ? 20 : S == 6 ? 16 : 12)
   const uint32_t nchan = (uint32_t)g.nchan;
   const int np = g.do_wgridding ? S : 1;
   const uint32_t tmask = (1u << g.log2tile) - 1u;
-  const uint32_t vmask = (1u << g.log2subv) - 1u;
+  const uint32_t se = (uint32_t)g.sube;
 
   float acc[S][2][4];
 #pragma unroll
@@ -1039,10 +1071,10 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 5 ? 20 : S == 6 ? 16 : 12)
         int64_t iu0, iv0;
         getpix(g, u, v, uf, vf, iu0, iv0);
         const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
-        const uint32_t sub = ((su & tmask) >> 3) * (uint32_t)g.nsub_v + ((sv & tmask) >> g.log2subv);
+        const uint32_t sa = (su & tmask) / se, sb = (sv & tmask) / se;
         key = (((su >> g.log2tile) * (uint32_t)g.ntv + (sv >> g.log2tile)) * (uint32_t)g.nbuckets + (uint32_t)mp) *
-                  (uint32_t)g.nsub + sub;
-        duv = (su & 7u) | ((sv & vmask) << 8);
+                  (uint32_t)g.nsub + sa * (uint32_t)g.nsub_side + sb;
+        duv = ((su & tmask) - sa * se) | (((sv & tmask) - sb * se) << 8);
         float ku[S], kv[S];
         const float x0 = (float)(-uf * 2.0 + ((double)S - 1.0));
         const float y0 = (float)(-vf * 2.0 + ((double)S - 1.0));
@@ -1050,7 +1082,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 5 ? 20 : S == 6 ? 16 : 12)
         cplx<float> val = unit_value<float>(g, b, imflip, f, in.wgt_kind != WGT_NONE, wgt_get<float>(in, idx));
         if (mode == VALUE_DATA) val = data_value<float>(vis_get<float>(in, idx), val, (float)imflip);
         float* cu = st.ku + lane * TC_USTRIDE + 8;
-        float2* cb = st.kb + lane * TC_VSTRIDE + 3;
+        float2* cb = st.kb + lane * TC_VSTRIDE + 4;
         float* cw = st.kw + lane * TC_WSTRIDE;
 #pragma unroll
         for (int i = 0; i < S; i++) {
@@ -1075,7 +1107,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 5 ? 20 : S == 6 ? 16 : 12)
     while (q < nb) {
       const uint32_t gk = st.key[q];
       if (gk != gcur) {
-        if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
+        if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc, fsc);
 #pragma unroll
         for (int j = 0; j < S; j++)
 #pragma unroll
@@ -1111,7 +1143,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 5 ? 20 : S == 6 ? 16 : 12)
           const float* u = st.ku + e[i] * TC_USTRIDE + gq - du + 8;
           ku0[i] = u[0];
           ku1[i] = u[8];
-          bv[i] = st.kb[e[i] * TC_VSTRIDE + gq - dv + 3];
+          bv[i] = st.kb[e[i] * TC_VSTRIDE + gq - dv + 4];
         }
         uint32_t brh0, brl0, bih0, bil0, brh1, brl1, bih1, bil1;
         split_bf16(bv[0].x, bv[1].x, brh0, brl0);
@@ -1168,7 +1200,7 @@ __global__ void __launch_bounds__(TC_BATCH, S <= 5 ? 20 : S == 6 ? 16 : 12)
       q += kbk;
     }
   }
-  if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc);
+  if (gcur != INACTIVE) tc_flush<S>(g, grids, pg0, su0, sv0, mpc, pact, acc, fsc);
 }
 
 // ------------------------------------------------------------------ degridding
@@ -1657,7 +1689,8 @@ void fft_touched_rows(FftPair& all, cplx<T>* plane, int nu, int nv, int b, int d
 template <class T, int S>
 void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, const Inputs& in, int mode,
                  const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
-                 const uint32_t* ntasks, cplx<T>* grids, int pg0, int npg, int gmax, int* err) {
+                 const uint32_t* ntasks, fast::FixCell* grids, int pg0, int npg, int gmax, int* err,
+                 fast::FixScale* fs) {
   if (nblocks == 0) return;
   const int batch = staging_batch<T, S>();
   const int total = smem + batch * (int)GridStaging<T, S>::bytes_per_vis();
@@ -1665,39 +1698,71 @@ void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, c
   {
     StageTimer timer_(ST_GRID, s);
     k_grid<T, S><<<nblocks, GridLayout<S>::THREADS, total, s>>>(g, in, mode, uvw, foc, sorted, tasks, ntasks, grids,
-                                                                pg0, npg, gmax, batch, err);
+                                                                pg0, npg, gmax, batch, err, fs);
   }
   check_cuda(cudaGetLastError(), "grid kernel");
 }
 
 template <int S>
 void launch_grid_tc(cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode, const double* uvw,
-                    const double* foc, const uint32_t* sorted, uint64_t kbase, uint64_t kend, cplx<float>* grids,
-                    int pg0, int npg) {
+                    const double* foc, const uint32_t* sorted, uint64_t kbase, uint64_t kend, fast::FixCell* grids,
+                    int pg0, int npg, const fast::FixScale* fs) {
   if (kend <= kbase) return;
   const int smem = (int)TcSlots::bytes();
   const unsigned nblocks = (unsigned)((kend - kbase + TC_CHUNK - 1) / TC_CHUNK);
   check_cuda(cudaFuncSetAttribute(k_grid_tc<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
   {
     StageTimer timer_(ST_GRID, s);
-    k_grid_tc<S><<<nblocks, TC_BATCH, smem, s>>>(g, in, mode, uvw, foc, sorted, kbase, kend, grids, pg0, npg);
+    k_grid_tc<S><<<nblocks, TC_BATCH, smem, s>>>(g, in, mode, uvw, foc, sorted, kbase, kend, grids, pg0, npg, fs);
   }
   check_cuda(cudaGetLastError(), "grid kernel (tensor cores)");
 }
 
 template <int S>
 void launch_grid_bf16(cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode, const double* uvw,
-                      const double* foc, const uint32_t* sorted, uint64_t kbase, uint64_t kend, cplx<float>* grids,
-                      int pg0, int npg) {
+                      const double* foc, const uint32_t* sorted, uint64_t kbase, uint64_t kend, fast::FixCell* grids,
+                      int pg0, int npg, const fast::FixScale* fs) {
   if (kend <= kbase) return;
   const int smem = (int)TcSlots::bytes();
   const unsigned nblocks = (unsigned)((kend - kbase + TC_CHUNK - 1) / TC_CHUNK);
   check_cuda(cudaFuncSetAttribute(k_grid_bf16<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
   {
     StageTimer timer_(ST_GRID, s);
-    k_grid_bf16<S><<<nblocks, TC_BATCH, smem, s>>>(g, in, mode, uvw, foc, sorted, kbase, kend, grids, pg0, npg);
+    k_grid_bf16<S><<<nblocks, TC_BATCH, smem, s>>>(g, in, mode, uvw, foc, sorted, kbase, kend, grids, pg0, npg, fs);
   }
   check_cuda(cudaGetLastError(), "grid kernel (tensor cores, 3 x BF16)");
+}
+
+template <int S>
+void launch_grid_i8(cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode, const fast::VisRecord* rec,
+                    const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins, fast::FixCell* grids,
+                    int pg0, int npg, fast::FixScale* fs) {
+  if (kend <= kbase) return;
+  const int smem = (int)fast::I8Slots::bytes();
+  const unsigned nblocks = (unsigned)((kend - kbase + fast::I8_CHUNK - 1) / fast::I8_CHUNK);
+  check_cuda(cudaFuncSetAttribute(fast::k_grid_i8<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
+  {
+    StageTimer timer_(ST_GRID, s);
+    fast::k_grid_i8<S><<<nblocks, fast::I8_BATCH, smem, s>>>(g, in, mode, rec, sorted, kbase, kend, nbins, grids,
+                                                             pg0, npg, fs);
+  }
+  check_cuda(cudaGetLastError(), "grid kernel (integer tensor cores)");
+}
+
+template <int S>
+void launch_degrid_h(cudaStream_t s, const Geom<float>& g, const Inputs& wts, const fast::VisRecord* rec,
+                     const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
+                     const cplx<float>* grids, int pg0, int npg, cplx<float>* vis, int first, int last) {
+  if (kend <= kbase) return;
+  const int smem = (int)fast::H16Slots::bytes();
+  const unsigned nblocks = (unsigned)((kend - kbase + fast::H16_CHUNK - 1) / fast::H16_CHUNK);
+  check_cuda(cudaFuncSetAttribute(fast::k_degrid_h<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
+  {
+    StageTimer timer_(ST_DEGRID, s);
+    fast::k_degrid_h<S><<<nblocks, fast::H16_BATCH, smem, s>>>(g, wts, rec, sorted, kbase, kend, nbins, grids, pg0,
+                                                               npg, vis, first, last);
+  }
+  check_cuda(cudaGetLastError(), "degrid kernel (tensor cores)");
 }
 
 template <class T, int S>
@@ -1753,7 +1818,7 @@ void check_cuda(cudaError_t e, const char* what) {
 }
 
 const char* const STAGE_NAMES[N_STAGES] = {"scan", "bin_count", "prefix", "bin_scatter", "tasks", "corr", "grid",
-                                           "fft", "project", "correct_input", "place", "degrid", "other"};
+                                           "fft", "project", "correct_input", "place", "degrid", "fixed_point", "other"};
 
 namespace {
 struct Profiler {
@@ -1850,7 +1915,7 @@ int grid_method() {
   if (m < 0) {
     const char* e = std::getenv("RANG_WGRIDDER_GPU_METHOD");
     const std::string v = e ? e : "";
-    m = v == "fp32" ? GRID_FP32 : v == "bf16x3" ? GRID_BF16X3 : GRID_TF32X3;
+    m = v == "fp32" ? GRID_FP32 : v == "bf16x3" ? GRID_BF16X3 : v == "tf32x3" ? GRID_TF32X3 : GRID_INT8;
     g_method = m;
   }
   return m;
@@ -1909,6 +1974,12 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
     std::memset(&info_, 0, sizeof(info_));
     return;
   }
+  bound_.alloc(sizeof(fast::ValueBound), s);
+  check_cuda(cudaMemsetAsync(bound_.get(), 0, sizeof(fast::ValueBound), s), "memset");
+  fast::k_bound_init<<<1, 1, 0, s>>>(bound_.as<fast::ValueBound>(), r.vmax_bits, r.wmax_bits);
+  scale_.alloc(sizeof(fast::FixScale), s);
+  scan_in_ = act;
+  scan_vis_ = with_vis;
   make_geom<T>(o, nrow, nchan, nvis_, wmin_d, wmax_d, r_l_, r_m_, g_, info_, kernel_);
   double umax_d = 0.0;  // metres; times the largest f / c
   std::memcpy(&umax_d, &r.u_bits, sizeof(double));
@@ -1946,7 +2017,13 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
   key_.alloc(n_ * 4, s);
   starts_.alloc((nkeys + 1) * 4, s);
   check_cuda(cudaMemsetAsync(starts_.get(), 0, (nkeys + 1) * 4, s), "memset");
-  {
+  if constexpr (sizeof(T) == 4) {  // with the records of the tensor-core kernels
+    rec_.alloc(n_ * sizeof(fast::VisRecord), s);
+    StageTimer timer_(ST_BIN_COUNT, s);
+    fast::k_bin_count_rec<<<blocks_for(n_, 256), 256, 0, s>>>(
+        g_, uvw_.as<double>(), foc_.as<double>(), act, with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>(),
+        rec_.as<fast::VisRecord>(), K > 1 ? (uint32_t)rows_per_chunk_ : 0u, (uint32_t)nbins_);
+  } else {
     StageTimer timer_(ST_BIN_COUNT, s);
     k_bin_count<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act,
                                                         with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>(),
@@ -2023,7 +2100,20 @@ bool Plan<T>::same_scan(const Inputs& act, bool with_vis, cudaStream_t s) const 
   check_cuda(cudaMemcpyAsync(&r, so.get(), sizeof(r), cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaStreamSynchronize(s), "scan");
   if (r.count != scan_[0] || r.finite != scan_[1]) return false;
-  return r.finite == 0 || (r.lo_bits == scan_[2] && r.hi_bits == scan_[3]);
+  if (!(r.finite == 0 || (r.lo_bits == scan_[2] && r.hi_bits == scan_[3]))) return false;
+  if (nvis_ && bound_.get()) {  // the same active set: this scan's value maxima hold for it
+    fast::k_bound_init<<<1, 1, 0, s>>>(bound_.as<fast::ValueBound>(), r.vmax_bits, r.wmax_bits);
+    scan_in_ = act;
+    scan_vis_ = with_vis;
+  }
+  return true;
+}
+
+template <class T>
+bool Plan<T>::bound_of(const Inputs& d, ValueMode mode) const {
+  if (d.wgt != scan_in_.wgt || d.wgt2 != scan_in_.wgt2 || d.wgt_kind != scan_in_.wgt_kind) return false;
+  if (mode == VALUE_UNIT) return true;
+  return scan_vis_ && d.vis == scan_in_.vis && d.vis_kind == scan_in_.vis_kind;
 }
 
 // The kernel's correction function at the image's pixel frequencies, cfu =
@@ -2076,89 +2166,133 @@ void Plan<T>::corrections(cudaStream_t s) {
   }
 }
 
+// Planes that fit at once: each takes `plane_bytes` (its grid and its image
+// columns, transposed); `fixed` bytes more are needed whatever the group.
 template <class T>
-size_t Plan<T>::plane_group(size_t cell_bytes) const {
+size_t Plan<T>::plane_group(size_t plane_bytes, size_t fixed) const {
   size_t nplanes = (size_t)std::max(g_.nplanes, 1);
-  size_t plane = ((size_t)g_.nu * g_.nv + (size_t)g_.ny * g_.nu) * cell_bytes;  // the plane and its columns, transposed
   size_t freeb = 0, total = 0;
   check_cuda(cudaMemGetInfo(&freeb, &total), "memory info");
   size_t budget = std::min<size_t>(freeb / 2, (size_t)64 << 30);
-  size_t group = std::max<size_t>(1, budget / plane);
+  budget = budget > fixed ? budget - fixed : 0;
+  size_t group = std::max<size_t>(1, budget / plane_bytes);
   return std::min(group, nplanes);
 }
 
 // Zeroes the rows of n planes that the gridder writes and the transforms
 // read: every row when `rows` is 0, else storage rows [0, rows) and
 // [nu - rows, nu) of each plane (the others are never read).
-template <class T>
-void zero_touched(cplx<T>* grids, int n, const Geom<T>& g, int rows, cudaStream_t s) {
-  const size_t plane = (size_t)g.nu * g.nv, row = (size_t)g.nv * sizeof(cplx<T>);
+void zero_touched(void* grids, size_t cell_bytes, int n, int nu, int nv, int rows, cudaStream_t s) {
+  const size_t plane = (size_t)nu * nv * cell_bytes, row = (size_t)nv * cell_bytes;
+  unsigned char* base = static_cast<unsigned char*>(grids);
   if (rows == 0) {
-    check_cuda(cudaMemsetAsync(grids, 0, (size_t)n * plane * sizeof(cplx<T>), s), "memset");
+    check_cuda(cudaMemsetAsync(base, 0, (size_t)n * plane, s), "memset");
     return;
   }
   for (int p = 0; p < n; p++) {
-    cplx<T>* pl = grids + (size_t)p * plane;
+    unsigned char* pl = base + (size_t)p * plane;
     check_cuda(cudaMemsetAsync(pl, 0, (size_t)rows * row, s), "memset");
-    check_cuda(cudaMemsetAsync(pl + (size_t)(g.nu - rows) * g.nv, 0, (size_t)rows * row, s), "memset");
+    check_cuda(cudaMemsetAsync(pl + (size_t)(nu - rows) * row, 0, (size_t)rows * row, s), "memset");
   }
 }
 
 template <class T>
-void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready) {
+void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready,
+                   bool scanned) {
   size_t npix = (size_t)o_.nx * o_.ny;
   if (nvis_ == 0) {
     check_cuda(cudaMemsetAsync(image, 0, npix * sizeof(T), s), "memset");
     return;
   }
+  using fast::FixCell;
   const size_t cell = sizeof(cplx<T>);
   const size_t nplanes = (size_t)std::max(g_.nplanes, 1);
-  const size_t group = plane_group(cell);
   const size_t plane = (size_t)g_.nu * g_.nv;
-  DevBuf grids(group * plane * cell, s);
   const size_t tplane = (size_t)g_.ny * g_.nu;  // a plane's image columns, transposed
+  const size_t group = plane_group(plane * sizeof(FixCell) + tplane * cell, plane * cell + npix * sizeof(T));
+  DevBuf grids(group * plane * sizeof(FixCell), s);
+  DevBuf fpl(plane * cell, s);  // the plane being transformed, in floating point
   DevBuf cols(group * tplane * cell, s);
   DevBuf acc(group < nplanes ? npix * sizeof(T) : 0, s);
   FftPair& fft = fft_plans<T>(g_.nu, g_.nv, g_.ny);
-  const int gmax = std::min<int>(max_window_planes(g_.L, sizeof(cplx<T>)), (int)std::min<size_t>(nplanes, 64));
-  const int smem = gmax * g_.L * g_.L * (int)sizeof(cplx<T>);
+  const int gmax =
+      std::min<int>(max_window_planes(g_.L, sizeof(FixCell)), (int)std::min<size_t>(nplanes, 64));
+  const int smem = gmax * g_.L * g_.L * (int)sizeof(FixCell);
   const double* corr = corr_.as<double>();
   const size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
+  const bool integer = sizeof(T) == 4 && grid_method() == GRID_INT8;
+  // The fixed-point scales: from the scan's value maxima when `data` is the
+  // scanned input, else from a pass over `data` (after all of it arrived).
+  if (ready)
+    for (int c = 0; c < nchunk_; c++) check_cuda(cudaStreamWaitEvent(s, ready[c], 0), "wait");
+  const fast::ValueBound* values = bound_.as<fast::ValueBound>();
+  DevBuf vb;
+  if (!(scanned && bound_of(data, mode))) {
+    vb.alloc(sizeof(fast::ValueBound), s);
+    check_cuda(cudaMemsetAsync(vb.get(), 0, sizeof(fast::ValueBound), s), "memset");
+    {
+      StageTimer timer_(ST_OTHER, s);
+      fast::k_value_max<T><<<blocks_for(n_, 256, 148u * 8u), 256, 0, s>>>(n_, data, key_.as<uint32_t>(),
+                                                                         vb.as<fast::ValueBound>());
+    }
+    check_cuda(cudaGetLastError(), "value bound");
+    values = vb.as<fast::ValueBound>();
+  }
+  {
+    StageTimer timer_(ST_OTHER, s);
+    fast::k_fix_scale<<<1, 1, 0, s>>>(values, mode == VALUE_UNIT ? 1 : 0, (unsigned long long)nvis_, integer ? 1 : 0,
+                                      scale_.as<fast::FixScale>());
+  }
+  check_cuda(cudaGetLastError(), "scale");
+  fast::FixScale* fs = scale_.as<fast::FixScale>();
+  const int rows = touched_row_count(urows_, g_.nu);
   for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
     int n = (int)std::min(group, nplanes - pg0);
-    zero_touched<T>(grids.as<cplx<T>>(), n, g_, touched_row_count(urows_, g_.nu), s);
+    zero_touched(grids.get(), sizeof(FixCell), n, g_.nu, g_.nv, rows, s);
+    FixCell* fg = grids.as<FixCell>();
     auto run = [&](auto S) {
       constexpr int SV = decltype(S)::value;
-      for (int c = 0; c < nchunk_; c++) {  // row chunk c once its rows are on the device
-        if (ready && pg0 == 0) check_cuda(cudaStreamWaitEvent(s, ready[c], 0), "wait");
+      for (int c = 0; c < nchunk_; c++) {
         if constexpr (sizeof(T) == 4) {
+          const uint64_t k0 = chunk_sorted_[c], k1 = chunk_sorted_[c + 1];
+          if (integer) {
+            if constexpr (SV <= 8)
+              launch_grid_i8<SV>(s, g_, data, (int)mode, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(), k0, k1,
+                                 (uint32_t)nbins_, fg, (int)pg0, n, fs);
+            continue;
+          }
           if (grid_method() == GRID_TF32X3) {
             launch_grid_tc<SV>(s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(), sorted_.as<uint32_t>(),
-                               chunk_sorted_[c], chunk_sorted_[c + 1], grids.as<cplx<T>>(), (int)pg0, n);
+                               k0, k1, fg, (int)pg0, n, fs);
             continue;
           }
           if (grid_method() == GRID_BF16X3) {
             launch_grid_bf16<SV>(s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(),
-                                 sorted_.as<uint32_t>(), chunk_sorted_[c], chunk_sorted_[c + 1],
-                                 grids.as<cplx<T>>(), (int)pg0, n);
+                                 sorted_.as<uint32_t>(), k0, k1, fg, (int)pg0, n, fs);
             continue;
           }
         }
         launch_grid<T, SV>(smem, chunk_tasks_[c + 1] - chunk_tasks_[c], s, g_, data, (int)mode, uvw_.as<double>(),
                            foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>() + chunk_tasks_[c],
-                           ntasks_.as<uint32_t>(), grids.as<cplx<T>>(), (int)pg0, n, gmax, err_.as<int>());
+                           ntasks_.as<uint32_t>(), fg, (int)pg0, n, gmax, err_.as<int>(), fs);
       }
     };
     if constexpr (sizeof(T) == 4)
       with_supp_float(g_.supp, run);
     else
       with_supp_double(g_.supp, run);
-    const int rows = touched_row_count(urows_, g_.nu);
     const dim3 tgrid((unsigned)((g_.nu + 31) / 32), (unsigned)((g_.ny + 31) / 32)), tblock(32, 8);
     FftPair& tf = fft_row_plan<T>(g_.nu, g_.ny);  // the image columns, transposed: ny transforms of length nu
     for (int p = 0; p < n; p++) {
-      cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
+      const FixCell* fpg = fg + (size_t)p * plane;
+      cplx<T>* pl = fpl.as<cplx<T>>();
       cplx<T>* tp = cols.as<cplx<T>>() + (size_t)p * tplane;
+      {
+        StageTimer timer_(ST_FIXED, s);
+        const uint64_t ncell = (uint64_t)(rows == 0 ? g_.nu : 2 * rows) * g_.nv;
+        fast::k_fix_to_plane<T><<<blocks_for(ncell, 256), 256, 0, s>>>(fpg, g_.nu, g_.nv, rows, fs, pl);
+      }
+      check_cuda(cudaGetLastError(), "fixed point");
       StageTimer timer_(ST_FFT, s, 3);
       fft_touched_rows<T>(fft, pl, g_.nu, g_.nv, rows, CUFFT_INVERSE, s);
       k_cols_to_t<T><<<tgrid, tblock, 0, s>>>(g_, pl, rows, tp);
@@ -2189,8 +2323,9 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
   const size_t npix = (size_t)o_.nx * o_.ny;
   const size_t cell = sizeof(cplx<T>);
   const size_t nplanes = (size_t)std::max(g_.nplanes, 1);
-  const size_t group = plane_group(cell);
   const size_t plane = (size_t)g_.nu * g_.nv;
+  const size_t tplane = (size_t)g_.ny * g_.nu;  // a plane's image columns, transposed
+  const size_t group = plane_group(plane * cell, tplane * cell + npix * sizeof(T));
   DevBuf grids(group * plane * cell, s);
   DevBuf img(npix * sizeof(T), s);
   FftPair& fft = fft_plans<T>(g_.nu, g_.nv, g_.ny);
@@ -2208,13 +2343,12 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
       (int)std::min<size_t>(nplanes, 64));
   const int smem = gmax * g_.L * Lp * (int)sizeof(cplx<T>);
   const int rows = touched_row_count(urows_, g_.nu);
-  const size_t tplane = (size_t)g_.ny * g_.nu;  // a plane's image columns, transposed
   DevBuf cols(tplane * cell, s);
   const dim3 tgrid((unsigned)((g_.nu + 31) / 32), (unsigned)((g_.ny + 31) / 32)), tblock(32, 8);
   FftPair& tf = fft_row_plan<T>(g_.nu, g_.ny);
   for (size_t pg0 = 0; pg0 < nplanes; pg0 += group) {
     int n = (int)std::min(group, nplanes - pg0);
-    zero_touched<T>(grids.as<cplx<T>>(), n, g_, rows, s);
+    zero_touched(grids.get(), cell, n, g_.nu, g_.nv, rows, s);
     for (int p = 0; p < n; p++) {
       cplx<T>* pl = grids.as<cplx<T>>() + (size_t)p * plane;
       check_cuda(cudaMemsetAsync(cols.get(), 0, tplane * cell, s), "memset");
@@ -2237,12 +2371,21 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
     }
     bool first = pg0 == 0, last = pg0 + n >= nplanes;
     auto run = [&](auto S) {
+      constexpr int SV = decltype(S)::value;
       for (int c = 0; c < nchunk_; c++) {  // row chunk c, final after the last plane group
-        launch_degrid<T, decltype(S)::value>(smem, chunk_tasks_[c + 1] - chunk_tasks_[c], s, g_, wts,
-                                             uvw_.as<double>(), foc_.as<double>(), sorted_.as<uint32_t>(),
-                                             tasks_.as<Task>() + chunk_tasks_[c], ntasks_.as<uint32_t>(),
-                                             grids.as<cplx<T>>(), (int)pg0, n, gmax,
-                                             reinterpret_cast<cplx<T>*>(vis), first, last, err_.as<int>());
+        bool fast_path = false;
+        if constexpr (sizeof(T) == 4 && SV <= 8) {
+          launch_degrid_h<SV>(s, g_, wts, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(), chunk_sorted_[c],
+                              chunk_sorted_[c + 1], (uint32_t)nbins_,
+                              reinterpret_cast<const cplx<float>*>(grids.as<cplx<T>>()), (int)pg0, n,
+                              reinterpret_cast<cplx<float>*>(vis), first, last);
+          fast_path = true;
+        }
+        if (!fast_path)
+          launch_degrid<T, SV>(smem, chunk_tasks_[c + 1] - chunk_tasks_[c], s, g_, wts, uvw_.as<double>(),
+                               foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>() + chunk_tasks_[c],
+                               ntasks_.as<uint32_t>(), grids.as<cplx<T>>(), (int)pg0, n, gmax,
+                               reinterpret_cast<cplx<T>*>(vis), first, last, err_.as<int>());
         if (done && last) check_cuda(cudaEventRecord(done[c], s), "record");
       }
     };
@@ -2267,11 +2410,21 @@ void Plan<T>::export_binning(uint32_t* key_host, uint32_t* sorted_host, cudaStre
   if (nvis_ == 0) return;
   if (nchunk_ != 1) throw DeviceError("binning export of a plan with row chunks");
   check_cuda(cudaMemcpyAsync(key_host, key_.get(), n_ * 4, cudaMemcpyDeviceToHost, s), "copy");
-  check_cuda(cudaMemcpyAsync(sorted_host, sorted_.get(), nvis_ * 4, cudaMemcpyDeviceToHost, s), "copy");
   check_cuda(cudaStreamSynchronize(s), "copy");
   // The reference's key, tile * nbuckets + plane, without the sub-tile.
   for (size_t i = 0; i < n_; i++)
     if (key_host[i] != INACTIVE) key_host[i] /= (uint32_t)g_.nsub;
+  // The reference's layout order (tile, first plane, row, channel): the
+  // device's keys ordered by a stable counting sort. The device's own sorted
+  // order leaves the order inside a bin free; gridding sums exact terms, so
+  // the results do not depend on it.
+  const size_t nref = (size_t)g_.ntu * g_.ntv * (size_t)g_.nbuckets;
+  std::vector<uint32_t> start(nref + 1, 0);
+  for (size_t i = 0; i < n_; i++)
+    if (key_host[i] != INACTIVE) start[key_host[i] + 1]++;
+  for (size_t b = 0; b < nref; b++) start[b + 1] += start[b];
+  for (size_t i = 0; i < n_; i++)
+    if (key_host[i] != INACTIVE) sorted_host[start[key_host[i]]++] = (uint32_t)i;
 }
 
 template <class T>

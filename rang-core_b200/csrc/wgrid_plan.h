@@ -78,8 +78,13 @@ class Plan {
 
   // vis2dirty into `image` (nx * ny, device): `data` gives the data and the
   // weights; VALUE_UNIT grids unit visibilities (the PSF). With `ready`
-  // (one event per row chunk), chunk c is gridded after ready[c].
-  void grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready = nullptr);
+  // (one event per row chunk), gridding waits for every ready[c]: the grid's
+  // fixed-point scale needs the largest value of all the data. `scanned`:
+  // `data` is the input this plan scanned (the same arrays, unchanged since),
+  // whose value bound the scan already took; otherwise one pass over `data`
+  // takes it.
+  void grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready = nullptr,
+            bool scanned = false);
   // dirty2vis of `image` into `vis` (nrow * nchan interleaved complex,
   // device, overwritten; inactive visibilities zero), times the weights of
   // `wts`. With `done` (one event per row chunk), done[c] is recorded once
@@ -111,7 +116,7 @@ class Plan {
   void build_layout(const Inputs& act, bool with_vis, cudaStream_t s);
   void corrections(cudaStream_t s);
   int touched_rows(double umax, double wmax) const;
-  size_t plane_group(size_t cell_bytes) const;
+  size_t plane_group(size_t plane_bytes, size_t fixed) const;
 
   WgridderOptions o_;
   size_t nrow_, nchan_, n_;
@@ -124,6 +129,9 @@ class Plan {
   DevBuf key_;      // u32 per visibility: bin or 0xffffffff
   DevBuf starts_;   // u32 per bin + 1: exclusive offsets
   DevBuf sorted_;   // u32 per active visibility: linear index
+  DevBuf rec_;      // single precision: a 32-byte record per active visibility, in sorted order
+  DevBuf bound_;    // the scan's largest |vis| |wgt| and |wgt|
+  DevBuf scale_;    // the fixed-point scales of the current gridding pass
   DevBuf tasks_;    // Task, at most max_tasks_
   DevBuf ntasks_;   // u32: tasks in use
   DevBuf corr_;     // double per pixel: the global correction
@@ -134,18 +142,28 @@ class Plan {
   std::vector<uint64_t> chunk_sorted_;  // nchunk_ + 1 offsets into the sorted order
   std::vector<uint32_t> chunk_tasks_;   // nchunk_ + 1 offsets into the task list
   unsigned long long scan_[4] = {0, 0, 0, 0};  // count, finite count, |w| min and max bits
+  // The arrays of the scan whose value maxima bound_ holds (with the
+  // visibilities when scan_vis_), to tell whether a gridding pass's data
+  // need their own bound.
+  mutable Inputs scan_in_{};
+  mutable bool scan_vis_ = false;
+  bool bound_of(const Inputs& data, ValueMode mode) const;
   // Grid rows (u) that footprints can touch: storage rows [0, urows_) and
   // [nu - urows_, nu); 0 means all rows (the v transforms run on these only).
   int urows_ = 0;
 };
 
-// How single-precision gridding accumulates footprints: split-precision
-// 3 x TF32 tensor-core products (default), split-precision 3 x BF16
-// tensor-core products (about 16 bits of each factor, for comparison), or
-// plain FP32 CUDA-core FMAs. Double precision always uses FP64 CUDA-core FMAs.
-// The environment variable RANG_WGRIDDER_GPU_METHOD (fp32 | tf32x3 | bf16x3)
-// sets the default.
-enum GridMethod : int { GRID_FP32 = 0, GRID_TF32X3 = 1, GRID_BF16X3 = 2 };
+// How single-precision gridding forms its sums: exact integer products of
+// 23-bit fixed-point factors on the integer tensor cores (default; results
+// independent of the visibilities' order), split-precision 3 x TF32 or
+// 3 x BF16 tensor-core products, or plain FP32 CUDA-core products (each term
+// rounded into the fixed-point grid, also order-independent). The float
+// tensor-core methods sum blocks of visibilities inside the tensor core, so
+// their results depend on the sorted order, which the counting sort's
+// atomics leave free. Double precision always uses FP64 CUDA-core products
+// rounded into the fixed-point grid. The environment variable
+// RANG_WGRIDDER_GPU_METHOD (int8 | fp32 | tf32x3 | bf16x3) sets the default.
+enum GridMethod : int { GRID_FP32 = 0, GRID_TF32X3 = 1, GRID_BF16X3 = 2, GRID_INT8 = 3 };
 int grid_method();
 void set_grid_method(int method);
 
@@ -155,7 +173,7 @@ int max_window_planes(int L, size_t cell_bytes);
 // Stages of the pipeline, for the launch counter and the event profiler.
 enum Stage : int {
   ST_SCAN = 0, ST_BIN_COUNT, ST_PREFIX, ST_BIN_SCATTER, ST_TASKS, ST_CORR, ST_GRID, ST_FFT, ST_PROJECT,
-  ST_CORRECT_INPUT, ST_PLACE, ST_DEGRID, ST_OTHER, N_STAGES
+  ST_CORRECT_INPUT, ST_PLACE, ST_DEGRID, ST_FIXED, ST_OTHER, N_STAGES
 };
 extern const char* const STAGE_NAMES[N_STAGES];
 

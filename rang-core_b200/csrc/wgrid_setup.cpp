@@ -330,14 +330,14 @@ void make_geom(const WgridderOptions& o, size_t nrow, size_t nchan, size_t nvis,
   g.ntu = (int32_t)((nu + tile - 1) / tile);
   g.ntv = (int32_t)((nv + tile - 1) / tile);
   g.L = tile + (int32_t)supp - 1;
-  // Sub-tiles group the visibilities whose footprints share one window of the
-  // tensor-core gridder: 16 rows along u (8 + supp - 1 <= 16) by 8 columns
-  // along v (2^log2subv + supp - 1 <= 8). Double precision, which has no
-  // tensor-core path, keeps 8 x 8.
-  g.nsub_side = tile >> 3;
-  g.log2subv = !single ? 3 : supp <= 5 ? 2 : supp <= 7 ? 1 : 0;
-  g.nsub_v = tile >> g.log2subv;
-  g.nsub = g.nsub_side * g.nsub_v;
+  // Sub-tiles group the visibilities whose footprints share one 8 x 8 window
+  // of the tensor-core gridder and degridder: sube = 9 - supp cells square
+  // (sube + supp - 1 = 8), ceil(tile / sube) of them along each side of a
+  // tile (the last one partial where sube does not divide the tile). Double
+  // precision, which has no tensor-core path, keeps 8 x 8 sub-tiles.
+  g.sube = single ? 9 - (int32_t)std::min<size_t>(supp, 8) : 8;
+  g.nsub_side = (tile + g.sube - 1) / g.sube;
+  g.nsub = g.nsub_side * g.nsub_side;
   g.do_wgridding = wgrid;
   g.lmshift = lmshift;
   g.shifting = lmshift || nshift != 0.0;

@@ -67,7 +67,9 @@ def test_chunked_dirty2vis_is_bit_identical(chunks, single, k):
 
 @pytest.mark.parametrize("single", [True, False])
 @pytest.mark.parametrize("k", [3, 7])
-def test_chunked_vis2dirty_matches(chunks, single, k):
+def test_chunked_vis2dirty_is_bit_identical(chunks, single, k):
+    """Gridding sums exact fixed-point terms, so a plan split into row chunks
+    (a different sorted order and split of the work) gives the same bits."""
     from rang import gridder as cw
 
     vis, wgt, mask, kw = _case(single)
@@ -76,7 +78,7 @@ def test_chunked_vis2dirty_matches(chunks, single, k):
     chunks(k)
     out, info2 = cw.vis2dirty(vis=vis, wgt=wgt, mask=mask, return_info=True, **kw)
     assert info1 == info2
-    assert rel_linf(out, ref) < (1e-6 if single else 1e-12)
+    assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
     oref = oracle.vis2dirty(vis=vis, wgt=wgt, mask=mask, **kw)
     assert rel_linf(out, oref) < TOL[single]
 
