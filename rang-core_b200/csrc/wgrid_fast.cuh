@@ -86,10 +86,14 @@ __global__ void k_bound_init(ValueBound* vb, unsigned long long vmax_bits, unsig
 // integer gridder's terms are at most 2^28 grid units (q = sb + 6), so int64
 // holds 2^34 of them. For the floating-point gridders a cell sums at most
 // nvis terms, each at most max |value| (taps are at most 1 + eps), and q
-// leaves 2 bits of headroom over that bound. The scales depend on nothing
+// leaves 2 bits of headroom over that bound in the cell's width (64 bits in
+// single precision, 128 in double: a 64-bit unit would sit about 2^-48 below
+// the largest term, which the wide-field correction factors amplify past
+// double precision's accuracy). The scales depend on nothing
 // but the values and the active count, so a plan split into row chunks
 // grids to the same bits as one without.
-__global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long long nvis, int integer, FixScale* fs) {
+__global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long long nvis, int integer, int wide,
+                            FixScale* fs) {
   double vmax = __longlong_as_double((long long)(unit ? values->wmax_bits : values->vmax_bits));
   if (!(vmax > 0.0) || !isfinite(vmax)) vmax = 1.0;
   const int ev = min(max(ilogb(vmax), -90), 90);  // vmax < 2^(ev + 1) (clamped: scales stay finite floats)
@@ -101,16 +105,90 @@ __global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long lo
     r.q = r.sb + 6;
   } else {
     r.sb = 0;
-    r.q = 60 - ev - ilogb((double)max(nvis, 1ull));  // nvis * vmax * 2^q < 2^62
+    // nvis * vmax * 2^q < 2^62 (int64 cells), < 2^126 (128-bit cells)
+    r.q = (wide ? 124 : 60) - ev - ilogb((double)max(nvis, 1ull));
   }
   *fs = r;
 }
 
+__device__ __forceinline__ void fix_add(FixCell* cell, long long re, long long im) {
+  if (re) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->re), (unsigned long long)re);
+  if (im) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->im), (unsigned long long)im);
+}
+
+// A 128-bit two's complement integer, hi * 2^64 + lo, and a double-precision
+// grid cell of two of them: value = (re + i im) * 2^-q.
+struct Fix128 {
+  unsigned long long lo;
+  long long hi;
+};
+struct FixCell2 {
+  Fix128 re, im;
+};
+
+__device__ __forceinline__ Fix128 add128(Fix128 a, Fix128 b) {
+  Fix128 r;
+  r.lo = a.lo + b.lo;
+  r.hi = a.hi + b.hi + (r.lo < a.lo ? 1 : 0);
+  return r;
+}
+
+// cell += v, exact mod 2^128 in any order: the carry out of each low-word
+// addition goes to the high word with that addition.
+__device__ __forceinline__ void fix_add128(Fix128* cell, Fix128 v) {
+  if (v.lo) {
+    const unsigned long long old = atomicAdd(&cell->lo, v.lo);
+    if (old + v.lo < old) v.hi += 1;
+  }
+  if (v.hi) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->hi), (unsigned long long)v.hi);
+}
+
+// The fixed-point cell and accumulator of each working precision.
+template <class T>
+struct FixTraits;
+template <>
+struct FixTraits<float> {
+  using Cell = FixCell;
+  using Acc = long long;
+  static constexpr int wide = 0;
+  // x * 2^q rounded to an integer (sc = 2^q)
+  static __device__ __forceinline__ float scale(int q) { return ldexpf(1.0f, q); }
+  static __device__ __forceinline__ Acc term(float x, float sc) { return __float2ll_rn(x * sc); }
+  static __device__ __forceinline__ Acc zero() { return 0; }
+  static __device__ __forceinline__ Acc add(Acc a, Acc b) { return a + b; }
+  static __device__ __forceinline__ bool nonzero(Acc a) { return a != 0; }
+  static __device__ __forceinline__ void flush(Cell* c, Acc re, Acc im) { fix_add(c, re, im); }
+  static __device__ __forceinline__ double value(long long v, int q) { return ldexp((double)v, -q); }
+};
+template <>
+struct FixTraits<double> {
+  using Cell = FixCell2;
+  using Acc = Fix128;
+  static constexpr int wide = 1;
+  // sc = 2^(q - 64): the high word is floor(x * sc), the low word the
+  // fraction times 2^64 (exact: the fraction of a double is a double)
+  static __device__ __forceinline__ double scale(int q) { return ldexp(1.0, q - 64); }
+  static __device__ __forceinline__ Acc term(double x, double sc) {
+    const double y = x * sc, h = floor(y);
+    return Fix128{__double2ull_rn((y - h) * 18446744073709551616.0), (long long)h};
+  }
+  static __device__ __forceinline__ Acc zero() { return Fix128{0ull, 0ll}; }
+  static __device__ __forceinline__ Acc add(Acc a, Acc b) { return add128(a, b); }
+  static __device__ __forceinline__ bool nonzero(Acc a) { return (a.lo | (unsigned long long)a.hi) != 0; }
+  static __device__ __forceinline__ void flush(Cell* c, Acc re, Acc im) {
+    fix_add128(&c->re, re);
+    fix_add128(&c->im, im);
+  }
+  static __device__ __forceinline__ double value(Fix128 v, int q) {
+    return ldexp((double)v.hi, 64 - q) + ldexp(__ull2double_rn(v.lo), -q);
+  }
+};
+
 // One plane of the fixed-point grid to floating point: rows [0, rows) and
 // [nu - rows, nu) (every row when rows is 0), each cell rounded once.
 template <class T>
-__global__ void k_fix_to_plane(const FixCell* __restrict__ fix, int nu, int nv, int rows, const FixScale* fs,
-                               cplx<T>* __restrict__ out) {
+__global__ void k_fix_to_plane(const typename FixTraits<T>::Cell* __restrict__ fix, int nu, int nv, int rows,
+                               const FixScale* fs, cplx<T>* __restrict__ out) {
   const int q = fs->q;
   const bool nan = fs->nonfinite != 0;
   const int nr = rows == 0 ? nu : 2 * rows;
@@ -118,20 +196,15 @@ __global__ void k_fix_to_plane(const FixCell* __restrict__ fix, int nu, int nv, 
   for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < n; c += (uint64_t)gridDim.x * blockDim.x) {
     const int r = (int)(c / nv);
     const uint64_t cell = (uint64_t)(rows == 0 || r < rows ? r : nu - 2 * rows + r) * nv + (c - (uint64_t)r * nv);
-    const FixCell f = fix[cell];
+    const auto f = fix[cell];
     cplx<T> v;
     if (nan) {
       v = {(T)__longlong_as_double(0x7ff8000000000000ll), (T)__longlong_as_double(0x7ff8000000000000ll)};
     } else {
-      v = {(T)ldexp((double)f.re, -q), (T)ldexp((double)f.im, -q)};
+      v = {(T)FixTraits<T>::value(f.re, q), (T)FixTraits<T>::value(f.im, q)};
     }
     out[cell] = v;
   }
-}
-
-__device__ __forceinline__ void fix_add(FixCell* cell, long long re, long long im) {
-  if (re) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->re), (unsigned long long)re);
-  if (im) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->im), (unsigned long long)im);
 }
 
 // ------------------------------------------------------------------ records
@@ -276,39 +349,118 @@ __device__ __forceinline__ void window_of(const Geom<float>& g, uint32_t key, ui
 
 // ------------------------------------------------------------------ integer gridder
 
+// ------------------------------------------------------------------ prefetch
+
+// The inputs of one staged record, copied asynchronously (cp.async) into
+// shared memory a round ahead of their use, so that the gathers of records,
+// visibilities and weights are in flight while the previous round is
+// contracted and take no registers.
+struct Prefetched {
+  uint4 rec[2];  // the record
+  uint4 vis;     // the visibility: complex64 in .x, .y or complex128
+  uint2 wgt;     // the weight: float32 in .x, float64, or the two float32 factors
+};
+
+__device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+  else if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Starts the copies of record `idx` and (with_vis, with_wgt) its value's inputs.
+__device__ __forceinline__ void prefetch(Prefetched* dst, const VisRecord* __restrict__ rec, const Inputs& in,
+                                         bool with_vis, bool with_wgt, uint32_t idx) {
+  const uint4* r = reinterpret_cast<const uint4*>(rec + idx);
+  cp_async(&dst->rec[0], r, 16);
+  cp_async(&dst->rec[1], r + 1, 16);
+  if (with_vis) {
+    if (in.vis_kind == VIS_C64)
+      cp_async(&dst->vis, reinterpret_cast<const float2*>(in.vis) + idx, 8);
+    else if (in.vis_kind == VIS_C128)
+      cp_async(&dst->vis, reinterpret_cast<const double2*>(in.vis) + idx, 16);
+  }
+  if (with_wgt) {
+    if (in.wgt_kind == WGT_F64) {
+      cp_async(&dst->wgt, reinterpret_cast<const double*>(in.wgt) + idx, 8);
+    } else if (in.wgt_kind == WGT_F32 || in.wgt_kind == WGT_F32_PRODUCT) {
+      cp_async(&dst->wgt.x, reinterpret_cast<const float*>(in.wgt) + idx, 4);
+      if (in.wgt_kind == WGT_F32_PRODUCT) cp_async(&dst->wgt.y, reinterpret_cast<const float*>(in.wgt2) + idx, 4);
+    }
+  }
+}
+
+__device__ __forceinline__ VisRecord prefetched_record(const Prefetched& p) {
+  const uint4 a = p.rec[0], b = p.rec[1];
+  return VisRecord{__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z), a.w,
+                   __uint_as_float(b.x), __uint_as_float(b.y), b.z, b.w};
+}
+// Weights::get and VisData::get (wgridder.rs:950-1005) of the copied values.
+__device__ __forceinline__ float prefetched_wgt(const Prefetched& p, const Inputs& in) {
+  switch (in.wgt_kind) {
+    case WGT_F32:
+      return __uint_as_float(p.wgt.x);
+    case WGT_F64:
+      return (float)__longlong_as_double((long long)(((unsigned long long)p.wgt.y << 32) | p.wgt.x));
+    case WGT_F32_PRODUCT:
+      return __uint_as_float(p.wgt.x) * __uint_as_float(p.wgt.y);
+    default:
+      return 1.0f;
+  }
+}
+__device__ __forceinline__ cplx<float> prefetched_vis(const Prefetched& p, const Inputs& in) {
+  if (in.vis_kind == VIS_C64) return {__uint_as_float(p.vis.x), __uint_as_float(p.vis.y)};
+  if (in.vis_kind == VIS_C128)
+    return {(float)__longlong_as_double((long long)(((unsigned long long)p.vis.y << 32) | p.vis.x)),
+            (float)__longlong_as_double((long long)(((unsigned long long)p.vis.w << 32) | p.vis.z))};
+  return {1.0f, 0.0f};
+}
+
+// ------------------------------------------------------------------ integer gridder
+
 constexpr int I8_BATCH = 32;         // records staged per round, one per lane
 constexpr uint32_t I8_CHUNK = 8192;  // sorted records per warp
-constexpr int I8_COL = 17;           // tap columns: taps at [8, 8 + S), read at 8 + row - offset (odd stride)
 constexpr float I8_ASCALE = 4194304.0f;  // 2^22
+// Integers x are formed as float(x + 0x8080) so that one cvt.rni gives the
+// offset that the balanced limbs need (|x| < 2^22 + 2^15, exact in FP32).
+constexpr float I8_OFFSET = 32896.0f;
+// Row strides (words) of the staging rows: with them the reads of the eight
+// records of a lane quad (slots 4 tq + j) fall in distinct banks.
+constexpr int I8_KU = 9;    // u taps placed on the window's 8 rows
+constexpr int I8_B = 9;     // float2: value * placed v taps * 2^sb + offset on the 8 columns
+constexpr int I8_KW = 10;   // w taps * 2^22 (8), as float2 pairs of planes
 
 // Staging of one round: per slot (record) the u taps and value * v taps
-// (scaled to integers' range) in zero-padded columns, the w taps times 2^22,
-// the window offsets and the key. Slot I8_BATCH stays zero.
+// placed on the window's rows and columns (zero, or the offset, elsewhere),
+// the w taps times 2^22 and the key. Slot I8_BATCH stays zero.
 struct I8Slots {
-  float* ku;     // [I8_BATCH + 1][I8_COL]
-  float2* bv;    // [I8_BATCH + 1][I8_COL]: value * kv * 2^sb
-  float* kw;     // [I8_BATCH + 1][8]: kw * 2^22, zero outside the pass's planes
-  uint32_t* key; // [I8_BATCH + 1]
-  uint32_t* off; // [I8_BATCH + 1]: du | dv << 8
+  float* ku;      // [I8_BATCH + 1][I8_KU]
+  float2* bv;     // [I8_BATCH + 1][I8_B]
+  float* kw;      // [I8_BATCH + 1][I8_KW]
+  uint32_t* key;  // [I8_BATCH + 1]
   __host__ __device__ static constexpr size_t bytes() {
-    return ((size_t)(I8_BATCH + 1) * (I8_COL * 4 + I8_COL * 8 + 8 * 4 + 8) + 15) / 16 * 16;
+    return ((size_t)(I8_BATCH + 1) * (I8_B * 8 + I8_KU * 4 + I8_KW * 4 + 4) + 15) / 16 * 16;
   }
+  // bv and kw are read as float2: both start on 8-byte boundaries.
   __device__ void carve(unsigned char* base) {
     bv = reinterpret_cast<float2*>(base);
-    ku = reinterpret_cast<float*>(bv + (I8_BATCH + 1) * I8_COL);
-    kw = ku + (I8_BATCH + 1) * I8_COL;
-    key = reinterpret_cast<uint32_t*>(kw + (I8_BATCH + 1) * 8);
-    off = key + (I8_BATCH + 1);
+    kw = reinterpret_cast<float*>(bv + (I8_BATCH + 1) * I8_B);
+    ku = kw + (I8_BATCH + 1) * I8_KW;
+    key = reinterpret_cast<uint32_t*>(ku + (I8_BATCH + 1) * I8_KU);
   }
 };
 
-// Three balanced 8-bit limbs of four integers |x| < 2^22 + 2^15, packed
-// per limb (byte j of limb register L holds limb L of x[j]).
-__device__ __forceinline__ void limbs4(int x0, int x1, int x2, int x3, uint32_t& l0, uint32_t& l1, uint32_t& l2) {
-  // y = x + 0x8080: bytes 0 and 1 of y are the low limbs plus 128, y >> 16
-  // (byte 2 of y, as a signed byte) is the top limb.
-  const uint32_t y0 = (uint32_t)(x0 + 0x8080), y1 = (uint32_t)(x1 + 0x8080);
-  const uint32_t y2 = (uint32_t)(x2 + 0x8080), y3 = (uint32_t)(x3 + 0x8080);
+// Three balanced 8-bit limbs of four integers y - 0x8080 (y = x + 0x8080,
+// |x| < 2^22 + 2^15), packed per limb (byte j of limb register L holds limb
+// L of x[j]): bytes 0 and 1 of y are the low limbs plus 128, y >> 16 (byte 2
+// of y, as a signed byte) is the top limb.
+__device__ __forceinline__ void limbs4(uint32_t y0, uint32_t y1, uint32_t y2, uint32_t y3, uint32_t& l0, uint32_t& l1,
+                                       uint32_t& l2) {
   const uint32_t a01 = __byte_perm(y0, y1, 0x5140), a23 = __byte_perm(y2, y3, 0x5140);  // b0 b0' b1 b1'
   l0 = __byte_perm(a01, a23, 0x5410) ^ 0x80808080u;
   l1 = __byte_perm(a01, a23, 0x7632) ^ 0x80808080u;
@@ -349,12 +501,14 @@ __device__ __forceinline__ void i8_flush(const Geom<float>& g, FixCell* __restri
 }
 
 // Gridding of records [kbase, kend) (single precision): each warp takes
-// I8_CHUNK consecutive records, stages I8_BATCH at a time, and per run of
-// one bin forms the integer limbs of A (rows: w tap x placed u tap of planes
-// 2h and 2h + 1, columns: the run's records) and B (rows: records, columns:
-// value x placed v tap) and adds their limb products into int32 fragments
-// on the tensor cores; at the end of a bin the fragments are combined into
-// int64 and added to the grid. Records outside the run read the zero slot.
+// I8_CHUNK consecutive sorted records, stages I8_BATCH at a time, and per run
+// of one bin forms the integer limbs of A (rows: w tap x placed u tap of
+// planes 2h and 2h + 1, columns: the run's records) and B (rows: records,
+// columns: value x placed v tap) and adds their limb products into int32
+// fragments on the tensor cores; at the end of a bin the fragments are
+// combined into int64 and added to the grid. Records outside the run read
+// the zero slot. The next round's records and values are loaded while the
+// current round is contracted.
 template <int S>
 __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
     k_grid_i8(const __grid_constant__ Geom<float> g, Inputs in, int mode, const VisRecord* __restrict__ rec,
@@ -366,10 +520,15 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
   I8Slots st;
   st.carve(smem);
   const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
-  for (int c = lane; c < (int)(I8Slots::bytes() / 16); c += I8_BATCH)
-    reinterpret_cast<float4*>(smem)[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  if (lane == 0) st.key[I8_BATCH] = INACTIVE;
-  __syncwarp();
+  {  // the zero slot: u and w taps 0, B rows at the offset (value 0)
+    float* zk = st.ku + I8_BATCH * I8_KU;
+    float2* zb = st.bv + I8_BATCH * I8_B;
+    float* zw = st.kw + I8_BATCH * I8_KW;
+    if (lane < I8_KU) zk[lane] = 0.0f;
+    if (lane < I8_B) zb[lane] = make_float2(I8_OFFSET, I8_OFFSET);
+    if (lane < I8_KW) zw[lane] = 0.0f;
+    if (lane == 0) st.key[I8_BATCH] = INACTIVE;
+  }
   const uint64_t k0 = kbase + (uint64_t)blockIdx.x * I8_CHUNK;
   const uint64_t k1 = min(kend, k0 + I8_CHUNK);
   const float bscale = ldexpf(1.0f, fs->sb);
@@ -387,24 +546,44 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
   uint32_t gcur = INACTIVE;
   int su0 = 0, sv0 = 0, mpc = 0;
 
+  // Rounds ahead: this round's inputs are in pre (copied asynchronously),
+  // nidx is the next round's index.
+  Prefetched* pre = reinterpret_cast<Prefetched*>(smem + I8Slots::bytes()) + lane;
+  const bool with_vis = mode == VALUE_DATA && in.vis_kind != VIS_UNIT, with_wgt = in.wgt_kind != WGT_NONE;
+  if (k0 + lane < k1) prefetch(pre, rec, in, with_vis, with_wgt, sorted[k0 + lane]);
+  cp_async_commit();
+  uint32_t nidx = (k0 + I8_BATCH + lane < k1) ? sorted[k0 + I8_BATCH + lane] : 0u;
+
   for (uint64_t kb = k0; kb < k1; kb += I8_BATCH) {
     const int nb = (int)min((uint64_t)I8_BATCH, k1 - kb);
+    cp_async_wait_all();
     __syncwarp();
     if (lane < nb) {  // staging, one record per lane
-      const VisRecord r = rec[sorted[kb + lane]];
+      const VisRecord r = prefetched_record(*pre);
+      const float wt = prefetched_wgt(*pre, in);
+      const cplx<float> vv = with_vis ? prefetched_vis(*pre, in) : cplx<float>{1.0f, 0.0f};
       float ku[S], kv[S], kw[S];
       eval_taps2<float, S>(g.coeff, g.ne, r.x0, r.y0, ku, kv);
       if (g.do_wgridding) eval_taps1<S>(g.coeff, r.xw, kw);
-      const cplx<float> val = record_value(r, in, mode);
-      const int mp = (int)(r.meta >> 16);
-      float* cu = st.ku + lane * I8_COL + 8;
-      float2* cb = st.bv + lane * I8_COL + 8;
-      float* cw = st.kw + lane * 8;
+      // record_value: value = vis * phase * wgt, imaginary part negated where w was flipped.
+      const float flip = (r.meta & 256u) ? -1.0f : 1.0f;
+      const float pr = r.ph_re * wt, pi = r.ph_im * wt;
+      const float vr = vv.re * pr - vv.im * pi, vi = (vv.re * pi + vv.im * pr) * flip;
+      bad |= !isfinite(vr) || !isfinite(vi) || !isfinite(r.x0) || !isfinite(r.y0) || !isfinite(r.xw);
+      const int mp = (int)(r.meta >> 16), du = (int)(r.meta & 15u), dv = (int)((r.meta >> 4) & 15u);
+      float* cu = st.ku + lane * I8_KU;
+      float2* cb = st.bv + lane * I8_B;
+      float* cw = st.kw + lane * I8_KW;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        cu[i] = 0.0f;
+        cb[i] = make_float2(I8_OFFSET, I8_OFFSET);
+      }
+      const float br = vr * bscale, bi = vi * bscale;
 #pragma unroll
       for (int i = 0; i < S; i++) {
-        cu[i] = ku[i];
-        cb[i] = make_float2(val.re * bscale * kv[i], val.im * bscale * kv[i]);
-        bad |= !isfinite(cb[i].x) || !isfinite(cb[i].y) || !isfinite(ku[i]);
+        cu[du + i] = ku[i];
+        cb[dv + i] = make_float2(fmaf(br, kv[i], I8_OFFSET), fmaf(bi, kv[i], I8_OFFSET));
       }
 #pragma unroll
       for (int j = 0; j < 8; j++) {
@@ -414,13 +593,15 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
         } else if (j == 0) {
           w = I8_ASCALE;
         }
-        bad |= !isfinite(w);
         cw[j] = w;
       }
       st.key[lane] = r.bin;
-      st.off[lane] = (r.meta & 15u) | (((r.meta >> 4) & 15u) << 8);
     }
+    // The next round's record and value, in flight while this one is contracted.
     __syncwarp();
+    if (kb + I8_BATCH + lane < k1) prefetch(pre, rec, in, with_vis, with_wgt, nidx);
+    cp_async_commit();
+    if (kb + 2 * I8_BATCH + lane < k1) nidx = sorted[kb + 2 * I8_BATCH + lane];
     int q = 0;
     while (q < nb) {
       const uint32_t gk = st.key[q];
@@ -448,39 +629,40 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
         slot[j] = (k >= q && k < q + len) ? k : I8_BATCH;
       }
       float kuv[8];
-      float2 bvv[8];
+      uint32_t b[2][3][2];  // B limbs per component: registers for k 4tq.. and 16 + 4tq..
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        const uint32_t o = st.off[slot[j]];
-        kuv[j] = st.ku[slot[j] * I8_COL + 8 + gq - (int)(o & 255u)];
-        bvv[j] = st.bv[slot[j] * I8_COL + 8 + gq - (int)(o >> 8)];
-      }
-      // B limbs per component: registers for k 4tq.. and 16 + 4tq..
-      uint32_t b[2][3][2];
+      for (int hf = 0; hf < 2; hf++) {
+        float2 bvv[4];
 #pragma unroll
-      for (int c = 0; c < 2; c++)
-#pragma unroll
-        for (int hf = 0; hf < 2; hf++) {
-          int x[4];
-#pragma unroll
-          for (int j = 0; j < 4; j++) x[j] = __float2int_rn(c ? bvv[4 * hf + j].y : bvv[4 * hf + j].x);
-          limbs4(x[0], x[1], x[2], x[3], b[c][0][hf], b[c][1][hf], b[c][2][hf]);
+        for (int j = 0; j < 4; j++) {
+          kuv[4 * hf + j] = st.ku[slot[4 * hf + j] * I8_KU + gq];
+          bvv[j] = st.bv[slot[4 * hf + j] * I8_B + gq];
         }
+        limbs4(__float2int_rn(bvv[0].x), __float2int_rn(bvv[1].x), __float2int_rn(bvv[2].x),
+               __float2int_rn(bvv[3].x), b[0][0][hf], b[0][1][hf], b[0][2][hf]);
+        limbs4(__float2int_rn(bvv[0].y), __float2int_rn(bvv[1].y), __float2int_rn(bvv[2].y),
+               __float2int_rn(bvv[3].y), b[1][0][hf], b[1][1][hf], b[1][2][hf]);
+      }
 #pragma unroll
       for (int h = 0; h < NP; h++) {
         uint32_t a[3][4];  // per limb: rows gq (plane 2h), gq + 8 (plane 2h + 1) x k halves
 #pragma unroll
-        for (int hf = 0; hf < 2; hf++)
+        for (int hf = 0; hf < 2; hf++) {
+          float2 w[4];
 #pragma unroll
-          for (int pl = 0; pl < 2; pl++) {
-            int x[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-              const float w = (2 * h + pl < S) ? st.kw[slot[4 * hf + j] * 8 + 2 * h + pl] : 0.0f;
-              x[j] = __float2int_rn(w * kuv[4 * hf + j]);
-            }
-            limbs4(x[0], x[1], x[2], x[3], a[0][2 * hf + pl], a[1][2 * hf + pl], a[2][2 * hf + pl]);
-          }
+          for (int j = 0; j < 4; j++)
+            w[j] = 2 * h < S ? *reinterpret_cast<const float2*>(st.kw + slot[4 * hf + j] * I8_KW + 2 * h)
+                             : make_float2(0.0f, 0.0f);
+          limbs4(__float2int_rn(fmaf(w[0].x, kuv[4 * hf], I8_OFFSET)),
+                 __float2int_rn(fmaf(w[1].x, kuv[4 * hf + 1], I8_OFFSET)),
+                 __float2int_rn(fmaf(w[2].x, kuv[4 * hf + 2], I8_OFFSET)),
+                 __float2int_rn(fmaf(w[3].x, kuv[4 * hf + 3], I8_OFFSET)), a[0][2 * hf], a[1][2 * hf], a[2][2 * hf]);
+          limbs4(__float2int_rn(fmaf(w[0].y, kuv[4 * hf], I8_OFFSET)),
+                 __float2int_rn(fmaf(w[1].y, kuv[4 * hf + 1], I8_OFFSET)),
+                 __float2int_rn(fmaf(w[2].y, kuv[4 * hf + 2], I8_OFFSET)),
+                 __float2int_rn(fmaf(w[3].y, kuv[4 * hf + 3], I8_OFFSET)), a[0][2 * hf + 1], a[1][2 * hf + 1],
+                 a[2][2 * hf + 1]);
+        }
 #pragma unroll
         for (int c = 0; c < 2; c++) {
           // weight 2^32: a2 b2; 2^24: a2 b1 + a1 b2; 2^16: a2 b0 + a1 b1 + a0 b2
@@ -503,26 +685,27 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
 
 constexpr int H16_BATCH = 32;
 constexpr uint32_t H16_CHUNK = 8192;
-constexpr int H16_COL = 17;  // tap columns as I8_COL
 constexpr float H16_BSCALE = 16384.0f;  // 2^14: v taps stay clear of FP16 subnormals
+constexpr int H16_KU = 9;   // u taps placed on the window's 8 rows
+constexpr int H16_KV = 10;  // v taps * 2^14 placed on the 8 columns (read as float2)
+constexpr int H16_KW = 12;  // w taps (8, read as float4)
 
 struct H16Slots {
-  float* ku;      // [H16_BATCH + 1][H16_COL]: u taps at [8, 8 + S)
-  float* kv;      // [H16_BATCH + 1][H16_COL]: v taps * 2^14
-  float* kw;      // [H16_BATCH + 1][8]: w taps (zero outside the pass's planes)
   float4* out;    // [H16_BATCH + 1]: conj(phase) * wgt (re, im), imflip, index bits
+  float* kw;      // [H16_BATCH + 1][H16_KW]: w taps (zero outside the pass's planes)
+  float* kv;      // [H16_BATCH + 1][H16_KV]
+  float* ku;      // [H16_BATCH + 1][H16_KU]
   uint32_t* key;  // [H16_BATCH + 1]
-  uint32_t* off;  // [H16_BATCH + 1]
   __host__ __device__ static constexpr size_t bytes() {
-    return ((size_t)(H16_BATCH + 1) * (H16_COL * 8 + 8 * 4 + 16 + 8) + 15) / 16 * 16;
+    return ((size_t)(H16_BATCH + 1) * (16 + H16_KW * 4 + H16_KV * 4 + H16_KU * 4 + 4) + 15) / 16 * 16;
   }
+  // out and kw are read as float4, kv as float2: their offsets are aligned.
   __device__ void carve(unsigned char* base) {
     out = reinterpret_cast<float4*>(base);
-    ku = reinterpret_cast<float*>(out + (H16_BATCH + 1));
-    kv = ku + (H16_BATCH + 1) * H16_COL;
-    kw = kv + (H16_BATCH + 1) * H16_COL;
-    key = reinterpret_cast<uint32_t*>(kw + (H16_BATCH + 1) * 8);
-    off = key + (H16_BATCH + 1);
+    kw = reinterpret_cast<float*>(out + (H16_BATCH + 1));
+    kv = kw + (H16_BATCH + 1) * H16_KW;
+    ku = kv + (H16_BATCH + 1) * H16_KV;
+    key = reinterpret_cast<uint32_t*>(ku + (H16_BATCH + 1) * H16_KU);
   }
 };
 
@@ -559,7 +742,8 @@ __device__ __forceinline__ void hmma(float (&d)[4], uint32_t a0, uint32_t a1, ui
 // rows with shuffles. Each output depends only on its own record and the
 // window, so the result does not depend on the grouping. With plane groups
 // (first / last) the partial sums accumulate in `vis` and the final factor
-// is applied with the last group.
+// is applied with the last group. The next round's records are loaded while
+// the current round is contracted.
 template <int S>
 __global__ void __launch_bounds__(H16_BATCH, 16)
     k_degrid_h(const __grid_constant__ Geom<float> g, Inputs wts, const VisRecord* __restrict__ rec,
@@ -572,10 +756,15 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
   H16Slots st;
   st.carve(smem);
   const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
-  for (int c = lane; c < (int)(H16Slots::bytes() / 16); c += H16_BATCH)
-    reinterpret_cast<float4*>(smem)[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  if (lane == 0) st.key[H16_BATCH] = INACTIVE;
-  __syncwarp();
+  {  // the zero slot
+    if (lane < H16_KW) st.kw[H16_BATCH * H16_KW + lane] = 0.0f;
+    if (lane < H16_KV) st.kv[H16_BATCH * H16_KV + lane] = 0.0f;
+    if (lane < H16_KU) st.ku[H16_BATCH * H16_KU + lane] = 0.0f;
+    if (lane == 0) {
+      st.key[H16_BATCH] = INACTIVE;
+      st.out[H16_BATCH] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+  }
   const uint64_t k0 = kbase + (uint64_t)blockIdx.x * H16_CHUNK;
   const uint64_t k1 = min(kend, k0 + H16_CHUNK);
   const size_t plane = (size_t)g.nu * g.nv;
@@ -584,22 +773,35 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
   float inv = 0.0f;                       // 1 / (window scale * 2^14)
   uint32_t gcur = INACTIVE;
 
+  Prefetched* pre = reinterpret_cast<Prefetched*>(smem + H16Slots::bytes()) + lane;
+  const bool with_wgt = wts.wgt_kind != WGT_NONE;
+  if (k0 + lane < k1) prefetch(pre, rec, wts, false, with_wgt, sorted[k0 + lane]);
+  cp_async_commit();
+  uint32_t nidx = (k0 + H16_BATCH + lane < k1) ? sorted[k0 + H16_BATCH + lane] : 0u;
+
   for (uint64_t kb = k0; kb < k1; kb += H16_BATCH) {
     const int nb = (int)min((uint64_t)H16_BATCH, k1 - kb);
+    cp_async_wait_all();
     __syncwarp();
     if (lane < nb) {
-      const VisRecord r = rec[sorted[kb + lane]];
+      const VisRecord r = prefetched_record(*pre);
+      const float tw = prefetched_wgt(*pre, wts);
       float ku[S], kv[S], kw[S];
       eval_taps2<float, S>(g.coeff, g.ne, r.x0, r.y0, ku, kv);
       if (g.do_wgridding) eval_taps1<S>(g.coeff, r.xw, kw);
-      const int mp = (int)(r.meta >> 16);
-      float* cu = st.ku + lane * H16_COL + 8;
-      float* cv = st.kv + lane * H16_COL + 8;
-      float* cw = st.kw + lane * 8;
+      const int mp = (int)(r.meta >> 16), du = (int)(r.meta & 15u), dv = (int)((r.meta >> 4) & 15u);
+      float* cu = st.ku + lane * H16_KU;
+      float* cv = st.kv + lane * H16_KV;
+      float* cw = st.kw + lane * H16_KW;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        cu[i] = 0.0f;
+        cv[i] = 0.0f;
+      }
 #pragma unroll
       for (int i = 0; i < S; i++) {
-        cu[i] = ku[i];
-        cv[i] = kv[i] * H16_BSCALE;
+        cu[du + i] = ku[i];
+        cv[dv + i] = kv[i] * H16_BSCALE;
       }
 #pragma unroll
       for (int j = 0; j < 8; j++) {
@@ -612,13 +814,14 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
         cw[j] = w;
       }
       // The final factor conj(phase) * wgt (shift_phase with sign -1).
-      const float tw = wts.wgt_kind != WGT_NONE ? wgt_get<float>(wts, r.idx) : 1.0f;
       st.out[lane] = make_float4(r.ph_re * tw, -r.ph_im * tw, (r.meta & 256u) ? -1.0f : 1.0f,
                                  __uint_as_float(r.idx));
       st.key[lane] = r.bin;
-      st.off[lane] = (r.meta & 15u) | (((r.meta >> 4) & 15u) << 8);
     }
     __syncwarp();
+    if (kb + H16_BATCH + lane < k1) prefetch(pre, rec, wts, false, with_wgt, nidx);
+    cp_async_commit();
+    if (kb + 2 * H16_BATCH + lane < k1) nidx = sorted[kb + 2 * H16_BATCH + lane];
     int q = 0;
     while (q < nb) {
       const uint32_t gk = st.key[q];
@@ -664,10 +867,9 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
       // Blocks of eight records of the run: this lane's B column is record gq.
       for (int k8 = q; k8 < q + len; k8 += 8) {
         const int sb = (k8 + gq < q + len) ? k8 + gq : H16_BATCH;
-        const uint32_t ob = st.off[sb];
-        const float* kvc = st.kv + sb * H16_COL + 8 - (int)(ob >> 8);
+        const float2 kvp = *reinterpret_cast<const float2*>(st.kv + sb * H16_KV + 2 * tq);
         uint32_t bhi, blo;
-        split_h2(kvc[2 * tq], kvc[2 * tq + 1], bhi, blo);
+        split_h2(kvp.x, kvp.y, bhi, blo);
         // This lane's outputs: records k8 + 2tq and k8 + 2tq + 1.
         int s2[2];
         float kwv[2][8], kuv[2];
@@ -675,10 +877,17 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
         for (int c = 0; c < 2; c++) {
           const int k = k8 + 2 * tq + c;
           s2[c] = (k < q + len) ? k : H16_BATCH;
-          const uint32_t o = st.off[s2[c]];
-          kuv[c] = st.ku[s2[c] * H16_COL + 8 + gq - (int)(o & 255u)];
-#pragma unroll
-          for (int j = 0; j < 8; j++) kwv[c][j] = st.kw[s2[c] * 8 + j];
+          kuv[c] = st.ku[s2[c] * H16_KU + gq];
+          const float4 w0 = *reinterpret_cast<const float4*>(st.kw + s2[c] * H16_KW);
+          const float4 w1 = *reinterpret_cast<const float4*>(st.kw + s2[c] * H16_KW + 4);
+          kwv[c][0] = w0.x;
+          kwv[c][1] = w0.y;
+          kwv[c][2] = w0.z;
+          kwv[c][3] = w0.w;
+          kwv[c][4] = w1.x;
+          kwv[c][5] = w1.y;
+          kwv[c][6] = w1.z;
+          kwv[c][7] = w1.w;
         }
         float tr[2] = {0.0f, 0.0f}, ti[2] = {0.0f, 0.0f};
 #pragma unroll
@@ -715,14 +924,14 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
 #pragma unroll
           for (int c = 0; c < 2; c++) {
             if (s2[c] == H16_BATCH) continue;
-            const float4 f = st.out[s2[c]];
-            const uint32_t idx = __float_as_uint(f.w);
-            cplx<float> accv{tr[c] * inv, ti[c] * inv * f.z};
+            const float4 fo = st.out[s2[c]];
+            const uint32_t idx = __float_as_uint(fo.w);
+            cplx<float> accv{tr[c] * inv, ti[c] * inv * fo.z};
             if (!first) {
               const cplx<float> prev = vis[idx];
               accv = {accv.re + prev.re, accv.im + prev.im};
             }
-            if (last) accv = {accv.re * f.x - accv.im * f.y, accv.re * f.y + accv.im * f.x};
+            if (last) accv = {accv.re * fo.x - accv.im * fo.y, accv.re * fo.y + accv.im * fo.x};
             vis[idx] = accv;
           }
         }

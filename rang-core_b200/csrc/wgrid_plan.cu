@@ -461,11 +461,6 @@ __global__ void k_task_emit(const uint32_t* __restrict__ starts, uint32_t stride
 
 // ------------------------------------------------------------------ gridding
 
-// One footprint term in the grid's fixed-point unit (`sc` = 2^q): the term
-// is rounded once in working precision, then scaled exactly and rounded to
-// an integer, so the sums below are exact and order-independent.
-__device__ __forceinline__ long long fix_term(float x, float sc) { return __float2ll_rn(x * sc); }
-__device__ __forceinline__ long long fix_term(double x, double sc) { return __double2ll_rn(x * sc); }
 
 // Thread layout of the gridding kernel. Thread (x, y, z) owns the window
 // cells whose u index is x mod S, v index y mod S and plane (z + k Z) mod S:
@@ -533,11 +528,17 @@ template <class T, int S>
 __global__ void __launch_bounds__(GridLayout<S>::THREADS)
     k_grid(const __grid_constant__ Geom<T> g, Inputs in, int mode, const double* __restrict__ uvw,
            const double* __restrict__ foc, const uint32_t* __restrict__ sorted, const Task* __restrict__ tasks,
-           const uint32_t* __restrict__ ntasks, fast::FixCell* __restrict__ grids, int pg0, int npg, int gmax,
-           int batch, int* __restrict__ err, fast::FixScale* __restrict__ fs) {
+           const uint32_t* __restrict__ ntasks, typename fast::FixTraits<T>::Cell* __restrict__ grids, int pg0,
+           int npg, int gmax, int batch, int* __restrict__ err, fast::FixScale* __restrict__ fs) {
   using Lay = GridLayout<S>;
   using St = GridStaging<T, S>;
-  using fast::FixCell;
+  // Each term is rounded once in working precision, then scaled exactly and
+  // rounded to an integer in the grid's unit, so the sums are exact.
+  using Fx = fast::FixTraits<T>;
+  using Acc = typename Fx::Acc;
+  struct FixCell {
+    Acc re, im;
+  };
   constexpr int S2 = S * S;
   if (blockIdx.x >= *ntasks) return;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
   FixCell* buf = reinterpret_cast<FixCell*>(smem);
   St st;
   st.carve(smem + (size_t)gmax * LL * sizeof(FixCell), batch);
-  const T sc = (T)ldexp(1.0, fs->q);
+  const T sc = Fx::scale(fs->q);
   bool bad = false;
   const Task t = tasks[blockIdx.x];
   const int tu = (int)(t.tile / (uint32_t)g.ntv), tv = (int)(t.tile - (uint32_t)tu * (uint32_t)g.ntv);
@@ -562,14 +563,14 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
   const int oz = tid % Lay::Z, oxy = tid / Lay::Z;
   for (int w0 = lo; w0 <= hi; w0 += gmax) {
     const int gw = min(gmax, hi - w0 + 1);
-    for (int c = tid; c < gw * LL; c += blockDim.x) buf[c] = FixCell{0, 0};
+    for (int c = tid; c < gw * LL; c += blockDim.x) buf[c] = FixCell{Fx::zero(), Fx::zero()};
     // The owner's running sums: consecutive contributions to one cell are
     // added in registers and the sum added to the window when the cell changes.
     FixCell acc[Lay::JPER];
     int cur[Lay::JPER];
 #pragma unroll
     for (int jj = 0; jj < Lay::JPER; jj++) {
-      acc[jj] = FixCell{0, 0};
+      acc[jj] = FixCell{Fx::zero(), Fx::zero()};
       cur[jj] = -1;
     }
     for (uint32_t kb = t.k0; kb < t.k1; kb += (uint32_t)batch) {
@@ -660,15 +661,15 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
             if (at != cur[jj]) {
               if (cur[jj] >= 0) {
                 FixCell o = buf[cur[jj]];
-                buf[cur[jj]] = FixCell{o.re + acc[jj].re, o.im + acc[jj].im};
+                buf[cur[jj]] = FixCell{Fx::add(o.re, acc[jj].re), Fx::add(o.im, acc[jj].im)};
               }
               cur[jj] = at;
-              acc[jj] = FixCell{0, 0};
+              acc[jj] = FixCell{Fx::zero(), Fx::zero()};
             }
             const T tr = pv.re * c.kk, ti = pv.im * c.kk;
             bad |= !isfinite(tr) || !isfinite(ti);
-            acc[jj].re += fix_term(tr, sc);
-            acc[jj].im += fix_term(ti, sc);
+            acc[jj].re = Fx::add(acc[jj].re, Fx::term(tr, sc));
+            acc[jj].im = Fx::add(acc[jj].im, Fx::term(ti, sc));
           }
         }
       }
@@ -678,16 +679,16 @@ __global__ void __launch_bounds__(GridLayout<S>::THREADS)
       for (int jj = 0; jj < Lay::JPER; jj++)
         if (cur[jj] >= 0) {
           FixCell o = buf[cur[jj]];
-          buf[cur[jj]] = FixCell{o.re + acc[jj].re, o.im + acc[jj].im};
+          buf[cur[jj]] = FixCell{Fx::add(o.re, acc[jj].re), Fx::add(o.im, acc[jj].im)};
         }
     }
     __syncthreads();
     for (int c = tid; c < gw * LL; c += blockDim.x) {
       const FixCell v = buf[c];
-      if (v.re == 0 && v.im == 0) continue;
+      if (!Fx::nonzero(v.re) && !Fx::nonzero(v.im)) continue;
       const int pl = c / LL, rem = c - pl * LL, i = rem / L, j = rem - i * L;
       const int row = (bu + i + g.nu / 2) % g.nu, col = (bv + j + g.nv / 2) % g.nv;
-      fast::fix_add(grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col, v.re, v.im);
+      Fx::flush(grids + ((size_t)(w0 + pl - pg0) * g.nu + row) * g.nv + col, v.re, v.im);
     }
     __syncthreads();
   }
@@ -1689,8 +1690,8 @@ void fft_touched_rows(FftPair& all, cplx<T>* plane, int nu, int nv, int b, int d
 template <class T, int S>
 void launch_grid(int smem, unsigned nblocks, cudaStream_t s, const Geom<T>& g, const Inputs& in, int mode,
                  const double* uvw, const double* foc, const uint32_t* sorted, const Task* tasks,
-                 const uint32_t* ntasks, fast::FixCell* grids, int pg0, int npg, int gmax, int* err,
-                 fast::FixScale* fs) {
+                 const uint32_t* ntasks, typename fast::FixTraits<T>::Cell* grids, int pg0, int npg, int gmax,
+                 int* err, fast::FixScale* fs) {
   if (nblocks == 0) return;
   const int batch = staging_batch<T, S>();
   const int total = smem + batch * (int)GridStaging<T, S>::bytes_per_vis();
@@ -1738,7 +1739,7 @@ void launch_grid_i8(cudaStream_t s, const Geom<float>& g, const Inputs& in, int 
                     const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins, fast::FixCell* grids,
                     int pg0, int npg, fast::FixScale* fs) {
   if (kend <= kbase) return;
-  const int smem = (int)fast::I8Slots::bytes();
+  const int smem = (int)(fast::I8Slots::bytes() + fast::I8_BATCH * sizeof(fast::Prefetched));
   const unsigned nblocks = (unsigned)((kend - kbase + fast::I8_CHUNK - 1) / fast::I8_CHUNK);
   check_cuda(cudaFuncSetAttribute(fast::k_grid_i8<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
   {
@@ -1754,7 +1755,7 @@ void launch_degrid_h(cudaStream_t s, const Geom<float>& g, const Inputs& wts, co
                      const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
                      const cplx<float>* grids, int pg0, int npg, cplx<float>* vis, int first, int last) {
   if (kend <= kbase) return;
-  const int smem = (int)fast::H16Slots::bytes();
+  const int smem = (int)(fast::H16Slots::bytes() + fast::H16_BATCH * sizeof(fast::Prefetched));
   const unsigned nblocks = (unsigned)((kend - kbase + fast::H16_CHUNK - 1) / fast::H16_CHUNK);
   check_cuda(cudaFuncSetAttribute(fast::k_degrid_h<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem");
   {
@@ -2204,7 +2205,7 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
     check_cuda(cudaMemsetAsync(image, 0, npix * sizeof(T), s), "memset");
     return;
   }
-  using fast::FixCell;
+  using FixCell = typename fast::FixTraits<T>::Cell;
   const size_t cell = sizeof(cplx<T>);
   const size_t nplanes = (size_t)std::max(g_.nplanes, 1);
   const size_t plane = (size_t)g_.nu * g_.nv;
@@ -2241,7 +2242,7 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
   {
     StageTimer timer_(ST_OTHER, s);
     fast::k_fix_scale<<<1, 1, 0, s>>>(values, mode == VALUE_UNIT ? 1 : 0, (unsigned long long)nvis_, integer ? 1 : 0,
-                                      scale_.as<fast::FixScale>());
+                                      fast::FixTraits<T>::wide, scale_.as<fast::FixScale>());
   }
   check_cuda(cudaGetLastError(), "scale");
   fast::FixScale* fs = scale_.as<fast::FixScale>();
