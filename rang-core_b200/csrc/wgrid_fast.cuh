@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256, 4)
   const uint64_t n = g.nrow * g.nchan;
   const uint64_t nround = (n + 31) & ~31ull;
   const uint32_t tmask = (1u << g.log2tile) - 1u;
-  const uint32_t se = (uint32_t)g.sube;
+  const uint32_t se = (uint32_t)g.sube, sdiv = (65536u + se - 1u) / se;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   RowCh rc(i, (uint32_t)g.nchan, (uint64_t)gridDim.x * blockDim.x);
   for (; i < nround; i += (uint64_t)gridDim.x * blockDim.x, rc.next((uint32_t)g.nchan)) {
@@ -248,7 +248,9 @@ __global__ void __launch_bounds__(256, 4)
         int64_t iu0, iv0;
         getpix(g, u, v, uf, vf, iu0, iv0);
         const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
-        const uint32_t sa = (su & tmask) / se, sb = (sv & tmask) / se;
+        // (x / sube) for x < 32 as a multiply and shift (exact: the error of
+        // ceil(2^16 / sube) stays below 2^-11 over 32 steps)
+        const uint32_t sa = ((su & tmask) * sdiv) >> 16, sb = ((sv & tmask) * sdiv) >> 16;
         const int mp = minplane(g, w);
         // The key of bin_of_rc (Setup::locate refined by the sub-tile).
         k = (((su >> g.log2tile) * (uint32_t)g.ntv + (sv >> g.log2tile)) * (uint32_t)g.nbuckets + (uint32_t)mp) *
@@ -347,6 +349,21 @@ __device__ __forceinline__ void window_of(const Geom<float>& g, uint32_t key, ui
               (uint32_t)g.nv);
 }
 
+// The taps t[0..S) placed at rows [off, off + S) of an 8-row window, zero
+// elsewhere, in registers (off < 9 - S is a runtime value, the candidates
+// compile-time: selects instead of indexed stores).
+template <int S, class V>
+__device__ __forceinline__ void place8(const V (&t)[S], int off, V zero, V (&row)[8]) {
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    V x = zero;
+#pragma unroll
+    for (int d = 0; d < 9 - S; d++)
+      if (j - d >= 0 && j - d < S && off == d) x = t[(j - d >= 0 && j - d < S) ? j - d : 0];
+    row[j] = x;
+  }
+}
+
 // ------------------------------------------------------------------ integer gridder
 
 // ------------------------------------------------------------------ prefetch
@@ -426,13 +443,18 @@ __device__ __forceinline__ cplx<float> prefetched_vis(const Prefetched& p, const
 constexpr int I8_BATCH = 32;         // records staged per round, one per lane
 constexpr uint32_t I8_CHUNK = 8192;  // sorted records per warp
 constexpr float I8_ASCALE = 4194304.0f;  // 2^22
-// Integers x are formed as float(x + 0x8080) so that one cvt.rni gives the
-// offset that the balanced limbs need (|x| < 2^22 + 2^15, exact in FP32).
-constexpr float I8_OFFSET = 32896.0f;
+// A's integers (w tap x u tap x 2^22, in [-2^16, 2^22 (1 + eps)]) are formed
+// without a conversion instruction: y = x + 2^23 + 2^16 + 0x8080 lies in
+// (2^23, 2^24), where FP32 spacing is 1, so the FFMA that forms x rounds it
+// to the nearest integer, and the bits of y are 0x4B010000 + rint(x) +
+// 0x8080: one IADD gives rint(x) with the offset the balanced limbs need.
+constexpr float I8_AOFF = 8487040.0f;      // 2^23 + 2^16 + 0x8080
+constexpr uint32_t I8_ABIAS = 0x4B010000u;  // bits of 2^23 + 2^16
+__device__ __forceinline__ uint32_t i8_aint(float y) { return __float_as_uint(y) - I8_ABIAS; }
 // Row strides (words) of the staging rows: with them the reads of the eight
 // records of a lane quad (slots 4 tq + j) fall in distinct banks.
-constexpr int I8_KU = 9;    // u taps placed on the window's 8 rows
-constexpr int I8_B = 9;     // float2: value * placed v taps * 2^sb + offset on the 8 columns
+constexpr int I8_KU = 10;   // u taps placed on the window's 8 rows
+constexpr int I8_B = 9;     // uint2: rint(value * placed v taps * 2^sb) + 0x8080 on the 8 columns
 constexpr int I8_KW = 10;   // w taps * 2^22 (8), as float2 pairs of planes
 
 // Staging of one round: per slot (record) the u taps and value * v taps
@@ -440,7 +462,7 @@ constexpr int I8_KW = 10;   // w taps * 2^22 (8), as float2 pairs of planes
 // the w taps times 2^22 and the key. Slot I8_BATCH stays zero.
 struct I8Slots {
   float* ku;      // [I8_BATCH + 1][I8_KU]
-  float2* bv;     // [I8_BATCH + 1][I8_B]
+  uint2* bv;      // [I8_BATCH + 1][I8_B]
   float* kw;      // [I8_BATCH + 1][I8_KW]
   uint32_t* key;  // [I8_BATCH + 1]
   __host__ __device__ static constexpr size_t bytes() {
@@ -448,7 +470,7 @@ struct I8Slots {
   }
   // bv and kw are read as float2: both start on 8-byte boundaries.
   __device__ void carve(unsigned char* base) {
-    bv = reinterpret_cast<float2*>(base);
+    bv = reinterpret_cast<uint2*>(base);
     kw = reinterpret_cast<float*>(bv + (I8_BATCH + 1) * I8_B);
     ku = kw + (I8_BATCH + 1) * I8_KW;
     key = reinterpret_cast<uint32_t*>(ku + (I8_BATCH + 1) * I8_KU);
@@ -522,10 +544,10 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
   const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
   {  // the zero slot: u and w taps 0, B rows at the offset (value 0)
     float* zk = st.ku + I8_BATCH * I8_KU;
-    float2* zb = st.bv + I8_BATCH * I8_B;
+    uint2* zb = st.bv + I8_BATCH * I8_B;
     float* zw = st.kw + I8_BATCH * I8_KW;
     if (lane < I8_KU) zk[lane] = 0.0f;
-    if (lane < I8_B) zb[lane] = make_float2(I8_OFFSET, I8_OFFSET);
+    if (lane < I8_B) zb[lane] = make_uint2(0x8080u, 0x8080u);
     if (lane < I8_KW) zw[lane] = 0.0f;
     if (lane == 0) st.key[I8_BATCH] = INACTIVE;
   }
@@ -571,20 +593,16 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
       const float vr = vv.re * pr - vv.im * pi, vi = (vv.re * pi + vv.im * pr) * flip;
       bad |= !isfinite(vr) || !isfinite(vi) || !isfinite(r.x0) || !isfinite(r.y0) || !isfinite(r.xw);
       const int mp = (int)(r.meta >> 16), du = (int)(r.meta & 15u), dv = (int)((r.meta >> 4) & 15u);
-      float* cu = st.ku + lane * I8_KU;
-      float2* cb = st.bv + lane * I8_B;
-      float* cw = st.kw + lane * I8_KW;
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        cu[i] = 0.0f;
-        cb[i] = make_float2(I8_OFFSET, I8_OFFSET);
-      }
       const float br = vr * bscale, bi = vi * bscale;
+      uint2 bt[S];
 #pragma unroll
-      for (int i = 0; i < S; i++) {
-        cu[du + i] = ku[i];
-        cb[dv + i] = make_float2(fmaf(br, kv[i], I8_OFFSET), fmaf(bi, kv[i], I8_OFFSET));
-      }
+      for (int i = 0; i < S; i++)
+        bt[i] = make_uint2((uint32_t)(__float2int_rn(br * kv[i]) + 0x8080), (uint32_t)(__float2int_rn(bi * kv[i]) + 0x8080));
+      float urow[8];
+      uint2 brow[8];
+      place8<S>(ku, du, 0.0f, urow);
+      place8<S>(bt, dv, make_uint2(0x8080u, 0x8080u), brow);
+      float wrow[8];
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         float w = 0.0f;
@@ -593,8 +611,18 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
         } else if (j == 0) {
           w = I8_ASCALE;
         }
-        cw[j] = w;
+        wrow[j] = w;
       }
+      float2* cu = reinterpret_cast<float2*>(st.ku + lane * I8_KU);
+      uint2* cb = st.bv + lane * I8_B;
+      float2* cw = reinterpret_cast<float2*>(st.kw + lane * I8_KW);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        cu[j] = make_float2(urow[2 * j], urow[2 * j + 1]);
+        cw[j] = make_float2(wrow[2 * j], wrow[2 * j + 1]);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) cb[j] = brow[j];
       st.key[lane] = r.bin;
     }
     // The next round's record and value, in flight while this one is contracted.
@@ -632,16 +660,14 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
       uint32_t b[2][3][2];  // B limbs per component: registers for k 4tq.. and 16 + 4tq..
 #pragma unroll
       for (int hf = 0; hf < 2; hf++) {
-        float2 bvv[4];
+        uint2 bvv[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
           kuv[4 * hf + j] = st.ku[slot[4 * hf + j] * I8_KU + gq];
           bvv[j] = st.bv[slot[4 * hf + j] * I8_B + gq];
         }
-        limbs4(__float2int_rn(bvv[0].x), __float2int_rn(bvv[1].x), __float2int_rn(bvv[2].x),
-               __float2int_rn(bvv[3].x), b[0][0][hf], b[0][1][hf], b[0][2][hf]);
-        limbs4(__float2int_rn(bvv[0].y), __float2int_rn(bvv[1].y), __float2int_rn(bvv[2].y),
-               __float2int_rn(bvv[3].y), b[1][0][hf], b[1][1][hf], b[1][2][hf]);
+        limbs4(bvv[0].x, bvv[1].x, bvv[2].x, bvv[3].x, b[0][0][hf], b[0][1][hf], b[0][2][hf]);
+        limbs4(bvv[0].y, bvv[1].y, bvv[2].y, bvv[3].y, b[1][0][hf], b[1][1][hf], b[1][2][hf]);
       }
 #pragma unroll
       for (int h = 0; h < NP; h++) {
@@ -653,15 +679,12 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
           for (int j = 0; j < 4; j++)
             w[j] = 2 * h < S ? *reinterpret_cast<const float2*>(st.kw + slot[4 * hf + j] * I8_KW + 2 * h)
                              : make_float2(0.0f, 0.0f);
-          limbs4(__float2int_rn(fmaf(w[0].x, kuv[4 * hf], I8_OFFSET)),
-                 __float2int_rn(fmaf(w[1].x, kuv[4 * hf + 1], I8_OFFSET)),
-                 __float2int_rn(fmaf(w[2].x, kuv[4 * hf + 2], I8_OFFSET)),
-                 __float2int_rn(fmaf(w[3].x, kuv[4 * hf + 3], I8_OFFSET)), a[0][2 * hf], a[1][2 * hf], a[2][2 * hf]);
-          limbs4(__float2int_rn(fmaf(w[0].y, kuv[4 * hf], I8_OFFSET)),
-                 __float2int_rn(fmaf(w[1].y, kuv[4 * hf + 1], I8_OFFSET)),
-                 __float2int_rn(fmaf(w[2].y, kuv[4 * hf + 2], I8_OFFSET)),
-                 __float2int_rn(fmaf(w[3].y, kuv[4 * hf + 3], I8_OFFSET)), a[0][2 * hf + 1], a[1][2 * hf + 1],
-                 a[2][2 * hf + 1]);
+          limbs4(i8_aint(fmaf(w[0].x, kuv[4 * hf], I8_AOFF)), i8_aint(fmaf(w[1].x, kuv[4 * hf + 1], I8_AOFF)),
+                 i8_aint(fmaf(w[2].x, kuv[4 * hf + 2], I8_AOFF)), i8_aint(fmaf(w[3].x, kuv[4 * hf + 3], I8_AOFF)),
+                 a[0][2 * hf], a[1][2 * hf], a[2][2 * hf]);
+          limbs4(i8_aint(fmaf(w[0].y, kuv[4 * hf], I8_AOFF)), i8_aint(fmaf(w[1].y, kuv[4 * hf + 1], I8_AOFF)),
+                 i8_aint(fmaf(w[2].y, kuv[4 * hf + 2], I8_AOFF)), i8_aint(fmaf(w[3].y, kuv[4 * hf + 3], I8_AOFF)),
+                 a[0][2 * hf + 1], a[1][2 * hf + 1], a[2][2 * hf + 1]);
         }
 #pragma unroll
         for (int c = 0; c < 2; c++) {
@@ -686,7 +709,7 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
 constexpr int H16_BATCH = 32;
 constexpr uint32_t H16_CHUNK = 8192;
 constexpr float H16_BSCALE = 16384.0f;  // 2^14: v taps stay clear of FP16 subnormals
-constexpr int H16_KU = 9;   // u taps placed on the window's 8 rows
+constexpr int H16_KU = 10;  // u taps placed on the window's 8 rows (read as float2)
 constexpr int H16_KV = 10;  // v taps * 2^14 placed on the 8 columns (read as float2)
 constexpr int H16_KW = 12;  // w taps (8, read as float4)
 
@@ -699,7 +722,7 @@ struct H16Slots {
   __host__ __device__ static constexpr size_t bytes() {
     return ((size_t)(H16_BATCH + 1) * (16 + H16_KW * 4 + H16_KV * 4 + H16_KU * 4 + 4) + 15) / 16 * 16;
   }
-  // out and kw are read as float4, kv as float2: their offsets are aligned.
+  // out and kw are read as float4, kv and ku as float2: their offsets are aligned.
   __device__ void carve(unsigned char* base) {
     out = reinterpret_cast<float4*>(base);
     kw = reinterpret_cast<float*>(out + (H16_BATCH + 1));
@@ -734,24 +757,24 @@ __device__ __forceinline__ void hmma(float (&d)[4], uint32_t a0, uint32_t a1, ui
 // Degridding of records [kbase, kend) (single precision, degrid_task_body,
 // wgridder.rs:2793-2901): per bin the warp holds the bin's 8 x 8 window of
 // each plane as FP16 hi + lo fragments (scaled by a power of two to the
-// window's largest value); per block of eight records the v contraction
-// T[p][u][k] = sum_v G[p][u][v] kv_k[v - dv_k] runs on the tensor cores as
-// hi*hi + hi*lo + lo*hi (mma.sync m16n8k8, FP32 accumulation, each block
-// from zero); the w and u contractions and the final phase and weight
-// (wgridder.rs:3146-3159) run on the CUDA cores, reduced over the window
-// rows with shuffles. Each output depends only on its own record and the
-// window, so the result does not depend on the grouping. With plane groups
-// (first / last) the partial sums accumulate in `vis` and the final factor
-// is applied with the last group. The next round's records are loaded while
-// the current round is contracted.
+// window's largest value); per block of sixteen records the v contraction
+// T[k][u] = sum_v kv_k[v - dv_k] G_p[u][v] of each plane runs on the tensor
+// cores as hi*hi + hi*lo + lo*hi (mma.sync m16n8k8, records along M, window
+// rows along N, FP32 accumulation, each block from zero); the u and w
+// contractions and the final phase and weight (wgridder.rs:3146-3159) run on
+// the CUDA cores, reduced over the four lanes that hold a record's window
+// rows. Each output depends only on its own record and the window, so the
+// result does not depend on the grouping. With plane groups (first / last)
+// the partial sums accumulate in `vis` and the final factor is applied with
+// the last group. The next round's records are copied while the current
+// round is contracted.
 template <int S>
-__global__ void __launch_bounds__(H16_BATCH, 16)
+__global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 16 : 12)
     k_degrid_h(const __grid_constant__ Geom<float> g, Inputs wts, const VisRecord* __restrict__ rec,
                const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
                const cplx<float>* __restrict__ grids, int pg0, int npg, cplx<float>* __restrict__ vis, int first,
                int last) {
   static_assert(S >= 1 && S <= 8, "8 x 8 windows");
-  constexpr int NP = (S + 1) / 2;
   extern __shared__ __align__(16) unsigned char smem[];
   H16Slots st;
   st.carve(smem);
@@ -769,8 +792,8 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
   const uint64_t k1 = min(kend, k0 + H16_CHUNK);
   const size_t plane = (size_t)g.nu * g.nv;
 
-  uint32_t ahi[NP][2][2], alo[NP][2][2];  // [pair][re/im][rows gq, gq + 8]
-  float inv = 0.0f;                       // 1 / (window scale * 2^14)
+  uint32_t bhi[S][2], blo[S][2];  // [plane][re/im]: window rows gq, columns 2tq, 2tq + 1
+  float inv = 0.0f;               // 1 / (window scale * 2^14)
   uint32_t gcur = INACTIVE;
 
   Prefetched* pre = reinterpret_cast<Prefetched*>(smem + H16Slots::bytes()) + lane;
@@ -790,19 +813,11 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
       eval_taps2<float, S>(g.coeff, g.ne, r.x0, r.y0, ku, kv);
       if (g.do_wgridding) eval_taps1<S>(g.coeff, r.xw, kw);
       const int mp = (int)(r.meta >> 16), du = (int)(r.meta & 15u), dv = (int)((r.meta >> 4) & 15u);
-      float* cu = st.ku + lane * H16_KU;
-      float* cv = st.kv + lane * H16_KV;
-      float* cw = st.kw + lane * H16_KW;
 #pragma unroll
-      for (int i = 0; i < 8; i++) {
-        cu[i] = 0.0f;
-        cv[i] = 0.0f;
-      }
-#pragma unroll
-      for (int i = 0; i < S; i++) {
-        cu[du + i] = ku[i];
-        cv[dv + i] = kv[i] * H16_BSCALE;
-      }
+      for (int i = 0; i < S; i++) kv[i] *= H16_BSCALE;
+      float urow[8], vrow[8], wrow[8];
+      place8<S>(ku, du, 0.0f, urow);
+      place8<S>(kv, dv, 0.0f, vrow);
 #pragma unroll
       for (int j = 0; j < 8; j++) {
         float w = 0.0f;
@@ -811,8 +826,18 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
         } else if (j == 0 && pg0 == 0) {
           w = 1.0f;
         }
-        cw[j] = w;
+        wrow[j] = w;
       }
+      float2* cu = reinterpret_cast<float2*>(st.ku + lane * H16_KU);
+      float2* cv = reinterpret_cast<float2*>(st.kv + lane * H16_KV);
+      float4* cw = reinterpret_cast<float4*>(st.kw + lane * H16_KW);
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        cu[j] = make_float2(urow[2 * j], urow[2 * j + 1]);
+        cv[j] = make_float2(vrow[2 * j], vrow[2 * j + 1]);
+      }
+      cw[0] = make_float4(wrow[0], wrow[1], wrow[2], wrow[3]);
+      cw[1] = make_float4(wrow[4], wrow[5], wrow[6], wrow[7]);
       // The final factor conj(phase) * wgt (shift_phase with sign -1).
       st.out[lane] = make_float4(r.ph_re * tw, -r.ph_im * tw, (r.meta & 256u) ? -1.0f : 1.0f,
                                  __uint_as_float(r.idx));
@@ -834,99 +859,85 @@ __global__ void __launch_bounds__(H16_BATCH, 16)
         int c0 = sv0 + 2 * tq, c1 = c0 + 1;
         if (c0 >= g.nv) c0 -= g.nv;
         if (c1 >= g.nv) c1 -= g.nv;
-        float2 v[NP][2][2];  // [pair][plane 2h + pl][column]
+        cplx<float> v[S][2];  // [plane][column]
         float m = 0.0f;
 #pragma unroll
-        for (int h = 0; h < NP; h++)
-#pragma unroll
-          for (int pl = 0; pl < 2; pl++) {
-            const int p = mp + 2 * h + pl;
-            const bool ok = (2 * h + pl < S) && p >= pg0 && p < pg0 + npg && (g.do_wgridding || p == 0);
-            const cplx<float>* src = grids + (size_t)(ok ? p - pg0 : 0) * plane + (size_t)row * g.nv;
-            const cplx<float> x0 = ok ? src[c0] : cplx<float>{0.0f, 0.0f};
-            const cplx<float> x1 = ok ? src[c1] : cplx<float>{0.0f, 0.0f};
-            v[h][pl][0] = make_float2(x0.re, x0.im);
-            v[h][pl][1] = make_float2(x1.re, x1.im);
-            m = fmaxf(m, fmaxf(fmaxf(fabsf(x0.re), fabsf(x0.im)), fmaxf(fabsf(x1.re), fabsf(x1.im))));
-          }
+        for (int p = 0; p < S; p++) {
+          const int pp = mp + p;
+          const bool ok = pp >= pg0 && pp < pg0 + npg && (g.do_wgridding || pp == 0);
+          const cplx<float>* src = grids + (size_t)(ok ? pp - pg0 : 0) * plane + (size_t)row * g.nv;
+          v[p][0] = ok ? src[c0] : cplx<float>{0.0f, 0.0f};
+          v[p][1] = ok ? src[c1] : cplx<float>{0.0f, 0.0f};
+          m = fmaxf(m, fmaxf(fmaxf(fabsf(v[p][0].re), fabsf(v[p][0].im)), fmaxf(fabsf(v[p][1].re), fabsf(v[p][1].im))));
+        }
         for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
         // Largest window value to about 2^14 (FP16 tops out at 65504).
         const int e = (m > 0.0f && isfinite(m)) ? ilogbf(m) : 0;
         const float sc = ldexpf(1.0f, 14 - e);
         inv = ldexpf(1.0f, e - 14) / H16_BSCALE;
 #pragma unroll
-        for (int h = 0; h < NP; h++)
-#pragma unroll
-          for (int pl = 0; pl < 2; pl++) {
-            split_h2(v[h][pl][0].x * sc, v[h][pl][1].x * sc, ahi[h][0][pl], alo[h][0][pl]);
-            split_h2(v[h][pl][0].y * sc, v[h][pl][1].y * sc, ahi[h][1][pl], alo[h][1][pl]);
-          }
+        for (int p = 0; p < S; p++) {
+          split_h2(v[p][0].re * sc, v[p][1].re * sc, bhi[p][0], blo[p][0]);
+          split_h2(v[p][0].im * sc, v[p][1].im * sc, bhi[p][1], blo[p][1]);
+        }
       }
       const unsigned mk = __ballot_sync(0xffffffffu, lane >= q && lane < nb && st.key[lane] == gk);
       const int len = __popc(mk);
-      // Blocks of eight records of the run: this lane's B column is record gq.
-      for (int k8 = q; k8 < q + len; k8 += 8) {
-        const int sb = (k8 + gq < q + len) ? k8 + gq : H16_BATCH;
-        const float2 kvp = *reinterpret_cast<const float2*>(st.kv + sb * H16_KV + 2 * tq);
-        uint32_t bhi, blo;
-        split_h2(kvp.x, kvp.y, bhi, blo);
-        // This lane's outputs: records k8 + 2tq and k8 + 2tq + 1.
-        int s2[2];
-        float kwv[2][8], kuv[2];
+      // Blocks of sixteen records of the run: rows gq and gq + 8 of the MMA.
+      for (int k16 = q; k16 < q + len; k16 += 16) {
+        int sr[2];
+        uint32_t ahi[2], alo[2];
+        float2 kup[2];
+        float kwv[2][8];
 #pragma unroll
-        for (int c = 0; c < 2; c++) {
-          const int k = k8 + 2 * tq + c;
-          s2[c] = (k < q + len) ? k : H16_BATCH;
-          kuv[c] = st.ku[s2[c] * H16_KU + gq];
-          const float4 w0 = *reinterpret_cast<const float4*>(st.kw + s2[c] * H16_KW);
-          const float4 w1 = *reinterpret_cast<const float4*>(st.kw + s2[c] * H16_KW + 4);
-          kwv[c][0] = w0.x;
-          kwv[c][1] = w0.y;
-          kwv[c][2] = w0.z;
-          kwv[c][3] = w0.w;
-          kwv[c][4] = w1.x;
-          kwv[c][5] = w1.y;
-          kwv[c][6] = w1.z;
-          kwv[c][7] = w1.w;
+        for (int h = 0; h < 2; h++) {
+          const int k = k16 + gq + 8 * h;
+          sr[h] = (k < q + len) ? k : H16_BATCH;
+          const float2 kvp = *reinterpret_cast<const float2*>(st.kv + sr[h] * H16_KV + 2 * tq);
+          split_h2(kvp.x, kvp.y, ahi[h], alo[h]);
+          kup[h] = *reinterpret_cast<const float2*>(st.ku + sr[h] * H16_KU + 2 * tq);
+          const float4 w0 = *reinterpret_cast<const float4*>(st.kw + sr[h] * H16_KW);
+          const float4 w1 = *reinterpret_cast<const float4*>(st.kw + sr[h] * H16_KW + 4);
+          kwv[h][0] = w0.x;
+          kwv[h][1] = w0.y;
+          kwv[h][2] = w0.z;
+          kwv[h][3] = w0.w;
+          kwv[h][4] = w1.x;
+          kwv[h][5] = w1.y;
+          kwv[h][6] = w1.z;
+          kwv[h][7] = w1.w;
         }
         float tr[2] = {0.0f, 0.0f}, ti[2] = {0.0f, 0.0f};
 #pragma unroll
-        for (int h = 0; h < NP; h++) {
+        for (int p = 0; p < S; p++) {
           float dre[4], dim[4];
-          hmma_zero(dre, ahi[h][0][0], ahi[h][0][1], bhi);
-          hmma(dre, ahi[h][0][0], ahi[h][0][1], blo);
-          hmma(dre, alo[h][0][0], alo[h][0][1], bhi);
-          hmma_zero(dim, ahi[h][1][0], ahi[h][1][1], bhi);
-          hmma(dim, ahi[h][1][0], ahi[h][1][1], blo);
-          hmma(dim, alo[h][1][0], alo[h][1][1], bhi);
-          // d[0], d[1]: plane 2h, columns 2tq, 2tq + 1; d[2], d[3]: plane 2h + 1
+          hmma_zero(dre, ahi[0], ahi[1], bhi[p][0]);
+          hmma(dre, ahi[0], ahi[1], blo[p][0]);
+          hmma(dre, alo[0], alo[1], bhi[p][0]);
+          hmma_zero(dim, ahi[0], ahi[1], bhi[p][1]);
+          hmma(dim, ahi[0], ahi[1], blo[p][1]);
+          hmma(dim, alo[0], alo[1], bhi[p][1]);
+          // d[0], d[1]: record gq, window rows 2tq, 2tq + 1; d[2], d[3]: record gq + 8
 #pragma unroll
-          for (int c = 0; c < 2; c++) {
-            tr[c] = fmaf(kwv[c][2 * h], dre[c], tr[c]);
-            ti[c] = fmaf(kwv[c][2 * h], dim[c], ti[c]);
-            if (2 * h + 1 < S) {
-              tr[c] = fmaf(kwv[c][2 * h + 1], dre[2 + c], tr[c]);
-              ti[c] = fmaf(kwv[c][2 * h + 1], dim[2 + c], ti[c]);
-            }
+          for (int h = 0; h < 2; h++) {
+            tr[h] = fmaf(kwv[h][p], fmaf(kup[h].x, dre[2 * h], kup[h].y * dre[2 * h + 1]), tr[h]);
+            ti[h] = fmaf(kwv[h][p], fmaf(kup[h].x, dim[2 * h], kup[h].y * dim[2 * h + 1]), ti[h]);
           }
         }
 #pragma unroll
-        for (int c = 0; c < 2; c++) {
-          tr[c] *= kuv[c];
-          ti[c] *= kuv[c];
+        for (int h = 0; h < 2; h++)
 #pragma unroll
-          for (int o = 4; o < 32; o <<= 1) {
-            tr[c] += __shfl_xor_sync(0xffffffffu, tr[c], o);
-            ti[c] += __shfl_xor_sync(0xffffffffu, ti[c], o);
+          for (int o = 1; o < 4; o <<= 1) {
+            tr[h] += __shfl_xor_sync(0xffffffffu, tr[h], o);
+            ti[h] += __shfl_xor_sync(0xffffffffu, ti[h], o);
           }
-        }
-        if (gq == 0) {
+        if (tq == 0) {
 #pragma unroll
-          for (int c = 0; c < 2; c++) {
-            if (s2[c] == H16_BATCH) continue;
-            const float4 fo = st.out[s2[c]];
+          for (int h = 0; h < 2; h++) {
+            if (sr[h] == H16_BATCH) continue;
+            const float4 fo = st.out[sr[h]];
             const uint32_t idx = __float_as_uint(fo.w);
-            cplx<float> accv{tr[c] * inv, ti[c] * inv * fo.z};
+            cplx<float> accv{tr[h] * inv, ti[h] * inv * fo.z};
             if (!first) {
               const cplx<float> prev = vis[idx];
               accv = {accv.re + prev.re, accv.im + prev.im};
