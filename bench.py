@@ -22,8 +22,16 @@ visibilities and mask: the reference's two stateless calls.
   event-timed average launch, against the measured copy bandwidth.
 * `cpu_baseline`: the CPU oracle (a C++/OpenMP restatement of the
   reference's Rust wgridder; the reference itself cannot be built here) on
-  the first eighth of the integrations with all host threads.
-* `accuracy`: the step's outputs against a float64 run at epsilon 1e-7.
+  every 64th integration of the workload (the same uv extent, w range and
+  plan, one sixty-fourth of the visibilities), all host threads.
+* `accuracy`: every gridding method's dirty image and visibilities on that
+  sample against the oracle's FP64 run at epsilon 1e-7, L-inf and RMS over
+  the peak with the image border (outer two pixels) apart from the interior
+  (eight pixels in), and each method's time at the full size.
+* `config1`: the 16.5 M-visibility, 1024^2 configuration on the GPU (f32 and
+  f64 at epsilon 1e-5) beside the CPU oracle run as the reference's own
+  harness runs it (a fresh process per repeat, three repeats, the median, all
+  threads and one, peak RSS and output SHA256).
 
 `--impl reference` times the CPU oracle alone, on the same workload sample.
 Multi-GPU (`--gpus N` under torchrun): independent replicas, one per GPU.
@@ -47,12 +55,16 @@ sys.path.insert(0, str(REPO / "rang-core_b200"))
 from rang import synth  # noqa: E402
 
 WORKLOAD = "ms2dirty+dirty2ms 1.06G vis 4096^2"
-# DRAM bytes (read + written) of one launch of the dominant kernels on this
-# workload, measured with ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-# on a B200: a profiler figure, not something this script can time.
-DRAM_TRAFFIC = {
-    (WORKLOAD, 1e-5, "k_grid_tc"): 20.79e9 + 0.70e9,
-    (WORKLOAD, 1e-5, "k_degrid"): 9.61e9 + 9.51e9,
+CONFIG1 = "ms2dirty 16.5M vis 1024^2"
+PROFILE_CASE = "ms2dirty+dirty2ms 132M vis 2048^2"
+# DRAM bytes (read + written) per launch of the dominant kernels, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of each on the
+# 132 M-visibility profiling case, as (bytes, active visibilities of that
+# launch): a launch of another workload is scaled by its active visibilities.
+# A profiler figure, not something this script can time.
+DRAM_CAPTURE = {
+    "k_grid_i8": None,
+    "k_degrid_h": None,
 }
 METRIC = "Mvis/s ms2dirty+dirty2ms @eps=1e-5 vs FP64"
 UNIT = "Mvis/s"
@@ -66,7 +78,11 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(synth.WORKLOADS))
     ap.add_argument("--epsilon", type=float, default=1e-5)
-    ap.add_argument("--cpu-fraction", type=float, default=0.125)
+    ap.add_argument("--cpu-stride", type=int, default=64,
+                    help="the CPU sample: every n-th integration of the workload")
+    ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--no-config1", action="store_true")
+    ap.add_argument("--fista-cap", type=int, default=3000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -141,6 +157,28 @@ def make_observation(wl, seed=0):
 
 # ------------------------------------------------------------------ CPU (oracle)
 
+NBL = 2016  # baselines of the 64-antenna array
+# The reference's published CPU figures for this path (dirty + PSF per image,
+# f64, epsilon 1e-6, 23.8 M gridded visibilities at 1024^2, Ryzen 7 7700X):
+# ns per visibility per image at 1, 4 and 16 threads.
+PUBLISHED_NS_PER_VIS = {"1": 477, "4": 149, "16": 81}
+
+
+def _oracle():
+    if str(REPO / "oracle") not in sys.path:
+        sys.path.insert(0, str(REPO / "oracle"))
+    import oracle
+
+    return oracle
+
+
+def sample_rows(ntime, stride):
+    """The rows of every `stride`-th integration, starting in the middle of
+    the first stride: the sample keeps the observation's uv extent and w
+    range, so its plan (kernel, grid, planes) is the full workload's."""
+    t = np.arange(stride // 2, ntime, stride)
+    return (t[:, None] * NBL + np.arange(NBL)[None, :]).ravel(), len(t)
+
 
 def cpu_round_trip(oracle, uvw, freq, vis, mask, npix, cell, eps):
     kw = dict(uvw=uvw, freq=freq, mask=mask, pixsize_x=cell, pixsize_y=cell, epsilon=eps)
@@ -163,17 +201,14 @@ def cpu_model():
     return f"{name}, {os.cpu_count()} logical cores"
 
 
-def cpu_sample(wl, fraction, seed=0):
-    """Host data of the first `fraction` of the integrations: visibilities
-    predicted from the point sky by the oracle's own degridder (float64,
-    epsilon 1e-6) plus seeded noise and flags."""
-    sys.path.insert(0, str(REPO / "oracle"))
-    import oracle
-
+def cpu_sample(wl, stride, seed=0):
+    """Host data of every `stride`-th integration: visibilities predicted
+    from the point sky by the oracle's degridder (float32, epsilon 1e-5)
+    plus seeded noise (sigma 0.1) and flags."""
+    oracle = _oracle()
     uvw, freq, sky = make_observation(wl, seed)
-    nbl = 2016
-    nt = max(1, int(round(wl["ntime"] * fraction)))
-    uvw = uvw[: nt * nbl]
+    rows, nt = sample_rows(wl["ntime"], stride)
+    uvw = np.ascontiguousarray(uvw[rows])
     cell = wl["cell_arcsec"] * synth.ARCSEC
     model = oracle.dirty2vis(uvw=uvw, freq=freq, dirty=sky.astype(np.float32), pixsize_x=cell, pixsize_y=cell,
                              epsilon=1e-5)
@@ -182,6 +217,123 @@ def cpu_sample(wl, fraction, seed=0):
     vis = (model + 0.1 * (rng.standard_normal(shape) + 1j * rng.standard_normal(shape))).astype(np.complex64)
     mask = (rng.uniform(size=shape) >= wl["flag"]).astype(np.uint8)
     return oracle, uvw, freq, vis, mask, nt
+
+
+def sample_text(wl, stride, nt, nvis):
+    full = NBL * wl["ntime"] * wl["nchan"]
+    return (f"every {stride}th integration: {nt} of {wl['ntime']} integrations ({nvis} visibilities, "
+            f"{100.0 * nvis / full:.2f} % of the workload, the same uv extent, w range and plan), "
+            f"full {wl['npix']}^2 image and grid")
+
+
+def workload_config(wl, name, eps, world):
+    """The `config` of both arms' lines: the workload, by what it is."""
+    nvis = NBL * wl["ntime"] * wl["nchan"]
+    return {"workload": name, "visibilities": nvis, "image": [wl["npix"], wl["npix"]],
+            "cell_arcsec": wl["cell_arcsec"], "epsilon": eps, "flags": wl["flag"],
+            "parallelism": f"replicas{world}",
+            "l2": f"inputs larger than L2 ({nvis * 8 / 1e9:.2f} GB of visibilities)"}
+
+
+def maxrss_mb():
+    import resource
+
+    return resource.getrusage(resource.RUSAGE_SELF).ru_maxrss / 1024.0
+
+
+def sha256(a):
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def strided(a, ntime, stride):
+    """Rows of every `stride`-th integration of a (ntime * NBL, ...) array."""
+    if stride <= 1:
+        return a
+    rows, _ = sample_rows(ntime, stride)
+    return np.ascontiguousarray(a[rows])
+
+
+def cpu_worker(spec_json):
+    """One timed oracle vis2dirty in this fresh process, as the reference's
+    harness times one image (`examples/bench_df2.py:568-615`): the inputs
+    from an .npz, the threads, precision, epsilon and sample from the spec;
+    prints wall and CPU time, peak RSS (after loading and at the end), the
+    load average before and after, and the image's SHA256."""
+    spec = json.loads(spec_json)
+    load0 = os.getloadavg()
+    oracle = _oracle()
+    d = np.load(spec["inputs"])
+    ntime = int(d["ntime"])
+    uvw = strided(d["uvw"], ntime, spec["stride"])
+    vis = strided(d["vis"], ntime, spec["stride"]).astype(np.complex64 if spec["single"] else np.complex128)
+    freq = d["freq"]
+    threads = oracle.set_threads(spec["threads"])
+    loaded = maxrss_mb()
+    cell = float(d["cell"])
+    w0, c0 = time.perf_counter(), time.process_time()
+    dirty = oracle.vis2dirty(uvw=uvw, freq=freq, vis=vis, npix_x=int(d["npix"]), npix_y=int(d["npix"]),
+                             pixsize_x=cell, pixsize_y=cell, epsilon=spec["epsilon"])
+    wall = time.perf_counter() - w0
+    print(json.dumps({"wall": wall, "cpu": time.process_time() - c0, "threads": threads, "visibilities": vis.size,
+                      "dirty_sha256": sha256(dirty), "max_rss_mb": maxrss_mb(), "rss_mb_after_loading": loaded,
+                      "loadavg_before_after": [load0, os.getloadavg()], "simd": oracle.simd_level()}), flush=True)
+
+
+def cpu_protocol(inputs, repeats=3, stride1=8):
+    """The CPU baseline as the reference's harness measures it
+    (`examples/bench_df2.py:618-673`): a fresh process per (threads,
+    precision, repeat), repeats interleaved, the median wall reported with
+    peak RSS, load average and output hashes. All host threads run the whole
+    configuration; one thread runs every `stride1`-th integration (a bounded
+    sample), and the same sample on all threads shows whether the bits depend
+    on the thread count."""
+    allth = os.cpu_count() or 1
+    cases = [(allth, True, 1), (allth, False, 1), (1, True, stride1), (1, False, stride1)]
+    runs = {c: [] for c in cases}
+    for _ in range(repeats):
+        for c in cases:
+            threads, single, stride = c
+            spec = json.dumps({"inputs": str(inputs), "threads": threads, "single": single, "stride": stride,
+                               "epsilon": 1e-5})
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            out = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--cpu-worker", spec], env=env,
+                                 capture_output=True, text=True, check=True)
+            runs[c].append(json.loads(out.stdout.strip().splitlines()[-1]))
+    same = {}
+    for single in (True, False):
+        spec = json.dumps({"inputs": str(inputs), "threads": allth, "single": single, "stride": stride1,
+                           "epsilon": 1e-5})
+        out = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--cpu-worker", spec],
+                             env=dict(os.environ, OMP_NUM_THREADS=str(allth)), capture_output=True, text=True,
+                             check=True)
+        rec = json.loads(out.stdout.strip().splitlines()[-1])
+        same["f32" if single else "f64"] = rec["dirty_sha256"] == runs[(1, single, stride1)][0]["dirty_sha256"]
+    rows = []
+    for (threads, single, stride), recs in runs.items():
+        walls = [r["wall"] for r in recs]
+        med = statistics.median(walls)
+        n = recs[0]["visibilities"]
+        rows.append({"threads": recs[0]["threads"], "precision": "f32" if single else "f64", "epsilon": 1e-5,
+                     "sample": "the whole configuration" if stride == 1 else
+                               f"every {stride}th integration ({n} visibilities)",
+                     "visibilities": n, "wall_median_s": med, "walls_s": [round(w, 4) for w in walls],
+                     "cpu_median_s": statistics.median(r["cpu"] for r in recs),
+                     "mvis_per_s": n / med / 1e6, "ns_per_vis": 1e9 * med / n,
+                     "max_rss_mb": max(r["max_rss_mb"] for r in recs),
+                     "rss_mb_after_loading": max(r["rss_mb_after_loading"] for r in recs),
+                     "loadavg_before_after": recs[0]["loadavg_before_after"],
+                     "hashes_identical_over_repeats": len({r["dirty_sha256"] for r in recs}) == 1,
+                     "dirty_sha256": recs[0]["dirty_sha256"]})
+    return {"harness": f"fresh process per (threads, precision, repeat), {repeats} interleaved repeats, median; "
+                       "oracle vis2dirty (the C++/OpenMP restatement of the reference's Rust wgridder)",
+            "cpu_model": cpu_model(), "simd": runs[cases[0]][0]["simd"], "runs": rows,
+            "bits_independent_of_threads": same,
+            "published_reference_ns_per_vis_per_image": {
+                "values": PUBLISHED_NS_PER_VIS,
+                "setting": "dirty + PSF, f64, epsilon 1e-6, 23.8 M visibilities at 1024^2, Ryzen 7 7700X "
+                           "(other hardware and data)"}}
 
 
 def replica_env():
@@ -221,11 +373,11 @@ def job_rate(world, units_per_rank, steps, seconds):
 
 
 def run_reference(args):
-    _, rank, _ = replica_env()
+    world, rank, _ = replica_env()
     if rank != 0:
         return  # the CPU reference runs once, on rank 0; the other ranks exit without work
     wl = synth.WORKLOADS[args.workload]
-    oracle, uvw, freq, vis, mask, nt = cpu_sample(wl, args.cpu_fraction)
+    oracle, uvw, freq, vis, mask, nt = cpu_sample(wl, args.cpu_stride)
     threads = oracle.set_threads(os.cpu_count() or 1)
     cell = wl["cell_arcsec"] * synth.ARCSEC
     for _ in range(args.warmup):
@@ -234,15 +386,16 @@ def run_reference(args):
     times = [cpu_round_trip(oracle, uvw, freq, vis, mask, wl["npix"], cell, args.epsilon) for _ in range(args.steps)]
     t = sum(times)
     value = vis.size * args.steps / t / 1e6
-    sample = f"first {nt} of {wl['ntime']} integrations ({vis.size} visibilities), full image and grid"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "epsilon": args.epsilon},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
-                         "cpu_model": cpu_model(), "median_step_s": statistics.median(times),
-                         "step_s": [round(x, 4) for x in times], "load_avg_before": list(load)},
+        "config": workload_config(wl, args.workload, args.epsilon, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample_text(wl, args.cpu_stride, nt, vis.size) + ", one round trip per step",
+                         "cpu_model": cpu_model(), "simd": oracle.simd_level(),
+                         "median_step_s": statistics.median(times), "step_s": [round(x, 4) for x in times],
+                         "load_avg_before": list(load)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line, default=_plain), flush=True)
@@ -251,16 +404,17 @@ def run_reference(args):
 # ------------------------------------------------------------------ FISTA
 
 
-def run_fista(dev, max_iterations=200, sigma=0.05, learn=None):
+def run_fista(dev, max_iterations=200, sigma=0.05, learn=None, cap=3000):
     """Plain FISTA (L1 with positivity, step 1 / ||A^H A|| from 30 power
     iterations) on 2048^2 at 1.5 arcsec: 300 point sources and 40 elliptical
     Gaussians predicted by the degridder onto the 64-antenna coverage of 128
     integrations at 256 channels (66 M visibilities), noise sigma 0.05 per
-    component. Reports the GPU time until the visibility residual RMS (per
-    real component) first reaches 1.2 sigma (null if it does not within the
-    iterations), plan and power iteration included, and the RMS every 20
-    iterations; with `learn`, learned-preconditioned FISTA on the same
-    measurement (`run_learned`)."""
+    component. Runs until the visibility residual RMS (per real component)
+    first reaches 1.2 sigma, or `cap` iterations; reports the GPU time to
+    that point (plan and power iteration included), the RMS after the
+    configuration's `max_iterations` iterations and every 20 iterations;
+    with `learn`, learned-preconditioned FISTA on the same measurement
+    (`run_learned`)."""
     import torch
 
     from rang import fista, wgrid_torch
@@ -286,36 +440,27 @@ def run_fista(dev, max_iterations=200, sigma=0.05, learn=None):
     ev[1].record()
     lmax, _ = fista.power_iteration(plan.gram, plan.shape, dev, max_iterations=30)
     ev[2].record()
-    trajectory, reached = [], {}
-    t_first = {}
-
-    marks = []
-
-    def stop(k, misfit):
-        rms = float(np.sqrt(max(2.0 * misfit, 0.0) / (2 * nvis)))
-        if k % 20 == 0 or k == max_iterations:
-            trajectory.append([k, rms])
-        reached["rms"], reached["k"] = rms, k
-        e = torch.cuda.Event(enable_timing=True)
-        e.record()
-        marks.append((rms, e))
-        if rms <= target and "event" not in t_first:
-            t_first["event"] = torch.cuda.Event(enable_timing=True)
-            t_first["event"].record()
-            t_first["k"] = k
-        return False  # all iterations run; the first one at the target is timed
-
     lam = 1e-4 * float(dirty.max())
-    x, gx, k, restarts = fista.solve(plan.gram, dirty, lam, 1.0 / lmax, max_iterations, q0=0.5 * q, stop=stop)
+    # rms = sqrt(2 misfit / (2 nvis)) per real component: the target's misfit.
+    res = fista.solve(plan.gram, dirty, lam, 1.0 / lmax, cap, q0=0.5 * q, target_misfit=target * target * nvis,
+                      events=True, check_every=10)
     ev[3].record()
     torch.cuda.synchronize()
+    x, restarts = res.x, res.restarts
+    rms = np.sqrt(np.maximum(2.0 * res.misfits.cpu().numpy(), 0.0) / (2 * nvis))
+    trajectory = [[k, float(rms[k])] for k in range(0, len(rms), 20)]
     t_setup = ev[0].elapsed_time(ev[1]) / 1e3
     t_power = ev[1].elapsed_time(ev[2]) / 1e3
     t_iter = ev[2].elapsed_time(ev[3]) / 1e3
-    t_target = ev[0].elapsed_time(t_first["event"]) / 1e3 if "event" in t_first else None
+    t_target = ev[0].elapsed_time(res.events[res.first]) / 1e3 if res.first is not None else None
     err = float((x - sky).norm() / sky.norm())
-    final_rms = reached.get("rms")
-    t_final = t_setup + t_power + ev[2].elapsed_time(next(e for r, e in marks if r <= final_rms)) / 1e3
+    # The learned solver's first comparison level: plain FISTA's RMS after the
+    # configuration's iterations, and plain FISTA's time to first reach it.
+    final_rms = float(rms[min(max_iterations, len(rms) - 1)])
+    t_final = ev[0].elapsed_time(res.events[int(np.argmax(rms <= final_rms))]) / 1e3
+    reached = {"rms_at_config_iterations": final_rms if len(rms) > max_iterations else None, "k": res.k,
+               "rms": float(rms[-1])}
+    t_first = {"k": res.first}
     learned_report = None
     if learn is not None:
         learned_report = run_learned(dev, plan, dirty, q, lmax, lam, sky, nvis, target, final_rms, t_final,
@@ -357,12 +502,22 @@ def run_fista(dev, max_iterations=200, sigma=0.05, learn=None):
     gram_report["exact_apply_ms"] = t0.elapsed_time(t1)
     del ones
     plan.close()
+    headline = None
+    if learned_report is not None:
+        lt = learned_report.get("time_to_target_s")
+        headline = {"plain_time_to_target_s": t_target, "learned_time_to_target_s": lt,
+                    "learned_over_plain": lt / t_target if lt and t_target else None,
+                    "target": f"residual RMS 1.2 sigma ({target})",
+                    "plain_cap_iterations": cap}
     return {"config": "2048^2 at 1.5 arcsec, 300 points + 40 Gaussians, 66 M visibilities, sigma 0.05, "
                       "L1 with positivity, lambda 1e-4 max(dirty), step 1/||A^H A|| from 30 power iterations",
             "target_rms": target, "time_to_target_s": t_target, "iterations_to_target": t_first.get("k"),
-            "iterations": max_iterations, "final_rms": reached.get("rms"), "rms_trajectory": trajectory,
+            "cap_iterations": cap, "config_iterations": max_iterations,
+            "rms_at_config_iterations": reached.get("rms_at_config_iterations"),
+            "iterations_run": reached.get("k"), "final_rms": reached.get("rms"), "rms_trajectory": trajectory,
             "restarts": int(restarts), "plan_and_dirty_s": t_setup, "power_iteration_s": t_power,
-            "fista_s": t_iter, "ms_per_iteration": 1e3 * t_iter / (max_iterations + 1),
+            "fista_s": t_iter, "ms_per_iteration": 1e3 * t_iter / (reached.get("k", 0) + 1),
+            "time_to_target_learned_vs_plain": headline,
             "model_rel_error": err, "time_to_final_rms_s": t_final, "gram_operator": gram_report,
             "learned": learned_report}
 
@@ -470,30 +625,27 @@ def run_learned(dev, plan, dirty, q, lmax, lam, sky, nvis, target, plain_rms, pl
                 "loss": losses}
     del data
     torch.cuda.empty_cache()
-    first = {}
-    trajectory = []
-
-    def stop(k, misfit):
-        rms = float(np.sqrt(max(2.0 * misfit, 0.0) / (2 * nvis)))
-        if k % 20 == 0:
-            trajectory.append([k, rms])
-        for name, level in (("plain", plain_rms), ("target", target)):
-            if rms <= level and name not in first:
-                first[name] = (k, torch.cuda.Event(enable_timing=True))
-                first[name][1].record()
-        return False
-
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     torch.cuda.synchronize()
     ev[0].record()
     psf, peak = learned.psf_patch(plan.grid(None))
     prop = learned.Proposer(net, npix)
-    x, gx, applies, st = learned.solve(plan.gram, dirty, lam, 1.0 / lmax, prop, psf, peak, max_iterations + 1,
-                                       q0=0.5 * q, stop=stop)
+    res = learned.solve(plan.gram, dirty, lam, 1.0 / lmax, prop, psf, peak, max_iterations + 1, q0=0.5 * q,
+                        events=True)
     ev[1].record()
     torch.cuda.synchronize()
-    rms = float(np.sqrt(max(2.0 * (0.5 * q - float(torch.dot(dirty.double().ravel(), x.double().ravel())) + 0.5 * float(
-        torch.dot(x.double().ravel(), gx.double().ravel()))), 0.0) / (2 * nvis)))
+    x, gx, applies, st = res
+    mis = res.misfits.cpu().numpy()
+    first = {}
+    trajectory = []
+    for k, e in res.events:
+        r = float(np.sqrt(max(2.0 * mis[k], 0.0) / (2 * nvis)))
+        if k % 20 == 0:
+            trajectory.append([k, r])
+        for name, level in (("plain", plain_rms), ("target", target)):
+            if r <= level and name not in first:
+                first[name] = (k, e)
+    rms = float(np.sqrt(max(2.0 * mis[applies], 0.0) / (2 * nvis)))
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     p0.record()
     prop(dirty, psf, 1.0 / peak)
@@ -621,16 +773,219 @@ def run_imaging_weights(wl, uvw_np, freq, mask, args):
     out = {"samples": nrow * nchan, "gpu_e2e_ms": 1e3 * t, "gpu_e2e_msamples_per_s": nrow * nchan / t / 1e6,
            "h2d_bytes": int(w_np.nbytes + uvw_np.nbytes), "d2h_bytes": int(w_np.nbytes)}
     if not args.no_cpu:
-        sys.path.insert(0, str(REPO / "oracle"))
-        import oracle
-
-        nt = max(1, int(round(wl["ntime"] * args.cpu_fraction)))
-        rows = nt * 2016
+        oracle = _oracle()
+        rows, nt = sample_rows(wl["ntime"], args.cpu_stride)
         t0 = time.perf_counter()
-        oracle.imaging_weights(uvw_np[:rows], wave, w_np[:rows], sel[:rows], **kw)
+        oracle.imaging_weights(uvw_np[rows], wave, w_np[rows], sel[rows], **kw)
         tc = time.perf_counter() - t0
-        out["cpu_oracle"] = {"samples": rows * nchan, "ms": 1e3 * tc, "msamples_per_s": rows * nchan / tc / 1e6,
-                             "cores": 1, "kind": "port"}
+        out["cpu_oracle"] = {"samples": rows.size * nchan, "ms": 1e3 * tc,
+                             "msamples_per_s": rows.size * nchan / tc / 1e6, "cores": 1, "kind": "port",
+                             "sample": f"every {args.cpu_stride}th integration ({nt} of {wl['ntime']})"}
+    return out
+
+
+# ------------------------------------------------------------------ accuracy and configuration 1
+
+
+def border_interior(x, ref):
+    """(border, interior, rms) of x - ref over max |ref|: L-inf over the
+    outer two pixels of the image, L-inf over the pixels eight or more in
+    from the edge, and the RMS over the whole image (the reference's edge
+    protocol, research/df2-wgridder-speed.md:446-487)."""
+    err = np.abs(np.asarray(x, np.float64) - ref)
+    peak = float(np.abs(ref).max())
+    inner = np.zeros(err.shape, bool)
+    inner[8:-8, 8:-8] = True
+    outer = np.ones(err.shape, bool)
+    outer[2:-2, 2:-2] = False
+    return (float(err[outer].max() / peak), float(err[inner].max() / peak),
+            float(np.sqrt(np.mean(err * err)) / peak))
+
+
+def vis_errors(v, ref):
+    """(L-inf, RMS) of the visibilities v - ref over max |ref|."""
+    err = np.abs(np.asarray(v, np.complex128) - ref)
+    peak = float(np.abs(ref).max())
+    return float(err.max() / peak), float(np.sqrt(np.mean(err * err)) / peak)
+
+
+# The gridding methods of the single-precision path (rang_b200_wgridder_set_method).
+METHODS = (("int8", 3), ("tf32x3", 1), ("bf16x3", 2), ("fp32", 0))
+
+
+def run_accuracy(dev, ext, wl, uvw, uvw_np, freq, vis, mask, common, args):
+    """Every gridding method against the oracle's FP64 run, and its time at
+    the full size.
+
+    Errors, on every `cpu_stride`-th integration of the workload's own data
+    (the same uv extent, w range and plan): the dirty image of the data, and
+    the visibilities of one fixed image (the oracle's FP64 dirty image,
+    rounded to float32), each against the oracle in float64 at epsilon 1e-7,
+    with the border apart from the interior. Times: one plan + grid and one
+    plan + degrid of the whole workload per method, after a warm-up, the
+    best of two. The single-precision kernels stop at epsilon 8.1e-7, so
+    1e-7 runs in double precision. Degridding has one single-precision
+    kernel for every method."""
+    import torch
+
+    from rang import gridder, wgrid_torch
+
+    oracle = _oracle()
+    oracle.set_threads(os.cpu_count() or 1)
+    rows, nt = sample_rows(wl["ntime"], args.cpu_stride)
+    ridx = torch.from_numpy(rows).to(dev)
+    s_vis = vis.index_select(0, ridx).cpu().numpy()
+    s_mask = mask.index_select(0, ridx).cpu().numpy()
+    npix, cell = common["npix_x"], common["pixsize_x"]
+    kw = dict(uvw=np.ascontiguousarray(uvw_np[rows]), freq=freq, mask=s_mask, pixsize_x=cell, pixsize_y=cell)
+    t0 = time.perf_counter()
+    d_ref = oracle.vis2dirty(vis=s_vis.astype(np.complex128), npix_x=npix, npix_y=npix, epsilon=1e-7, **kw)
+    img = d_ref.astype(np.float32)
+    v_ref = oracle.dirty2vis(dirty=img.astype(np.float64), epsilon=1e-7, **kw)
+    t_oracle = time.perf_counter() - t0
+    cases = [(e, name, code, True) for e in (1e-5, 1e-6) for name, code in METHODS]
+    cases += [(1e-5, "fp64", 3, False), (1e-7, "fp64", 3, False)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    methods = []
+    for eps_m, name, code, single in cases:
+        ext.wgridder_set_method(code)
+        d = gridder.vis2dirty(vis=s_vis if single else s_vis.astype(np.complex128), npix_x=npix, npix_y=npix,
+                              epsilon=eps_m, **kw)
+        v = gridder.dirty2vis(dirty=img if single else img.astype(np.float64), epsilon=eps_m, **kw)
+        b, i, r = border_interior(d, d_ref)
+        vl, vr = vis_errors(v, v_ref)
+        entry = {"method": name, "precision": "f32" if single else "f64", "epsilon": eps_m,
+                 "dirty_border_linf": b, "dirty_interior_linf": i, "dirty_rms": r, "vis_linf": vl, "vis_rms": vr}
+        del d, v
+        vin = vis if single else vis.to(torch.complex128)
+        iin = torch.from_numpy(img).to(dev) if single else torch.from_numpy(img).to(dev, torch.float64)
+        best = [float("inf"), float("inf")]
+        for rep in range(3):  # the first is a warm-up; the best of the other two is kept
+            torch.cuda.synchronize()
+            ev[0].record()
+            pa = wgrid_torch.DevicePlan(uvw, freq, vis=vin, mask=mask, epsilon=eps_m, single=single, **common)
+            dm = pa.grid(vin)
+            ev[1].record()
+            pb = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=eps_m, single=single, **common)
+            vm = pb.degrid(iin)
+            ev[2].record()
+            torch.cuda.synchronize()
+            supp = pa.info["supp"]
+            pa.close()
+            pb.close()
+            if rep > 0:
+                best = [min(best[0], ev[0].elapsed_time(ev[1])), min(best[1], ev[1].elapsed_time(ev[2]))]
+            del dm, vm
+        entry.update({"supp": int(supp), "vis2dirty_ms": best[0], "dirty2vis_ms": best[1]})
+        methods.append(entry)
+        del vin, iin
+    ext.wgridder_set_method(3)
+    # The methods on sparse data, where the split error of a single footprint
+    # does not average away: the dirty image of one and of eight visibilities
+    # (seeded baselines up to 2 km, 1 GHz, 256^2 at 4 arcsec) against the FP64
+    # direct Fourier transform.
+    srng = np.random.default_rng(11)
+    sparse = []
+    for nsparse in (1, 8):
+        suvw = srng.uniform(-2000.0, 2000.0, size=(nsparse, 3)) * np.array([1.0, 1.0, 0.2])
+        svis = srng.standard_normal((nsparse, 1)) + 1j * srng.standard_normal((nsparse, 1))
+        px = 4.0 * np.pi / 648000.0
+        skw = dict(uvw=suvw, freq=np.array([1.0e9]), npix_x=256, npix_y=256, pixsize_x=px, pixsize_y=px)
+        ref = oracle.dft_dirty(suvw, np.array([1.0e9]), svis, 256, 256, px, px)
+        for eps_m in (1e-5, 1e-6):
+            entry = {"visibilities": nsparse, "epsilon": eps_m}
+            for name, code in METHODS:
+                ext.wgridder_set_method(code)
+                dm = gridder.vis2dirty(vis=svis.astype(np.complex64), epsilon=eps_m, **skw)
+                entry[name + "_dirty_linf"] = float(np.abs(dm - ref).max() / np.abs(ref).max())
+            sparse.append(entry)
+    ext.wgridder_set_method(3)
+    return {"reference": "the oracle's FP64 run at epsilon 1e-7 on the sample; errors over the reference's peak",
+            "sample": sample_text(wl, args.cpu_stride, nt, s_vis.size), "oracle_s": t_oracle,
+            "methods": methods, "methods_sparse": sparse,
+            "methods_sparse_reference": "FP64 direct Fourier transform"}
+
+
+def run_config1(dev, args):
+    """The 16.5 M-visibility configuration: 64 antennas x 128 integrations x 64
+    channels, 50 point sources plus noise (sigma 0.1), unit weights, no flags,
+    1024^2 at 1.5 arcsec, epsilon 1e-5, f32 and f64. The GPU's vis2dirty
+    through the host-array API (copies included) and on device-resident
+    inputs, each the median of five after two warm-ups, with the output's
+    SHA256 over the repeats; the errors against the oracle's FP64 run at
+    epsilon 1e-7 (border apart); and the CPU oracle as the reference's
+    harness runs it, beside it."""
+    import torch
+
+    from rang import gridder, wgrid_torch
+
+    wl = synth.WORKLOADS[CONFIG1]
+    npix, cell = wl["npix"], wl["cell_arcsec"] * synth.ARCSEC
+    uvw_np = synth.uvw_tracks(nant=64, ntime=wl["ntime"], tint=8.0, dec_deg=-30.0, seed=7)
+    freq = synth.channels(wl["nchan"])
+    sky = synth.point_sky(npix, nsrc=50, seed=11)
+    kw = dict(uvw=uvw_np, freq=freq, pixsize_x=cell, pixsize_y=cell)
+    model = gridder.dirty2vis(dirty=sky, epsilon=1e-9, **kw)
+    rng = np.random.default_rng(101)
+    vis = (model + 0.1 * (rng.standard_normal(model.shape) + 1j * rng.standard_normal(model.shape))).astype(
+        np.complex64)
+    del model
+    nvis = vis.size
+    uvw = torch.from_numpy(uvw_np).to(dev)
+    common = dict(npix_x=npix, npix_y=npix, pixsize_x=cell, pixsize_y=cell)
+    out = {"configuration": "64 antennas x 128 integrations x 64 channels (16,515,072 visibilities), 50 point "
+                            "sources + noise sigma 0.1, unit weights, no flags, 1024^2 at 1.5 arcsec",
+           "gpu": []}
+    images = {}
+    for single, eps in ((True, 1e-5), (False, 1e-5), (False, 1e-7)):
+        hv = vis if single else vis.astype(np.complex128)
+        walls, hashes = [], set()
+        for rep in range(7):
+            t0 = time.perf_counter()
+            d = gridder.vis2dirty(vis=hv, npix_x=npix, npix_y=npix, epsilon=eps, **kw)
+            if rep >= 2:
+                walls.append(time.perf_counter() - t0)
+                hashes.add(sha256(d))
+        images[(single, eps)] = d
+        dv = torch.from_numpy(hv).to(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        times = []
+        for rep in range(7):
+            ev[0].record()
+            p = wgrid_torch.DevicePlan(uvw, freq, vis=dv, epsilon=eps, single=single, **common)
+            p.grid(dv)
+            ev[1].record()
+            torch.cuda.synchronize()
+            p.close()
+            if rep >= 2:
+                times.append(ev[0].elapsed_time(ev[1]) / 1e3)
+        del dv
+        w, t = statistics.median(walls), statistics.median(times)
+        out["gpu"].append({"precision": "f32" if single else "f64", "epsilon": eps,
+                           "e2e_s": w, "e2e_mvis_per_s": nvis / w / 1e6,
+                           "h2d_bytes": int(hv.nbytes + uvw_np.nbytes + freq.nbytes), "d2h_bytes": int(d.nbytes),
+                           "device_s": t, "device_mvis_per_s": nvis / t / 1e6,
+                           "dirty_sha256": sorted(hashes)[0], "identical_over_repeats": len(hashes) == 1})
+    if not args.no_cpu:
+        oracle = _oracle()
+        oracle.set_threads(os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        ref = oracle.vis2dirty(vis=vis.astype(np.complex128), npix_x=npix, npix_y=npix, epsilon=1e-7, **kw)
+        out["oracle_fp64_s"] = time.perf_counter() - t0
+        for g in out["gpu"]:
+            b, i, r = border_interior(images[(g["precision"] == "f32", g["epsilon"])], ref)
+            g.update({"vs_oracle_fp64_1e-7": {"border_linf": b, "interior_linf": i, "rms": r}})
+        with tempfile.TemporaryDirectory() as tmp:
+            path = Path(tmp) / "config1.npz"
+            np.savez(path, uvw=uvw_np, freq=freq, vis=vis, ntime=wl["ntime"], npix=npix, cell=cell)
+            cpu = cpu_protocol(path)
+        out["cpu"] = cpu
+        allth = {r["precision"]: r for r in cpu["runs"] if r["sample"] == "the whole configuration"}
+        for g in out["gpu"]:
+            c = allth.get(g["precision"]) if g["epsilon"] == 1e-5 else None
+            if c:
+                g["e2e_vs_cpu_all_threads"] = g["e2e_mvis_per_s"] / c["mvis_per_s"]
+                g["cpu_same_bits"] = None  # the GPU's exact integer sums and the CPU's float sums differ in rounding
     return out
 
 
@@ -729,7 +1084,7 @@ def run_b200(args):
     grid_bytes = nplanes * plan_info["nu"] * plan_info["nv"] * 8
     alg = {"grid": nact * (8 + 4) + nrow * 24 + grid_bytes, "degrid": nact * (8 + 4) + nrow * 24 + grid_bytes}
     dom = max(("grid", "degrid"), key=lambda k: prof[k][1])
-    kernel = {"grid": "k_grid_tc", "degrid": "k_degrid"}[dom]
+    kernel = {"grid": "k_grid_i8", "degrid": "k_degrid_h"}[dom]
     dom_launches, dom_ms = prof[dom]
     per_launch_s = dom_ms / max(dom_launches, 1) / 1e3
     achieved = alg[dom] / per_launch_s / 1e9
@@ -739,11 +1094,14 @@ def run_b200(args):
     # clock; the HBM bound and this bound together are the kernel's roofline.
     flops = 4.0 * supp**3 * nact
     fp32_peak = 148 * 128 * 2 * 1965e6 / 1e12
-    traffic = DRAM_TRAFFIC.get((args.workload, args.epsilon, kernel))
+    cap = DRAM_CAPTURE.get(kernel)
+    traffic = cap[0] * nact / cap[1] if cap and args.epsilon == 1e-5 else None
     roofline = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": peak_kind,
-                "traffic": traffic, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
-                                                      "one launch of this workload" if traffic else None,
+                "traffic": traffic,
+                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the "
+                                   f"{PROFILE_CASE} case ({cap[0] / 1e9:.2f} GB for {cap[1]} active visibilities), "
+                                   f"scaled by the active visibilities") if traffic else None,
                 "algorithmic_bytes_per_launch": alg[dom], "avg_launch_ms": per_launch_s * 1e3,
                 "share_of_step": dom_ms / max(total_prof, 1e-9),
                 "compute": {"useful_tflop_per_launch": flops / 1e12, "achieved_tflops": flops / per_launch_s / 1e12,
@@ -799,138 +1157,41 @@ def run_b200(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te / args.steps}
         del vis_h, mask_h, out_h, dirty_h
 
-    # Error of the float32 step against a float64 run at epsilon 1e-7.
     accuracy = None
-    if not args.no_accuracy:
-        p64 = wgrid_torch.DevicePlan(uvw, freq, vis=vis, mask=mask, epsilon=1e-7, single=False, **common)
-        d64 = p64.grid(vis)
-        p64.close()
-        dd = (dirty32.double() - d64)
-        peak = d64.abs().max()
-        q64 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=1e-7, single=False, **common)
-        v64 = q64.degrid(dirty32.double())
-        q64.close()
-        dv = vis32.to(torch.complex128) - v64
-        vpeak = v64.abs().max()
-        accuracy = {
-            "reference": "float64 GPU run at epsilon 1e-7 on the same inputs",
-            "dirty_rel_linf": float(dd.abs().max() / peak), "dirty_rel_rms": float(dd.pow(2).mean().sqrt() / peak),
-            "vis_rel_linf": float(dv.abs().max() / vpeak),
-            "vis_rel_rms": float(dv.abs().pow(2).mean().sqrt() / vpeak),
-        }
-        del v64, dd, dv
-
-        # The tensor-core (3 x TF32, 3 x BF16) and CUDA-core (FP32) gridders at epsilon
-        # 1e-5 (support 6) and 1e-6 (support 8; the single-precision kernels
-        # stop at 8.1e-7, so 1e-7 needs double precision, timed last): one
-        # plan + grid and one plan + degrid each (after a warm-up), errors
-        # against float64 at epsilon 1e-7 on the same inputs: the dirty image
-        # of the data, and the visibilities of one fixed image (the float64
-        # dirty image in float32). Degridding has one kernel for all three methods.
-        img = d64.float()
-        q64 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=1e-7, single=False, **common)
-        v64 = q64.degrid(img.double())
-        q64.close()
-        vpeak = v64.abs().max()
-        methods = []
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        cases = [(1e-5, "tf32x3", 1, True), (1e-5, "bf16x3", 2, True), (1e-5, "fp32", 0, True),
-                 (1e-6, "tf32x3", 1, True), (1e-6, "bf16x3", 2, True), (1e-6, "fp32", 0, True),
-                 (1e-7, "fp64", 1, False)]
-        for eps_m, name, code, single in cases:
-            ext.wgridder_set_method(code)
-            vin = vis if single else vis.to(torch.complex128)
-            iin = img if single else img.double()
-            best = [float("inf"), float("inf")]
-            for rep in range(3):  # the first is a warm-up; the best of the other two is kept
-                torch.cuda.synchronize()
-                ev[0].record()
-                pa = wgrid_torch.DevicePlan(uvw, freq, vis=vin, mask=mask, epsilon=eps_m, single=single, **common)
-                dm = pa.grid(vin)
-                ev[1].record()
-                pb = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=eps_m, single=single, **common)
-                vm = pb.degrid(iin)
-                ev[2].record()
-                torch.cuda.synchronize()
-                supp = pa.info["supp"]
-                pa.close()
-                pb.close()
-                if rep > 0:
-                    best = [min(best[0], ev[0].elapsed_time(ev[1])), min(best[1], ev[1].elapsed_time(ev[2]))]
-                if rep < 2:
-                    del dm, vm
-            entry = {"method": name, "epsilon": eps_m, "supp": int(supp),
-                     "vis2dirty_ms": best[0], "dirty2vis_ms": best[1]}
-            if single:
-                dd = dm.double() - d64
-                dv = vm.to(torch.complex128) - v64
-                entry.update({"dirty_rel_linf": float(dd.abs().max() / peak),
-                              "dirty_rel_rms": float(dd.pow(2).mean().sqrt() / peak),
-                              "vis_rel_linf": float(dv.abs().max() / vpeak),
-                              "vis_rel_rms": float(dv.abs().pow(2).mean().sqrt() / vpeak)})
-                del dd, dv
-            methods.append(entry)
-            del dm, vm, vin, iin
-        ext.wgridder_set_method(1)
-        accuracy["methods"] = methods
-        accuracy["methods_reference"] = "float64 GPU run at epsilon 1e-7; errors near 1e-7 are at that reference's level"
-        del d64, v64, img
-        # The same methods on sparse data, where the split error of a single
-        # footprint does not average away: the dirty image of one and of
-        # eight visibilities (seeded baselines up to 2 km, 1 GHz, 256^2 at
-        # 4 arcsec), relative L-inf error against float64 at epsilon 1e-12.
-        from rang import gridder
-
-        srng = np.random.default_rng(11)
-        sparse = []
-        for nvis in (1, 8):
-            suvw = srng.uniform(-2000.0, 2000.0, size=(nvis, 3)) * np.array([1.0, 1.0, 0.2])
-            svis = srng.standard_normal((nvis, 1)) + 1j * srng.standard_normal((nvis, 1))
-            skw = dict(uvw=suvw, freq=np.array([1.0e9]), npix_x=256, npix_y=256,
-                       pixsize_x=4.0 * np.pi / 648000.0, pixsize_y=4.0 * np.pi / 648000.0)
-            ref = gridder.vis2dirty(vis=svis, epsilon=1e-12, **skw)
-            for eps_m in (1e-5, 1e-6):
-                entry = {"visibilities": nvis, "epsilon": eps_m}
-                for name, code in (("fp32", 0), ("tf32x3", 1), ("bf16x3", 2)):
-                    ext.wgridder_set_method(code)
-                    dm = gridder.vis2dirty(vis=svis.astype(np.complex64), epsilon=eps_m, **skw)
-                    entry[name + "_dirty_rel_linf"] = float(np.abs(dm - ref).max() / np.abs(ref).max())
-                sparse.append(entry)
-        ext.wgridder_set_method(1)
-        accuracy["methods_sparse"] = sparse
+    if world == 1 and not args.no_accuracy:
+        accuracy = run_accuracy(dev, ext, wl, uvw, uvw_np, freq, vis, mask, common, args)
 
     fst = None
-    if rank == 0 and not args.no_fista:
+    if world == 1 and not args.no_fista:
         learn = None if args.no_learned else {"patches": args.learned_patches, "steps": args.learned_steps, "batch": 16}
-        fst = run_fista(dev, learn=learn)
+        fst = run_fista(dev, learn=learn, cap=args.fista_cap)
 
+    # The CPU oracle on a bounded sample of the same workload (one process,
+    # all host threads: one warm-up and three timed round trips).
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        oracle, suvw, sfreq, svis, smask, nt = cpu_sample(wl, args.cpu_fraction)
+    if world == 1 and not args.no_cpu:
+        oracle, suvw, sfreq, svis, smask, nt = cpu_sample(wl, args.cpu_stride)
         threads = oracle.set_threads(os.cpu_count() or 1)
+        cpu_round_trip(oracle, suvw, sfreq, svis, smask, npix, cell, eps)
         load = os.getloadavg()
-        t = cpu_round_trip(oracle, suvw, sfreq, svis, smask, npix, cell, eps)
+        times = [cpu_round_trip(oracle, suvw, sfreq, svis, smask, npix, cell, eps) for _ in range(3)]
+        t = statistics.median(times)
         cpu = {"value": svis.size / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"first {nt} of {wl['ntime']} integrations ({svis.size} visibilities), one round trip, "
-                         f"full {npix}^2 image and grid, {threads} threads",
-               "cpu_model": cpu_model(), "load_avg_before": list(load),
-               "ns_per_vis": 1e9 * t / svis.size}
-        # One core, on the first 4 integrations (a bounded sample of the same workload).
-        rows1 = 4 * 2016
-        oracle.set_threads(1)
-        t1 = cpu_round_trip(oracle, suvw[:rows1], sfreq, svis[:rows1], smask[:rows1], npix, cell, eps)
-        oracle.set_threads(threads)
-        cpu["single_core"] = {"value": svis[:rows1].size / t1 / 1e6, "unit": UNIT, "cores": 1,
-                              "sample": f"first 4 of {wl['ntime']} integrations ({svis[:rows1].size} visibilities), "
-                                        f"one round trip, full {npix}^2 image and grid (at this size the FFTs "
-                                        f"of the full grid take most of the time)"}
+               "sample": sample_text(wl, args.cpu_stride, nt, svis.size) + ", median of three round trips",
+               "cpu_model": cpu_model(), "simd": oracle.simd_level(), "load_avg_before": list(load),
+               "step_s": [round(x, 4) for x in times], "ns_per_vis": 1e9 * t / svis.size}
+        del svis, smask
+
+    config1 = None
+    if world == 1 and not args.no_config1:
+        config1 = run_config1(dev, args)
 
     weights_leg = None
-    if rank == 0 and world == 1 and not args.no_weights:
+    if world == 1 and not args.no_weights:
         weights_leg = run_imaging_weights(wl, uvw_np, freq, mask, args)
 
     msv4_leg = None
-    if rank == 0 and world == 1 and not args.no_msv4:
+    if world == 1 and not args.no_msv4:
         msv4_leg = run_msv4()
 
     if rank == 0:
@@ -938,13 +1199,11 @@ def run_b200(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "visibilities": nvis, "active": nact, "image": [npix, npix],
-                       "cell_arcsec": wl["cell_arcsec"], "epsilon": eps, "flags": wl["flag"],
-                       "parallelism": f"replicas{world}",
-                       "l2": f"inputs larger than L2 ({nvis * 8 / 1e9:.2f} GB of visibilities)",
-                       "plan": {k: plan_info[k] for k in ("kernel_index", "supp", "nu", "nv", "nplanes")}},
+            "config": workload_config(wl, args.workload, eps, world),
+            "plan": dict({k: plan_info[k] for k in ("kernel_index", "supp", "nu", "nv", "nplanes")}, active=nact),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk, "accuracy": accuracy, "fista": fst, "imaging_weights": weights_leg, "msv4_ingest": msv4_leg,
+            "clocks": clk, "accuracy": accuracy, "config1": config1, "fista": fst, "imaging_weights": weights_leg,
+            "msv4_ingest": msv4_leg,
             "stages_ms": {k: round(v[1], 3) for k, v in prof.items() if v[0]},
         }
         print(json.dumps(line, default=_plain), flush=True)
@@ -955,7 +1214,9 @@ def run_b200(args):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.cpu_worker:
+        cpu_worker(args.cpu_worker)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

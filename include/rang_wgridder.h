@@ -147,6 +147,54 @@ int32_t rang_b200_wgridder_plan_status(RangWgridPlan* plan, void* stream);
 int32_t rang_b200_wgridder_plan_info(const RangWgridPlan* plan, double* info);
 void rang_b200_wgridder_plan_destroy(RangWgridPlan* plan);
 
+/* Prepared::residual / residual_sorted (wgridder.rs:3232-3278): the residual
+ * image of `data_dev` against the image `model_dev` (nx * ny in the plan's
+ * precision; null: the data alone) into image_dev, gridded with the weights
+ * (kinds as for plan_grid), and sum w |d - A model|^2 into *misfit_dev (one
+ * double on the device; null: not formed). The prediction is degridded
+ * without weights. sorted = 0: data and weights are nrow * nchan; 1: they
+ * hold the plan's active visibilities in its sorted order
+ * (rang_b200_wgridder_plan_sorted). The values live in the plan's stored
+ * work space (sorted order), so no visibility-sized buffer is allocated per
+ * call, and nothing waits for the device: the call is asynchronous on
+ * `stream`. Passes of one plan must run in stream order (they share that
+ * work space). */
+int32_t rang_b200_wgridder_plan_residual(RangWgridPlan* plan, const void* data_dev, int32_t vis_kind,
+                                         const void* wgt_dev, const void* wgt2_dev, int32_t wgt_kind,
+                                         const void* model_dev, int32_t sorted, void* image_dev, double* misfit_dev,
+                                         void* stream);
+/* The Gram operator A^H W A of the plan (the reference's gram_apply,
+ * clean_certified.rs:233-236) on x_dev (nx * ny) into image_dev, W the
+ * weights (sorted as for plan_residual), and x^T A^H W A x = sum w |A x|^2
+ * into *xgx_dev (null: not formed). Asynchronous on `stream`. */
+int32_t rang_b200_wgridder_plan_gram(RangWgridPlan* plan, const void* x_dev, const void* wgt_dev,
+                                     const void* wgt2_dev, int32_t wgt_kind, int32_t sorted, void* image_dev,
+                                     double* xgx_dev, void* stream);
+/* Prepared::sorted (wgridder.rs:3287-3302): dense_dev (nrow * nchan elements
+ * of elem_bytes = 1, 4, 8 or 16) at the active visibilities, in the plan's
+ * sorted order, into out_dev (plan_active elements). */
+int32_t rang_b200_wgridder_plan_sorted(const RangWgridPlan* plan, const void* dense_dev, int32_t elem_bytes,
+                                       void* out_dev, void* stream);
+/* Prepared::active: the number of active visibilities. */
+int32_t rang_b200_wgridder_plan_active(const RangWgridPlan* plan, size_t* active);
+/* Prepared::memory (wgridder.rs:3397-3430): device bytes held per buffer
+ * into bytes[0, n); returns the number of buffers (names from
+ * plan_memory_name), or -1 for a null plan. */
+int32_t rang_b200_wgridder_plan_memory(const RangWgridPlan* plan, size_t* bytes, int32_t n);
+const char* rang_b200_wgridder_plan_memory_name(int32_t index);
+/* Prepared::release_grids (wgridder.rs:3432-3440): frees the stored values
+ * that residual and Gram passes keep; the next pass allocates them again. */
+void rang_b200_wgridder_plan_release_work(RangWgridPlan* plan);
+/* `plan` and `gridding_footprint` (wgridder.rs:3527-3588) on HOST arrays:
+ * the kernel and grid a call would choose (info, 14 doubles; the activity as
+ * for rang_b200_wgridder_binning, with_vis when vis_kind is not 0), without
+ * binning or gridding, and in *footprint (may be null) the device bytes of
+ * a gridding pass's work space for `nout` images. */
+int32_t rang_b200_wgridder_plan_only(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                     const double* freq, const void* vis, int32_t vis_kind, const void* wgt,
+                                     const void* wgt2, int32_t wgt_kind, const uint8_t* mask, int32_t single,
+                                     int32_t nout, double* info, size_t* footprint);
+
 /* The visibility binning of a call on HOST arrays, for parity tests: per
  * visibility (row-major) iu0, iv0 (-1 when inactive) and the bin key
  * tile * max(nplanes, 1) + first plane (0xffffffff when inactive), and the

@@ -44,12 +44,36 @@ class Options(ctypes.Structure):
     ]
 
 
+LIB_AVX512 = HERE / "liboracle_avx512.so"
+# CPU flags the x86-64-v4 build may use.
+_AVX512_FLAGS = ("avx512f", "avx512vl", "avx512bw", "avx512dq", "avx512cd")
+
+
 def build():
-    """Compile liboracle.so with the committed Makefile (idempotent)."""
+    """Compile both libraries with the committed Makefile (idempotent)."""
     srcs = [HERE / "wgridder_oracle.cpp", HERE / "weights_oracle.cpp"]
-    if not LIB.exists() or any(LIB.stat().st_mtime < src.stat().st_mtime for src in srcs):
+    if any(not p.exists() or any(p.stat().st_mtime < s.stat().st_mtime for s in srcs) for p in (LIB, LIB_AVX512)):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
+
+
+def simd_level():
+    """The instruction set of the library `lib()` loads, chosen as the
+    reference chooses its gridding loops (`core/src/wgridder.rs:1592-1625`):
+    "avx512" where the host has AVX-512 (the x86-64-v4 set), else "avx2";
+    RANG_WGRIDDER_SIMD=avx2 caps it. The oracle has no variant below AVX2."""
+    if os.environ.get("RANG_WGRIDDER_SIMD") in ("avx2", "baseline"):
+        return "avx2"
+    try:
+        flags = set()
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+    except OSError:
+        return "avx2"
+    return "avx512" if all(x in flags for x in _AVX512_FLAGS) else "avx2"
 
 
 _lib = None
@@ -59,7 +83,7 @@ def lib():
     global _lib
     if _lib is None:
         build()
-        _lib = ctypes.CDLL(str(LIB))
+        _lib = ctypes.CDLL(str(LIB_AVX512 if simd_level() == "avx512" else LIB))
         P = ctypes.c_void_p
         S = ctypes.c_size_t
         I = ctypes.c_int

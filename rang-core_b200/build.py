@@ -30,9 +30,11 @@ NVCC = str(CUDA / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = PKG / "librang_wgrid_b200.so"
 
-CU_SOURCES = ["wgrid_plan.cu", "wgrid_capi.cu", "wgrid_weights.cu", "wgrid_gram.cu", "nn_kernels.cu", "nn_conv_tc.cu"]
+CU_SOURCES = ["wgrid_plan.cu", "wgrid_capi.cu", "wgrid_weights.cu", "wgrid_gram.cu", "wgrid_solver.cu", "nn_kernels.cu",
+              "nn_conv_tc.cu"]
 CXX_SOURCES = ["wgrid_setup.cpp", "msv4_codec.cpp"]
-HEADERS = ["wgrid_common.h", "wgrid_device.cuh", "wgrid_plan.h", "wgrid_setup.h", "kernel_db.inc", "nn_conv_tc.h"]
+HEADERS = ["wgrid_common.h", "wgrid_device.cuh", "wgrid_fast.cuh", "wgrid_plan.h", "wgrid_setup.h", "kernel_db.inc",
+           "nn_conv_tc.h"]
 
 
 def ext_path():
@@ -52,7 +54,8 @@ def _run(cmd):
 
 
 def build_lib(force=False, jobs=None):
-    deps = [CSRC / s for s in CU_SOURCES + CXX_SOURCES + HEADERS] + [INCLUDE / "rang_wgridder.h", INCLUDE / "rang_weights.h", INCLUDE / "rang_gram.h", INCLUDE / "rang_nn.h", INCLUDE / "rang_msv4.h"]
+    deps = [CSRC / s for s in CU_SOURCES + CXX_SOURCES + HEADERS] + [INCLUDE / "rang_wgridder.h", INCLUDE / "rang_weights.h", INCLUDE / "rang_gram.h", INCLUDE / "rang_nn.h", INCLUDE / "rang_msv4.h",
+            INCLUDE / "rang_solver.h"]
     deps.append(Path(__file__))
     if not force and not _stale(LIB, deps):
         return LIB

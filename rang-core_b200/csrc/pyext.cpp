@@ -345,6 +345,65 @@ PYBIND11_MODULE(_core, m) {
     py::gil_scoped_release release;
     rang_b200_wgridder_plan_destroy(reinterpret_cast<RangWgridPlan*>(plan));
   });
+  m.def("wgridder_plan_residual",
+        [](uintptr_t plan, uintptr_t data, int vis_kind, uintptr_t wgt, uintptr_t wgt2, int wgt_kind, uintptr_t model,
+           int sorted, uintptr_t image, uintptr_t misfit, uintptr_t stream) {
+          py::gil_scoped_release release;
+          return rang_b200_wgridder_plan_residual(reinterpret_cast<RangWgridPlan*>(plan), ptr(data), vis_kind,
+                                                  ptr(wgt), ptr(wgt2), wgt_kind, ptr(model), sorted, (void*)image,
+                                                  (double*)misfit, (void*)stream);
+        });
+  m.def("wgridder_plan_gram", [](uintptr_t plan, uintptr_t x, uintptr_t wgt, uintptr_t wgt2, int wgt_kind, int sorted,
+                                 uintptr_t image, uintptr_t xgx, uintptr_t stream) {
+    py::gil_scoped_release release;
+    return rang_b200_wgridder_plan_gram(reinterpret_cast<RangWgridPlan*>(plan), ptr(x), ptr(wgt), ptr(wgt2), wgt_kind,
+                                        sorted, (void*)image, (double*)xgx, (void*)stream);
+  });
+  m.def("wgridder_plan_sorted", [](uintptr_t plan, uintptr_t dense, int elem_bytes, uintptr_t out, uintptr_t stream) {
+    py::gil_scoped_release release;
+    return rang_b200_wgridder_plan_sorted(reinterpret_cast<RangWgridPlan*>(plan), ptr(dense), elem_bytes,
+                                          (void*)out, (void*)stream);
+  });
+  m.def("wgridder_plan_active", [](uintptr_t plan) {
+    size_t n = 0;
+    int st = rang_b200_wgridder_plan_active(reinterpret_cast<RangWgridPlan*>(plan), &n);
+    return py::make_tuple(st, n);
+  });
+  m.def("wgridder_plan_memory", [](uintptr_t plan) {
+    size_t b[32];
+    int n = rang_b200_wgridder_plan_memory(reinterpret_cast<RangWgridPlan*>(plan), b, 32);
+    py::list out;
+    for (int i = 0; i < n && i < 32; i++)
+      out.append(py::make_tuple(std::string(rang_b200_wgridder_plan_memory_name(i)), b[i]));
+    return out;
+  });
+  m.def("wgridder_plan_release_work",
+        [](uintptr_t plan) { rang_b200_wgridder_plan_release_work(reinterpret_cast<RangWgridPlan*>(plan)); });
+  m.def("wgridder_plan_only", [](std::vector<double> opts, py::object uvw, py::object freq, py::object vis,
+                                 py::object wgt, py::object wgt2, py::object mask, int single, int nout) {
+    WgridderOptions o = options(opts);
+    size_t nuvw, nfreq, nvis = 0, nwgt = 0, nwgt2 = 0, nmask = 0;
+    const double* puvw = ro<double>(uvw, "uvw", &nuvw);
+    const double* pfreq = ro<double>(freq, "freq", &nfreq);
+    int vkind, wkind;
+    const void* pvis = vis_arg(vis, &vkind, &nvis);
+    const void* pwgt = wgt_arg(wgt, &wkind, &nwgt);
+    const void* pwgt2 = nullptr;
+    if (!wgt2.is_none()) {
+      pwgt2 = ro<float>(wgt2, "wgt2", &nwgt2);
+      wkind = WGRIDDER_WGT_F32_PRODUCT;
+    }
+    const uint8_t* pmask = mask.is_none() ? nullptr : ro<uint8_t>(mask, "mask", &nmask);
+    py::array_t<double> info(14);
+    size_t fp = 0;
+    int32_t st;
+    {
+      py::gil_scoped_release release;
+      st = rang_b200_wgridder_plan_only(&o, nuvw / 3, nfreq, puvw, pfreq, pvis, vkind, pwgt, pwgt2, wkind, pmask,
+                                        single, nout, info.mutable_data(), &fp);
+    }
+    return py::make_tuple(st, info, fp);
+  });
   m.def("wgridder_set_method", [](int m) { return (int)rang_b200_wgridder_set_method(m); });
   m.def("wgridder_launch_count", []() { return (long long)rang_b200_wgridder_launch_count(); });
   m.def("wgridder_profile", [](int on) { rang_b200_wgridder_profile(on); });

@@ -24,8 +24,8 @@ void weight_grid_shape(size_t width, size_t height, double super_weight, size_t*
 size_t padded_size(size_t trimmed, double padding);
 void stokes_i(const StokesIInputs& in, StokesIOutputs& out, cudaStream_t s);
 void imaging_weights(const ImagingWeightInputs& in, ImagingWeightOutputs& out, cudaStream_t s);
-int32_t gram_guarded(const std::function<void()>& f);
-cudaStream_t gram_stream(void* stream);
+int32_t status_guarded(const std::function<void()>& f);
+cudaStream_t stream_of(void* stream);
 }  // namespace wg
 
 using namespace wg;
@@ -329,10 +329,11 @@ void host_dirty2vis(const WgridderOptions* o, size_t nrow, size_t nchan, const d
 
 std::string* wg::last_error_slot() { return &g_last_error; }
 
-// The Gram operator's entry points (wgrid_gram.cu) share the status mapping,
+// The Gram operator's and the solver's entry points (wgrid_gram.cu,
+// wgrid_solver.cu) share the status mapping,
 // the per-thread message and the per-thread stream.
-int32_t wg::gram_guarded(const std::function<void()>& f) { return guarded(f); }
-cudaStream_t wg::gram_stream(void* stream) {
+int32_t wg::status_guarded(const std::function<void()>& f) { return guarded(f); }
+cudaStream_t wg::stream_of(void* stream) {
   int dev = 0;
   check_cuda(cudaGetDevice(&dev), "no CUDA device");
   configure_pool(dev);
@@ -552,6 +553,104 @@ int32_t rang_b200_wgridder_plan_info(const RangWgridPlan* plan, double* info) {
 }
 
 void rang_b200_wgridder_plan_destroy(RangWgridPlan* plan) { delete plan; }
+
+int32_t rang_b200_wgridder_plan_residual(RangWgridPlan* plan, const void* data_dev, int32_t vis_kind,
+                                         const void* wgt_dev, const void* wgt2_dev, int32_t wgt_kind,
+                                         const void* model_dev, int32_t sorted, void* image_dev, double* misfit_dev,
+                                         void* stream) {
+  return guarded([&] {
+    if (!plan || !image_dev) throw InvalidArgument("null array");
+    if (vis_kind == VIS_UNIT) throw InvalidArgument("the residual needs data");
+    vis_bytes(vis_kind, data_dev);
+    wgt_bytes(wgt_kind, wgt_dev, wgt2_dev);
+    Inputs in{data_dev, vis_kind, wgt_dev, wgt2_dev, wgt_kind, nullptr};
+    if (plan->single)
+      plan->f->residual(in, sorted != 0, (const float*)model_dev, (float*)image_dev, misfit_dev, (cudaStream_t)stream);
+    else
+      plan->d->residual(in, sorted != 0, (const double*)model_dev, (double*)image_dev, misfit_dev,
+                        (cudaStream_t)stream);
+  });
+}
+
+int32_t rang_b200_wgridder_plan_gram(RangWgridPlan* plan, const void* x_dev, const void* wgt_dev,
+                                     const void* wgt2_dev, int32_t wgt_kind, int32_t sorted, void* image_dev,
+                                     double* xgx_dev, void* stream) {
+  return guarded([&] {
+    if (!plan || !x_dev || !image_dev) throw InvalidArgument("null array");
+    wgt_bytes(wgt_kind, wgt_dev, wgt2_dev);
+    Inputs in{nullptr, VIS_UNIT, wgt_dev, wgt2_dev, wgt_kind, nullptr};
+    if (plan->single)
+      plan->f->gram((const float*)x_dev, in, sorted != 0, (float*)image_dev, xgx_dev, (cudaStream_t)stream);
+    else
+      plan->d->gram((const double*)x_dev, in, sorted != 0, (double*)image_dev, xgx_dev, (cudaStream_t)stream);
+  });
+}
+
+int32_t rang_b200_wgridder_plan_sorted(const RangWgridPlan* plan, const void* dense_dev, int32_t elem_bytes,
+                                       void* out_dev, void* stream) {
+  return guarded([&] {
+    if (!plan || !dense_dev || !out_dev) throw InvalidArgument("null array");
+    if (plan->single)
+      plan->f->gather_sorted(dense_dev, elem_bytes, out_dev, (cudaStream_t)stream);
+    else
+      plan->d->gather_sorted(dense_dev, elem_bytes, out_dev, (cudaStream_t)stream);
+  });
+}
+
+int32_t rang_b200_wgridder_plan_active(const RangWgridPlan* plan, size_t* active) {
+  if (!plan || !active) return 1;
+  *active = plan->single ? plan->f->nvis() : plan->d->nvis();
+  return 0;
+}
+
+int32_t rang_b200_wgridder_plan_memory(const RangWgridPlan* plan, size_t* bytes, int32_t n) {
+  if (!plan) return -1;
+  const auto m = plan->single ? plan->f->memory() : plan->d->memory();
+  for (int32_t i = 0; i < n && i < (int32_t)m.size(); i++) bytes[i] = m[i].second;
+  return (int32_t)m.size();
+}
+
+const char* rang_b200_wgridder_plan_memory_name(int32_t index) {
+  static const auto names = Plan<float>::memory_names();
+  return index >= 0 && index < (int32_t)names.size() ? names[index] : nullptr;
+}
+
+void rang_b200_wgridder_plan_release_work(RangWgridPlan* plan) {
+  if (!plan) return;
+  if (plan->single)
+    plan->f->release_work();
+  else
+    plan->d->release_work();
+}
+
+int32_t rang_b200_wgridder_plan_only(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
+                                     const double* freq, const void* vis, int32_t vis_kind, const void* wgt,
+                                     const void* wgt2, int32_t wgt_kind, const uint8_t* mask, int32_t single,
+                                     int32_t nout, double* info, size_t* footprint) {
+  return guarded([&] {
+    if (!opts) throw InvalidArgument("null options");
+    if (!uvw || !freq || !info) throw InvalidArgument("null array");
+    vis_bytes(vis_kind, vis);
+    wgt_bytes(wgt_kind, wgt, wgt2);
+    check_common(*opts, nrow, nchan);
+    f_over_c(freq, nchan);
+    cudaStream_t s = call_stream();
+    Uploaded u = upload_inputs(nrow, nchan, uvw, vis, vis_kind, wgt, wgt2, wgt_kind, mask, s);
+    const bool with_vis = vis_kind != VIS_UNIT;
+    size_t fp = 0;
+    if (single) {
+      Plan<float> plan(*opts, nrow, nchan, u.uvw.as<double>(), freq, u.in, with_vis, s, 1, false);
+      std::memcpy(info, plan.info().v, sizeof(plan.info().v));
+      fp = plan.footprint(nout);
+    } else {
+      Plan<double> plan(*opts, nrow, nchan, u.uvw.as<double>(), freq, u.in, with_vis, s, 1, false);
+      std::memcpy(info, plan.info().v, sizeof(plan.info().v));
+      fp = plan.footprint(nout);
+    }
+    if (footprint) *footprint = fp;
+    check_cuda(cudaStreamSynchronize(s), "plan");
+  });
+}
 
 int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
                                    const double* freq, const void* vis, int32_t vis_kind, const void* wgt,

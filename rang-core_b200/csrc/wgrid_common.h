@@ -16,7 +16,9 @@
 namespace wg {
 
 // Data kinds of the `_ex` entry points (ffi_wgridder.rs:297-310).
-enum VisKind : int { VIS_UNIT = 0, VIS_C64 = 1, VIS_C128 = 2 };
+// VIS_SORTED is internal: complex float values indexed by sorted position
+// (a plan's stored values); no entry point accepts it from a caller.
+enum VisKind : int { VIS_UNIT = 0, VIS_C64 = 1, VIS_C128 = 2, VIS_SORTED = 3 };
 enum WgtKind : int { WGT_NONE = 0, WGT_F32 = 1, WGT_F64 = 2, WGT_F32_PRODUCT = 3 };
 
 constexpr double C_LIGHT = 299792458.0;  // wgridder.rs:58

@@ -390,14 +390,17 @@ __device__ __forceinline__ void cp_async(void* dst, const void* src, int bytes) 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Starts the copies of record `idx` and (with_vis, with_wgt) its value's inputs.
+// Starts the copies of record `idx` (at sorted position k) and (with_vis,
+// with_wgt) its value's inputs.
 __device__ __forceinline__ void prefetch(Prefetched* dst, const VisRecord* __restrict__ rec, const Inputs& in,
-                                         bool with_vis, bool with_wgt, uint32_t idx) {
+                                         bool with_vis, bool with_wgt, uint32_t idx, uint64_t k) {
   const uint4* r = reinterpret_cast<const uint4*>(rec + idx);
   cp_async(&dst->rec[0], r, 16);
   cp_async(&dst->rec[1], r + 1, 16);
   if (with_vis) {
-    if (in.vis_kind == VIS_C64)
+    if (in.vis_kind == VIS_SORTED)
+      cp_async(&dst->vis, reinterpret_cast<const float2*>(in.vis) + k, 8);
+    else if (in.vis_kind == VIS_C64)
       cp_async(&dst->vis, reinterpret_cast<const float2*>(in.vis) + idx, 8);
     else if (in.vis_kind == VIS_C128)
       cp_async(&dst->vis, reinterpret_cast<const double2*>(in.vis) + idx, 16);
@@ -431,7 +434,7 @@ __device__ __forceinline__ float prefetched_wgt(const Prefetched& p, const Input
   }
 }
 __device__ __forceinline__ cplx<float> prefetched_vis(const Prefetched& p, const Inputs& in) {
-  if (in.vis_kind == VIS_C64) return {__uint_as_float(p.vis.x), __uint_as_float(p.vis.y)};
+  if (in.vis_kind == VIS_C64 || in.vis_kind == VIS_SORTED) return {__uint_as_float(p.vis.x), __uint_as_float(p.vis.y)};
   if (in.vis_kind == VIS_C128)
     return {(float)__longlong_as_double((long long)(((unsigned long long)p.vis.y << 32) | p.vis.x)),
             (float)__longlong_as_double((long long)(((unsigned long long)p.vis.w << 32) | p.vis.z))};
@@ -572,7 +575,7 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
   // nidx is the next round's index.
   Prefetched* pre = reinterpret_cast<Prefetched*>(smem + I8Slots::bytes()) + lane;
   const bool with_vis = mode == VALUE_DATA && in.vis_kind != VIS_UNIT, with_wgt = in.wgt_kind != WGT_NONE;
-  if (k0 + lane < k1) prefetch(pre, rec, in, with_vis, with_wgt, sorted[k0 + lane]);
+  if (k0 + lane < k1) prefetch(pre, rec, in, with_vis, with_wgt, sorted[k0 + lane], k0 + lane);
   cp_async_commit();
   uint32_t nidx = (k0 + I8_BATCH + lane < k1) ? sorted[k0 + I8_BATCH + lane] : 0u;
 
@@ -627,7 +630,7 @@ __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
     }
     // The next round's record and value, in flight while this one is contracted.
     __syncwarp();
-    if (kb + I8_BATCH + lane < k1) prefetch(pre, rec, in, with_vis, with_wgt, nidx);
+    if (kb + I8_BATCH + lane < k1) prefetch(pre, rec, in, with_vis, with_wgt, nidx, kb + I8_BATCH + lane);
     cp_async_commit();
     if (kb + 2 * I8_BATCH + lane < k1) nidx = sorted[kb + 2 * I8_BATCH + lane];
     int q = 0;
@@ -754,6 +757,26 @@ __device__ __forceinline__ void hmma(float (&d)[4], uint32_t a0, uint32_t a1, ui
       : "r"(a0), "r"(a1), "r"(b0));
 }
 
+// Where the degridder's results go. DEGRID_TO_VIS: vis[visibility index],
+// times the weights of the call. The two other modes write the plan's stored
+// values, indexed by sorted position, for the gridder to read back
+// (Prepared::residual, wgridder.rs:3297-3395): DEGRID_GRAM stores w A x
+// (the prediction times the weight of `data`), DEGRID_RESIDUAL stores
+// w (d - A x) with d the visibility of `data`; both add w |stored / w|^2 into
+// an FP64 partial per block (partials[block0 + block], summed by the warp in
+// a fixed order) and the largest |stored| into `bound`.
+enum DegridMode : int { DEGRID_TO_VIS = 0, DEGRID_GRAM = 1, DEGRID_RESIDUAL = 2 };
+struct DegridOut {
+  int mode = DEGRID_TO_VIS;
+  cplx<float>* vis = nullptr;     // DEGRID_TO_VIS
+  cplx<float>* stored = nullptr;  // the other modes
+  Inputs data;                    // weights (and visibilities) of the stored modes
+  int sorted_data = 0;            // data and weights by sorted position, not by visibility index
+  double* partials = nullptr;
+  uint32_t block0 = 0;
+  ValueBound* bound = nullptr;
+};
+
 // Degridding of records [kbase, kend) (single precision, degrid_task_body,
 // wgridder.rs:2793-2901): per bin the warp holds the bin's 8 x 8 window of
 // each plane as FP16 hi + lo fragments (scaled by a power of two to the
@@ -767,13 +790,13 @@ __device__ __forceinline__ void hmma(float (&d)[4], uint32_t a0, uint32_t a1, ui
 // result does not depend on the grouping. With plane groups (first / last)
 // the partial sums accumulate in `vis` and the final factor is applied with
 // the last group. The next round's records are copied while the current
-// round is contracted.
+// round is contracted. `out` says where the results go (DegridOut).
 template <int S>
 __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 16 : 12)
     k_degrid_h(const __grid_constant__ Geom<float> g, Inputs wts, const VisRecord* __restrict__ rec,
                const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
-               const cplx<float>* __restrict__ grids, int pg0, int npg, cplx<float>* __restrict__ vis, int first,
-               int last) {
+               const cplx<float>* __restrict__ grids, int pg0, int npg, const __grid_constant__ DegridOut out,
+               int first, int last) {
   static_assert(S >= 1 && S <= 8, "8 x 8 windows");
   extern __shared__ __align__(16) unsigned char smem[];
   H16Slots st;
@@ -795,10 +818,11 @@ __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 16 : 12)
   uint32_t bhi[S][2], blo[S][2];  // [plane][re/im]: window rows gq, columns 2tq, 2tq + 1
   float inv = 0.0f;               // 1 / (window scale * 2^14)
   uint32_t gcur = INACTIVE;
+  double part = 0.0, vmax = 0.0;  // the stored modes' misfit partial and largest |stored|
 
   Prefetched* pre = reinterpret_cast<Prefetched*>(smem + H16Slots::bytes()) + lane;
   const bool with_wgt = wts.wgt_kind != WGT_NONE;
-  if (k0 + lane < k1) prefetch(pre, rec, wts, false, with_wgt, sorted[k0 + lane]);
+  if (k0 + lane < k1) prefetch(pre, rec, wts, false, with_wgt, sorted[k0 + lane], k0 + lane);
   cp_async_commit();
   uint32_t nidx = (k0 + H16_BATCH + lane < k1) ? sorted[k0 + H16_BATCH + lane] : 0u;
 
@@ -844,7 +868,7 @@ __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 16 : 12)
       st.key[lane] = r.bin;
     }
     __syncwarp();
-    if (kb + H16_BATCH + lane < k1) prefetch(pre, rec, wts, false, with_wgt, nidx);
+    if (kb + H16_BATCH + lane < k1) prefetch(pre, rec, wts, false, with_wgt, nidx, kb + H16_BATCH + lane);
     cp_async_commit();
     if (kb + 2 * H16_BATCH + lane < k1) nidx = sorted[kb + 2 * H16_BATCH + lane];
     int q = 0;
@@ -937,19 +961,95 @@ __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 16 : 12)
             if (sr[h] == H16_BATCH) continue;
             const float4 fo = st.out[sr[h]];
             const uint32_t idx = __float_as_uint(fo.w);
+            const uint64_t k = kb + (uint64_t)sr[h];
+            cplx<float>* dst = out.mode == DEGRID_TO_VIS ? out.vis + idx : out.stored + k;
             cplx<float> accv{tr[h] * inv, ti[h] * inv * fo.z};
             if (!first) {
-              const cplx<float> prev = vis[idx];
+              const cplx<float> prev = *dst;
               accv = {accv.re + prev.re, accv.im + prev.im};
             }
-            if (last) accv = {accv.re * fo.x - accv.im * fo.y, accv.re * fo.y + accv.im * fo.x};
-            vis[idx] = accv;
+            if (last) {
+              accv = {accv.re * fo.x - accv.im * fo.y, accv.re * fo.y + accv.im * fo.x};
+              if (out.mode != DEGRID_TO_VIS) {
+                const uint64_t di = out.sorted_data ? k : (uint64_t)idx;
+                const float w = wgt_get<float>(out.data, di);
+                if (out.mode == DEGRID_RESIDUAL) {
+                  const cplx<float> d = vis_get<float>(out.data, di);
+                  accv = {d.re - accv.re, d.im - accv.im};
+                }
+                part += (double)w * ((double)accv.re * (double)accv.re + (double)accv.im * (double)accv.im);
+                accv = {accv.re * w, accv.im * w};
+                vmax = fmax(vmax, sqrt((double)accv.re * (double)accv.re + (double)accv.im * (double)accv.im));
+              }
+            }
+            *dst = accv;
           }
         }
       }
       q += len;
     }
   }
+  if (out.mode != DEGRID_TO_VIS && last) {
+    for (int o = 16; o > 0; o >>= 1) {
+      part += __shfl_down_sync(0xffffffffu, part, o);
+      vmax = fmax(vmax, __shfl_down_sync(0xffffffffu, vmax, o));
+    }
+    if (lane == 0) {
+      out.partials[out.block0 + blockIdx.x] = part;
+      atomic_max_double(&out.bound->vmax_bits, vmax);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ residual without a model, and sums
+
+constexpr uint32_t STORE_CHUNK = 8192;  // sorted positions per block of k_store_values
+constexpr int STORE_THREADS = 256;
+
+// Fixed-order sum of one value per thread of a block into thread 0.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  return sh[0];
+}
+
+// The residual of the data alone (no model): stored[k] = w d for the
+// visibility at sorted position k, w |d|^2 summed into partials[block]
+// (each block takes STORE_CHUNK positions, each thread a fixed stride of
+// them, then a fixed tree), and the largest |stored| into `bound`.
+__global__ void __launch_bounds__(STORE_THREADS)
+    k_store_values(uint64_t n, const uint32_t* __restrict__ sorted, Inputs data, int sorted_data,
+                   cplx<float>* __restrict__ stored, double* __restrict__ partials, ValueBound* bound) {
+  __shared__ double sh[STORE_THREADS];
+  const uint64_t k0 = (uint64_t)blockIdx.x * STORE_CHUNK, k1 = min(n, k0 + STORE_CHUNK);
+  double part = 0.0, vmax = 0.0;
+  for (uint64_t k = k0 + threadIdx.x; k < k1; k += STORE_THREADS) {
+    const uint64_t di = sorted_data ? k : (uint64_t)sorted[k];
+    const float w = wgt_get<float>(data, di);
+    const cplx<float> d = vis_get<float>(data, di);
+    part += (double)w * ((double)d.re * (double)d.re + (double)d.im * (double)d.im);
+    const cplx<float> v{d.re * w, d.im * w};
+    vmax = fmax(vmax, sqrt((double)v.re * (double)v.re + (double)v.im * (double)v.im));
+    stored[k] = v;
+  }
+  const double sum = block_sum(part, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = sum;
+  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_down_sync(0xffffffffu, vmax, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_double(&bound->vmax_bits, vmax);
+}
+
+// out = sum of partials[0, n) in a fixed order (one block).
+__global__ void __launch_bounds__(STORE_THREADS) k_sum_partials(const double* __restrict__ partials, uint32_t n,
+                                                                 double* out) {
+  __shared__ double sh[STORE_THREADS];
+  double v = 0.0;
+  for (uint32_t i = threadIdx.x; i < n; i += STORE_THREADS) v += partials[i];
+  const double s = block_sum(v, sh);
+  if (threadIdx.x == 0) *out = s;
 }
 
 }  // namespace fast

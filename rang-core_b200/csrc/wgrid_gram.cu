@@ -559,15 +559,15 @@ struct RangGram {
 
 namespace wg {
 // Status mapping and the per-thread message, shared with the gridder's ABI.
-int32_t gram_guarded(const std::function<void()>& f);
-cudaStream_t gram_stream(void* stream);
+int32_t status_guarded(const std::function<void()>& f);
+cudaStream_t stream_of(void* stream);
 }  // namespace wg
 
 extern "C" {
 
 int32_t rang_b200_gram_expansion(size_t stencil, double theta, double ridge, double* table, double* sup_error,
                                  double* lebesgue) {
-  return gram_guarded([&] {
+  return status_guarded([&] {
     WExpansionHost ex(stencil, theta, ridge);
     if (table) std::memcpy(table, ex.table.data(), ex.table.size() * sizeof(double));
     if (sup_error) *sup_error = ex.sup_error;
@@ -581,8 +581,8 @@ int32_t rang_b200_gram_create(const WgridderOptions* opts, size_t nrow, size_t n
                               RangGram** out, double* stats) {
   if (!opts || !out) return 1;
   *out = nullptr;
-  return gram_guarded([&] {
-    cudaStream_t s = gram_stream(stream);
+  return status_guarded([&] {
+    cudaStream_t s = stream_of(stream);
     std::unique_ptr<WExpansionHost> ex;
     if (!no_w) ex = std::make_unique<WExpansionHost>(stencil, theta, ridge);
     auto g = std::make_unique<RangGram>();
@@ -597,24 +597,24 @@ int32_t rang_b200_gram_create(const WgridderOptions* opts, size_t nrow, size_t n
 
 int32_t rang_b200_gram_apply(RangGram* op, const double* m_dev, double* out_dev, void* stream) {
   if (!op || !m_dev || !out_dev) return 1;
-  return gram_guarded([&] { op->op->apply(m_dev, out_dev, gram_stream(stream)); });
+  return status_guarded([&] { op->op->apply(m_dev, out_dev, stream_of(stream)); });
 }
 
 int32_t rang_b200_gram_inverse_filter(const RangGram* op, double rho, void* stream, RangGram** out) {
   if (!op || !out) return 1;
   *out = nullptr;
-  return gram_guarded([&] {
+  return status_guarded([&] {
     auto g = std::make_unique<RangGram>();
-    g->op = op->op->inverse_filter(rho, gram_stream(stream));
+    g->op = op->op->inverse_filter(rho, stream_of(stream));
     *out = g.release();
   });
 }
 
 int32_t rang_b200_gram_psf_no_w(const RangGram* op, double* out_dev, void* stream) {
   if (!op || !out_dev) return 1;
-  return gram_guarded([&] {
+  return status_guarded([&] {
     const size_t big = 2 * (size_t)op->op->n;
-    cudaStream_t s = gram_stream(stream);
+    cudaStream_t s = stream_of(stream);
     if (!op->op->psf_no_w()) throw InvalidArgument("no PSF kept by this operator");
     check_cuda(cudaMemcpyAsync(out_dev, op->op->psf_no_w(), big * big * sizeof(double), cudaMemcpyDeviceToDevice, s),
                "copy");

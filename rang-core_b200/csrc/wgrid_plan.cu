@@ -1753,7 +1753,7 @@ void launch_grid_i8(cudaStream_t s, const Geom<float>& g, const Inputs& in, int 
 template <int S>
 void launch_degrid_h(cudaStream_t s, const Geom<float>& g, const Inputs& wts, const fast::VisRecord* rec,
                      const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
-                     const cplx<float>* grids, int pg0, int npg, cplx<float>* vis, int first, int last) {
+                     const cplx<float>* grids, int pg0, int npg, const fast::DegridOut& out, int first, int last) {
   if (kend <= kbase) return;
   const int smem = (int)(fast::H16Slots::bytes() + fast::H16_BATCH * sizeof(fast::Prefetched));
   const unsigned nblocks = (unsigned)((kend - kbase + fast::H16_CHUNK - 1) / fast::H16_CHUNK);
@@ -1761,7 +1761,7 @@ void launch_degrid_h(cudaStream_t s, const Geom<float>& g, const Inputs& wts, co
   {
     StageTimer timer_(ST_DEGRID, s);
     fast::k_degrid_h<S><<<nblocks, fast::H16_BATCH, smem, s>>>(g, wts, rec, sorted, kbase, kend, nbins, grids, pg0,
-                                                               npg, vis, first, last);
+                                                               npg, out, first, last);
   }
   check_cuda(cudaGetLastError(), "degrid kernel (tensor cores)");
 }
@@ -1931,7 +1931,7 @@ int max_window_planes(int L, size_t cell_bytes) {
 
 template <class T>
 Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw_dev, const double* freq_host,
-              const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks)
+              const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks, bool layout)
     : o_(o), nrow_(nrow), nchan_(nchan), n_(nrow * nchan) {
   rows_per_chunk_ = chunk_rows(nrow, row_chunks);
   nchunk_ = (int)((std::max<size_t>(nrow, 1) + rows_per_chunk_ - 1) / rows_per_chunk_);
@@ -1985,7 +1985,7 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   double umax_d = 0.0;  // metres; times the largest f / c
   std::memcpy(&umax_d, &r.u_bits, sizeof(double));
   urows_ = touched_rows(umax_d * *std::max_element(foc.begin(), foc.end()), wmax_d);
-  build_layout(act, with_vis, s);
+  if (layout) build_layout(act, with_vis, s);
 }
 
 // The grid rows footprints can reach, from the scan's largest |u| and |w|
@@ -2197,20 +2197,44 @@ void zero_touched(void* grids, size_t cell_bytes, int n, int nu, int nv, int row
   }
 }
 
+// A gridding pass's work space: per plane of a group its fixed-point grid and
+// its image columns (transposed), and whatever the group the floating-point
+// plane being transformed and the image accumulator.
+template <class T>
+void Plan<T>::grid_sizes(size_t& plane_bytes, size_t& fixed, size_t& group) const {
+  using FixCell = typename fast::FixTraits<T>::Cell;
+  const size_t npix = (size_t)o_.nx * o_.ny;
+  const size_t plane = (size_t)g_.nu * g_.nv;
+  const size_t tplane = (size_t)g_.ny * g_.nu;
+  plane_bytes = plane * sizeof(FixCell) + tplane * sizeof(cplx<T>);
+  fixed = plane * sizeof(cplx<T>) + npix * sizeof(T);
+  group = plane_group(plane_bytes, fixed);
+}
+
+template <class T>
+size_t Plan<T>::footprint(int nout) const {
+  if (nvis_ == 0) return 0;
+  size_t plane_bytes, fixed, group;
+  grid_sizes(plane_bytes, fixed, group);
+  return (size_t)std::max(nout, 1) * (group * plane_bytes + fixed);
+}
+
 template <class T>
 void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready,
-                   bool scanned) {
+                   bool scanned, const void* bound) {
   size_t npix = (size_t)o_.nx * o_.ny;
   if (nvis_ == 0) {
     check_cuda(cudaMemsetAsync(image, 0, npix * sizeof(T), s), "memset");
     return;
   }
+  if (!sorted_.get()) throw InvalidArgument("this plan was made without the visibility layout");
   using FixCell = typename fast::FixTraits<T>::Cell;
   const size_t cell = sizeof(cplx<T>);
   const size_t nplanes = (size_t)std::max(g_.nplanes, 1);
   const size_t plane = (size_t)g_.nu * g_.nv;
   const size_t tplane = (size_t)g_.ny * g_.nu;  // a plane's image columns, transposed
-  const size_t group = plane_group(plane * sizeof(FixCell) + tplane * cell, plane * cell + npix * sizeof(T));
+  size_t plane_bytes, fixed, group;
+  grid_sizes(plane_bytes, fixed, group);
   DevBuf grids(group * plane * sizeof(FixCell), s);
   DevBuf fpl(plane * cell, s);  // the plane being transformed, in floating point
   DevBuf cols(group * tplane * cell, s);
@@ -2228,7 +2252,11 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
     for (int c = 0; c < nchunk_; c++) check_cuda(cudaStreamWaitEvent(s, ready[c], 0), "wait");
   const fast::ValueBound* values = bound_.as<fast::ValueBound>();
   DevBuf vb;
-  if (!(scanned && bound_of(data, mode))) {
+  if (data.vis_kind == VIS_SORTED && !(integer && bound))
+    throw DeviceError("stored values need the integer gridder and their bound");
+  if (bound) {
+    values = static_cast<const fast::ValueBound*>(bound);
+  } else if (!(scanned && bound_of(data, mode))) {
     vb.alloc(sizeof(fast::ValueBound), s);
     check_cuda(cudaMemsetAsync(vb.get(), 0, sizeof(fast::ValueBound), s), "memset");
     {
@@ -2315,7 +2343,14 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
 
 template <class T>
 void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, cudaEvent_t* done) {
-  check_cuda(cudaMemsetAsync(vis, 0, n_ * 2 * sizeof(T), s), "memset");
+  degrid_to(image, wts, vis, nullptr, s, done);
+}
+
+template <class T>
+void Plan<T>::degrid_to(const T* image, const Inputs& wts, T* vis, const void* fused, cudaStream_t s,
+                        cudaEvent_t* done) {
+  if (vis) check_cuda(cudaMemsetAsync(vis, 0, n_ * 2 * sizeof(T), s), "memset");
+  if (nvis_ > 0 && !sorted_.get()) throw InvalidArgument("this plan was made without the visibility layout");
   if (nvis_ == 0) {
     if (done)
       for (int c = 0; c < nchunk_; c++) check_cuda(cudaEventRecord(done[c], s), "record");
@@ -2373,15 +2408,25 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
     bool first = pg0 == 0, last = pg0 + n >= nplanes;
     auto run = [&](auto S) {
       constexpr int SV = decltype(S)::value;
+      uint32_t block0 = 0;  // the stored modes' partial sums: blocks of the earlier chunks
       for (int c = 0; c < nchunk_; c++) {  // row chunk c, final after the last plane group
         bool fast_path = false;
         if constexpr (sizeof(T) == 4 && SV <= 8) {
+          fast::DegridOut out;
+          if (fused) {
+            out = *static_cast<const fast::DegridOut*>(fused);
+            out.block0 = block0;
+            block0 += (uint32_t)((chunk_sorted_[c + 1] - chunk_sorted_[c] + fast::H16_CHUNK - 1) / fast::H16_CHUNK);
+          } else {
+            out.vis = reinterpret_cast<cplx<float>*>(vis);
+          }
           launch_degrid_h<SV>(s, g_, wts, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(), chunk_sorted_[c],
                               chunk_sorted_[c + 1], (uint32_t)nbins_,
-                              reinterpret_cast<const cplx<float>*>(grids.as<cplx<T>>()), (int)pg0, n,
-                              reinterpret_cast<cplx<float>*>(vis), first, last);
+                              reinterpret_cast<const cplx<float>*>(grids.as<cplx<T>>()), (int)pg0, n, out, first,
+                              last);
           fast_path = true;
         }
+        if (!fast_path && fused) throw DeviceError("stored values need the tensor-core degridder");
         if (!fast_path)
           launch_degrid<T, SV>(smem, chunk_tasks_[c + 1] - chunk_tasks_[c], s, g_, wts, uvw_.as<double>(),
                                foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>() + chunk_tasks_[c],
@@ -2395,6 +2440,192 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
     else
       with_supp_double(g_.supp, run);
   }
+}
+
+namespace {
+
+// The residual or Gram values of the paths without the tensor-core kernels
+// (double precision, other single-precision methods), by visibility index:
+// work[idx] holds the unweighted prediction (has_model) and becomes
+// w (d - prediction), w d or, for the Gram operator, w prediction; the
+// weighted squares w |value / w|^2 are summed per block as k_store_values
+// sums them (fixed order).
+template <class T>
+__global__ void __launch_bounds__(fast::STORE_THREADS)
+    k_values_dense(uint64_t n, const uint32_t* __restrict__ sorted, Inputs data, int sorted_data, int has_model,
+                   int gram, cplx<T>* __restrict__ work, double* __restrict__ partials) {
+  __shared__ double sh[fast::STORE_THREADS];
+  const uint64_t k0 = (uint64_t)blockIdx.x * fast::STORE_CHUNK, k1 = min(n, k0 + fast::STORE_CHUNK);
+  double part = 0.0;
+  for (uint64_t k = k0 + threadIdx.x; k < k1; k += fast::STORE_THREADS) {
+    const uint64_t idx = sorted[k], di = sorted_data ? k : idx;
+    const T w = wgt_get<T>(data, di);
+    cplx<T> v = has_model ? work[idx] : cplx<T>{(T)0, (T)0};
+    if (!gram) {
+      const cplx<T> d = vis_get<T>(data, di);
+      v = {d.re - v.re, d.im - v.im};
+    }
+    part += (double)w * ((double)v.re * (double)v.re + (double)v.im * (double)v.im);
+    work[idx] = {v.re * w, v.im * w};
+  }
+  const double sum = fast::block_sum(part, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = sum;
+}
+
+// out[k] = dense[sorted[k]] for elements of B bytes.
+template <class E>
+__global__ void k_gather_sorted(uint64_t n, const uint32_t* __restrict__ sorted, const E* __restrict__ dense,
+                                E* __restrict__ out) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+    out[k] = dense[sorted[k]];
+}
+
+}  // namespace
+
+template <class T>
+bool Plan<T>::fused_values() const {
+  return sizeof(T) == 4 && g_.supp <= 8 && grid_method() == GRID_INT8;
+}
+
+template <class T>
+void Plan<T>::values_pass(bool gram, const Inputs& data, bool sorted_data, const T* model, T* image, double* sum,
+                          cudaStream_t s) {
+  const size_t npix = (size_t)o_.nx * o_.ny;
+  if (nvis_ == 0) {
+    check_cuda(cudaMemsetAsync(image, 0, npix * sizeof(T), s), "memset");
+    if (sum) check_cuda(cudaMemsetAsync(sum, 0, sizeof(double), s), "memset");
+    return;
+  }
+  if (!sorted_.get()) throw InvalidArgument("this plan was made without the visibility layout");
+  const uint64_t nblk = (nvis_ + fast::STORE_CHUNK - 1) / fast::STORE_CHUNK;
+  // Partial sums: one per block of the degridder (its chunks rounded up
+  // separately) or of the value kernels.
+  const size_t nparts_max = nblk + (size_t)nchunk_ + 1;
+  if (partials_.size() < nparts_max * sizeof(double)) partials_.alloc(nparts_max * sizeof(double), s);
+  if (!res_bound_.get()) res_bound_.alloc(sizeof(fast::ValueBound), s);
+  double* partials = partials_.as<double>();
+  uint32_t nparts = (uint32_t)nblk;
+  const Inputs none{};
+  if (fused_values()) {
+    if (!stored_.get()) stored_.alloc(nvis_ * sizeof(cplx<float>), s);
+    check_cuda(cudaMemsetAsync(res_bound_.get(), 0, sizeof(fast::ValueBound), s), "memset");
+    cplx<float>* stored = stored_.as<cplx<float>>();
+    if (model) {
+      fast::DegridOut out;
+      out.mode = gram ? fast::DEGRID_GRAM : fast::DEGRID_RESIDUAL;
+      out.stored = stored;
+      out.data = data;
+      out.sorted_data = sorted_data ? 1 : 0;
+      out.partials = partials;
+      out.bound = res_bound_.as<fast::ValueBound>();
+      degrid_to(model, none, nullptr, &out, s, nullptr);
+      nparts = 0;
+      for (int c = 0; c < nchunk_; c++)
+        nparts += (uint32_t)((chunk_sorted_[c + 1] - chunk_sorted_[c] + fast::H16_CHUNK - 1) / fast::H16_CHUNK);
+    } else {
+      {
+        StageTimer timer_(ST_OTHER, s);
+        fast::k_store_values<<<(unsigned)nblk, fast::STORE_THREADS, 0, s>>>(
+            nvis_, sorted_.as<uint32_t>(), data, sorted_data ? 1 : 0, stored, partials,
+            res_bound_.as<fast::ValueBound>());
+      }
+      check_cuda(cudaGetLastError(), "stored values");
+    }
+    const Inputs vals{stored, VIS_SORTED, nullptr, nullptr, WGT_NONE, nullptr};
+    grid(vals, VALUE_DATA, image, s, nullptr, false, res_bound_.get());
+  } else {
+    if (!work_.get()) work_.alloc(n_ * sizeof(cplx<T>), s);
+    cplx<T>* work = work_.as<cplx<T>>();
+    if (model) degrid_to(model, none, reinterpret_cast<T*>(work), nullptr, s, nullptr);
+    {
+      StageTimer timer_(ST_OTHER, s);
+      k_values_dense<T><<<(unsigned)nblk, fast::STORE_THREADS, 0, s>>>(
+          nvis_, sorted_.as<uint32_t>(), data, sorted_data ? 1 : 0, model ? 1 : 0, gram ? 1 : 0, work, partials);
+    }
+    check_cuda(cudaGetLastError(), "residual values");
+    const Inputs vals{work, sizeof(T) == 4 ? VIS_C64 : VIS_C128, nullptr, nullptr, WGT_NONE, nullptr};
+    grid(vals, VALUE_DATA, image, s, nullptr, false);
+  }
+  if (sum) {
+    {
+      StageTimer timer_(ST_OTHER, s);
+      fast::k_sum_partials<<<1, fast::STORE_THREADS, 0, s>>>(partials, nparts, sum);
+    }
+    check_cuda(cudaGetLastError(), "misfit sum");
+  }
+}
+
+template <class T>
+void Plan<T>::residual(const Inputs& data, bool sorted_data, const T* model, T* image, double* misfit,
+                       cudaStream_t s) {
+  values_pass(false, data, sorted_data, model, image, misfit, s);
+}
+
+template <class T>
+void Plan<T>::gram(const T* x, const Inputs& wts, bool sorted_wts, T* image, double* xgx, cudaStream_t s) {
+  Inputs w = wts;
+  w.vis = nullptr;
+  w.vis_kind = VIS_UNIT;
+  values_pass(true, w, sorted_wts, x, image, xgx, s);
+}
+
+template <class T>
+void Plan<T>::gather_sorted(const void* dense, int elem_bytes, void* out, cudaStream_t s) const {
+  if (nvis_ == 0) return;
+  if (!sorted_.get()) throw InvalidArgument("this plan was made without the visibility layout");
+  const uint32_t* srt = sorted_.as<uint32_t>();
+  const unsigned nb = blocks_for(nvis_, 256);
+  switch (elem_bytes) {
+    case 1:
+      k_gather_sorted<uint8_t><<<nb, 256, 0, s>>>(nvis_, srt, (const uint8_t*)dense, (uint8_t*)out);
+      break;
+    case 4:
+      k_gather_sorted<uint32_t><<<nb, 256, 0, s>>>(nvis_, srt, (const uint32_t*)dense, (uint32_t*)out);
+      break;
+    case 8:
+      k_gather_sorted<uint2><<<nb, 256, 0, s>>>(nvis_, srt, (const uint2*)dense, (uint2*)out);
+      break;
+    case 16:
+      k_gather_sorted<uint4><<<nb, 256, 0, s>>>(nvis_, srt, (const uint4*)dense, (uint4*)out);
+      break;
+    default:
+      throw InvalidArgument("element size must be 1, 4, 8 or 16 bytes");
+  }
+  check_cuda(cudaGetLastError(), "gather");
+}
+
+template <class T>
+std::vector<const char*> Plan<T>::memory_names() {
+  return {"gridder: coordinates (uvw per row, f/c per channel)",
+          "gridder: bin keys and offsets",
+          "gridder: sorted visibility index",
+          "gridder: visibility records",
+          "gridder: tasks",
+          "gridder: corrections",
+          "gridder: stored sorted values",
+          "gridder: scalars and partial sums"};
+}
+
+template <class T>
+std::vector<std::pair<const char*, size_t>> Plan<T>::memory() const {
+  const std::vector<const char*> n = memory_names();
+  const size_t b[] = {uvw_.size() + foc_.size(),
+                      key_.size() + starts_.size(),
+                      sorted_.size(),
+                      rec_.size(),
+                      tasks_.size() + ntasks_.size(),
+                      corr_.size(),
+                      stored_.size() + work_.size(),
+                      bound_.size() + scale_.size() + err_.size() + partials_.size() + res_bound_.size()};
+  std::vector<std::pair<const char*, size_t>> out;
+  for (size_t i = 0; i < n.size(); i++) out.emplace_back(n[i], b[i]);
+  return out;
+}
+
+template <class T>
+void Plan<T>::release_work() {
+  stored_.release();
+  work_.release();
 }
 
 template <class T>

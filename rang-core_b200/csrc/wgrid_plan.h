@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "wgrid_common.h"
@@ -68,8 +69,11 @@ class Plan {
   // the sorted order is chunk-major (each range's visibilities contiguous,
   // binned among themselves), so that gridding can start on the rows that
   // have arrived and degridding can hand out finished rows early.
+  // `layout` false stops after the kernel and grid choice (the reference's
+  // `plan` and `gridding_footprint`): such a plan reports `info` and
+  // `footprint` but cannot grid.
   Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw_dev, const double* freq_host,
-       const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks = 1);
+       const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks = 1, bool layout = true);
 
   bool empty() const { return nvis_ == 0; }
   const PlanInfo& info() const { return info_; }
@@ -83,13 +87,43 @@ class Plan {
   // `data` is the input this plan scanned (the same arrays, unchanged since),
   // whose value bound the scan already took; otherwise one pass over `data`
   // takes it.
+  // `bound`, when given, is the device value bound (fast::ValueBound) of
+  // `data`, formed by the caller's kernels.
   void grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s, const cudaEvent_t* ready = nullptr,
-            bool scanned = false);
+            bool scanned = false, const void* bound = nullptr);
   // dirty2vis of `image` into `vis` (nrow * nchan interleaved complex,
   // device, overwritten; inactive visibilities zero), times the weights of
   // `wts`. With `done` (one event per row chunk), done[c] is recorded once
   // the rows of chunk c are final.
   void degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, cudaEvent_t* done = nullptr);
+
+  // The residual image of `data` against the image `model` (null: the data
+  // alone), gridded with the weights of `data`, and the weighted misfit
+  // sum w |d - A model|^2 into `misfit` (one device double; null: not
+  // formed): the reference's Prepared::residual and residual_sorted
+  // (wgridder.rs:3232-3395). The prediction is degridded without weights.
+  // With `sorted_data`, the data and weights hold the active visibilities in
+  // the plan's sorted order (`gather_sorted`) instead of nrow * nchan.
+  // Asynchronous on `s`: nothing waits for the device.
+  void residual(const Inputs& data, bool sorted_data, const T* model, T* image, double* misfit, cudaStream_t s);
+  // A^H W A x into `image`, with W the weights of `wts` (sorted as for
+  // `residual`), and x^T A^H W A x = sum w |A x|^2 into `xgx` (null: not
+  // formed): the prediction, weighted, is gridded from the stored values.
+  void gram(const T* x, const Inputs& wts, bool sorted_wts, T* image, double* xgx, cudaStream_t s);
+  // `dense` (nrow * nchan elements of `elem_bytes`: 1, 4, 8 or 16) at the
+  // active visibilities in the sorted order (the reference's Prepared::sorted).
+  void gather_sorted(const void* dense, int elem_bytes, void* out, cudaStream_t s) const;
+  // Device bytes held, by buffer (the reference's Prepared::memory), in the
+  // order of memory_names().
+  std::vector<std::pair<const char*, size_t>> memory() const;
+  static std::vector<const char*> memory_names();
+  // Frees the values the residual and Gram passes keep between calls; the
+  // next pass allocates them again.
+  void release_work();
+  // Device bytes of a gridding pass's work space for `nout` images (the
+  // reference's gridding_footprint): the fixed-point and transform planes of
+  // one plane group, and the image accumulator.
+  size_t footprint(int nout) const;
 
   // Rows per chunk when `nrow` rows are asked to be split `row_chunks` ways.
   static size_t chunk_rows(size_t nrow, int row_chunks) {
@@ -114,6 +148,17 @@ class Plan {
 
  private:
   void build_layout(const Inputs& act, bool with_vis, cudaStream_t s);
+  // Degridding into `vis` (by visibility index), or, with `fused` (a
+  // fast::DegridOut), into the stored values by sorted position.
+  void degrid_to(const T* image, const Inputs& wts, T* vis, const void* fused, cudaStream_t s, cudaEvent_t* done);
+  // The residual (gram false) or Gram (true) values, gridded into `image`.
+  void values_pass(bool gram, const Inputs& data, bool sorted_data, const T* model, T* image, double* sum,
+                   cudaStream_t s);
+  // The single-precision tensor-core kernels serve the pass (the degridder
+  // writes the stored values in sorted order, the integer gridder reads them).
+  bool fused_values() const;
+  // Bytes of one gridding plane group and of the fixed part, and the group.
+  void grid_sizes(size_t& plane_bytes, size_t& fixed, size_t& group) const;
   void corrections(cudaStream_t s);
   int touched_rows(double umax, double wmax) const;
   size_t plane_group(size_t plane_bytes, size_t fixed) const;
@@ -136,6 +181,10 @@ class Plan {
   DevBuf ntasks_;   // u32: tasks in use
   DevBuf corr_;     // double per pixel: the global correction
   DevBuf err_;      // int: kernel-detected inconsistencies
+  DevBuf stored_;   // residual / Gram values by sorted position (single precision, tensor-core path)
+  DevBuf work_;     // residual / Gram values by visibility index (the other paths)
+  DevBuf partials_; // FP64 per-block partial sums of the misfit
+  DevBuf res_bound_;  // the largest |value| of a residual or Gram pass
   size_t nbins_ = 0, ntiles_ = 0, max_tasks_ = 0;
   int nchunk_ = 1;
   size_t rows_per_chunk_ = 0;

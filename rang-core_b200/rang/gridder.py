@@ -223,3 +223,39 @@ def kernel_table():
         table.append(row)
         row = kernel_row(len(table))
     return table
+
+
+def plan(*, uvw, freq, npix_x, npix_y, pixsize_x, pixsize_y, epsilon, vis=None, wgt=None, wgt2=None, mask=None,
+         single=False, **kw):
+    """The kernel and grid a call would choose, without binning or gridding
+    (the reference's `plan`, core/src/wgridder.rs:3527-3551): the plan
+    report of `vis2dirty` on these arrays (the activity |vis|^2 wgt mask != 0
+    with `vis`, else wgt mask != 0)."""
+    info, _ = _plan_only(uvw, freq, npix_x, npix_y, pixsize_x, pixsize_y, epsilon, vis, wgt, wgt2, mask, single, 1,
+                         kw)
+    return info
+
+
+def gridding_footprint(*, uvw, freq, wgt, npix_x, npix_y, pixsize_x, pixsize_y, epsilon, nout=1, single=False,
+                       **kw):
+    """The plan a gridding pass would choose on the weights `wgt` (a
+    visibility is active where its weight is non-zero) and the device bytes
+    of its work space for `nout` images, without gridding (the reference's
+    `gridding_footprint`, core/src/wgridder.rs:3553-3588). Returns
+    (plan report, bytes)."""
+    return _plan_only(uvw, freq, npix_x, npix_y, pixsize_x, pixsize_y, epsilon, None, wgt, None, None, single, nout,
+                      kw)
+
+
+def _plan_only(uvw, freq, npix_x, npix_y, pixsize_x, pixsize_y, epsilon, vis, wgt, wgt2, mask, single, nout, kw):
+    call = _Call(uvw, freq)
+    v = call.vis(vis)
+    if wgt2 is not None:
+        w, w2 = (call._sized(np.ascontiguousarray(a, dtype=np.float32), n) for a, n in ((wgt, "wgt"), (wgt2, "wgt2")))
+    else:
+        w, w2 = call.weights(wgt)
+    opts = Options.make(npix_x, npix_y, pixsize_x, pixsize_y, epsilon, kw)
+    st, info, footprint = extension().wgridder_plan_only(opts.packed(), call.uvw, call.freq, v, w, w2, call.mask(mask),
+                                                         int(bool(single)), int(nout))
+    _raise_on(st)
+    return info_dict(info), int(footprint)

@@ -442,14 +442,8 @@ def make_training_set(device, n_patches=20000, n_coverages=8, nant=(32, 64), npi
             vis += sigma * math.sqrt(2.0) * torch.randn(vis.shape, dtype=vis.dtype, device=dev, generator=g)
             dirty, q = plan.residual(vis, None)
             del vis
-            snaps = {}
-
-            def keep(it, x, gx, misfit):
-                if it in snapshots:
-                    snaps[it] = (x.clone(), gx.clone())
-
-            fista.solve(plan.gram, dirty, 1e-4 * float(dirty.max()), 1.0 / lmax, max(snapshots), q0=0.5 * q,
-                        observer=keep)
+            snaps = fista.solve(plan.gram, dirty, 1e-4 * float(dirty.max()), 1.0 / lmax, max(snapshots),
+                                q0=0.5 * q, keep=snapshots).snapshots
             for it in snapshots:
                 x, gx = snaps[it]
                 r = _patches((dirty - gx) / peak)
@@ -534,16 +528,26 @@ class Proposer:
 
 
 def _blur(img, sigma):
-    """A periodic Gaussian blur of standard deviation `sigma` pixels (FFT)."""
-    n0, n1 = img.shape
-    f0 = torch.fft.fftfreq(n0, device=img.device, dtype=torch.float64)
-    f1 = torch.fft.rfftfreq(n1, device=img.device, dtype=torch.float64)
-    k = torch.exp(-2.0 * math.pi**2 * sigma**2 * (f0[:, None] ** 2 + f1[None, :] ** 2)).to(torch.float32)
-    return torch.fft.irfft2(torch.fft.rfft2(img) * k, s=(n0, n1))
+    """The periodic Gaussian blur of standard deviation `sigma` pixels (the
+    library's cuFFT low-pass)."""
+    return fista.gaussian_lowpass(img.float(), sigma)
+
+
+class LearnedSolve:
+    """The outcome of `solve`: the iterate `x` and `gx` = G x, the applies of
+    G made, the proposal statistics, the misfit after each apply (`misfits`,
+    a float64 CUDA tensor, NaN where an apply was a proposal's) and, with
+    `events`, a CUDA event recorded after each apply's iteration."""
+
+    def __init__(self, x, gx, applies, stats, misfits, events):
+        self.x, self.gx, self.applies, self.stats, self.misfits, self.events = x, gx, applies, stats, misfits, events
+
+    def __iter__(self):  # (x, G x, applies, statistics), as the earlier tuple
+        return iter((self.x, self.gx, self.applies, self.stats))
 
 
 def solve(gram, dirty, lam, step, proposer, psf, peak, max_iterations, q0=0.0, cycle=40, bands=2, sigma=4.0,
-          first=0, stop=None, observer=None):
+          first=0, stop=None, observer=None, events=False, check_every=20):
     """Learned-preconditioned FISTA on the misfit Q(x) = Q(0) - <dirty, x> +
     <x, G x> / 2 with the L1 prior and positivity (the FISTA of `rang.fista`,
     with gradient restart), where at iteration `first` and every `cycle`
@@ -555,32 +559,51 @@ def solve(gram, dirty, lam, step, proposer, psf, peak, max_iterations, q0=0.0, c
     minimiser of Q over the pair (two applies). The step is kept only when
     Q decreases, and then shifts the iterate, the previous iterate and the
     extrapolated point alike, so that FISTA's momentum carries on.
-    `stop(k, misfit)` and `observer(k, x, gx, misfit)` see every iterate, k
-    counting applies of G. Returns (x, G x, applies, proposal statistics)."""
-    dd = dirty.double().ravel()
 
-    def misfit_of(x, gx):
-        xd = x.double().ravel()
-        return q0 - float(torch.dot(dd, xd)) + 0.5 * float(torch.dot(xd, gx.double().ravel()))
-
-    def dot(a, b):
-        return float(torch.dot(a.double().ravel(), b.double().ravel()))
-
+    The plain iterations run on the library's step kernels with their
+    scalars on the device; a proposal reads its inner products back (one
+    wait per proposal). `stop(k, misfit)` is tested on the recorded misfits
+    every `check_every` applies (k counts applies of G) and `observer(k, x,
+    gx, misfit)` sees every iterate (a wait each). Returns a `LearnedSolve`
+    (which unpacks as (x, G x, applies, proposal statistics))."""
+    lib = fista._library()
+    dev = dirty.device
+    single = fista._single(dirty)
+    n = dirty.numel()
+    s = fista._stream(dev)
+    ws = fista.Workspace(dev)
     x = torch.zeros_like(dirty)
-    x_prev = x.clone()
     y = x.clone()
     g_x_prev = torch.zeros_like(dirty)
-    t, beta = 1.0, 0.0
+    g_x = torch.empty_like(dirty)
+    x_next = torch.empty_like(dirty)
+    y_next = torch.empty_like(dirty)
+    state = torch.empty(fista._STATE, dtype=torch.float64, device=dev)
+    q0_dev = q0.to(dev, torch.float64).reshape(()) if torch.is_tensor(q0) else None
+    fista._check(lib.rang_b200_fista_init(state.data_ptr(), None if q0_dev is None else q0_dev.data_ptr(),
+                                          0.0 if q0_dev is not None else float(q0), float(step), float(lam), 0, 0.0,
+                                          s), "fista init")
+    q0v = q0_dev if q0_dev is not None else torch.tensor(float(q0), dtype=torch.float64, device=dev)
+    misfits = torch.full((max_iterations + 1,), float("nan"), dtype=torch.float64, device=dev)
+    iters = torch.full((max_iterations + 1,), float("nan"), dtype=torch.float64, device=dev)
+    evs = []
     applies = 0
     stats = {"proposals": 0, "accepted": 0, "steps": [], "misfit_drops": []}
     k = 0
+    checked = 0
+
+    def host_dot(a, b):
+        return float(fista.dot(a, b, ws=ws))
+
     while True:
         g_y = gram(y)
         applies += 1
-        g_x = g_y if beta == 0.0 else (g_y + beta * g_x_prev) / (1.0 + beta)
-        misfit = misfit_of(x, g_x)
         if k >= first and (k - first) % cycle == 0 and applies + bands <= max_iterations:
-            r = dirty - g_x
+            # G x and the misfit of the current iterate (beta from the device state).
+            beta = state[1].to(dirty.dtype)
+            gx_now = torch.where(beta == 0, g_y, (g_y + beta * g_x_prev) / (1.0 + beta))
+            misfit = float(fista.misfit_of(dirty, x, gx_now, q0v, ws))
+            r = dirty - gx_now
             d = torch.clamp(x + proposer(r, psf, 1.0 / peak), min=0.0) - x
             parts = [d] if bands == 1 else [_blur(d, sigma), None]
             if bands != 1:
@@ -588,8 +611,8 @@ def solve(gram, dirty, lam, step, proposer, psf, peak, max_iterations, q0=0.0, c
             gparts = [gram(p) for p in parts]
             applies += len(parts)
             stats["proposals"] += 1
-            b = np.array([dot(p, r) for p in parts])
-            m = np.array([[dot(p, q) for q in gparts] for p in parts])
+            b = np.array([host_dot(p, r) for p in parts])
+            m = np.array([[host_dot(p, q) for q in gparts] for p in parts])
             try:
                 coef = np.linalg.solve(m, b)
             except np.linalg.LinAlgError:
@@ -598,31 +621,36 @@ def solve(gram, dirty, lam, step, proposer, psf, peak, max_iterations, q0=0.0, c
             if np.all(np.isfinite(coef)) and drop > 0.0:
                 shift = sum(c * p for c, p in zip(coef, parts))
                 gshift = sum(c * g for c, g in zip(coef, gparts))
-                x_try, g_try = x + shift, g_x + gshift
-                m_try = misfit_of(x_try, g_try)
+                x_try, g_try = x + shift, gx_now + gshift
+                m_try = float(fista.misfit_of(dirty, x_try, g_try, q0v, ws))
                 if m_try < misfit:
                     stats["accepted"] += 1
                     stats["steps"].append([round(float(c), 4) for c in coef])
                     stats["misfit_drops"].append(misfit - m_try)
-                    x, g_x, misfit = x_try, g_try, m_try
-                    x_prev, g_x_prev = x_prev + shift, g_x_prev + gshift
+                    # The iterate, the previous iterate's G and the extrapolated
+                    # point move alike; the step kernel forms G x from them.
+                    x = x_try
+                    g_x_prev = g_x_prev + gshift
                     y, g_y = y + shift, g_y + gshift
+        fista._check(lib.rang_b200_fista_step(single, n, dirty.data_ptr(), x.data_ptr(), y.data_ptr(), g_y.data_ptr(),
+                                              g_x_prev.data_ptr(), g_x.data_ptr(), x_next.data_ptr(),
+                                              y_next.data_ptr(), state.data_ptr(), iters.data_ptr(), k, 0, 1, 1,
+                                              ws.partials.data_ptr(), s), "fista step")
+        misfits[applies:applies + 1].copy_(iters[k:k + 1])
+        if events:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record()
+            evs.append((applies, e))
         if observer is not None:
-            observer(applies, x, g_x, misfit)
-        if applies >= max_iterations or (stop is not None and stop(applies, misfit)):
-            return x, g_x, applies, stats
-        z = y + step * (dirty - g_y)
-        x_next = fista.soft_threshold(z, step * lam, False)
-        next_beta = 0.0
-        inner = float(torch.sum((y - x_next) * (x_next - x)))
-        if inner > 0.0:
-            t = 1.0
-        else:
-            t_next = 0.5 * (1.0 + math.sqrt(1.0 + 4.0 * t * t))
-            next_beta = (t - 1.0) / t_next
-            t = t_next
-        g_x_prev = g_x
-        x_prev, x = x, x_next
-        y = x + next_beta * (x - x_prev)
-        beta = next_beta
+            observer(applies, x, g_x, float(misfits[applies]))
+        done = applies >= max_iterations
+        if not done and stop is not None and applies - checked >= check_every:
+            vals = misfits[checked + 1:applies + 1].tolist()
+            done = any(stop(checked + 1 + j, v) for j, v in enumerate(vals) if v == v)
+            checked = applies
+        if done:
+            return LearnedSolve(x, g_x, applies, stats, misfits[:applies + 1], evs)
+        x, x_next = x_next, x
+        g_x_prev, g_x = g_x, g_x_prev
+        y, y_next = y_next, y
         k += 1

@@ -121,27 +121,71 @@ class DevicePlan:
                                                      _stream(self.device)))
         return out
 
-    def residual(self, data, wgt, model=None, mask=None, out=None):
+    def residual(self, data, wgt=None, model=None, out=None, misfit=None, sorted=False):
         """The residual image of `data` against the image `model` (None: the
         data alone), gridded with weights `wgt`, and the misfit
         sum w |data - A model|^2 over the active visibilities (the
         reference's Prepared::residual, core/src/wgridder.rs:3232-3395: the
         prediction is degridded without weights, the residual gridded with
-        them). Returns (image, misfit as a Python float)."""
-        r = data if model is None else data - self.degrid(model)
-        w = torch.ones_like(r.real) if wgt is None else wgt.to(r.real.dtype)
-        act = w != 0
-        if mask is not None:
-            act = act & (mask != 0)
-        q = torch.sum(torch.where(act, w.double() * (r.real.double() ** 2 + r.imag.double() ** 2), 0.0))
-        r = r.to(self.cplx).contiguous()
-        return self.grid(r, wgt, out=out), float(q)
+        them). The values pass through the plan's stored work space in the
+        sorted order; no visibility-sized tensor is made and nothing waits for
+        the device. `sorted`: `data` and `wgt` hold the active visibilities in
+        the plan's sorted order (`sorted_values`, the reference's
+        residual_sorted). Returns (image, misfit as a 0-dimensional float64
+        CUDA tensor)."""
+        if out is None:
+            out = torch.empty(self.shape, dtype=self.real, device=self.device)
+        q = torch.empty((), dtype=torch.float64, device=self.device) if misfit is None else misfit
+        data = data.contiguous()
+        w, w2, wk = _wgt(None if wgt is None else wgt.contiguous())
+        m = None if model is None else model.to(self.real).contiguous()
+        _check(core.extension().wgridder_plan_residual(self._handle, data.data_ptr(), _VIS_KIND[data.dtype], _ptr(w),
+                                                       _ptr(w2), wk, _ptr(m), int(bool(sorted)), out.data_ptr(),
+                                                       q.data_ptr(), _stream(self.device)))
+        return out, q
 
-    def gram(self, x, wgt=None, out=None):
-        """A^H W A x: the image of the unweighted prediction of `x`, gridded
-        with the weights (the reference's gram_apply,
-        core/src/clean_certified.rs:233-236)."""
-        return self.grid(self.degrid(x).contiguous(), wgt, out=out)
+    def gram(self, x, wgt=None, out=None, xgx=None, sorted=False):
+        """A^H W A x: the image of the unweighted prediction of `x`, weighted
+        and gridded (the reference's gram_apply,
+        core/src/clean_certified.rs:233-236), through the plan's stored work
+        space; with `xgx` (a 0-dimensional float64 CUDA tensor) also
+        x^T A^H W A x = sum w |A x|^2."""
+        if out is None:
+            out = torch.empty(self.shape, dtype=self.real, device=self.device)
+        x = x.to(self.real).contiguous()
+        w, w2, wk = _wgt(None if wgt is None else wgt.contiguous())
+        _check(core.extension().wgridder_plan_gram(self._handle, x.data_ptr(), _ptr(w), _ptr(w2), wk,
+                                                   int(bool(sorted)), out.data_ptr(), _ptr(xgx),
+                                                   _stream(self.device)))
+        return out
+
+    @property
+    def active(self):
+        """The number of active visibilities (the sorted layout's length)."""
+        st, n = core.extension().wgridder_plan_active(self._handle)
+        _check(st)
+        return int(n)
+
+    def sorted_values(self, dense):
+        """`dense` ((nrow, nchan) CUDA tensor) at the active visibilities in
+        the plan's sorted order (the reference's Prepared::sorted)."""
+        dense = dense.contiguous()
+        if tuple(dense.shape[:2]) != (self.nrow, self.nchan):
+            raise ValueError(f"expected ({self.nrow}, {self.nchan}), got {tuple(dense.shape)}")
+        out = torch.empty((self.active,), dtype=dense.dtype, device=self.device)
+        _check(core.extension().wgridder_plan_sorted(self._handle, dense.data_ptr(), dense.element_size(),
+                                                     out.data_ptr(), _stream(self.device)))
+        return out
+
+    def memory(self):
+        """Device bytes held by the plan, per buffer (the reference's
+        Prepared::memory)."""
+        return dict(core.extension().wgridder_plan_memory(self._handle))
+
+    def release_work(self):
+        """Frees the stored values that residual and Gram passes keep (the
+        reference's Prepared::release_grids)."""
+        core.extension().wgridder_plan_release_work(self._handle)
 
     def status(self):
         """Waits for the stream; raises if a kernel flagged an inconsistency."""

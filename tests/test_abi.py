@@ -52,6 +52,46 @@ def test_library_exports_every_weights_symbol(built):
         assert hasattr(lib, name), name
 
 
+def test_library_exports_every_solver_symbol(built):
+    text = (REPO / "include" / "rang_solver.h").read_text()
+    names = sorted(set(re.findall(r"^\w+\s+(rang_b200_\w+)\s*\(", text, re.M)))
+    assert names == ["rang_b200_dot", "rang_b200_fista_init", "rang_b200_fista_partials", "rang_b200_fista_step",
+                     "rang_b200_gaussian_lowpass"]
+    lib = ctypes.CDLL(str(built.LIB))
+    for name in names:
+        assert hasattr(lib, name), name
+
+
+def test_solver_entry_points_refuse_null_arrays(built):
+    lib = ctypes.CDLL(str(built.LIB))
+    P = ctypes.c_void_p
+    lib.rang_b200_fista_step.argtypes = [ctypes.c_int32, ctypes.c_size_t] + [P] * 10 + [ctypes.c_int32] * 4 + [P, P]
+    assert lib.rang_b200_fista_step(1, 16, *([None] * 10), 0, 0, 1, 1, None, None) == 1
+    lib.rang_b200_gaussian_lowpass.argtypes = [ctypes.c_size_t, ctypes.c_size_t, P, P, ctypes.c_double, P]
+    assert lib.rang_b200_gaussian_lowpass(8, 8, None, None, 1.0, None) == 1
+    assert lib.rang_b200_fista_partials() > 0
+
+
+def test_plan_extension_entry_points_refuse_null_plans(built):
+    lib = ctypes.CDLL(str(built.LIB))
+    P = ctypes.c_void_p
+    lib.rang_b200_wgridder_plan_residual.argtypes = [P, P, ctypes.c_int32, P, P, ctypes.c_int32, P, ctypes.c_int32,
+                                                     P, P, P]
+    assert lib.rang_b200_wgridder_plan_residual(None, None, 1, None, None, 0, None, 0, None, None, None) == 1
+    lib.rang_b200_wgridder_plan_gram.argtypes = [P, P, P, P, ctypes.c_int32, ctypes.c_int32, P, P, P]
+    assert lib.rang_b200_wgridder_plan_gram(None, None, None, None, 0, 0, None, None, None) == 1
+    lib.rang_b200_wgridder_plan_memory.argtypes = [P, P, ctypes.c_int32]
+    assert lib.rang_b200_wgridder_plan_memory(None, None, 0) == -1
+    lib.rang_b200_wgridder_plan_memory_name.restype = ctypes.c_char_p
+    names = []
+    while True:
+        n = lib.rang_b200_wgridder_plan_memory_name(len(names))
+        if n is None:
+            break
+        names.append(n.decode())
+    assert len(names) == 8 and all(n.startswith("gridder: ") for n in names)
+
+
 def test_library_exports_every_gram_symbol(built):
     text = (REPO / "include" / "rang_gram.h").read_text()
     names = sorted(set(re.findall(r"^\w+\s+(rang_b200_gram_\w+)\s*\(", text, re.M)))

@@ -109,7 +109,7 @@ def test_residual_matches_the_composition_and_the_oracle(single):
     ref = oracle.vis2dirty(vis=r, wgt=ww, npix_x=kw["npix_x"], npix_y=kw["npix_y"], **okw)
     assert rel_linf(img.cpu().numpy(), ref) < (1e-4 if single else 1e-9)
     qref = float(np.sum(wgt * np.abs(r.astype(np.complex128)) ** 2))
-    assert abs(q - qref) / qref < (1e-5 if single else 1e-12)
+    assert abs(float(q) - qref) / qref < (1e-5 if single else 1e-12)
 
 
 def _numpy_fista(gram, dirty, lam, step, iters):
@@ -199,4 +199,5 @@ def test_fista_reaches_the_noise():
     x, gx, k, _ = fista.solve(lambda x: plan.gram(x, tw), dirty, 1e-4 * float(dirty.max()), 1.0 / lmax, 200,
                               q0=0.5 * q0, stop=lambda k, m: rms(m) <= 1.2 * sigma)
     _, q = plan.residual(tv, tw, x)
+    q = float(q)
     assert np.sqrt(q / (2 * nvis)) <= 1.25 * sigma, (k, np.sqrt(q / (2 * nvis)))

@@ -180,3 +180,41 @@ def test_binning_is_a_stable_sort_by_tile_and_plane():
     act = np.flatnonzero(b["tile"] >= 0)
     expect = act[np.lexsort((act, key[act]))]
     assert np.array_equal(b["sorted"], expect)
+
+
+_SIMD_PROBE = """
+import hashlib, sys
+import numpy as np
+sys.path[:0] = sys.argv[1:3]
+import oracle
+from cases import small_case
+uvw, freq, vis, wgt, nx, ny, dx = small_case(nx=64, ny=48, nrow=400, seed=9)
+out = [oracle.simd_level()]
+for single in (True, False):
+    v = vis.astype(np.complex64) if single else vis
+    kw = dict(uvw=uvw, freq=freq, pixsize_x=dx, pixsize_y=dx, epsilon=1e-5 if single else 1e-9)
+    d = oracle.vis2dirty(vis=v, wgt=wgt, npix_x=nx, npix_y=ny, **kw)
+    m = oracle.dirty2vis(dirty=d, **kw)
+    out += [hashlib.sha256(d.tobytes()).hexdigest(), hashlib.sha256(m.tobytes()).hexdigest()]
+print(" ".join(out))
+"""
+
+
+def test_instruction_sets_give_the_same_bits():
+    """The AVX-512 and AVX2 builds of the oracle return the same bits, as the
+    reference's instruction-set variants do (`core/src/wgridder.rs:1592-1597`)."""
+    import os
+    import subprocess
+    import sys
+
+    if oracle.simd_level() != "avx512":
+        pytest.skip("the host has no AVX-512")
+    here = Path(__file__).resolve().parent
+    runs = {}
+    for cap in ("avx512", "avx2"):
+        env = dict(os.environ, RANG_WGRIDDER_SIMD=cap)
+        out = subprocess.run([sys.executable, "-c", _SIMD_PROBE, str(here.parent / "oracle"), str(here)], env=env,
+                             capture_output=True, text=True, check=True).stdout.split()
+        runs[out[0]] = out[1:]
+    assert set(runs) == {"avx512", "avx2"}
+    assert runs["avx512"] == runs["avx2"]
