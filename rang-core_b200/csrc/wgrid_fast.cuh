@@ -334,7 +334,8 @@ __device__ __forceinline__ cplx<float> record_value(const VisRecord& r, const In
 
 // The window of a bin key: the grid row and column of its cell (0, 0) (the
 // sub-tile's first cell; windows are 8 x 8) and its first plane.
-__device__ __forceinline__ void window_of(const Geom<float>& g, uint32_t key, uint32_t nbins, int& su0, int& sv0,
+template <class T>
+__device__ __forceinline__ void window_of(const Geom<T>& g, uint32_t key, uint32_t nbins, int& su0, int& sv0,
                                           int& mp) {
   const uint32_t bin = key % nbins;
   const uint32_t sub = bin % (uint32_t)g.nsub, t = bin / (uint32_t)g.nsub;

@@ -24,6 +24,8 @@
 #include <cuda_fp16.h>
 #include <cufft.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cstdlib>
 #include <atomic>
@@ -301,6 +303,11 @@ __global__ void __launch_bounds__(256, 8) k_bin_count(const __grid_constant__ Ge
 // Each thread takes four indices a grid-stride apart per round, so that four
 // independent atomics (each returning its run's base) are in flight at once:
 // the kernel is bound by their latency. The order within a bin is free.
+__global__ void k_iota(uint64_t n, uint32_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)i;
+}
+
 __global__ void k_bin_scatter(uint64_t n, const uint32_t* __restrict__ key, uint32_t* __restrict__ cursor,
                               uint32_t* __restrict__ sorted) {
   constexpr int U = 4;
@@ -322,6 +329,7 @@ __global__ void k_bin_scatter(uint64_t n, const uint32_t* __restrict__ key, uint
 }
 
 #include "wgrid_fast.cuh"
+#include "wgrid_f64.cuh"
 
 // ------------------------------------------------------------------ exclusive scan (u32)
 
@@ -1751,6 +1759,21 @@ void launch_grid_i8(cudaStream_t s, const Geom<float>& g, const Inputs& in, int 
 }
 
 template <int S>
+void launch_grid_f64(cudaStream_t s, const Geom<double>& g, const Inputs& in, int mode, const double* uvw,
+                     const double* foc, const uint32_t* key, const uint32_t* sorted, uint64_t kbase, uint64_t kend,
+                     uint32_t nbins, fast::FixCell2* grids, int pg0, int npg, fast::FixScale* fs) {
+  if (kend <= kbase) return;
+  const int smem = (int)fast::F64Slots::bytes();
+  const unsigned nblocks = (unsigned)((kend - kbase + fast::F64_CHUNK - 1) / fast::F64_CHUNK);
+  {
+    StageTimer timer_(ST_GRID, s);
+    fast::k_grid_f64<S><<<nblocks, fast::F64_BATCH, smem, s>>>(g, in, mode, uvw, foc, key, sorted, kbase, kend, nbins,
+                                                               grids, pg0, npg, fs);
+  }
+  check_cuda(cudaGetLastError(), "grid kernel (FP64 tensor cores)");
+}
+
+template <int S>
 void launch_degrid_h(cudaStream_t s, const Geom<float>& g, const Inputs& wts, const fast::VisRecord* rec,
                      const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
                      const cplx<float>* grids, int pg0, int npg, const fast::DegridOut& out, int first, int last) {
@@ -2032,7 +2055,32 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
   }
   check_cuda(cudaGetLastError(), "bin count");
   exclusive_scan(starts_.as<uint32_t>(), starts_.as<uint32_t>(), nkeys + 1, s);
-  {
+  if constexpr (sizeof(T) == 8) {
+    // A stable radix sort of the visibility indices by bin key: inside a bin
+    // the visibilities keep their index order (the reference's layout
+    // order), so the double-precision gridder's sums, which follow this
+    // order, come out the same on every call. Inactive keys (all ones in
+    // the sorted bits: 2^bits - 1 exceeds every bin key) sort last.
+    int bits = 1;
+    while (bits < 32 && ((1ull << bits) - 1ull) < (unsigned long long)nkeys) bits++;
+    DevBuf iota(n_ * 4, s), keys_out(n_ * 4, s), vals_out(n_ * 4, s);
+    {
+      StageTimer timer_(ST_BIN_SCATTER, s);
+      k_iota<<<blocks_for(n_, 256), 256, 0, s>>>(n_, iota.as<uint32_t>());
+      size_t temp = 0;
+      check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, temp, key_.as<uint32_t>(), keys_out.as<uint32_t>(),
+                                                 iota.as<uint32_t>(), vals_out.as<uint32_t>(), (long long)n_, 0, bits,
+                                                 s),
+                 "radix sort");
+      DevBuf work(temp, s);
+      check_cuda(cub::DeviceRadixSort::SortPairs(work.get(), temp, key_.as<uint32_t>(), keys_out.as<uint32_t>(),
+                                                 iota.as<uint32_t>(), vals_out.as<uint32_t>(), (long long)n_, 0, bits,
+                                                 s),
+                 "radix sort");
+    }
+    sorted_.alloc(nvis_ * 4, s);
+    check_cuda(cudaMemcpyAsync(sorted_.get(), vals_out.get(), nvis_ * 4, cudaMemcpyDeviceToDevice, s), "copy");
+  } else {
     DevBuf cursor((nkeys + 1) * 4, s);
     check_cuda(cudaMemcpyAsync(cursor.get(), starts_.get(), (nkeys + 1) * 4, cudaMemcpyDeviceToDevice, s), "copy");
     sorted_.alloc(nvis_ * 4, s);
@@ -2300,6 +2348,11 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
                                  sorted_.as<uint32_t>(), k0, k1, fg, (int)pg0, n, fs);
             continue;
           }
+        } else if constexpr (SV <= 8) {
+          launch_grid_f64<SV>(s, g_, data, (int)mode, uvw_.as<double>(), foc_.as<double>(), key_.as<uint32_t>(),
+                              sorted_.as<uint32_t>(), chunk_sorted_[c], chunk_sorted_[c + 1], (uint32_t)nbins_, fg,
+                              (int)pg0, n, fs);
+          continue;
         }
         launch_grid<T, SV>(smem, chunk_tasks_[c + 1] - chunk_tasks_[c], s, g_, data, (int)mode, uvw_.as<double>(),
                            foc_.as<double>(), sorted_.as<uint32_t>(), tasks_.as<Task>() + chunk_tasks_[c],

@@ -335,7 +335,7 @@ void make_geom(const WgridderOptions& o, size_t nrow, size_t nchan, size_t nvis,
   // (sube + supp - 1 = 8), ceil(tile / sube) of them along each side of a
   // tile (the last one partial where sube does not divide the tile). Double
   // precision, which has no tensor-core path, keeps 8 x 8 sub-tiles.
-  g.sube = single ? 9 - (int32_t)std::min<size_t>(supp, 8) : 8;
+  g.sube = (single || supp <= 8) ? 9 - (int32_t)std::min<size_t>(supp, 8) : 8;
   g.nsub_side = (tile + g.sube - 1) / g.sube;
   g.nsub = g.nsub_side * g.nsub_side;
   g.do_wgridding = wgrid;

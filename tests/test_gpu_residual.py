@@ -33,7 +33,8 @@ def _problem(single, method=None, npix=128, seed=0, nant=32, ntime=6, nchan=12):
     plan = wgrid_torch.DevicePlan(torch.from_numpy(uvw).to(dev), freq, wgt=t_wgt, single=single, **kw)
     d = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
     model = np.zeros(plan.shape)
-    model[40, 70], model[90, 20], model[64, 64] = 2.0, -1.0, 0.5
+    n = npix
+    model[5 * n // 16, 9 * n // 16], model[11 * n // 16, n // 8], model[n // 2, n // 2] = 2.0, -1.0, 0.5
     return plan, uvw, freq, wgt, t_wgt, kw, dev, d, model
 
 
