@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD, choices=sorted(synth.WORKLOADS))
     ap.add_argument("--epsilon", type=float, default=1e-5)
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
+                    help="working precision of the timed step (f64: complex128 visibilities)")
     ap.add_argument("--cpu-stride", type=int, default=64,
                     help="the CPU sample: every n-th integration of the workload")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
@@ -226,11 +228,11 @@ def sample_text(wl, stride, nt, nvis):
             f"full {wl['npix']}^2 image and grid")
 
 
-def workload_config(wl, name, eps, world):
+def workload_config(wl, name, eps, world, precision="f32"):
     """The `config` of both arms' lines: the workload, by what it is."""
     nvis = NBL * wl["ntime"] * wl["nchan"]
     return {"workload": name, "visibilities": nvis, "image": [wl["npix"], wl["npix"]],
-            "cell_arcsec": wl["cell_arcsec"], "epsilon": eps, "flags": wl["flag"],
+            "cell_arcsec": wl["cell_arcsec"], "epsilon": eps, "precision": precision, "flags": wl["flag"],
             "parallelism": f"replicas{world}",
             "l2": f"inputs larger than L2 ({nvis * 8 / 1e9:.2f} GB of visibilities)"}
 
@@ -378,6 +380,8 @@ def run_reference(args):
         return  # the CPU reference runs once, on rank 0; the other ranks exit without work
     wl = synth.WORKLOADS[args.workload]
     oracle, uvw, freq, vis, mask, nt = cpu_sample(wl, args.cpu_stride)
+    if args.precision == "f64":
+        vis = vis.astype(np.complex128)
     threads = oracle.set_threads(os.cpu_count() or 1)
     cell = wl["cell_arcsec"] * synth.ARCSEC
     for _ in range(args.warmup):
@@ -389,8 +393,8 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(wl, args.workload, args.epsilon, world),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
+        "data": "synthetic", "config": workload_config(wl, args.workload, args.epsilon, world, args.precision),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample_text(wl, args.cpu_stride, nt, vis.size) + ", one round trip per step",
                          "cpu_model": cpu_model(), "simd": oracle.simd_level(),
@@ -1028,12 +1032,14 @@ def run_b200(args):
         b = min(nrow, a + 65536)
         vis[a:b] += 0.1 * torch.randn((b - a, nchan), dtype=torch.complex64, device=dev, generator=g) * np.sqrt(2.0)
     mask = (torch.rand((nrow, nchan), device=dev, generator=g) >= wl["flag"]).to(torch.uint8)
+    single = args.precision == "f32"
+    svis = vis if single else vis.to(torch.complex128)
     torch.cuda.synchronize()
 
     def step():
-        p1 = wgrid_torch.DevicePlan(uvw, freq, vis=vis, mask=mask, epsilon=eps, single=True, **common)
-        dirty = p1.grid(vis)
-        p2 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=eps, single=True, **common)
+        p1 = wgrid_torch.DevicePlan(uvw, freq, vis=svis, mask=mask, epsilon=eps, single=single, **common)
+        dirty = p1.grid(svis)
+        p2 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=eps, single=single, **common)
         out = p2.degrid(dirty)
         return p1, p2, dirty, out
 
@@ -1081,10 +1087,11 @@ def run_b200(args):
     nact = int(plan_info["nvis"])
     nplanes = max(int(plan_info["nplanes"]), 1)
     supp = int(plan_info["supp"])
-    grid_bytes = nplanes * plan_info["nu"] * plan_info["nv"] * 8
-    alg = {"grid": nact * (8 + 4) + nrow * 24 + grid_bytes, "degrid": nact * (8 + 4) + nrow * 24 + grid_bytes}
+    vb = 8 if single else 16  # a complex visibility or grid cell in the working precision
+    grid_bytes = nplanes * plan_info["nu"] * plan_info["nv"] * vb
+    alg = {"grid": nact * (vb + 4) + nrow * 24 + grid_bytes, "degrid": nact * (vb + 4) + nrow * 24 + grid_bytes}
     dom = max(("grid", "degrid"), key=lambda k: prof[k][1])
-    kernel = {"grid": "k_grid_i8", "degrid": "k_degrid_h"}[dom]
+    kernel = ({"grid": "k_grid_i8", "degrid": "k_degrid_h"} if single else {"grid": "k_grid_f64", "degrid": "k_degrid"})[dom]
     dom_launches, dom_ms = prof[dom]
     per_launch_s = dom_ms / max(dom_launches, 1) / 1e3
     achieved = alg[dom] / per_launch_s / 1e9
@@ -1116,10 +1123,11 @@ def run_b200(args):
         # Each rank pins about 18 GB of host memory; if any rank cannot, every
         # rank skips this leg together (its timing is a collective).
         try:
-            pinned = [torch.empty((nrow, nchan), dtype=torch.complex64, pin_memory=True),
+            cdt, rdt = (torch.complex64, torch.float32) if single else (torch.complex128, torch.float64)
+            pinned = [torch.empty((nrow, nchan), dtype=cdt, pin_memory=True),
                       torch.empty((nrow, nchan), dtype=torch.uint8, pin_memory=True),
-                      torch.empty((nrow, nchan), dtype=torch.complex64, pin_memory=True),
-                      torch.empty((npix, npix), dtype=torch.float32, pin_memory=True)]
+                      torch.empty((nrow, nchan), dtype=cdt, pin_memory=True),
+                      torch.empty((npix, npix), dtype=rdt, pin_memory=True)]
         except RuntimeError as exc:
             pinned = None
             reason = f"pinned host memory: {exc}".splitlines()[0][:200]
@@ -1131,17 +1139,20 @@ def run_b200(args):
 
         vis_h, mask_h, out_h, dirty_h = pinned
         pinned = None
-        vis_h.copy_(vis)
+        vis_h.copy_(svis)
         mask_h.copy_(mask)
         vis_np, mask_np, out_np, dirty_np = vis_h.numpy(), mask_h.numpy(), out_h.numpy(), dirty_h.numpy()
         opts = options_list(npix, npix, cell, cell, eps, {})
         info = np.empty(14)
 
+        v2d = ext.wgridder_vis2dirty_f32 if single else ext.wgridder_vis2dirty_f64
+        d2v = ext.wgridder_dirty2vis_f32 if single else ext.wgridder_dirty2vis_f64
+        real = np.float32 if single else np.float64
+
         def e2e_step():
-            st = ext.wgridder_vis2dirty_f32(opts, uvw_np, freq, vis_np, None, None, mask_np, dirty_np, None, info)
+            st = v2d(opts, uvw_np, freq, vis_np, None, None, mask_np, dirty_np, None, info)
             assert st == 0, ext.wgridder_last_error()
-            st = ext.wgridder_dirty2vis_f32(opts, uvw_np, freq, dirty_np, None, mask_np, out_np.view(np.float32),
-                                            info)
+            st = d2v(opts, uvw_np, freq, dirty_np, None, mask_np, out_np.view(real), info)
             assert st == 0, ext.wgridder_last_error()
 
         for _ in range(args.warmup):
@@ -1198,8 +1209,8 @@ def run_b200(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(wl, args.workload, eps, world),
+            "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+            "config": workload_config(wl, args.workload, eps, world, args.precision),
             "plan": dict({k: plan_info[k] for k in ("kernel_index", "supp", "nu", "nv", "nplanes")}, active=nact),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk, "accuracy": accuracy, "config1": config1, "fista": fst, "imaging_weights": weights_leg,

@@ -80,15 +80,19 @@ __device__ __forceinline__ bool is_active(const Inputs& in, bool with_vis, uint6
 
 // Baselines::new then FixW (wgridder.rs:568-586): the row's coordinates in
 // metres with flips and recentring, flipped to w >= 0; returns the sign.
-__device__ __forceinline__ double row_coord(const double* uvw, uint64_t row, double fu, double fv,
-                                            double fw, double r_l, double r_m, double b[3]) {
-  double tu = fu * uvw[3 * row], tv = fv * uvw[3 * row + 1], tw = fw * uvw[3 * row + 2];
+__device__ __forceinline__ double row_coord_of(double u, double v, double w, double fu, double fv, double fw,
+                                               double r_l, double r_m, double b[3]) {
+  double tu = fu * u, tv = fv * v, tw = fw * w;
   double c0 = tu + r_l * tw, c1 = tv + r_m * tw, c2 = tw;
   double res = 1.0 - 2.0 * (double)(c2 < 0.0 ? 1 : 0);
   b[0] = c0 * res;
   b[1] = c1 * res;
   b[2] = c2 * res;
   return res;
+}
+__device__ __forceinline__ double row_coord(const double* uvw, uint64_t row, double fu, double fv,
+                                            double fw, double r_l, double r_m, double b[3]) {
+  return row_coord_of(uvw[3 * row], uvw[3 * row + 1], uvw[3 * row + 2], fu, fv, fw, r_l, r_m, b);
 }
 
 // Setup::getpix (wgridder.rs:757-767).

@@ -44,6 +44,68 @@ struct F64Slots {
   }
 };
 
+// The inputs of one staged visibility, copied asynchronously (cp.async) a
+// round ahead of their use: its row's uvw, its channel's f / c, its value,
+// its weight and its bin key.
+struct Prefetched64 {
+  double uvw[3];
+  double foc;
+  uint4 vis;  // complex128, or complex64 in .x, .y
+  uint2 wgt;  // float64, float32 in .x, or the two float32 factors
+  uint32_t key;
+  uint32_t idx;
+};
+static_assert(sizeof(Prefetched64) == 64, "one 64-byte slot per lane");
+
+__device__ __forceinline__ void prefetch64(Prefetched64* dst, const double* __restrict__ uvw,
+                                           const double* __restrict__ foc, const Inputs& in, bool with_vis,
+                                           bool with_wgt, const uint32_t* __restrict__ key, uint32_t idx,
+                                           uint32_t nchan) {
+  const uint32_t row = idx / nchan, ch = idx - row * nchan;
+  const double* u = uvw + 3 * (size_t)row;
+  cp_async(&dst->uvw[0], u, 8);
+  cp_async(&dst->uvw[1], u + 1, 8);
+  cp_async(&dst->uvw[2], u + 2, 8);
+  cp_async(&dst->foc, foc + ch, 8);
+  if (with_vis) {
+    if (in.vis_kind == VIS_C128)
+      cp_async(&dst->vis, reinterpret_cast<const double2*>(in.vis) + idx, 16);
+    else if (in.vis_kind == VIS_C64)
+      cp_async(&dst->vis, reinterpret_cast<const float2*>(in.vis) + idx, 8);
+  }
+  if (with_wgt) {
+    if (in.wgt_kind == WGT_F64) {
+      cp_async(&dst->wgt, reinterpret_cast<const double*>(in.wgt) + idx, 8);
+    } else {
+      cp_async(&dst->wgt.x, reinterpret_cast<const float*>(in.wgt) + idx, 4);
+      if (in.wgt_kind == WGT_F32_PRODUCT) cp_async(&dst->wgt.y, reinterpret_cast<const float*>(in.wgt2) + idx, 4);
+    }
+  }
+  cp_async(&dst->key, key + idx, 4);
+  dst->idx = idx;
+}
+
+// Weights::get and VisData::get (wgridder.rs:950-1005) in double precision.
+__device__ __forceinline__ double prefetched_wgt64(const Prefetched64& p, const Inputs& in) {
+  switch (in.wgt_kind) {
+    case WGT_F64:
+      return __longlong_as_double((long long)(((unsigned long long)p.wgt.y << 32) | p.wgt.x));
+    case WGT_F32:
+      return (double)__uint_as_float(p.wgt.x);
+    case WGT_F32_PRODUCT:
+      return (double)(__uint_as_float(p.wgt.x) * __uint_as_float(p.wgt.y));
+    default:
+      return 1.0;
+  }
+}
+__device__ __forceinline__ cplx<double> prefetched_vis64(const Prefetched64& p, const Inputs& in) {
+  if (in.vis_kind == VIS_C128)
+    return {__longlong_as_double((long long)(((unsigned long long)p.vis.y << 32) | p.vis.x)),
+            __longlong_as_double((long long)(((unsigned long long)p.vis.w << 32) | p.vis.z))};
+  if (in.vis_kind == VIS_C64) return {(double)__uint_as_float(p.vis.x), (double)__uint_as_float(p.vis.y)};
+  return {1.0, 0.0};
+}
+
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(d[0]), "+d"(d[1])
@@ -114,15 +176,23 @@ __global__ void __launch_bounds__(F64_BATCH, 12)
   uint32_t gcur = INACTIVE;
   int su0 = 0, sv0 = 0, mpc = 0;
 
+  // This round's inputs are in pre (copied asynchronously); nidx is the next
+  // round's index.
+  Prefetched64* pre = reinterpret_cast<Prefetched64*>(smem + F64Slots::bytes()) + lane;
+  const bool with_vis = mode == VALUE_DATA && in.vis_kind != VIS_UNIT;
+  if (k0 + lane < k1) prefetch64(pre, uvw, foc, in, with_vis, with_wgt, key, sorted[k0 + lane], nchan);
+  cp_async_commit();
+  uint32_t nidx = (k0 + F64_BATCH + lane < k1) ? sorted[k0 + F64_BATCH + lane] : 0u;
+
   for (uint64_t kb = k0; kb < k1; kb += F64_BATCH) {
     const int nb = (int)min((uint64_t)F64_BATCH, k1 - kb);
+    cp_async_wait_all();
     __syncwarp();
     if (lane < nb) {  // staging, one record per lane
-      const uint32_t idx = sorted[kb + lane];
-      const uint32_t row = idx / nchan, ch = idx - row * nchan;
+      const Prefetched64& pr = *pre;
       double b[3];
-      const double imflip = row_coord(uvw, row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
-      const double f = foc[ch];
+      const double imflip = row_coord_of(pr.uvw[0], pr.uvw[1], pr.uvw[2], g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+      const double f = pr.foc;
       const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
       double uf, vf;
       int64_t iu0, iv0;
@@ -132,8 +202,8 @@ __global__ void __launch_bounds__(F64_BATCH, 12)
       const int du = (int)(su % (uint32_t)g.sube), dv = (int)(sv % (uint32_t)g.sube);
       double ku[S], kv[S];
       eval_taps2<double, S>(g.coeff, g.ne, -uf * 2.0 + ((double)S - 1.0), -vf * 2.0 + ((double)S - 1.0), ku, kv);
-      cplx<double> val = unit_value<double>(g, b, imflip, f, with_wgt, wgt_get<double>(in, idx));
-      if (mode == VALUE_DATA) val = data_value<double>(vis_get<double>(in, idx), val, imflip);
+      cplx<double> val = unit_value<double>(g, b, imflip, f, with_wgt, prefetched_wgt64(pr, in));
+      if (mode == VALUE_DATA) val = data_value<double>(prefetched_vis64(pr, in), val, imflip);
       bad |= !isfinite(val.re) || !isfinite(val.im) || !isfinite(uf) || !isfinite(vf) || !isfinite(w);
       double* cu = st.ku + lane * F64_ROW;
       double* cr = st.bre + lane * F64_ROW;
@@ -167,9 +237,13 @@ __global__ void __launch_bounds__(F64_BATCH, 12)
         }
         cw[j] = kwj;
       }
-      st.key[lane] = key[idx];
+      st.key[lane] = pr.key;
     }
+    // The next round's inputs, in flight while this one is contracted.
     __syncwarp();
+    if (kb + F64_BATCH + lane < k1) prefetch64(pre, uvw, foc, in, with_vis, with_wgt, key, nidx, nchan);
+    cp_async_commit();
+    if (kb + 2 * F64_BATCH + lane < k1) nidx = sorted[kb + 2 * F64_BATCH + lane];
     int q = 0;
     while (q < nb) {
       const uint32_t gk = st.key[q];

@@ -87,11 +87,12 @@ __global__ void k_bound_init(ValueBound* vb, unsigned long long vmax_bits, unsig
 // holds 2^34 of them. For the floating-point gridders a cell sums at most
 // nvis terms, each at most max |value| (taps are at most 1 + eps), and q
 // leaves 2 bits of headroom over that bound in the cell's width (64 bits in
-// single precision, 128 in double: a 64-bit unit would sit about 2^-48 below
-// the largest term, which the wide-field correction factors amplify past
-// double precision's accuracy). The scales depend on nothing
-// but the values and the active count, so a plan split into row chunks
-// grids to the same bits as one without.
+// single precision; 94 bits of hi * 2^32 + lo in double, where the unit is
+// 2^-(92 - log2 nvis) of the largest value, 2^-60 or finer: a 64-bit cell's
+// unit would sit about 2^-48 below the largest term, which the wide-field
+// correction factors amplify past double precision's accuracy). The scales
+// depend on nothing but the values and the active count, so a plan split
+// into row chunks grids to the same bits as one without.
 __global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long long nvis, int integer, int wide,
                             FixScale* fs) {
   double vmax = __longlong_as_double((long long)(unit ? values->wmax_bits : values->vmax_bits));
@@ -105,8 +106,8 @@ __global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long lo
     r.q = r.sb + 6;
   } else {
     r.sb = 0;
-    // nvis * vmax * 2^q < 2^62 (int64 cells), < 2^126 (128-bit cells)
-    r.q = (wide ? 124 : 60) - ev - ilogb((double)max(nvis, 1ull));
+    // nvis * vmax * 2^q < 2^62 (int64 cells), < 2^94 (hi * 2^32 + lo cells)
+    r.q = (wide ? 92 : 60) - ev - ilogb((double)max(nvis, 1ull));
   }
   *fs = r;
 }
@@ -116,30 +117,23 @@ __device__ __forceinline__ void fix_add(FixCell* cell, long long re, long long i
   if (im) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->im), (unsigned long long)im);
 }
 
-// A 128-bit two's complement integer, hi * 2^64 + lo, and a double-precision
-// grid cell of two of them: value = (re + i im) * 2^-q.
-struct Fix128 {
-  unsigned long long lo;
-  long long hi;
+// A double-precision grid value in fixed point: hi * 2^32 + lo, two int64
+// words, and a complex cell of two of them. A term, x * 2^q rounded once to
+// an integer t, is split as t_hi = floor(t / 2^32) and t_lo = t - t_hi 2^32 in
+// [0, 2^32]; the words sum their parts independently, so adding a term is two
+// integer adds that need no carry and no returned value (red.global.add),
+// exact in any order. lo stays below 2^63 for fewer than 2^31 terms per cell
+// (runs, not visibilities, are the terms), hi below 2^62 by the scale's
+// headroom (k_fix_scale).
+struct FixWide {
+  long long lo, hi;
 };
 struct FixCell2 {
-  Fix128 re, im;
+  FixWide re, im;
 };
 
-__device__ __forceinline__ Fix128 add128(Fix128 a, Fix128 b) {
-  Fix128 r;
-  r.lo = a.lo + b.lo;
-  r.hi = a.hi + b.hi + (r.lo < a.lo ? 1 : 0);
-  return r;
-}
-
-// cell += v, exact mod 2^128 in any order: the carry out of each low-word
-// addition goes to the high word with that addition.
-__device__ __forceinline__ void fix_add128(Fix128* cell, Fix128 v) {
-  if (v.lo) {
-    const unsigned long long old = atomicAdd(&cell->lo, v.lo);
-    if (old + v.lo < old) v.hi += 1;
-  }
+__device__ __forceinline__ void fix_add_wide(FixWide* cell, FixWide v) {
+  if (v.lo) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->lo), (unsigned long long)v.lo);
   if (v.hi) atomicAdd(reinterpret_cast<unsigned long long*>(&cell->hi), (unsigned long long)v.hi);
 }
 
@@ -163,24 +157,25 @@ struct FixTraits<float> {
 template <>
 struct FixTraits<double> {
   using Cell = FixCell2;
-  using Acc = Fix128;
+  using Acc = FixWide;
   static constexpr int wide = 1;
-  // sc = 2^(q - 64): the high word is floor(x * sc), the low word the
-  // fraction times 2^64 (exact: the fraction of a double is a double)
-  static __device__ __forceinline__ double scale(int q) { return ldexp(1.0, q - 64); }
+  // sc = 2^(q - 32): y = x * sc (exact), hi = floor(y) (exact; every double
+  // from 2^52 up is an integer), lo = rint((y - hi) 2^32) (the fraction is
+  // exact, the one rounding is to the grid's unit).
+  static __device__ __forceinline__ double scale(int q) { return ldexp(1.0, q - 32); }
   static __device__ __forceinline__ Acc term(double x, double sc) {
     const double y = x * sc, h = floor(y);
-    return Fix128{__double2ull_rn((y - h) * 18446744073709551616.0), (long long)h};
+    return FixWide{__double2ll_rn((y - h) * 4294967296.0), __double2ll_rn(h)};
   }
-  static __device__ __forceinline__ Acc zero() { return Fix128{0ull, 0ll}; }
-  static __device__ __forceinline__ Acc add(Acc a, Acc b) { return add128(a, b); }
-  static __device__ __forceinline__ bool nonzero(Acc a) { return (a.lo | (unsigned long long)a.hi) != 0; }
+  static __device__ __forceinline__ Acc zero() { return FixWide{0ll, 0ll}; }
+  static __device__ __forceinline__ Acc add(Acc a, Acc b) { return FixWide{a.lo + b.lo, a.hi + b.hi}; }
+  static __device__ __forceinline__ bool nonzero(Acc a) { return (a.lo | a.hi) != 0; }
   static __device__ __forceinline__ void flush(Cell* c, Acc re, Acc im) {
-    fix_add128(&c->re, re);
-    fix_add128(&c->im, im);
+    fix_add_wide(&c->re, re);
+    fix_add_wide(&c->im, im);
   }
-  static __device__ __forceinline__ double value(Fix128 v, int q) {
-    return ldexp((double)v.hi, 64 - q) + ldexp(__ull2double_rn(v.lo), -q);
+  static __device__ __forceinline__ double value(FixWide v, int q) {
+    return ldexp((double)v.hi, 32 - q) + ldexp((double)v.lo, -q);
   }
 };
 
@@ -218,6 +213,24 @@ struct VisRecord {
 };
 static_assert(sizeof(VisRecord) == 32, "records are one 32-byte sector");
 
+// The inputs of is_active<float> for visibility i, loaded ahead of their use.
+struct ActivityIn {
+  float vn = 1.0f;   // |vis|^2 in single precision (1 without visibilities)
+  float w = 1.0f;    // the weight (1 without weights)
+  float m = 1.0f;    // the mask (1 without a mask)
+  __device__ bool active() const { return (double)vn * (double)w * (double)m != 0.0; }
+};
+__device__ __forceinline__ ActivityIn activity_in(const Inputs& in, bool with_vis, uint64_t i) {
+  ActivityIn a;
+  if (with_vis) {
+    const cplx<float> v = vis_get<float>(in, i);
+    a.vn = v.re * v.re + v.im * v.im;
+  }
+  if (in.wgt_kind != WGT_NONE) a.w = wgt_get<float>(in, i);
+  if (in.mask) a.m = (float)in.mask[i];
+  return a;
+}
+
 // The count pass of the counting sort (k_bin_count) for single precision,
 // writing as well the record of each active visibility at its own index
 // (coalesced): its coordinates and taps' arguments are formed here once. The
@@ -232,13 +245,18 @@ __global__ void __launch_bounds__(256, 4)
   const uint64_t nround = (n + 31) & ~31ull;
   const uint32_t tmask = (1u << g.log2tile) - 1u;
   const uint32_t se = (uint32_t)g.sube, sdiv = (65536u + se - 1u) / se;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  RowCh rc(i, (uint32_t)g.nchan, (uint64_t)gridDim.x * blockDim.x);
-  for (; i < nround; i += (uint64_t)gridDim.x * blockDim.x, rc.next((uint32_t)g.nchan)) {
+  RowCh rc(i, (uint32_t)g.nchan, stride);
+  // The activity inputs (value, weight, mask) of the next index are loaded
+  // while this one is processed: the streamed loads were the kernel's stall.
+  ActivityIn cur = i < n ? activity_in(in, with_vis != 0, i) : ActivityIn{};
+  for (; i < nround; i += stride, rc.next((uint32_t)g.nchan)) {
     bool act = false;
     uint32_t k = INACTIVE;
+    const ActivityIn nxt = i + stride < n ? activity_in(in, with_vis != 0, i + stride) : ActivityIn{};
     if (i < n) {
-      act = is_active<float>(in, with_vis != 0, i);
+      act = cur.active();
       if (act) {
         double b[3];
         const double imflip = row_coord(uvw, rc.row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
@@ -283,6 +301,7 @@ __global__ void __launch_bounds__(256, 4)
       }
       key[i] = k;
     }
+    cur = nxt;
     warp_aggregated_add(counts, k, act);
   }
 }

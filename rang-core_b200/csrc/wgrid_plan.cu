@@ -300,14 +300,15 @@ __global__ void __launch_bounds__(256, 8) k_bin_count(const __grid_constant__ Ge
   }
 }
 
-// Each thread takes four indices a grid-stride apart per round, so that four
-// independent atomics (each returning its run's base) are in flight at once:
-// the kernel is bound by their latency. The order within a bin is free.
+// out[i] = i: the values of the double-precision plan's radix sort.
 __global__ void k_iota(uint64_t n, uint32_t* __restrict__ out) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     out[i] = (uint32_t)i;
 }
 
+// Each thread takes four indices a grid-stride apart per round, so that four
+// independent atomics (each returning its run's base) are in flight at once:
+// the kernel is bound by their latency. The order within a bin is free.
 __global__ void k_bin_scatter(uint64_t n, const uint32_t* __restrict__ key, uint32_t* __restrict__ cursor,
                               uint32_t* __restrict__ sorted) {
   constexpr int U = 4;
@@ -1763,7 +1764,7 @@ void launch_grid_f64(cudaStream_t s, const Geom<double>& g, const Inputs& in, in
                      const double* foc, const uint32_t* key, const uint32_t* sorted, uint64_t kbase, uint64_t kend,
                      uint32_t nbins, fast::FixCell2* grids, int pg0, int npg, fast::FixScale* fs) {
   if (kend <= kbase) return;
-  const int smem = (int)fast::F64Slots::bytes();
+  const int smem = (int)(fast::F64Slots::bytes() + fast::F64_BATCH * sizeof(fast::Prefetched64));
   const unsigned nblocks = (unsigned)((kend - kbase + fast::F64_CHUNK - 1) / fast::F64_CHUNK);
   {
     StageTimer timer_(ST_GRID, s);
