@@ -63,8 +63,8 @@ PROFILE_CASE = "ms2dirty+dirty2ms 132M vis 2048^2"
 # launch): a launch of another workload is scaled by its active visibilities.
 # A profiler figure, not something this script can time.
 DRAM_CAPTURE = {
-    "k_grid_i8": None,
-    "k_degrid_h": None,
+    "k_grid_i8": (7.865368e9 + 0.639403e9, 105697663),
+    "k_degrid_h": (6.765928e9 + 1.254083e9, 105697663),
 }
 METRIC = "Mvis/s ms2dirty+dirty2ms @eps=1e-5 vs FP64"
 UNIT = "Mvis/s"
@@ -868,7 +868,7 @@ def run_accuracy(dev, ext, wl, uvw, uvw_np, freq, vis, mask, common, args):
             torch.cuda.synchronize()
             ev[0].record()
             pa = wgrid_torch.DevicePlan(uvw, freq, vis=vin, mask=mask, epsilon=eps_m, single=single, **common)
-            dm = pa.grid(vin)
+            dm = pa.grid(vin, scanned=True)
             ev[1].record()
             pb = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=eps_m, single=single, **common)
             vm = pb.degrid(iin)
@@ -957,7 +957,7 @@ def run_config1(dev, args):
         for rep in range(7):
             ev[0].record()
             p = wgrid_torch.DevicePlan(uvw, freq, vis=dv, epsilon=eps, single=single, **common)
-            p.grid(dv)
+            p.grid(dv, scanned=True)
             ev[1].record()
             torch.cuda.synchronize()
             p.close()
@@ -1038,7 +1038,7 @@ def run_b200(args):
 
     def step():
         p1 = wgrid_torch.DevicePlan(uvw, freq, vis=svis, mask=mask, epsilon=eps, single=single, **common)
-        dirty = p1.grid(svis)
+        dirty = p1.grid(svis, scanned=True)
         p2 = wgrid_torch.DevicePlan(uvw, freq, mask=mask, epsilon=eps, single=single, **common)
         out = p2.degrid(dirty)
         return p1, p2, dirty, out
@@ -1192,6 +1192,20 @@ def run_b200(args):
                "cpu_model": cpu_model(), "simd": oracle.simd_level(), "load_avg_before": list(load),
                "step_s": [round(x, 4) for x in times], "ns_per_vis": 1e9 * t / svis.size}
         del svis, smask
+        # The sample pays the full grid's FFTs, a fixed cost, for a fraction of
+        # the visibilities. A second sample of twice the integrations separates
+        # the two: t = a + b n, and the whole workload would take a + b N.
+        if args.cpu_stride >= 2:
+            _, uv2, fr2, vis2, mask2, nt2 = cpu_sample(wl, args.cpu_stride // 2)
+            t2 = cpu_round_trip(oracle, uv2, fr2, vis2, mask2, npix, cell, eps)
+            n1, n2 = NBL * nt * wl["nchan"], vis2.size
+            b = (t2 - t) / (n2 - n1) if n2 > n1 else float("nan")
+            a = t - b * n1
+            cpu["two_sample_model"] = {
+                "samples": [[n1, t], [n2, t2]], "fixed_s": a, "ns_per_vis": 1e9 * b,
+                "whole_workload_mvis_per_s": nvis / (a + b * nvis) / 1e6 if a + b * nvis > 0 else None,
+                "note": "fixed cost (plan, FFTs of the full grid) and per-visibility cost fitted to two samples"}
+            del vis2, mask2
 
     config1 = None
     if world == 1 and not args.no_config1:

@@ -130,11 +130,15 @@ int32_t rang_b200_wgridder_plan_create(const WgridderOptions* opts, size_t nrow,
                                        int32_t single, void* stream, RangWgridPlan** plan,
                                        double* info);
 /* vis2dirty with the plan into image_dev (nx * ny, the plan's precision):
- * unit = 0 grids the data (vis_dev of vis_kind), unit = 1 unit visibilities
- * (the PSF); weights as in the _ex2 entry points. Asynchronous on `stream`. */
+ * weights as in the _ex2 entry points. `flags`: bit 0 (1) grids unit
+ * visibilities (the PSF) instead of vis_dev; bit 1 (2) tells that vis_dev,
+ * wgt_dev and wgt2_dev are the arrays the plan was created with, unchanged
+ * since, so the plan's scan already holds their largest value and the pass
+ * over the data that finds it is skipped (a plan checks the pointers; the
+ * caller vouches for the contents). Asynchronous on `stream`. */
 int32_t rang_b200_wgridder_plan_grid(RangWgridPlan* plan, const void* vis_dev, int32_t vis_kind,
                                      const void* wgt_dev, const void* wgt2_dev, int32_t wgt_kind,
-                                     int32_t unit, void* image_dev, void* stream);
+                                     int32_t flags, void* image_dev, void* stream);
 /* dirty2vis with the plan: image_dev (nx * ny) to vis_dev (nrow * nchan
  * interleaved complex, overwritten; inactive visibilities zero), times the
  * weights. Asynchronous on `stream`. */

@@ -326,10 +326,10 @@ PYBIND11_MODULE(_core, m) {
         return py::make_tuple(st, reinterpret_cast<uintptr_t>(plan), info);
       });
   m.def("wgridder_plan_grid", [](uintptr_t plan, uintptr_t vis, int vis_kind, uintptr_t wgt, uintptr_t wgt2,
-                                 int wgt_kind, int unit, uintptr_t image, uintptr_t stream) {
+                                 int wgt_kind, int flags, uintptr_t image, uintptr_t stream) {
     py::gil_scoped_release release;
     return rang_b200_wgridder_plan_grid(reinterpret_cast<RangWgridPlan*>(plan), ptr(vis), vis_kind, ptr(wgt),
-                                        ptr(wgt2), wgt_kind, unit, (void*)image, (void*)stream);
+                                        ptr(wgt2), wgt_kind, flags, (void*)image, (void*)stream);
   });
   m.def("wgridder_plan_degrid",
         [](uintptr_t plan, uintptr_t image, uintptr_t wgt, int wgt_kind, uintptr_t vis, uintptr_t stream) {

@@ -509,18 +509,19 @@ int32_t rang_b200_wgridder_plan_create(const WgridderOptions* opts, size_t nrow,
 }
 
 int32_t rang_b200_wgridder_plan_grid(RangWgridPlan* plan, const void* vis_dev, int32_t vis_kind, const void* wgt_dev,
-                                     const void* wgt2_dev, int32_t wgt_kind, int32_t unit, void* image_dev,
+                                     const void* wgt2_dev, int32_t wgt_kind, int32_t flags, void* image_dev,
                                      void* stream) {
   return guarded([&] {
     if (!plan || !image_dev) throw InvalidArgument("null array");
+    const bool unit = (flags & 1) != 0, scanned = (flags & 2) != 0;
     if (!unit) vis_bytes(vis_kind, vis_dev);
     wgt_bytes(wgt_kind, wgt_dev, wgt2_dev);
     Inputs in{vis_dev, vis_kind, wgt_dev, wgt2_dev, wgt_kind, nullptr};
     ValueMode m = unit ? VALUE_UNIT : VALUE_DATA;
     if (plan->single)
-      plan->f->grid(in, m, (float*)image_dev, (cudaStream_t)stream);
+      plan->f->grid(in, m, (float*)image_dev, (cudaStream_t)stream, nullptr, scanned);
     else
-      plan->d->grid(in, m, (double*)image_dev, (cudaStream_t)stream);
+      plan->d->grid(in, m, (double*)image_dev, (cudaStream_t)stream, nullptr, scanned);
   });
 }
 

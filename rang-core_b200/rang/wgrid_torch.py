@@ -99,15 +99,20 @@ class DevicePlan:
         except Exception:
             pass
 
-    def grid(self, vis=None, wgt=None, wgt2=None, out=None):
+    def grid(self, vis=None, wgt=None, wgt2=None, out=None, scanned=False):
         """vis2dirty of `vis` (complex CUDA tensor (nrow, nchan); None: unit
-        visibilities, the PSF) with weights `wgt` into a new or given image."""
+        visibilities, the PSF) with weights `wgt` into a new or given image.
+        `scanned`: `vis` (and the weights) are the tensors this plan was made
+        with, unchanged since, so the plan's scan bounds their values and the
+        pass over the data that would find the bound is skipped (as in the
+        reference's stateless call, which plans and grids one set of data)."""
         if out is None:
             out = torch.empty(self.shape, dtype=self.real, device=self.device)
         w, w2, wk = _wgt(wgt, wgt2)
         vk = 0 if vis is None else _VIS_KIND[vis.dtype]
-        _check(core.extension().wgridder_plan_grid(self._handle, _ptr(vis), vk, _ptr(w), _ptr(w2), wk,
-                                                   int(vis is None), out.data_ptr(), _stream(self.device)))
+        flags = (1 if vis is None else 0) | (2 if scanned else 0)
+        _check(core.extension().wgridder_plan_grid(self._handle, _ptr(vis), vk, _ptr(w), _ptr(w2), wk, flags,
+                                                   out.data_ptr(), _stream(self.device)))
         return out
 
     def degrid(self, image, wgt=None, out=None):

@@ -212,3 +212,25 @@ def test_device_fista_matches_a_numpy_run_with_its_misfits():
     assert rel_linf(res.x.cpu().numpy(), x) < 1e-10
     assert np.allclose(res.misfits.cpu().numpy(), misfits, rtol=1e-10, atol=1e-12 * abs(q0))
     plan.close()
+
+
+@pytest.mark.parametrize("single", [True, False])
+def test_grid_of_the_scanned_data_skips_its_bound_pass_with_the_same_bits(single):
+    """A plan made with the visibilities grids them with the scan's value bound
+    (`scanned=True`) to the same bits as with the bound pass over the data."""
+    import torch
+
+    from rang import wgrid_torch
+
+    uvw, freq = meerkat_like(nant=24, ntime=6, nchan=10, seed=4)
+    rng = np.random.default_rng(8)
+    shape = (uvw.shape[0], freq.size)
+    vis = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    dev = torch.device("cuda", 0)
+    tv = torch.from_numpy(vis).to(dev, torch.complex64 if single else torch.complex128)
+    kw = dict(npix_x=128, npix_y=96, pixsize_x=2e-5, pixsize_y=2e-5, epsilon=1e-5 if single else 1e-9)
+    plan = wgrid_torch.DevicePlan(torch.from_numpy(uvw).to(dev), freq, vis=tv, single=single, **kw)
+    a = plan.grid(tv)
+    b = plan.grid(tv, scanned=True)
+    assert torch.equal(a, b)
+    plan.close()
