@@ -866,6 +866,9 @@ def run_accuracy(dev, ext, wl, uvw, uvw_np, freq, vis, mask, common, args):
         best = [float("inf"), float("inf")]
         for rep in range(3):  # the first is a warm-up; the best of the other two is kept
             torch.cuda.synchronize()
+            if rep == 1:
+                ext.wgridder_profile_read()
+                ext.wgridder_profile(1)
             ev[0].record()
             pa = wgrid_torch.DevicePlan(uvw, freq, vis=vin, mask=mask, epsilon=eps_m, single=single, **common)
             dm = pa.grid(vin, scanned=True)
@@ -880,7 +883,11 @@ def run_accuracy(dev, ext, wl, uvw, uvw_np, freq, vis, mask, common, args):
             if rep > 0:
                 best = [min(best[0], ev[0].elapsed_time(ev[1])), min(best[1], ev[1].elapsed_time(ev[2]))]
             del dm, vm
-        entry.update({"supp": int(supp), "vis2dirty_ms": best[0], "dirty2vis_ms": best[1]})
+        ext.wgridder_profile(0)
+        prof = ext.wgridder_profile_read()
+        entry.update({"supp": int(supp), "vis2dirty_ms": best[0], "dirty2vis_ms": best[1],
+                      "stages_per_round_trip": {k: [v[0] / 2, round(v[1] / 2, 3)] for k, v in prof.items() if v[0]},
+                      "stages_note": "[launches, ms] per plan + grid + plan + degrid"})
         methods.append(entry)
         del vin, iin
     ext.wgridder_set_method(3)

@@ -78,6 +78,14 @@ __device__ __forceinline__ bool is_active(const Inputs& in, bool with_vis, uint6
   return tnorm * twgt * tmask != 0.0;
 }
 
+// |vis|^2 |w|^2 in double precision: the square of a value's bound. The
+// scan and the value-bound pass form it alike and take one square root of
+// their maximum, so a plan's bound of its own data equals a pass over it.
+template <class T>
+__device__ __forceinline__ double value_bound_sq(cplx<T> v, double aw) {
+  return ((double)v.re * (double)v.re + (double)v.im * (double)v.im) * (aw * aw);
+}
+
 // Baselines::new then FixW (wgridder.rs:568-586): the row's coordinates in
 // metres with flips and recentring, flipped to w >= 0; returns the sign.
 __device__ __forceinline__ double row_coord_of(double u, double v, double w, double fu, double fv, double fw,

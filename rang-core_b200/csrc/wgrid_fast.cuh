@@ -60,8 +60,7 @@ __global__ void k_value_max(uint64_t n, Inputs in, const uint32_t* __restrict__ 
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     if (key[i] == INACTIVE) continue;
     const double w = fabs((double)wgt_get<T>(in, i));
-    const cplx<T> v = vis_get<T>(in, i);
-    const double a = sqrt((double)v.re * (double)v.re + (double)v.im * (double)v.im) * w;
+    const double a = value_bound_sq(vis_get<T>(in, i), w);
     // NaN compares false and is dropped here; the gridder flags it.
     vm = a > vm ? a : vm;
     wm = w > wm ? w : wm;
@@ -71,6 +70,7 @@ __global__ void k_value_max(uint64_t n, Inputs in, const uint32_t* __restrict__ 
     wm = fmax(wm, __shfl_down_sync(0xffffffffu, wm, o));
   }
   if ((threadIdx.x & 31) == 0) {
+    vm = sqrt(vm);
     atomic_max_double(&vb->vmax_bits, vm);
     atomic_max_double(&vb->wmax_bits, wm);
   }
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(256, 4)
       key[i] = k;
     }
     cur = nxt;
-    warp_aggregated_add(counts, k, act);
+    warp_aggregated_count(counts, k, act);
   }
 }
 

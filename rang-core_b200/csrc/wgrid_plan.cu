@@ -182,7 +182,8 @@ __global__ void __launch_bounds__(256, 6) k_scan(uint32_t nrow, uint32_t nchan, 
         if (act[u]) {
           const double aw = fabs(twgt);
           wm = aw > wm ? aw : wm;
-          const double av = sqrt(tnorm) * aw;
+          // |vis|^2 |wgt|^2, the value bound's square (value_bound_sq)
+          const double av = with_vis ? value_bound_sq(vis_get<T>(in, i), aw) : aw * aw;
           vm = av > vm ? av : vm;
         }
       }
@@ -209,6 +210,7 @@ __global__ void __launch_bounds__(256, 6) k_scan(uint32_t nrow, uint32_t nchan, 
   vm = warp_max(vm);
   wm = warp_max(wm);
   if ((threadIdx.x & 31) == 0 && cnt) {
+    vm = sqrt(vm);  // one square root per warp: the largest |vis| |wgt|
     if (vm > 0.0) atomicMax(&out->vmax_bits, (unsigned long long)__double_as_longlong(vm));
     if (wm > 0.0) atomicMax(&out->wmax_bits, (unsigned long long)__double_as_longlong(wm));
     atomicAdd(&out->count, cnt);
@@ -255,6 +257,16 @@ __device__ __forceinline__ uint32_t bin_of(const Geom<T>& g, const double* __res
   return bin_of_rc(g, uvw, foc, row, ch, piu0, piv0);
 }
 
+// One counting atomic per distinct counter in the warp, without waiting for
+// its result (the count pass needs no positions).
+__device__ __forceinline__ void warp_aggregated_count(uint32_t* counters, uint32_t key, bool active) {
+  const unsigned mask = __ballot_sync(0xffffffffu, active);
+  if (active) {
+    const unsigned peers = __match_any_sync(mask, key);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counters[key], (uint32_t)__popc(peers));
+  }
+}
+
 // One atomic per distinct counter in the warp; each active lane gets the
 // counter's old value plus its rank among the lanes with the same counter.
 __device__ __forceinline__ uint32_t warp_aggregated_add(uint32_t* counters, uint32_t key, bool active) {
@@ -296,7 +308,7 @@ __global__ void __launch_bounds__(256, 8) k_bin_count(const __grid_constant__ Ge
       }
       key[i] = k;
     }
-    warp_aggregated_add(counts, k, act);
+    warp_aggregated_count(counts, k, act);
   }
 }
 
@@ -2223,6 +2235,15 @@ size_t Plan<T>::plane_group(size_t plane_bytes, size_t fixed) const {
   size_t nplanes = (size_t)std::max(g_.nplanes, 1);
   size_t freeb = 0, total = 0;
   check_cuda(cudaMemGetInfo(&freeb, &total), "memory info");
+  // Memory the stream-ordered pool holds without using it is this
+  // library's to reuse, though the device does not count it as free.
+  int dev = 0;
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+    freeb += (size_t)(reserved - used);
   size_t budget = std::min<size_t>(freeb / 2, (size_t)64 << 30);
   budget = budget > fixed ? budget - fixed : 0;
   size_t group = std::max<size_t>(1, budget / plane_bytes);
