@@ -58,6 +58,12 @@ int32_t rang_b200_nn_set_conv_path(int32_t path);
  * 0 none, 3 one did (the flag is cleared), 2 a CUDA error. */
 int32_t rang_b200_nn_device_status(void* stream);
 
+/* The timeout path of the tcgen05 convolutions, for tests: one block holds
+ * TMEM and waits on an mbarrier that nothing completes until the wait gives
+ * up after limit_ns (at most 10 s), then frees its TMEM and sets the flag
+ * that rang_b200_nn_device_status reports as 3. 0, 1 (bad limit) or 2. */
+int32_t rang_b200_nn_wait_probe(int64_t limit_ns, void* stream);
+
 /* wt[ci, tap, co] = w[co, 8 - tap, ci]: the weights with which conv3 computes
  * the gradient with respect to its input. */
 int32_t rang_b200_nn_conv3_flip(const void* w, void* wt, int32_t cin, int32_t cout, void* stream);

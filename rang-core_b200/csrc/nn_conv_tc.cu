@@ -61,8 +61,8 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
 }
-// True once the phase of this parity has completed; false after WAIT_NS.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// True once the phase of this parity has completed; false after limit_ns.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, unsigned long long limit_ns) {
   const uint32_t a = saddr(bar);
   unsigned long long t0 = 0;
   for (uint32_t i = 0;; i++) {
@@ -79,11 +79,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
       const unsigned long long t = now_ns();
       if (i == 0)
         t0 = t;
-      else if (t - t0 > WAIT_NS)
+      else if (t - t0 > limit_ns)
         return false;
     }
   }
 }
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) { return mbar_wait_for(bar, parity, WAIT_NS); }
 
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2,
                                             int c3) {
@@ -565,6 +566,44 @@ bool conv3_tc_supported(const TcConvArgs& a) {
 
 int conv3_tc(const TcConvArgs& a, cudaStream_t s) {
   return a.Cin % 64 == 0 ? launch_kc<64>(a, s) : launch_kc<32>(a, s);
+}
+
+// The timeout path of the convolutions' waits, exercised: a block holds TMEM
+// as a convolution does, waits on an mbarrier on which nothing arrives until
+// the wait gives up after limit_ns, sets the flag, frees its TMEM and
+// returns. Nothing else runs in the block, so nothing is left in flight.
+__global__ void __launch_bounds__(128) k_wait_probe(unsigned long long limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int gave_up;
+  const int warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    gave_up = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&tmem_slot)),
+                 "r"(32u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  if (threadIdx.x == 0 && !mbar_wait_for(&bar, 0, limit_ns)) gave_up = 1;
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u));
+  }
+  if (threadIdx.x == 0 && gave_up) atomicExch(&g_conv_tc_error, 1);
+}
+
+int conv3_tc_wait_probe(unsigned long long limit_ns, cudaStream_t s) {
+  k_wait_probe<<<1, 128, 0, s>>>(limit_ns);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 int conv3_tc_status(cudaStream_t s) {

@@ -24,6 +24,9 @@ int conv3_tc(const TcConvArgs& a, cudaStream_t s);
 // Waits for s and reads (and clears) the device flag that a block sets when
 // one of its waits gave up: 0, 3 (a wait gave up) or 2 (CUDA error).
 int conv3_tc_status(cudaStream_t s);
+// One block that holds TMEM and waits on an mbarrier nothing completes, with
+// the given limit: the convolutions' timeout path, for the tests.
+int conv3_tc_wait_probe(unsigned long long limit_ns, cudaStream_t s);
 
 struct TcDwArgs {
   const __nv_bfloat16* in;  // NHWC forward input of the layer, pixel stride ld_in

@@ -706,6 +706,11 @@ int32_t rang_b200_nn_conv3_weight_grad(const void* in, int64_t ld_in, const void
 
 int32_t rang_b200_nn_set_conv_path(int32_t path) { return g_conv_path.exchange(path == 1 ? 1 : 0); }
 
+int32_t rang_b200_nn_wait_probe(int64_t limit_ns, void* stream) {
+  if (limit_ns < 0 || limit_ns > 10000000000ll) return 1;
+  return conv3_tc_wait_probe((unsigned long long)limit_ns, (cudaStream_t)stream);
+}
+
 int32_t rang_b200_nn_device_status(void* stream) { return conv3_tc_status((cudaStream_t)stream); }
 
 int32_t rang_b200_nn_conv3_flip(const void* w, void* wt, int32_t cin, int32_t cout, void* stream) {

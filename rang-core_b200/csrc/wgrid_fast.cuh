@@ -213,21 +213,22 @@ struct VisRecord {
 };
 static_assert(sizeof(VisRecord) == 32, "records are one 32-byte sector");
 
-// The inputs of is_active<float> for visibility i, loaded ahead of their use.
+// The inputs of is_active<float> for visibility i, loaded ahead of their use
+// and combined only when used, so that nothing waits on the loads early.
 struct ActivityIn {
-  float vn = 1.0f;   // |vis|^2 in single precision (1 without visibilities)
-  float w = 1.0f;    // the weight (1 without weights)
-  float m = 1.0f;    // the mask (1 without a mask)
-  __device__ bool active() const { return (double)vn * (double)w * (double)m != 0.0; }
+  cplx<float> v{1.0f, 0.0f};  // the visibility ((1, 0) without visibilities)
+  float w = 1.0f;             // the weight (1 without weights)
+  uint32_t m = 1u;            // the mask (1 without a mask)
+  __device__ bool active() const {
+    const float vn = v.re * v.re + v.im * v.im;
+    return (double)vn * (double)w * (double)m != 0.0;
+  }
 };
 __device__ __forceinline__ ActivityIn activity_in(const Inputs& in, bool with_vis, uint64_t i) {
   ActivityIn a;
-  if (with_vis) {
-    const cplx<float> v = vis_get<float>(in, i);
-    a.vn = v.re * v.re + v.im * v.im;
-  }
+  if (with_vis) a.v = vis_get<float>(in, i);
   if (in.wgt_kind != WGT_NONE) a.w = wgt_get<float>(in, i);
-  if (in.mask) a.m = (float)in.mask[i];
+  if (in.mask) a.m = in.mask[i];
   return a;
 }
 
@@ -274,30 +275,27 @@ __global__ void __launch_bounds__(256, 4)
         k = (((su >> g.log2tile) * (uint32_t)g.ntv + (sv >> g.log2tile)) * (uint32_t)g.nbuckets + (uint32_t)mp) *
                 (uint32_t)g.nsub + sa * (uint32_t)g.nsub_side + sb;
         if (rows_per_chunk) k += (rc.row / rows_per_chunk) * nbins;
-        VisRecord r;
+        // The record's two 16-byte halves, formed in registers (VisRecord's
+        // field order).
         const double s1 = (double)g.supp - 1.0;
-        r.x0 = (float)(-uf * 2.0 + s1);
-        r.y0 = (float)(-vf * 2.0 + s1);
+        const float x0 = (float)(-uf * 2.0 + s1);
+        const float y0 = (float)(-vf * 2.0 + s1);
+        float xw = 0.0f;
         if (g.do_wgridding) {  // w_factor's argument for the first plane (nth 0)
           const float z = (float)(g.xdw * ((g.wmin + (double)mp * g.dw) - w));
-          r.xw = z * 2.0f + (float)s1;
-        } else {
-          r.xw = 0.0f;
+          xw = z * 2.0f + (float)s1;
         }
-        r.idx = (uint32_t)i;
+        float ph_re = 1.0f, ph_im = 0.0f;
         if (g.shifting) {
           const cplx<float> ph = shift_phase<float>(g, b, imflip, f, 1.0);
-          r.ph_re = ph.re;
-          r.ph_im = ph.im;
-        } else {
-          r.ph_re = 1.0f;
-          r.ph_im = 0.0f;
+          ph_re = ph.re;
+          ph_im = ph.im;
         }
-        r.meta = ((su & tmask) - sa * se) | (((sv & tmask) - sb * se) << 4) | (imflip < 0.0 ? 256u : 0u) |
-                 ((uint32_t)mp << 16);
-        r.bin = k;
-        reinterpret_cast<uint4*>(rec + i)[0] = *reinterpret_cast<const uint4*>(&r.x0);
-        reinterpret_cast<uint4*>(rec + i)[1] = *reinterpret_cast<const uint4*>(&r.ph_re);
+        const uint32_t meta = ((su & tmask) - sa * se) | (((sv & tmask) - sb * se) << 4) |
+                              (imflip < 0.0 ? 256u : 0u) | ((uint32_t)mp << 16);
+        reinterpret_cast<uint4*>(rec + i)[0] =
+            make_uint4(__float_as_uint(x0), __float_as_uint(y0), __float_as_uint(xw), (uint32_t)i);
+        reinterpret_cast<uint4*>(rec + i)[1] = make_uint4(__float_as_uint(ph_re), __float_as_uint(ph_im), meta, k);
       }
       key[i] = k;
     }

@@ -2235,19 +2235,25 @@ size_t Plan<T>::plane_group(size_t plane_bytes, size_t fixed) const {
   size_t nplanes = (size_t)std::max(g_.nplanes, 1);
   size_t freeb = 0, total = 0;
   check_cuda(cudaMemGetInfo(&freeb, &total), "memory info");
-  // Memory the stream-ordered pool holds without using it is this
-  // library's to reuse, though the device does not count it as free.
-  int dev = 0;
-  cudaMemPool_t pool;
-  uint64_t reserved = 0, used = 0;
-  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
-      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
-      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
-    freeb += (size_t)(reserved - used);
-  size_t budget = std::min<size_t>(freeb / 2, (size_t)64 << 30);
-  budget = budget > fixed ? budget - fixed : 0;
-  size_t group = std::max<size_t>(1, budget / plane_bytes);
-  return std::min(group, nplanes);
+  auto group_of = [&](size_t avail) {
+    size_t budget = std::min<size_t>(avail / 2, (size_t)64 << 30);
+    budget = budget > fixed ? budget - fixed : 0;
+    return std::min(std::max<size_t>(1, budget / plane_bytes), nplanes);
+  };
+  size_t group = group_of(freeb);
+  if (group < nplanes) {
+    // Memory the stream-ordered pool holds without using it is this
+    // library's to reuse, though the device does not count it as free. (The
+    // query waits for the device, so it is made only when it can matter.)
+    int dev = 0;
+    cudaMemPool_t pool;
+    uint64_t reserved = 0, used = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+      group = group_of(freeb + (size_t)(reserved - used));
+  }
+  return group;
 }
 
 // Zeroes the rows of n planes that the gridder writes and the transforms
@@ -2852,6 +2858,11 @@ void bin_noalloc(const WgridderOptions& o, size_t nrow, size_t nchan, const doub
   PlanInfo pi;
   EsKernel* kernel = nullptr;
   make_geom<T>(o, nrow, nchan, r.count, wmin_d, wmax_d, r_l, r_m, g, pi, kernel);
+  // The export orders by (tile, first plane) only: one sub-tile per tile, so
+  // the counters are one per (tile, plane), the reference's bins.
+  g.sube = 1 << g.log2tile;
+  g.nsub_side = 1;
+  g.nsub = 1;
   const uint64_t nbins = (uint64_t)g.ntu * g.ntv * g.nbuckets * g.nsub;
   const uint64_t need_words = 2 * (nbins + 1) + scan_tmp_words(nbins + 1);
   const uint64_t have_words = (NOALLOC_SCRATCH_BYTES - words_off) / sizeof(uint32_t);

@@ -94,6 +94,7 @@ _SIGNATURES = {
     "to_bf16": "PPLP",
     "set_conv_path": "I",
     "device_status": "P",
+    "wait_probe": "LP",
 }
 
 

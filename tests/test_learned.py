@@ -62,7 +62,7 @@ def test_library_exports_every_nn_symbol():
 
     text = (REPO / "include" / "rang_nn.h").read_text()
     names = sorted(set(re.findall(r"^\w+\s+(rang_b200_nn_\w+)\s*\(", text, re.M)))
-    assert len(names) == 16
+    assert len(names) == 17
     lib = ctypes.CDLL(core.library_path())
     for name in names:
         assert hasattr(lib, name), name
@@ -165,6 +165,42 @@ def conv_path():
     old = lib.rang_b200_nn_set_conv_path(0)
     yield lib
     lib.rang_b200_nn_set_conv_path(old)
+
+
+@pytest.mark.gpu
+def test_a_tcgen05_wait_that_runs_out_reports_status_3_and_the_context_stays_usable(conv_path):
+    """The convolutions' bounded wait, run out on purpose: one block holds TMEM
+    and waits 20 ms on an mbarrier that nothing completes; the wait gives up,
+    the block frees its TMEM, and the host reads status 3 once (the flag is
+    then cleared). A tcgen05 convolution afterwards runs with status 0."""
+    import torch
+
+    from rang import learned
+
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.current_stream().cuda_stream
+    assert conv_path.rang_b200_nn_device_status(s) == 0
+    assert conv_path.rang_b200_nn_wait_probe(-1, s) == 1
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    assert conv_path.rang_b200_nn_wait_probe(20_000_000, s) == 0
+    t1.record()
+    assert conv_path.rang_b200_nn_device_status(s) == 3
+    assert t0.elapsed_time(t1) >= 19.0
+    assert conv_path.rang_b200_nn_device_status(s) == 0
+    rng = np.random.default_rng(0)
+    cin = cout = 64
+    x = nno.bf16(rng.standard_normal((1, 8, 16, cin)))
+    w = nno.bf16(rng.standard_normal((cout, 9, cin)) / np.sqrt(9 * cin))
+    b = np.zeros(cout, np.float32)
+    xt, wt, bt = _bf16_tensor(x.reshape(-1, cin), dev), _bf16_tensor(w, dev), torch.from_numpy(b).to(dev)
+    out = torch.zeros((8 * 16, cout), dtype=torch.bfloat16, device=dev)
+    learned._call("conv3", xt.data_ptr(), cin, wt.data_ptr(), bt.data_ptr(), out.data_ptr(), cout, None, 0, 1, 8, 16,
+                  cin, cout, 0, 0, s)
+    assert conv_path.rang_b200_nn_device_status(s) == 0
+    ref = nno.conv3(x, w, b.astype(np.float64))
+    assert np.abs(_np(out).reshape(1, 8, 16, cout) - ref).max() <= 2.0**-7 * np.abs(ref).max()
 
 
 @pytest.mark.gpu
