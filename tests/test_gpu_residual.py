@@ -234,3 +234,28 @@ def test_grid_of_the_scanned_data_skips_its_bound_pass_with_the_same_bits(single
     b = plan.grid(tv, scanned=True)
     assert torch.equal(a, b)
     plan.close()
+
+
+@pytest.mark.parametrize("single", [True, False])
+def test_residual_and_gram_of_a_plan_with_nothing_active(single):
+    """All weights zero: the plan is empty, the residual and Gram images are
+    zero, the misfit and x^T G x are zero, and nothing is stored."""
+    import torch
+
+    from rang import wgrid_torch
+
+    uvw, freq = meerkat_like(nant=8, ntime=2, nchan=4, seed=2)
+    dev = torch.device("cuda", 0)
+    rt = torch.float32 if single else torch.float64
+    w = torch.zeros((uvw.shape[0], freq.size), dtype=rt, device=dev)
+    plan = wgrid_torch.DevicePlan(torch.from_numpy(uvw).to(dev), freq, wgt=w, single=single, npix_x=64, npix_y=64,
+                                  pixsize_x=2e-5, pixsize_y=2e-5, epsilon=1e-5 if single else 1e-9)
+    assert plan.active == 0
+    d = torch.ones((uvw.shape[0], freq.size), dtype=plan.cplx, device=dev)
+    img, q = plan.residual(d, w, torch.ones(plan.shape, dtype=rt, device=dev))
+    assert float(img.abs().max()) == 0.0 and float(q) == 0.0
+    xgx = torch.full((), 7.0, dtype=torch.float64, device=dev)
+    g = plan.gram(torch.ones(plan.shape, dtype=rt, device=dev), w, xgx=xgx)
+    assert float(g.abs().max()) == 0.0 and float(xgx) == 0.0
+    assert plan.memory()["gridder: stored sorted values"] == 0
+    plan.close()
