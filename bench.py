@@ -80,8 +80,9 @@ def parse():
     ap.add_argument("--epsilon", type=float, default=1e-5)
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
                     help="working precision of the timed step (f64: complex128 visibilities)")
-    ap.add_argument("--cpu-stride", type=int, default=64,
-                    help="the CPU sample: every n-th integration of the workload")
+    ap.add_argument("--cpu-stride", type=int, default=None,
+                    help="the CPU sample: every n-th integration of the workload (default: 64 for the CPU "
+                         "baseline leg; for --impl reference, 16, 32 or 64 as the step count allows)")
     ap.add_argument("--cpu-worker", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--no-config1", action="store_true")
     ap.add_argument("--fista-cap", type=int, default=3000)
@@ -374,10 +375,23 @@ def job_rate(world, units_per_rank, steps, seconds):
     return world * units_per_rank * steps / seconds / 1e6
 
 
+def reference_stride(steps, warmup):
+    """The reference arm's sample: as large as the run's length allows. A
+    sample pays the full grid's plan and FFTs (about 3.4 s on the 16 threads
+    of the GPU box) however few visibilities it has, so a small one
+    understates the CPU's rate on the whole workload; every 16th integration
+    (66 M visibilities, about 10 s a round trip) when the run has at most 24
+    steps, else every 32nd or 64th, keeps the run within a few minutes."""
+    n = steps + warmup
+    return 16 if n <= 24 else 32 if n <= 48 else 64
+
+
 def run_reference(args):
     world, rank, _ = replica_env()
     if rank != 0:
         return  # the CPU reference runs once, on rank 0; the other ranks exit without work
+    if args.cpu_stride is None:
+        args.cpu_stride = reference_stride(args.steps, args.warmup)
     wl = synth.WORKLOADS[args.workload]
     oracle, uvw, freq, vis, mask, nt = cpu_sample(wl, args.cpu_stride)
     if args.precision == "f64":
@@ -1245,6 +1259,8 @@ def run_b200(args):
 
 def main():
     args = parse()
+    if args.impl != "reference" and args.cpu_stride is None:
+        args.cpu_stride = 64
     if args.cpu_worker:
         cpu_worker(args.cpu_worker)
     elif args.impl == "reference":

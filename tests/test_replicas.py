@@ -89,3 +89,10 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
 
     assert bench.run_reference(Args()) is None  # returns before any work
     assert capsys.readouterr().out == ""
+
+
+def test_reference_sample_is_as_large_as_the_run_allows():
+    bench = _bench()
+    assert bench.reference_stride(20, 3) == 16
+    assert bench.reference_stride(40, 3) == 32
+    assert bench.reference_stride(100, 5) == 64
