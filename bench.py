@@ -1107,9 +1107,15 @@ def run_b200(args):
     nact = int(plan_info["nvis"])
     nplanes = max(int(plan_info["nplanes"]), 1)
     supp = int(plan_info["supp"])
-    vb = 8 if single else 16  # a complex visibility or grid cell in the working precision
-    grid_bytes = nplanes * plan_info["nu"] * plan_info["nv"] * vb
-    alg = {"grid": nact * (vb + 4) + nrow * 24 + grid_bytes, "degrid": nact * (vb + 4) + nrow * 24 + grid_bytes}
+    # The algorithmic bytes of one direction, per unit as the hot-path survey
+    # counts them: every visibility's value (8 B; 16 in double), weight (4 B)
+    # and flag (1 B) read (or the value written, degridding), 24 B of uvw per
+    # row, each plane's grid written and read once (2 x 8 B per cell; 16 in
+    # double) and the image (4 B per pixel; 8 in double).
+    vb = 8 if single else 16
+    per_direction = (nvis * (vb + 4 + 1) + nrow * 24 + nplanes * plan_info["nu"] * plan_info["nv"] * vb * 2
+                     + npix * npix * vb // 2)
+    alg = {"grid": per_direction, "degrid": per_direction}
     dom = max(("grid", "degrid"), key=lambda k: prof[k][1])
     kernel = ({"grid": "k_grid_i8", "degrid": "k_degrid_h"} if single else {"grid": "k_grid_f64", "degrid": "k_degrid"})[dom]
     dom_launches, dom_ms = prof[dom]
