@@ -222,9 +222,9 @@ int32_t rang_b200_wgridder_binning(const WgridderOptions* opts, size_t nrow, siz
  * lives in one 16 MiB array that the library holds on each GPU that loads it
  * (NOALLOC_SCRATCH_BYTES); a call whose bin counters and scan do not fit in
  * it fails with status 1 and says how many bytes it needed. The first call on
- * a device looks up that array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture. Every call reads the scan's
- * count back to the host and waits for `stream` before it returns. All calls
+ * a device looks up that array's device address (cudaGetSymbolAddress).
+ * Every call reads the scan's count back to the host and waits for `stream`
+ * before it returns, so no call can be made inside a stream capture. All calls
  * share the array, so calls whose GPU work overlaps race: run them on one
  * stream, or wait for one before starting another. The call clears what must
  * start at zero.
