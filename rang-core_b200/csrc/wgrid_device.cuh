@@ -103,20 +103,25 @@ __device__ __forceinline__ double row_coord(const double* uvw, uint64_t row, dou
   return row_coord_of(uvw[3 * row], uvw[3 * row + 1], uvw[3 * row + 2], fu, fv, fw, r_l, r_m, b);
 }
 
-// Setup::getpix (wgridder.rs:757-767).
-template <class T>
-__device__ __forceinline__ void getpix(const Geom<T>& g, double uin, double vin, double& uf, double& vf,
-                                       int64_t& iu0, int64_t& iv0) {
+// Setup::getpix (wgridder.rs:757-767), in 32-bit integers: u - floor(u)
+// lies in [0, 1] (or is NaN), so u + ushift lies in (0, 2 nu + 1] and every
+// intermediate fits an int; NaN converts to 0 in either width. The indices
+// equal the reference's 64-bit ones, and I may be int or int64_t.
+template <class T, class I>
+__device__ __forceinline__ void getpix(const Geom<T>& g, double uin, double vin, double& uf, double& vf, I& iu0,
+                                       I& iv0) {
   double u = uin * g.pixsize_x;
   u = (u - floor(u)) * (double)g.nu;
-  iu0 = min((int64_t)(u + g.ushift) - (int64_t)g.nu, g.maxiu0);
-  u -= (double)iu0;
+  const int a = min((int)(u + g.ushift) - g.nu, (int)g.maxiu0);
+  u -= (double)a;
   double v = vin * g.pixsize_y;
   v = (v - floor(v)) * (double)g.nv;
-  iv0 = min((int64_t)(v + g.vshift) - (int64_t)g.nv, g.maxiv0);
-  v -= (double)iv0;
+  const int b = min((int)(v + g.vshift) - g.nv, (int)g.maxiv0);
+  v -= (double)b;
   uf = u;
   vf = v;
+  iu0 = a;
+  iv0 = b;
 }
 
 // Setup::minplane and the clamp of Setup::locate (wgridder.rs:770-776, 1253-1254).
@@ -136,6 +141,12 @@ __device__ __forceinline__ int shifted(int64_t i0, int n) {
   if (r >= 0 && r < 2 * (int64_t)n) return (int)(r >= n ? r - n : r);
   r %= n;
   return (int)(r < 0 ? r + n : r);
+}
+__device__ __forceinline__ int shifted(int i0, int n) {  // getpix's 32-bit indices (|i0| < 2^30)
+  int r = i0 + n / 2;
+  if (r >= 0 && r < 2 * n) return r >= n ? r - n : r;
+  r %= n;
+  return r < 0 ? r + n : r;
 }
 
 // `offset` (wgridder.rs:1183-1192).

@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(F64_BATCH, 12)
       const double f = pr.foc;
       const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
       double uf, vf;
-      int64_t iu0, iv0;
+      int iu0, iv0;
       getpix(g, u, v, uf, vf, iu0, iv0);
       const int mp = minplane(g, w);
       const uint32_t su = (uint32_t)shifted(iu0, g.nu) & tmask, sv = (uint32_t)shifted(iv0, g.nv) & tmask;

@@ -213,34 +213,33 @@ struct VisRecord {
 };
 static_assert(sizeof(VisRecord) == 32, "records are one 32-byte sector");
 
-// The inputs of is_active<float> for visibility i, loaded ahead of their use
-// and combined only when used, so that nothing waits on the loads early.
-struct ActivityIn {
-  cplx<float> v{1.0f, 0.0f};  // the visibility ((1, 0) without visibilities)
-  float w = 1.0f;             // the weight (1 without weights)
-  uint32_t m = 1u;            // the mask (1 without a mask)
-  __device__ bool active() const {
-    const float vn = v.re * v.re + v.im * v.im;
-    return (double)vn * (double)w * (double)m != 0.0;
-  }
+// The loads of one visibility of the count pass: its word of the scan's
+// active bits, its row's coordinates and its channel's f / c, issued an
+// iteration ahead of their use (the pass otherwise waited on them).
+struct CountIn {
+  uint32_t word = 0;
+  double u = 0.0, v = 0.0, w = 0.0, f = 0.0;
 };
-__device__ __forceinline__ ActivityIn activity_in(const Inputs& in, bool with_vis, uint64_t i) {
-  ActivityIn a;
-  if (with_vis) a.v = vis_get<float>(in, i);
-  if (in.wgt_kind != WGT_NONE) a.w = wgt_get<float>(in, i);
-  if (in.mask) a.m = in.mask[i];
-  return a;
+__device__ __forceinline__ CountIn count_in(const uint32_t* __restrict__ bits, const double* __restrict__ uvw,
+                                            const double* __restrict__ foc, uint64_t i, uint32_t row, uint32_t ch) {
+  CountIn c;
+  c.word = bits[i >> 5];
+  c.u = uvw[3 * (uint64_t)row];
+  c.v = uvw[3 * (uint64_t)row + 1];
+  c.w = uvw[3 * (uint64_t)row + 2];
+  c.f = foc[ch];
+  return c;
 }
 
 // The count pass of the counting sort (k_bin_count) for single precision,
 // writing as well the record of each active visibility at its own index
 // (coalesced): its coordinates and taps' arguments are formed here once. The
 // scatter then moves only the 4-byte indices, and the gridder and degridder
-// read each record through the sorted index. Five blocks per SM (51
-// registers) measured 7 % faster than four (56).
-__global__ void __launch_bounds__(256, 5)
+// read each record through the sorted index. The active set comes from the
+// scan's bits (bit i: visibility i), one word per 32 visibilities.
+__global__ void __launch_bounds__(256, 4)
     k_bin_count_rec(const __grid_constant__ Geom<float> g, const double* __restrict__ uvw,
-                    const double* __restrict__ foc, Inputs in, int with_vis, uint32_t* __restrict__ key,
+                    const double* __restrict__ foc, const uint32_t* __restrict__ bits, uint32_t* __restrict__ key,
                     uint32_t* __restrict__ counts, VisRecord* __restrict__ rec, uint32_t rows_per_chunk,
                     uint32_t nbins) {
   const uint64_t n = g.nrow * g.nchan;
@@ -250,22 +249,22 @@ __global__ void __launch_bounds__(256, 5)
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   RowCh rc(i, (uint32_t)g.nchan, stride);
-  // The activity inputs (value, weight, mask) of the next index are loaded
-  // while this one is processed: the streamed loads were the kernel's stall.
-  ActivityIn cur = i < n ? activity_in(in, with_vis != 0, i) : ActivityIn{};
-  for (; i < nround; i += stride, rc.next((uint32_t)g.nchan)) {
+  CountIn cur = i < n ? count_in(bits, uvw, foc, i, rc.row, rc.ch) : CountIn{};
+  for (; i < nround; i += stride) {
+    RowCh nrc = rc;
+    nrc.next((uint32_t)g.nchan);
+    const CountIn nxt = i + stride < n ? count_in(bits, uvw, foc, i + stride, nrc.row, nrc.ch) : CountIn{};
     bool act = false;
     uint32_t k = INACTIVE;
-    const ActivityIn nxt = i + stride < n ? activity_in(in, with_vis != 0, i + stride) : ActivityIn{};
     if (i < n) {
-      act = cur.active();
+      act = ((cur.word >> (i & 31)) & 1u) != 0;
       if (act) {
         double b[3];
-        const double imflip = row_coord(uvw, rc.row, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
-        const double f = foc[rc.ch];
+        const double imflip = row_coord_of(cur.u, cur.v, cur.w, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+        const double f = cur.f;
         const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
         double uf, vf;
-        int64_t iu0, iv0;
+        int iu0, iv0;
         getpix(g, u, v, uf, vf, iu0, iv0);
         const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
         // (x / sube) for x < 32 as a multiply and shift (exact: the error of
@@ -300,8 +299,9 @@ __global__ void __launch_bounds__(256, 5)
       }
       key[i] = k;
     }
-    cur = nxt;
     warp_aggregated_count(counts, k, act);
+    cur = nxt;
+    rc = nrc;
   }
 }
 

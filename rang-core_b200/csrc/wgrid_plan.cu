@@ -127,92 +127,210 @@ __global__ void k_scan_init(ScanOut* so) {
   so->wmax_bits = 0;
 }
 
-// The scan gives each warp runs of 32 x SCAN_ROUNDS consecutive visibilities,
-// a grid stride apart; in round u of a run lane l takes visibility
-// base + 32 u + l. The rounds' loads are independent, so a lane keeps
-// SCAN_ROUNDS of them in flight: the mask is one byte per visibility, and one
-// load at a time left the pass waiting on memory. Four rounds measured best
-// (one: 7.9 ms per step of two scans on 1.06 G visibilities; four: 6.1;
-// eight: 6.4; sixteen: 7.6).
-constexpr int SCAN_ROUNDS = 4;
-
-// Row and channel of a lane's visibility, advanced by one round (32 visibilities).
-struct RoundStep {
-  uint32_t srow, sch;
-  __device__ explicit RoundStep(uint32_t nchan) : srow(32u / nchan), sch(32u % nchan) {}
-  __device__ __forceinline__ void next(uint32_t& row, uint32_t& ch, uint32_t nchan) const {
-    row += srow;
-    ch += sch;
-    if (ch >= nchan) {
-      ch -= nchan;
-      row++;
-    }
-  }
+// The activity inputs of four consecutive visibilities e .. e + 3 (e a
+// multiple of 4): by 16-byte loads when `vec` (every input 16-byte aligned)
+// and all four exist, else one by one; those at or past n get mask 0.
+template <class T>
+struct Quad {
+  cplx<T> v[4];
+  T w[4];
+  uint32_t m;  // the four mask bytes, visibility e in the low byte
 };
 
-// scan (wgridder.rs:1051-1077): the count is exact and min/max are order
-// independent, so the result is the reference's bit for bit.
 template <class T>
-__global__ void __launch_bounds__(256, 6) k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__ uvw,
-                       const double* __restrict__ foc, double fw, Inputs in, int with_vis, ScanOut* out) {
-  const uint64_t n = (uint64_t)nrow * nchan;
-  const uint64_t run = 32ull * SCAN_ROUNDS;
-  const uint64_t wid = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t wstride = (((uint64_t)gridDim.x * blockDim.x) >> 5) * run;
-  unsigned long long cnt = 0, fin = 0;
-  double lo = 1e300, hi = 0.0, vm = 0.0, wm = 0.0;
-  uint64_t i0 = wid * run + (threadIdx.x & 31);
-  RowCh rc(i0, nchan, wstride);
-  const RoundStep step(nchan);
-  for (; i0 < n; i0 += wstride, rc.next(nchan)) {
-    bool act[SCAN_ROUNDS];
+__device__ __forceinline__ void load_quad(const Inputs& in, bool with_vis, bool vec, uint64_t e, uint64_t n,
+                                          Quad<T>& q) {
 #pragma unroll
-    for (int u = 0; u < SCAN_ROUNDS; u++) {
-      const uint64_t i = i0 + 32u * u;
-      act[u] = false;
-      if (i < n) {  // is_active, keeping the magnitudes for the value bound
-        double tnorm = 1.0;
-        if (with_vis) {
-          const cplx<T> v = vis_get<T>(in, i);
-          tnorm = (double)(v.re * v.re + v.im * v.im);
-        }
-        const double twgt = in.wgt_kind != WGT_NONE ? (double)wgt_get<T>(in, i) : 1.0;
-        const double tmask = in.mask ? (double)in.mask[i] : 1.0;
-        act[u] = tnorm * twgt * tmask != 0.0;
-        if (act[u]) {
-          const double aw = fabs(twgt);
-          wm = aw > wm ? aw : wm;
+  for (int k = 0; k < 4; k++) {
+    q.v[k] = {(T)1, (T)0};
+    q.w[k] = (T)1;
+  }
+  if (vec && e + 4 <= n) {
+    if (with_vis && in.vis_kind == VIS_C64) {
+      const float4 a = reinterpret_cast<const float4*>(in.vis)[e / 2];
+      const float4 b = reinterpret_cast<const float4*>(in.vis)[e / 2 + 1];
+      q.v[0] = {(T)a.x, (T)a.y};
+      q.v[1] = {(T)a.z, (T)a.w};
+      q.v[2] = {(T)b.x, (T)b.y};
+      q.v[3] = {(T)b.z, (T)b.w};
+    } else if (with_vis && in.vis_kind == VIS_C128) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const double2 d = reinterpret_cast<const double2*>(in.vis)[e + k];
+        q.v[k] = {(T)d.x, (T)d.y};
+      }
+    }
+    if (in.wgt_kind == WGT_F32 || in.wgt_kind == WGT_F32_PRODUCT) {
+      float4 a = reinterpret_cast<const float4*>(in.wgt)[e / 4];
+      if (in.wgt_kind == WGT_F32_PRODUCT) {
+        const float4 b = reinterpret_cast<const float4*>(in.wgt2)[e / 4];
+        a = make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
+      }
+      q.w[0] = (T)a.x;
+      q.w[1] = (T)a.y;
+      q.w[2] = (T)a.z;
+      q.w[3] = (T)a.w;
+    } else if (in.wgt_kind == WGT_F64) {
+      const double2 a = reinterpret_cast<const double2*>(in.wgt)[e / 2];
+      const double2 b = reinterpret_cast<const double2*>(in.wgt)[e / 2 + 1];
+      q.w[0] = (T)a.x;
+      q.w[1] = (T)a.y;
+      q.w[2] = (T)b.x;
+      q.w[3] = (T)b.y;
+    }
+    q.m = in.mask ? reinterpret_cast<const uint32_t*>(in.mask)[e / 4] : 0x01010101u;
+    return;
+  }
+  q.m = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (e + k < n) {
+      if (with_vis) q.v[k] = vis_get<T>(in, e + k);
+      q.w[k] = wgt_get<T>(in, e + k);
+      q.m |= (in.mask ? (uint32_t)in.mask[e + k] : 1u) << (8 * k);
+    }
+  }
+}
+
+// is_active's test, (double) |vis|^2 * (double) wgt * (double) mask != 0,
+// for single-precision factors: a double product of floats neither
+// overflows nor underflows, so it is zero exactly when a factor is zero and
+// none is infinite or NaN. Double-precision factors take the product.
+__device__ __forceinline__ bool active_of(float vn, float w, uint32_t m) {
+  return !isfinite(vn) || !isfinite(w) || (vn != 0.0f && w != 0.0f && m != 0u);
+}
+__device__ __forceinline__ bool active_of(double vn, double w, uint32_t m) { return vn * w * (double)m != 0.0; }
+
+// Whether every channel factor f / c is finite (they are positive): the
+// scan's |w| range then takes two products per group of four.
+bool all_finite(const std::vector<double>& foc) {
+  for (double f : foc)
+    if (!std::isfinite(f)) return false;
+  return true;
+}
+
+// Whether the scan's 16-byte loads may be used: every input present is
+// 16-byte aligned (the mask 4-byte).
+bool scan_vectors(const Inputs& in, bool with_vis) {
+  auto al = [](const void* p, uintptr_t a) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % a) == 0; };
+  return (!with_vis || in.vis_kind == VIS_UNIT || al(in.vis, 16)) &&
+         (in.wgt_kind == WGT_NONE || (al(in.wgt, 16) && al(in.wgt2, 16))) && al(in.mask, 4);
+}
+
+// Groups of four visibilities each lane has in flight (half as many in
+// double precision, whose values take twice the registers): at four blocks
+// per SM that is 72 bytes per lane, 73 KB per SM, of complex64 values and
+// mask in flight; more groups spill.
+constexpr int SCAN_GROUPS = 2;
+
+// scan (wgridder.rs:1051-1077): the count is exact and min/max are order
+// independent, so the result is the reference's bit for bit. A warp takes
+// blocks of 128 G consecutive visibilities, a grid stride apart; in group q
+// of a block lane l takes the four visibilities from 128 q + 4 l, its inputs
+// in 16-byte loads (one byte per lane per load left the pass waiting on
+// memory at a third of the HBM rate). With `bits`, bit i of the u32 array is
+// set when visibility i is active (is_active): the count pass then reads one
+// word per 32 visibilities instead of their inputs.
+//
+// The |w| range of a group inside one row needs two products, not four:
+// |w| = |(fw w_row) f_c| with the channels' f_c ascending and, when `clean`
+// (every f_c finite; they are positive), rounding is monotone, so the
+// smallest and largest |w| of the group's active visibilities are those of
+// its first and last active channel, and each is NaN exactly when
+// fw w_row is.
+template <class T>
+__global__ void __launch_bounds__(256, 3) k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__ uvw,
+                       const double* __restrict__ foc, double fw, Inputs in, int with_vis, int vec, int clean,
+                       ScanOut* out, uint32_t* __restrict__ bits) {
+  const uint64_t n = (uint64_t)nrow * nchan;
+  constexpr int G = sizeof(T) == 4 ? SCAN_GROUPS : SCAN_GROUPS / 2;
+  constexpr uint64_t BLOCK = 128ull * G;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t wid = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t wstride = (((uint64_t)gridDim.x * blockDim.x) >> 5) * BLOCK;
+  uint32_t cnt32 = 0, fin32 = 0;  // per thread: far below 2^32
+  double lo = 1e300, hi = 0.0, vm = 0.0;
+  T wm = (T)0;  // max |wgt|: the conversion to double is exact and monotone
+  uint64_t b0 = wid * BLOCK;
+  RowCh rc(b0 + 4 * lane, nchan, wstride);
+  const uint32_t srow = 128u / nchan, sch = 128u % nchan;  // one group: 128 visibilities
+  for (; b0 < n; b0 += wstride, rc.next(nchan)) {
+    Quad<T> q[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) load_quad<T>(in, with_vis != 0, vec != 0, b0 + 128 * g + 4 * lane, n, q[g]);
+    uint32_t row = rc.row, ch = rc.ch;
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      uint32_t nib = 0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        // is_active, keeping the magnitudes for the value bound
+        const T vn = with_vis ? q[g].v[k].re * q[g].v[k].re + q[g].v[k].im * q[g].v[k].im : (T)1;
+        if (active_of(vn, q[g].w[k], (q[g].m >> (8 * k)) & 0xffu)) {
+          nib |= 1u << k;
+          const T awt = fabs(q[g].w[k]);
+          wm = awt > wm ? awt : wm;
           // |vis|^2 |wgt|^2, the value bound's square (value_bound_sq)
-          const double av = with_vis ? value_bound_sq(vis_get<T>(in, i), aw) : aw * aw;
+          const double aw = (double)awt;
+          const double av = with_vis ? value_bound_sq(q[g].v[k], aw) : aw * aw;
           vm = av > vm ? av : vm;
         }
       }
-    }
-    uint32_t row = rc.row, ch = rc.ch;
+      if (nib) {
+        cnt32 += __popc(nib);
+        if (clean && ch + 3 < nchan) {  // one row
+          const double a = fw * uvw[3 * (uint64_t)row + 2];
+          if (!isnan(a)) {
+            fin32 += __popc(nib);
+            lo = fmin(lo, fabs(a * foc[ch + __ffs(nib) - 1]));
+            hi = fmax(hi, fabs(a * foc[ch + 31 - __clz(nib)]));
+          }
+        } else {
+          uint32_t r = row, c = ch;
 #pragma unroll
-    for (int u = 0; u < SCAN_ROUNDS; u++) {
-      if (act[u]) {
-        double w = fabs(fw * uvw[3 * (uint64_t)row + 2] * foc[ch]);
-        cnt++;
-        if (!isnan(w)) {
-          fin++;
-          lo = fmin(lo, w);
-          hi = fmax(hi, w);
+          for (int k = 0; k < 4; k++) {
+            if (nib & (1u << k)) {
+              const double w = fabs(fw * uvw[3 * (uint64_t)r + 2] * foc[c]);
+              if (!isnan(w)) {
+                fin32++;
+                lo = fmin(lo, w);
+                hi = fmax(hi, w);
+              }
+            }
+            if (++c == nchan) {
+              c = 0;
+              r++;
+            }
+          }
         }
       }
-      step.next(row, ch, nchan);
+      if (bits) {  // eight lanes' nibbles make the word of 32 visibilities
+        uint32_t x = nib << (4 * (lane & 7));
+        x |= __shfl_xor_sync(0xffffffffu, x, 1);
+        x |= __shfl_xor_sync(0xffffffffu, x, 2);
+        x |= __shfl_xor_sync(0xffffffffu, x, 4);
+        const uint64_t e = b0 + 128 * g + 4 * lane;
+        if ((lane & 7) == 0 && e < n) bits[e >> 5] = x;
+      }
+      row += srow;
+      ch += sch;
+      if (ch >= nchan) {
+        ch -= nchan;
+        row++;
+      }
     }
   }
+  unsigned long long cnt = cnt32, fin = fin32;
   cnt = warp_sum(cnt);
   fin = warp_sum(fin);
   lo = warp_min(lo);
   hi = warp_max(hi);
   vm = warp_max(vm);
-  wm = warp_max(wm);
+  double wmd = warp_max((double)wm);
   if ((threadIdx.x & 31) == 0 && cnt) {
     vm = sqrt(vm);  // one square root per warp: the largest |vis| |wgt|
     if (vm > 0.0) atomicMax(&out->vmax_bits, (unsigned long long)__double_as_longlong(vm));
-    if (wm > 0.0) atomicMax(&out->wmax_bits, (unsigned long long)__double_as_longlong(wm));
+    if (wmd > 0.0) atomicMax(&out->wmax_bits, (unsigned long long)__double_as_longlong(wmd));
     atomicAdd(&out->count, cnt);
     if (fin) {
       atomicAdd(&out->finite, fin);
@@ -238,7 +356,7 @@ __device__ __forceinline__ uint32_t bin_of_rc(const Geom<T>& g, const double* __
   double f = foc[ch];
   double u = b[0] * f, v = b[1] * f, w = b[2] * f;
   double uf, vf;
-  int64_t iu0, iv0;
+  int iu0, iv0;
   getpix(g, u, v, uf, vf, iu0, iv0);
   const uint32_t su = (uint32_t)shifted(iu0, g.nu), sv = (uint32_t)shifted(iv0, g.nv);
   const uint32_t tu = su >> g.log2tile, tv = sv >> g.log2tile;
@@ -286,13 +404,15 @@ __device__ __forceinline__ uint32_t warp_aggregated_add(uint32_t* counters, uint
 }
 
 // With rows_per_chunk > 0 the key is chunk * nbins + bin, chunk = row / rows_per_chunk.
-// Capped at 32 registers (eight 256-thread blocks, every warp slot of an SM):
+// With `bits` the active set is the scan's (bit i: visibility i), else each
+// visibility's inputs are read. Capped at 32 registers (eight 256-thread blocks, every warp slot of an SM):
 // the kernel is bound by instruction issue, and the extra warps measured 11 %
 // faster than 36 registers (6 blocks) despite a 4-byte spill.
 template <class T>
 __global__ void __launch_bounds__(256, 8) k_bin_count(const __grid_constant__ Geom<T> g, const double* __restrict__ uvw,
                             const double* __restrict__ foc, Inputs in, int with_vis, uint32_t* __restrict__ key,
-                            uint32_t* __restrict__ counts, uint32_t rows_per_chunk = 0, uint32_t nbins = 0) {
+                            uint32_t* __restrict__ counts, uint32_t rows_per_chunk = 0, uint32_t nbins = 0,
+                            const uint32_t* __restrict__ bits = nullptr) {
   uint64_t n = g.nrow * g.nchan;
   uint64_t nround = (n + 31) & ~31ull;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -301,7 +421,7 @@ __global__ void __launch_bounds__(256, 8) k_bin_count(const __grid_constant__ Ge
     bool act = false;
     uint32_t k = INACTIVE;
     if (i < n) {
-      act = is_active<T>(in, with_vis != 0, i);
+      act = bits ? ((bits[i >> 5] >> (i & 31)) & 1u) != 0 : is_active<T>(in, with_vis != 0, i);
       if (act) {
         k = bin_of_rc(g, uvw, foc, rc.row, rc.ch);
         if (rows_per_chunk) k += (rc.row / rows_per_chunk) * nbins;
@@ -1929,16 +2049,144 @@ DevBuf& DevBuf::operator=(DevBuf&& o) noexcept {
   return *this;
 }
 
+namespace {
+// A released buffer kept for reuse: free once `ready` (recorded on the
+// releasing stream) has passed.
+struct CachedBuf {
+  void* p;
+  size_t bytes;
+  int dev;
+  cudaEvent_t ready;
+};
+std::mutex g_cache_mu;
+std::vector<CachedBuf> g_cache;  // oldest first
+
+constexpr size_t CACHED_MAX = 128;
+
+// The device's memory in bytes (looked up once per device).
+size_t device_bytes(int dev) {
+  static std::mutex mu;
+  static std::map<int, size_t> total;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = total.find(dev);
+  if (it != total.end()) return it->second;
+  size_t f = 0, t = 0;
+  if (cudaMemGetInfo(&f, &t) != cudaSuccess) t = 0;
+  total[dev] = t;
+  return t;
+}
+
+// Returns one cached buffer to the pool, ordered after its release.
+void free_cached(const CachedBuf& b, cudaStream_t s) {
+  cudaStreamWaitEvent(s, b.ready, 0);
+  cudaEventDestroy(b.ready);
+  cudaFreeAsync(b.p, s);
+}
+}  // namespace
+
+size_t cached_free_bytes(int dev) {
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  size_t t = 0;
+  for (const CachedBuf& b : g_cache)
+    if (b.dev == dev) t += b.bytes;
+  return t;
+}
+
+void flush_cache(int dev) {
+  std::vector<CachedBuf> out;
+  {
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    auto keep = std::stable_partition(g_cache.begin(), g_cache.end(), [&](const CachedBuf& b) { return b.dev != dev; });
+    out.assign(keep, g_cache.end());
+    g_cache.erase(keep, g_cache.end());
+  }
+  for (const CachedBuf& b : out) free_cached(b, nullptr);
+  if (!out.empty()) cudaStreamSynchronize(nullptr);  // the pool has them back before a retry
+}
+
 void DevBuf::alloc(size_t bytes, cudaStream_t s) {
   release();
   if (bytes == 0) return;
-  check_cuda(cudaMallocAsync(&p_, bytes, s), "device memory");
+  int dev = 0;
+  check_cuda(cudaGetDevice(&dev), "no CUDA device");
+  if (bytes >= CACHED_MIN) {
+    bool hit = false;
+    CachedBuf b{};
+    {
+      std::lock_guard<std::mutex> lock(g_cache_mu);
+      for (size_t i = g_cache.size(); i-- > 0;)  // the most recent of this size
+        if (g_cache[i].dev == dev && g_cache[i].bytes == bytes) {
+          b = g_cache[i];
+          g_cache.erase(g_cache.begin() + (std::ptrdiff_t)i);
+          hit = true;
+          break;
+        }
+    }
+    if (hit) {
+      const cudaError_t e = cudaStreamWaitEvent(s, b.ready, 0);
+      cudaEventDestroy(b.ready);
+      if (e != cudaSuccess) {
+        cudaFreeAsync(b.p, nullptr);
+        check_cuda(e, "device memory");
+      }
+      p_ = b.p;
+      n_ = bytes;
+      s_ = s;
+      return;
+    }
+  }
+  cudaError_t e = cudaMallocAsync(&p_, bytes, s);
+  if (e == cudaErrorMemoryAllocation && cached_free_bytes(dev) > 0) {
+    cudaGetLastError();
+    flush_cache(dev);
+    e = cudaMallocAsync(&p_, bytes, s);
+  }
+  if (e != cudaSuccess) p_ = nullptr;
+  check_cuda(e, "device memory");
   n_ = bytes;
   s_ = s;
 }
 
 void DevBuf::release() {
-  if (p_) cudaFreeAsync(p_, s_);
+  if (!p_) return;
+  cudaEvent_t ev = nullptr;
+  int dev = 0;
+  if (n_ >= CACHED_MIN && cudaGetDevice(&dev) == cudaSuccess &&
+      cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+    if (cudaEventRecord(ev, s_) == cudaSuccess) {
+      std::vector<CachedBuf> old;
+      {
+        // At most CACHED_MAX buffers and three quarters of the device's
+        // memory per device (a step of two plans holds about 100 GB at 1 G
+        // visibilities); the oldest go back to the pool.
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        g_cache.push_back(CachedBuf{p_, n_, dev, ev});
+        size_t count = 0, bytes = 0;
+        for (const CachedBuf& b : g_cache)
+          if (b.dev == dev) {
+            count++;
+            bytes += b.bytes;
+          }
+        const size_t cap = device_bytes(dev) / 4 * 3;
+        for (size_t i = 0; i < g_cache.size() && (count > CACHED_MAX || bytes > cap);) {
+          if (g_cache[i].dev != dev) {
+            i++;
+            continue;
+          }
+          count--;
+          bytes -= g_cache[i].bytes;
+          old.push_back(g_cache[i]);
+          g_cache.erase(g_cache.begin() + (std::ptrdiff_t)i);
+        }
+      }
+      for (const CachedBuf& b : old) free_cached(b, s_);
+      p_ = nullptr;
+      n_ = 0;
+      return;
+    }
+    cudaEventDestroy(ev);
+  }
+  cudaFreeAsync(p_, s_);
   p_ = nullptr;
   n_ = 0;
 }
@@ -1975,6 +2223,7 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   if (n_ >= 0xffffffffull) throw InvalidArgument("too many visibilities for one call (at most 2^32 - 2)");
   recentring(o, r_l_, r_m_);
   std::vector<double> foc = f_over_c(freq_host, nchan);
+  foc_finite_ = all_finite(foc);
   uvw_.alloc(nrow * 3 * sizeof(double), s);
   foc_.alloc(nchan * sizeof(double), s);
   if (nrow) check_cuda(cudaMemcpyAsync(uvw_.get(), uvw_dev, nrow * 3 * sizeof(double), cudaMemcpyDeviceToDevice, s), "copy uvw");
@@ -1985,11 +2234,16 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   DevBuf so(sizeof(ScanOut), s);
   k_scan_init<<<1, 1, 0, s>>>(so.as<ScanOut>());
   double fw = o.flip_w ? 1.0 : -1.0;
+  // The active set as bits, for the count pass (one bit per visibility).
+  DevBuf bits;
+  if (layout && n_) bits.alloc((n_ + 31) / 32 * 4, s);
   if (n_) {
     {
       StageTimer timer_(ST_SCAN, s);
       k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw_.as<double>(),
-                                                    foc_.as<double>(), fw, act, with_vis ? 1 : 0, so.as<ScanOut>());
+                                                    foc_.as<double>(), fw, act, with_vis ? 1 : 0,
+                                                    scan_vectors(act, with_vis) ? 1 : 0, foc_finite_ ? 1 : 0,
+                                                    so.as<ScanOut>(), bits.as<uint32_t>());
       k_umax<<<blocks_for(nrow, 256, 148u * 8u), 256, 0, s>>>((uint32_t)nrow, uvw_.as<double>(), so.as<ScanOut>());
     }
     check_cuda(cudaGetLastError(), "scan kernel");
@@ -2021,7 +2275,7 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   double umax_d = 0.0;  // metres; times the largest f / c
   std::memcpy(&umax_d, &r.u_bits, sizeof(double));
   urows_ = touched_rows(umax_d * *std::max_element(foc.begin(), foc.end()), wmax_d);
-  if (layout) build_layout(act, with_vis, s);
+  if (layout) build_layout(act, with_vis, bits.as<uint32_t>(), s);
 }
 
 // The grid rows footprints can reach, from the scan's largest |u| and |w|
@@ -2042,7 +2296,7 @@ int Plan<T>::touched_rows(double umax, double wmax) const {
 }
 
 template <class T>
-void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
+void Plan<T>::build_layout(const Inputs& act, bool with_vis, const uint32_t* bits, cudaStream_t s) {
   ntiles_ = (size_t)g_.ntu * g_.ntv;
   nbins_ = ntiles_ * (size_t)g_.nbuckets * (size_t)g_.nsub;
   if (nbins_ >= 0xffffffffull) throw InvalidArgument("too many uv tiles and w-planes for one call");
@@ -2058,13 +2312,14 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, cudaStream_t s) {
     rec_.alloc(n_ * sizeof(fast::VisRecord), s);
     StageTimer timer_(ST_BIN_COUNT, s);
     fast::k_bin_count_rec<<<blocks_for(n_, 256), 256, 0, s>>>(
-        g_, uvw_.as<double>(), foc_.as<double>(), act, with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>(),
+        g_, uvw_.as<double>(), foc_.as<double>(), bits, key_.as<uint32_t>(), starts_.as<uint32_t>(),
         rec_.as<fast::VisRecord>(), K > 1 ? (uint32_t)rows_per_chunk_ : 0u, (uint32_t)nbins_);
   } else {
     StageTimer timer_(ST_BIN_COUNT, s);
     k_bin_count<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act,
                                                         with_vis ? 1 : 0, key_.as<uint32_t>(), starts_.as<uint32_t>(),
-                                                        K > 1 ? (uint32_t)rows_per_chunk_ : 0u, (uint32_t)nbins_);
+                                                        K > 1 ? (uint32_t)rows_per_chunk_ : 0u, (uint32_t)nbins_,
+                                                        bits);
   }
   check_cuda(cudaGetLastError(), "bin count");
   exclusive_scan(starts_.as<uint32_t>(), starts_.as<uint32_t>(), nkeys + 1, s);
@@ -2154,7 +2409,8 @@ bool Plan<T>::same_scan(const Inputs& act, bool with_vis, cudaStream_t s) const 
       StageTimer timer_(ST_SCAN, s);
       k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow_, (uint32_t)nchan_, uvw_.as<double>(),
                                                     foc_.as<double>(), o_.flip_w ? 1.0 : -1.0, act, with_vis ? 1 : 0,
-                                                    so.as<ScanOut>());
+                                                    scan_vectors(act, with_vis) ? 1 : 0, foc_finite_ ? 1 : 0,
+                                                    so.as<ScanOut>(), nullptr);
     }
     check_cuda(cudaGetLastError(), "scan kernel");
   }
@@ -2240,6 +2496,8 @@ size_t Plan<T>::plane_group(size_t plane_bytes, size_t fixed) const {
     budget = budget > fixed ? budget - fixed : 0;
     return std::min(std::max<size_t>(1, budget / plane_bytes), nplanes);
   };
+  int cur = 0;
+  if (cudaGetDevice(&cur) == cudaSuccess) freeb += cached_free_bytes(cur);  // this library's to reuse
   size_t group = group_of(freeb);
   if (group < nplanes) {
     // Memory the stream-ordered pool holds without using it is this
@@ -2836,7 +3094,9 @@ void bin_noalloc(const WgridderOptions& o, size_t nrow, size_t nchan, const doub
   check_cuda(cudaMemcpyAsync(dfoc, foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, s), "copy");
   const double fw = o.flip_w ? 1.0 : -1.0;
   if (n) {
-    k_scan<T><<<blocks_for(n, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw, dfoc, fw, act, 0, so);
+    k_scan<T><<<blocks_for(n, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw, dfoc, fw, act, 0,
+                                                  scan_vectors(act, false) ? 1 : 0, all_finite(foc) ? 1 : 0, so,
+                                                  nullptr);
     check_cuda(cudaGetLastError(), "scan kernel");
   }
   ScanOut r;
