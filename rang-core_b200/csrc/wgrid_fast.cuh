@@ -52,12 +52,13 @@ __device__ __forceinline__ void atomic_max_double(unsigned long long* a, double 
   if (v > 0.0) atomicMax(a, (unsigned long long)__double_as_longlong(v));
 }
 
-// max |vis| |wgt| and max |wgt| over the visibilities the plan keeps
-// (key != INACTIVE), for gridding data other than the plan's own.
+// max |vis| |wgt| and max |wgt| over visibilities [i0, i1) that the plan
+// keeps (key != INACTIVE), for gridding data other than the plan's own.
 template <class T>
-__global__ void k_value_max(uint64_t n, Inputs in, const uint32_t* __restrict__ key, ValueBound* vb) {
+__global__ void k_value_max(uint64_t i0, uint64_t i1, Inputs in, const uint32_t* __restrict__ key, ValueBound* vb) {
   double vm = 0.0, wm = 0.0;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+  for (uint64_t i = i0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < i1;
+       i += (uint64_t)gridDim.x * blockDim.x) {
     if (key[i] == INACTIVE) continue;
     const double w = fabs((double)wgt_get<T>(in, i));
     const double a = value_bound_sq(vis_get<T>(in, i), w);
@@ -93,11 +94,15 @@ __global__ void k_bound_init(ValueBound* vb, unsigned long long vmax_bits, unsig
 // correction factors amplify past double precision's accuracy). The scales
 // depend on nothing but the values and the active count, so a plan split
 // into row chunks grids to the same bits as one without.
-__global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long long nvis, int integer, int wide,
-                            FixScale* fs) {
+// The exponent the scales take from `values`: vmax < 2^(ev + 1) (clamped,
+// so that the scales stay finite floats).
+__device__ __forceinline__ int bound_exponent(const ValueBound* values, int unit) {
   double vmax = __longlong_as_double((long long)(unit ? values->wmax_bits : values->vmax_bits));
   if (!(vmax > 0.0) || !isfinite(vmax)) vmax = 1.0;
-  const int ev = min(max(ilogb(vmax), -90), 90);  // vmax < 2^(ev + 1) (clamped: scales stay finite floats)
+  return min(max(ilogb(vmax), -90), 90);
+}
+
+__device__ __forceinline__ FixScale scale_of(int ev, unsigned long long nvis, int integer, int wide) {
   FixScale r;
   r.nonfinite = 0;
   r.pad = 0;
@@ -109,7 +114,49 @@ __global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long lo
     // nvis * vmax * 2^q < 2^62 (int64 cells), < 2^94 (hi * 2^32 + lo cells)
     r.q = (wide ? 92 : 60) - ev - ilogb((double)max(nvis, 1ull));
   }
-  *fs = r;
+  return r;
+}
+
+__global__ void k_fix_scale(const ValueBound* values, int unit, unsigned long long nvis, int integer, int wide,
+                            FixScale* fs) {
+  *fs = scale_of(bound_exponent(values, unit), nvis, integer, wide);
+}
+
+// Gridding row chunks as they arrive, before the bound of all the values
+// is known: the scale depends on the bound only through its exponent, so
+// the chunks are gridded with the exponent of the values seen so far, and
+// when a chunk changes it, the planes are cleared and the chunks before it
+// gridded again (`redo`, which their launches test). After the last chunk
+// the exponent, and every term, is the one-pass gridding's.
+struct SpecState {
+  int ev;
+  int redo;
+};
+__global__ void k_spec_scale(const ValueBound* values, int first, int unit, unsigned long long nvis, int integer,
+                             int wide, SpecState* st, FixScale* fs) {
+  const int ev = bound_exponent(values, unit);
+  if (first || ev != st->ev) {
+    st->redo = first ? 0 : 1;
+    st->ev = ev;
+    *fs = scale_of(ev, nvis, integer, wide);
+  } else {
+    st->redo = 0;
+  }
+}
+
+// Zeroes n planes' rows as zero_touched does, when *flag is set.
+template <class Cell>
+__global__ void k_zero_touched_if(const int* __restrict__ flag, Cell* __restrict__ grids, int n, int nu, int nv,
+                                  int rows) {
+  if (*flag == 0) return;
+  const uint64_t prow = rows == 0 ? (uint64_t)nu : 2ull * rows;  // rows cleared per plane
+  const uint64_t total = (uint64_t)n * prow * nv;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t p = i / (prow * nv), r = (i / nv) % prow, c = i % nv;
+    const uint64_t row = (rows == 0 || r < (uint64_t)rows) ? r : (uint64_t)nu - 2ull * rows + r;
+    grids[(p * nu + row) * nv + c] = Cell{};
+  }
 }
 
 __device__ __forceinline__ void fix_add(FixCell* cell, long long re, long long im) {
@@ -557,8 +604,10 @@ template <int S>
 __global__ void __launch_bounds__(I8_BATCH, S <= 4 ? 16 : S <= 6 ? 12 : 8)
     k_grid_i8(const __grid_constant__ Geom<float> g, Inputs in, int mode, const VisRecord* __restrict__ rec,
               const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
-              FixCell* __restrict__ grids, int pg0, int npg, FixScale* __restrict__ fs) {
+              FixCell* __restrict__ grids, int pg0, int npg, FixScale* __restrict__ fs,
+              const int* __restrict__ run) {
   static_assert(S >= 1 && S <= 8, "8 x 8 windows");
+  if (run && *run == 0) return;  // a speculative pass's regridding, not needed
   constexpr int NP = (S + 1) / 2;  // plane pairs
   extern __shared__ __align__(16) unsigned char smem[];
   I8Slots st;

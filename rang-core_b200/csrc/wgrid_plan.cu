@@ -1878,7 +1878,7 @@ void launch_grid_bf16(cudaStream_t s, const Geom<float>& g, const Inputs& in, in
 template <int S>
 void launch_grid_i8(cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode, const fast::VisRecord* rec,
                     const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins, fast::FixCell* grids,
-                    int pg0, int npg, fast::FixScale* fs) {
+                    int pg0, int npg, fast::FixScale* fs, const int* run = nullptr) {
   if (kend <= kbase) return;
   const int smem = (int)(fast::I8Slots::bytes() + fast::I8_BATCH * sizeof(fast::Prefetched));
   const unsigned nblocks = (unsigned)((kend - kbase + fast::I8_CHUNK - 1) / fast::I8_CHUNK);
@@ -1886,7 +1886,7 @@ void launch_grid_i8(cudaStream_t s, const Geom<float>& g, const Inputs& in, int 
   {
     StageTimer timer_(ST_GRID, s);
     fast::k_grid_i8<S><<<nblocks, fast::I8_BATCH, smem, s>>>(g, in, mode, rec, sorted, kbase, kend, nbins, grids,
-                                                             pg0, npg, fs);
+                                                             pg0, npg, fs, run);
   }
   check_cuda(cudaGetLastError(), "grid kernel (integer tensor cores)");
 }
@@ -2580,28 +2580,35 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
   const double* corr = corr_.as<double>();
   const size_t nu2 = (size_t)g_.nx / 2 + 1, nv2 = (size_t)g_.ny / 2 + 1;
   const bool integer = sizeof(T) == 4 && grid_method() == GRID_INT8;
-  // The fixed-point scales: from the scan's value maxima when `data` is the
-  // scanned input, else from a pass over `data` (after all of it arrived).
-  if (ready)
-    for (int c = 0; c < nchunk_; c++) check_cuda(cudaStreamWaitEvent(s, ready[c], 0), "wait");
-  const fast::ValueBound* values = bound_.as<fast::ValueBound>();
-  DevBuf vb;
   if (data.vis_kind == VIS_SORTED && !(integer && bound))
     throw DeviceError("stored values need the integer gridder and their bound");
+  const bool own_bound = !bound && !(scanned && bound_of(data, mode));
+  // Row chunks arriving (`ready`) are gridded as they come when the integer
+  // gridder takes all planes at once (k_spec_scale); otherwise the pass
+  // waits for all of them.
+  const bool speculate = ready && integer && own_bound && nchunk_ > 1 && group >= nplanes && g_.supp <= 8;
+  if (ready && !speculate)
+    for (int c = 0; c < nchunk_; c++) check_cuda(cudaStreamWaitEvent(s, ready[c], 0), "wait");
+  // The fixed-point scales: from the scan's value maxima when `data` is the
+  // scanned input, else from a pass over `data`.
+  const fast::ValueBound* values = bound_.as<fast::ValueBound>();
+  DevBuf vb, spec;
   if (bound) {
     values = static_cast<const fast::ValueBound*>(bound);
-  } else if (!(scanned && bound_of(data, mode))) {
+  } else if (own_bound) {
     vb.alloc(sizeof(fast::ValueBound), s);
     check_cuda(cudaMemsetAsync(vb.get(), 0, sizeof(fast::ValueBound), s), "memset");
-    {
+    if (!speculate) {
       StageTimer timer_(ST_OTHER, s);
-      fast::k_value_max<T><<<blocks_for(n_, 256, 148u * 8u), 256, 0, s>>>(n_, data, key_.as<uint32_t>(),
+      fast::k_value_max<T><<<blocks_for(n_, 256, 148u * 8u), 256, 0, s>>>(0, n_, data, key_.as<uint32_t>(),
                                                                          vb.as<fast::ValueBound>());
     }
     check_cuda(cudaGetLastError(), "value bound");
     values = vb.as<fast::ValueBound>();
   }
-  {
+  if (speculate) {
+    spec.alloc(sizeof(fast::SpecState), s);
+  } else {
     StageTimer timer_(ST_OTHER, s);
     fast::k_fix_scale<<<1, 1, 0, s>>>(values, mode == VALUE_UNIT ? 1 : 0, (unsigned long long)nvis_, integer ? 1 : 0,
                                       fast::FixTraits<T>::wide, scale_.as<fast::FixScale>());
@@ -2618,6 +2625,33 @@ void Plan<T>::grid(const Inputs& data, ValueMode mode, T* image, cudaStream_t s,
       for (int c = 0; c < nchunk_; c++) {
         if constexpr (sizeof(T) == 4) {
           const uint64_t k0 = chunk_sorted_[c], k1 = chunk_sorted_[c + 1];
+          if (speculate) {
+            if constexpr (SV <= 8) {
+              check_cuda(cudaStreamWaitEvent(s, ready[c], 0), "wait");
+              fast::SpecState* st = spec.as<fast::SpecState>();
+              {
+                StageTimer timer_(ST_OTHER, s);
+                fast::k_value_max<T><<<blocks_for(n_ / nchunk_ + 1, 256, 148u * 8u), 256, 0, s>>>(
+                    (uint64_t)row_begin(c) * nchan_, (uint64_t)row_begin(c + 1) * nchan_, data, key_.as<uint32_t>(),
+                    vb.as<fast::ValueBound>());
+                fast::k_spec_scale<<<1, 1, 0, s>>>(vb.as<fast::ValueBound>(), c == 0 ? 1 : 0,
+                                                   mode == VALUE_UNIT ? 1 : 0, (unsigned long long)nvis_, 1,
+                                                   fast::FixTraits<T>::wide, st, fs);
+              }
+              check_cuda(cudaGetLastError(), "scale");
+              if (c > 0) {
+                fast::k_zero_touched_if<FixCell><<<148u * 8u, 256, 0, s>>>(&st->redo, fg, n, g_.nu, g_.nv, rows);
+                check_cuda(cudaGetLastError(), "zero");
+                for (int j = 0; j < c; j++)
+                  launch_grid_i8<SV>(s, g_, data, (int)mode, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(),
+                                     chunk_sorted_[j], chunk_sorted_[j + 1], (uint32_t)nbins_, fg, (int)pg0, n, fs,
+                                     &st->redo);
+              }
+              launch_grid_i8<SV>(s, g_, data, (int)mode, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(), k0, k1,
+                                 (uint32_t)nbins_, fg, (int)pg0, n, fs);
+            }
+            continue;
+          }
           if (integer) {
             if constexpr (SV <= 8)
               launch_grid_i8<SV>(s, g_, data, (int)mode, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(), k0, k1,

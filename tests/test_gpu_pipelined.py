@@ -94,3 +94,31 @@ def test_chunked_vis2dirty_with_zero_visibilities_falls_back(chunks, single):
     assert info == oinfo
     oref = oracle.vis2dirty(vis=vis, wgt=wgt, mask=mask, **kw)
     assert rel_linf(out, oref) < TOL[single]
+
+
+@pytest.mark.parametrize("k", [3, 7])
+@pytest.mark.parametrize("change", ["later chunk larger", "first rows flagged", "later chunk smaller"])
+def test_chunked_vis2dirty_regrids_when_the_bound_changes(chunks, k, change):
+    """The chunked gridder grids each row chunk as it arrives, with the
+    fixed-point scale of the values seen so far (the scale depends on their
+    bound only through its exponent). A chunk that changes the exponent makes
+    it clear the planes and grid the chunks before it again, so the image
+    still equals the one-pass gridding's bit for bit."""
+    from rang import gridder as cw
+
+    vis, wgt, mask, kw = _case(True, seed=8)
+    nrow = vis.shape[0]
+    if change == "later chunk larger":
+        vis[nrow * 2 // 3:] *= np.float32(1000.0)
+    elif change == "first rows flagged":
+        mask[: nrow // 2] = 0
+    else:
+        vis[nrow // 3:] *= np.float32(1e-4)
+    chunks(1)
+    ref, info1 = cw.vis2dirty(vis=vis, wgt=wgt, mask=mask, return_info=True, **kw)
+    chunks(k)
+    out, info2 = cw.vis2dirty(vis=vis, wgt=wgt, mask=mask, return_info=True, **kw)
+    assert info1 == info2
+    assert np.array_equal(out.view(np.uint8), ref.view(np.uint8))
+    oref = oracle.vis2dirty(vis=vis, wgt=wgt, mask=mask, **kw)
+    assert rel_linf(out, oref) < TOL[True]
