@@ -35,6 +35,7 @@
 #include <memory>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 
 #include "wgrid_plan.h"
 
@@ -1875,6 +1876,32 @@ void launch_grid_bf16(cudaStream_t s, const Geom<float>& g, const Inputs& in, in
   check_cuda(cudaGetLastError(), "grid kernel (tensor cores, 3 x BF16)");
 }
 
+// The record count pass for the plan's w-planes, shift and row chunks.
+void launch_count_rec(const Geom<float>& g, const double* uvw, const double* foc, const uint32_t* bits, uint32_t* key,
+                      uint32_t* counts, fast::VisRecord* rec, uint32_t rows_per_chunk, uint32_t nbins, uint64_t n,
+                      cudaStream_t s) {
+  auto go = [&](auto wpl, auto shift, auto chunked) {
+    fast::k_bin_count_rec<decltype(wpl)::value, decltype(shift)::value, decltype(chunked)::value>
+        <<<blocks_for(n, 256), 256, 0, s>>>(g, uvw, foc, bits, key, counts, rec, rows_per_chunk, nbins);
+  };
+  using T_ = std::true_type;
+  using F_ = std::false_type;
+  const bool w = g.do_wgridding != 0, sh = g.shifting != 0, ch = rows_per_chunk != 0;
+  if (w) {
+    if (sh) {
+      if (ch) go(T_{}, T_{}, T_{}); else go(T_{}, T_{}, F_{});
+    } else {
+      if (ch) go(T_{}, F_{}, T_{}); else go(T_{}, F_{}, F_{});
+    }
+  } else {
+    if (sh) {
+      if (ch) go(F_{}, T_{}, T_{}); else go(F_{}, T_{}, F_{});
+    } else {
+      if (ch) go(F_{}, F_{}, T_{}); else go(F_{}, F_{}, F_{});
+    }
+  }
+}
+
 template <int S>
 void launch_grid_i8(cudaStream_t s, const Geom<float>& g, const Inputs& in, int mode, const fast::VisRecord* rec,
                     const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins, fast::FixCell* grids,
@@ -2311,9 +2338,8 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, const uint32_t* bit
   if constexpr (sizeof(T) == 4) {  // with the records of the tensor-core kernels
     rec_.alloc(n_ * sizeof(fast::VisRecord), s);
     StageTimer timer_(ST_BIN_COUNT, s);
-    fast::k_bin_count_rec<<<blocks_for(n_, 256), 256, 0, s>>>(
-        g_, uvw_.as<double>(), foc_.as<double>(), bits, key_.as<uint32_t>(), starts_.as<uint32_t>(),
-        rec_.as<fast::VisRecord>(), K > 1 ? (uint32_t)rows_per_chunk_ : 0u, (uint32_t)nbins_);
+    launch_count_rec(g_, uvw_.as<double>(), foc_.as<double>(), bits, key_.as<uint32_t>(), starts_.as<uint32_t>(),
+                     rec_.as<fast::VisRecord>(), K > 1 ? (uint32_t)rows_per_chunk_ : 0u, (uint32_t)nbins_, n_, s);
   } else {
     StageTimer timer_(ST_BIN_COUNT, s);
     k_bin_count<T><<<blocks_for(n_, 256), 256, 0, s>>>(g_, uvw_.as<double>(), foc_.as<double>(), act,
