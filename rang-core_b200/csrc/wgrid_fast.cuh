@@ -865,8 +865,10 @@ struct DegridOut {
 // the partial sums accumulate in `vis` and the final factor is applied with
 // the last group. The next round's records are copied while the current
 // round is contracted. `out` says where the results go (DegridOut). Up to
-// support 6, 24 warps per SM (80 registers, a 32-byte spill) measured 4 %
-// faster than 16 (122 registers) and 20 (96).
+// support 6, 24 warps per SM (80 registers) measured 4 % faster than 16 (122
+// registers) and 20 (96), and as fast as 28. The w contraction before the u
+// taps and one output lane per record (two lanes of each quad) measured 10 %
+// faster than u first and one lane writing both records.
 template <int S>
 __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 24 : 12)
     k_degrid_h(const __grid_constant__ Geom<float> g, Inputs wts, const VisRecord* __restrict__ rec,
@@ -1007,7 +1009,9 @@ __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 24 : 12)
           kwv[h][6] = w1.z;
           kwv[h][7] = w1.w;
         }
-        float tr[2] = {0.0f, 0.0f}, ti[2] = {0.0f, 0.0f};
+        // The w contraction first (per window row, over the planes), then the
+        // u taps: two FMAs per plane and output instead of three.
+        float wr[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}}, wi[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
 #pragma unroll
         for (int p = 0; p < S; p++) {
           float dre[4], dim[4];
@@ -1019,10 +1023,18 @@ __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 24 : 12)
           hmma(dim, alo[0], alo[1], bhi[p][1]);
           // d[0], d[1]: record gq, window rows 2tq, 2tq + 1; d[2], d[3]: record gq + 8
 #pragma unroll
-          for (int h = 0; h < 2; h++) {
-            tr[h] = fmaf(kwv[h][p], fmaf(kup[h].x, dre[2 * h], kup[h].y * dre[2 * h + 1]), tr[h]);
-            ti[h] = fmaf(kwv[h][p], fmaf(kup[h].x, dim[2 * h], kup[h].y * dim[2 * h + 1]), ti[h]);
-          }
+          for (int h = 0; h < 2; h++)
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+              wr[h][c] = fmaf(kwv[h][p], dre[2 * h + c], wr[h][c]);
+              wi[h][c] = fmaf(kwv[h][p], dim[2 * h + c], wi[h][c]);
+            }
+        }
+        float tr[2], ti[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          tr[h] = fmaf(kup[h].x, wr[h][0], kup[h].y * wr[h][1]);
+          ti[h] = fmaf(kup[h].x, wi[h][0], kup[h].y * wi[h][1]);
         }
 #pragma unroll
         for (int h = 0; h < 2; h++)
@@ -1031,15 +1043,15 @@ __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 24 : 12)
             tr[h] += __shfl_xor_sync(0xffffffffu, tr[h], o);
             ti[h] += __shfl_xor_sync(0xffffffffu, ti[h], o);
           }
-        if (tq == 0) {
-#pragma unroll
-          for (int h = 0; h < 2; h++) {
-            if (sr[h] == H16_BATCH) continue;
-            const float4 fo = st.out[sr[h]];
+        // Every lane of a quad holds both records' sums: lane tq = h writes record h.
+        const int slot = tq ? sr[1] : sr[0];
+        if (tq < 2 && slot != H16_BATCH) {
+          {
+            const float4 fo = st.out[slot];
             const uint32_t idx = __float_as_uint(fo.w);
-            const uint64_t k = kb + (uint64_t)sr[h];
+            const uint64_t k = kb + (uint64_t)slot;
             cplx<float>* dst = out.mode == DEGRID_TO_VIS ? out.vis + idx : out.stored + k;
-            cplx<float> accv{tr[h] * inv, ti[h] * inv * fo.z};
+            cplx<float> accv{(tq ? tr[1] : tr[0]) * inv, (tq ? ti[1] : ti[0]) * inv * fo.z};
             if (!first) {
               const cplx<float> prev = *dst;
               accv = {accv.re + prev.re, accv.im + prev.im};
