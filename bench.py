@@ -63,8 +63,8 @@ PROFILE_CASE = "ms2dirty+dirty2ms 132M vis 2048^2"
 # launch): a launch of another workload is scaled by its active visibilities.
 # A profiler figure, not something this script can time.
 DRAM_CAPTURE = {
-    "k_grid_i8": (7.865368e9 + 0.639403e9, 105697663),
-    "k_degrid_h": (6.765928e9 + 1.254083e9, 105697663),
+    "k_grid_i8": (7.865198e9 + 0.640229e9, 105697663),
+    "k_degrid_h": (6.992914e9 + 1.269871e9, 105697663),
 }
 METRIC = "Mvis/s ms2dirty+dirty2ms @eps=1e-5 vs FP64"
 UNIT = "Mvis/s"
