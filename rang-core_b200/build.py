@@ -33,8 +33,8 @@ LIB = PKG / "librang_wgrid_b200.so"
 CU_SOURCES = ["wgrid_plan.cu", "wgrid_capi.cu", "wgrid_weights.cu", "wgrid_gram.cu", "wgrid_solver.cu", "nn_kernels.cu",
               "nn_conv_tc.cu"]
 CXX_SOURCES = ["wgrid_setup.cpp", "msv4_codec.cpp"]
-HEADERS = ["wgrid_common.h", "wgrid_device.cuh", "wgrid_fast.cuh", "wgrid_plan.h", "wgrid_setup.h", "kernel_db.inc",
-           "nn_conv_tc.h"]
+HEADERS = ["wgrid_common.h", "wgrid_device.cuh", "wgrid_fast.cuh", "wgrid_f64.cuh", "wgrid_plan.h", "wgrid_setup.h",
+           "kernel_db.inc", "nn_conv_tc.h"]
 
 
 def ext_path():
