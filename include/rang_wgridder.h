@@ -189,6 +189,17 @@ const char* rang_b200_wgridder_plan_memory_name(int32_t index);
 /* Prepared::release_grids (wgridder.rs:3432-3440): frees the stored values
  * that residual and Gram passes keep; the next pass allocates them again. */
 void rang_b200_wgridder_plan_release_work(RangWgridPlan* plan);
+/* No counterpart in the reference (whose buffers are host memory freed at
+ * the end of each call). The library keeps released device buffers of 64 MB
+ * or more for the next request of the same size, so that repeated calls of
+ * one shape allocate nothing; the device memory they hold (and what the
+ * stream-ordered pool keeps) is not available to other allocators in the
+ * process, such as PyTorch's. rang_b200_wgridder_cached_bytes reports the
+ * bytes held on the current device; rang_b200_wgridder_release_cached
+ * returns them, and the pool's unused memory, to the device (status 0, 2 on
+ * a CUDA error), after the work already queued that uses them. */
+size_t rang_b200_wgridder_cached_bytes(void);
+int32_t rang_b200_wgridder_release_cached(void);
 /* `plan` and `gridding_footprint` (wgridder.rs:3527-3588) on HOST arrays:
  * the kernel and grid a call would choose (info, 14 doubles; the activity as
  * for rang_b200_wgridder_binning, with_vis when vis_kind is not 0), without

@@ -377,6 +377,8 @@ PYBIND11_MODULE(_core, m) {
       out.append(py::make_tuple(std::string(rang_b200_wgridder_plan_memory_name(i)), b[i]));
     return out;
   });
+  m.def("wgridder_cached_bytes", []() { return rang_b200_wgridder_cached_bytes(); });
+  m.def("wgridder_release_cached", []() { return rang_b200_wgridder_release_cached(); });
   m.def("wgridder_plan_release_work",
         [](uintptr_t plan) { rang_b200_wgridder_plan_release_work(reinterpret_cast<RangWgridPlan*>(plan)); });
   m.def("wgridder_plan_only", [](std::vector<double> opts, py::object uvw, py::object freq, py::object vis,

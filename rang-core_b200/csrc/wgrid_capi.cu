@@ -624,6 +624,23 @@ void rang_b200_wgridder_plan_release_work(RangWgridPlan* plan) {
     plan->d->release_work();
 }
 
+size_t rang_b200_wgridder_cached_bytes(void) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  return cached_free_bytes(dev);
+}
+
+int32_t rang_b200_wgridder_release_cached(void) {
+  return guarded([&] {
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "no CUDA device");
+    flush_cache(dev);  // frees in stream order and waits for those frees
+    cudaMemPool_t pool;
+    check_cuda(cudaDeviceGetDefaultMemPool(&pool, dev), "memory pool");
+    check_cuda(cudaMemPoolTrimTo(pool, 0), "memory pool");
+  });
+}
+
 int32_t rang_b200_wgridder_plan_only(const WgridderOptions* opts, size_t nrow, size_t nchan, const double* uvw,
                                      const double* freq, const void* vis, int32_t vis_kind, const void* wgt,
                                      const void* wgt2, int32_t wgt_kind, const uint8_t* mask, int32_t single,

@@ -259,3 +259,29 @@ def test_residual_and_gram_of_a_plan_with_nothing_active(single):
     assert float(g.abs().max()) == 0.0 and float(xgx) == 0.0
     assert plan.memory()["gridder: stored sorted values"] == 0
     plan.close()
+
+
+def test_cached_buffers_are_reused_and_released():
+    """Buffers of 64 MB or more stay cached for the next call of the same
+    shape (no allocation then), and release_cached gives them back to the
+    device, so that other allocators in the process can use the memory."""
+    import torch
+
+    from rang import core, gridder as cw
+
+    ext = core.extension()
+    uvw, freq = meerkat_like(nant=64, ntime=16, nchan=64, seed=3)  # 2 M visibilities: 64 MB of records
+    rng = np.random.default_rng(3)
+    vis = (rng.standard_normal((uvw.shape[0], freq.size)) + 1j).astype(np.complex64)
+    kw = dict(uvw=uvw, freq=freq, npix_x=256, npix_y=256, pixsize_x=3e-5, pixsize_y=3e-5, epsilon=1e-5)
+    first = cw.vis2dirty(vis=vis, **kw)
+    held = ext.wgridder_cached_bytes()
+    assert held >= 64 << 20
+    again = cw.vis2dirty(vis=vis, **kw)
+    assert np.array_equal(first, again)
+    assert ext.wgridder_cached_bytes() == held  # the same buffers, taken and returned
+    free_before, _ = torch.cuda.mem_get_info(0)
+    assert ext.wgridder_release_cached() == 0
+    assert ext.wgridder_cached_bytes() == 0
+    free_after, _ = torch.cuda.mem_get_info(0)
+    assert free_after >= free_before + held
