@@ -295,7 +295,10 @@ void host_dirty2vis(const WgridderOptions* o, size_t nrow, size_t nchan, const d
   size_t n = nrow * nchan, npix = o->nx * o->ny;
   cudaStream_t s = call_stream();
   Uploaded u = upload_inputs(nrow, nchan, uvw, nullptr, VIS_UNIT, wgt, nullptr, wgt_kind, mask, s);
-  Plan<T> plan(*o, nrow, nchan, u.uvw.as<double>(), freq, u.in, false, s, host_row_chunks(n * 2 * sizeof(T)));
+  // Row chunks are binned one at a time, each just before it is degridded.
+  const int chunks = host_row_chunks(n * 2 * sizeof(T));
+  Plan<T> plan(*o, nrow, nchan, u.uvw.as<double>(), freq, u.in, false, s, chunks,
+               chunks > 1 ? Plan<T>::LAYOUT_STREAMED : Plan<T>::LAYOUT_FULL);
   std::memcpy(info, plan.info().v, sizeof(plan.info().v));
   if (plan.empty()) {
     std::memset(vis, 0, n * 2 * sizeof(T));
@@ -312,7 +315,7 @@ void host_dirty2vis(const WgridderOptions* o, size_t nrow, size_t nchan, const d
   // Each row chunk's visibilities go back while the next chunk is degridded.
   cudaStream_t sc = copy_stream();
   Events done(plan.chunks());
-  plan.degrid(img.as<T>(), u.in, out.as<T>(), s, done.e.data());
+  plan.degrid_streamed(img.as<T>(), u.in, out.as<T>(), s, done.e.data());
   const size_t rowb = nchan * 2 * sizeof(T);
   for (int c = 0; c < plan.chunks(); c++) {
     const size_t r0 = plan.row_begin(c), r1 = plan.row_begin(c + 1);

@@ -294,13 +294,13 @@ __global__ void __launch_bounds__(256, COUNT_BLOCKS)
     k_bin_count_rec(const __grid_constant__ Geom<float> g, const double* __restrict__ uvw,
                     const double* __restrict__ foc, const uint32_t* __restrict__ bits, uint32_t* __restrict__ key,
                     uint32_t* __restrict__ counts, VisRecord* __restrict__ rec, uint32_t rows_per_chunk,
-                    uint32_t nbins) {
-  const uint64_t n = g.nrow * g.nchan;
-  const uint64_t nround = (n + 31) & ~31ull;
+                    uint32_t nbins, uint64_t i0, uint64_t n, uint32_t koff) {
+  // Visibilities [i0, n); bin k is counted in counts[k - koff].
+  const uint64_t nround = i0 + ((n - i0 + 31) & ~31ull);
   const uint32_t tmask = (1u << g.log2tile) - 1u;
   const uint32_t se = (uint32_t)g.sube, sdiv = (65536u + se - 1u) / se;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  uint64_t i = i0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   RowCh rc(i, (uint32_t)g.nchan, stride);
   CountIn cur = i < n ? count_in(bits, uvw, foc, i, rc.row, rc.ch) : CountIn{};
   for (; i < nround; i += stride) {
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(256, COUNT_BLOCKS)
       }
       key[i] = k;
     }
-    warp_aggregated_count(counts, k, act);
+    warp_aggregated_count(counts, k - koff, act);
     cur = nxt;
     rc = nrc;
   }
@@ -874,8 +874,13 @@ __global__ void __launch_bounds__(H16_BATCH, S <= 6 ? 24 : 12)
     k_degrid_h(const __grid_constant__ Geom<float> g, Inputs wts, const VisRecord* __restrict__ rec,
                const uint32_t* __restrict__ sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
                const cplx<float>* __restrict__ grids, int pg0, int npg, const __grid_constant__ DegridOut out,
-               int first, int last) {
+               int first, int last, const uint32_t* __restrict__ kb_ptr, const uint32_t* __restrict__ ke_ptr) {
   static_assert(S >= 1 && S <= 8, "8 x 8 windows");
+  if (kb_ptr) {  // a range the device computed: the grid covers its largest size
+    kbase = *kb_ptr;
+    kend = *ke_ptr;
+    if (kbase + (uint64_t)blockIdx.x * H16_CHUNK >= kend) return;
+  }
   extern __shared__ __align__(16) unsigned char smem[];
   H16Slots st;
   st.carve(smem);

@@ -442,12 +442,13 @@ __global__ void k_iota(uint64_t n, uint32_t* __restrict__ out) {
 // Each thread takes four indices a grid-stride apart per round, so that four
 // independent atomics (each returning its run's base) are in flight at once:
 // the kernel is bound by their latency. The order within a bin is free.
+// Visibilities [i0, n); bin k's cursor is cursor[k - koff].
 __global__ void k_bin_scatter(uint64_t n, const uint32_t* __restrict__ key, uint32_t* __restrict__ cursor,
-                              uint32_t* __restrict__ sorted) {
+                              uint32_t* __restrict__ sorted, uint64_t i0 = 0, uint32_t koff = 0) {
   constexpr int U = 4;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32: warps stay aligned
-  const uint64_t nround = (n + 31) & ~31ull;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nround; i += U * stride) {
+  const uint64_t nround = i0 + ((n - i0 + 31) & ~31ull);
+  for (uint64_t i = i0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nround; i += U * stride) {
     uint32_t k[U], pos[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
@@ -455,7 +456,7 @@ __global__ void k_bin_scatter(uint64_t n, const uint32_t* __restrict__ key, uint
       k[u] = j < n ? key[j] : INACTIVE;
     }
 #pragma unroll
-    for (int u = 0; u < U; u++) pos[u] = warp_aggregated_add(cursor, k[u], k[u] != INACTIVE);
+    for (int u = 0; u < U; u++) pos[u] = warp_aggregated_add(cursor, k[u] - koff, k[u] != INACTIVE);
 #pragma unroll
     for (int u = 0; u < U; u++)
       if (k[u] != INACTIVE) sorted[pos[u]] = (uint32_t)(i + u * stride);
@@ -535,6 +536,17 @@ void exclusive_scan(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t 
       k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, sums.as<uint32_t>());
     }
     check_cuda(cudaGetLastError(), "scan");
+  }
+}
+
+// a[i] += base[c] for i < n, and base[c + 1] = the new a[n - 1]: one row
+// chunk's bin offsets after the earlier chunks' visibilities.
+__global__ void k_add_base(uint32_t* __restrict__ a, uint64_t n, uint32_t* __restrict__ base, int c) {
+  const uint32_t b = base[c];
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = a[i] + b;
+    a[i] = v;
+    if (i == n - 1) base[c + 1] = v;
   }
 }
 
@@ -1879,10 +1891,11 @@ void launch_grid_bf16(cudaStream_t s, const Geom<float>& g, const Inputs& in, in
 // The record count pass for the plan's w-planes, shift and row chunks.
 void launch_count_rec(const Geom<float>& g, const double* uvw, const double* foc, const uint32_t* bits, uint32_t* key,
                       uint32_t* counts, fast::VisRecord* rec, uint32_t rows_per_chunk, uint32_t nbins, uint64_t n,
-                      cudaStream_t s) {
+                      cudaStream_t s, uint64_t i0 = 0, uint32_t koff = 0) {
   auto go = [&](auto wpl, auto shift, auto chunked) {
     fast::k_bin_count_rec<decltype(wpl)::value, decltype(shift)::value, decltype(chunked)::value>
-        <<<blocks_for(n, 256), 256, 0, s>>>(g, uvw, foc, bits, key, counts, rec, rows_per_chunk, nbins);
+        <<<blocks_for(n - i0, 256), 256, 0, s>>>(g, uvw, foc, bits, key, counts, rec, rows_per_chunk, nbins, i0, n,
+                                                 koff);
   };
   using T_ = std::true_type;
   using F_ = std::false_type;
@@ -1936,7 +1949,10 @@ void launch_grid_f64(cudaStream_t s, const Geom<double>& g, const Inputs& in, in
 template <int S>
 void launch_degrid_h(cudaStream_t s, const Geom<float>& g, const Inputs& wts, const fast::VisRecord* rec,
                      const uint32_t* sorted, uint64_t kbase, uint64_t kend, uint32_t nbins,
-                     const cplx<float>* grids, int pg0, int npg, const fast::DegridOut& out, int first, int last) {
+                     const cplx<float>* grids, int pg0, int npg, const fast::DegridOut& out, int first, int last,
+                     const uint32_t* kb_ptr = nullptr, const uint32_t* ke_ptr = nullptr) {
+  // With kb_ptr / ke_ptr the range is read on the device; [kbase, kend)
+  // then only bounds its size (the grid covers kend - kbase records).
   if (kend <= kbase) return;
   const int smem = (int)(fast::H16Slots::bytes() + fast::H16_BATCH * sizeof(fast::Prefetched));
   const unsigned nblocks = (unsigned)((kend - kbase + fast::H16_CHUNK - 1) / fast::H16_CHUNK);
@@ -1944,7 +1960,7 @@ void launch_degrid_h(cudaStream_t s, const Geom<float>& g, const Inputs& wts, co
   {
     StageTimer timer_(ST_DEGRID, s);
     fast::k_degrid_h<S><<<nblocks, fast::H16_BATCH, smem, s>>>(g, wts, rec, sorted, kbase, kend, nbins, grids, pg0,
-                                                               npg, out, first, last);
+                                                               npg, out, first, last, kb_ptr, ke_ptr);
   }
   check_cuda(cudaGetLastError(), "degrid kernel (tensor cores)");
 }
@@ -2242,7 +2258,7 @@ int max_window_planes(int L, size_t cell_bytes) {
 
 template <class T>
 Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw_dev, const double* freq_host,
-              const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks, bool layout)
+              const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks, int layout)
     : o_(o), nrow_(nrow), nchan_(nchan), n_(nrow * nchan) {
   rows_per_chunk_ = chunk_rows(nrow, row_chunks);
   nchunk_ = (int)((std::max<size_t>(nrow, 1) + rows_per_chunk_ - 1) / rows_per_chunk_);
@@ -2302,7 +2318,11 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   double umax_d = 0.0;  // metres; times the largest f / c
   std::memcpy(&umax_d, &r.u_bits, sizeof(double));
   urows_ = touched_rows(umax_d * *std::max_element(foc.begin(), foc.end()), wmax_d);
-  if (layout) build_layout(act, with_vis, bits.as<uint32_t>(), s);
+  if (layout == LAYOUT_FULL) build_layout(act, with_vis, bits.as<uint32_t>(), s);
+  if (layout == LAYOUT_STREAMED) {
+    bits_ = std::move(bits);
+    streamed_ = true;
+  }
 }
 
 // The grid rows footprints can reach, from the scan's largest |u| and |w|
@@ -2746,10 +2766,81 @@ void Plan<T>::degrid(const T* image, const Inputs& wts, T* vis, cudaStream_t s, 
 }
 
 template <class T>
+void Plan<T>::degrid_streamed(const T* image, const Inputs& wts, T* vis, cudaStream_t s, cudaEvent_t* done) {
+  if (!streamed_) throw InvalidArgument("this plan was not made for a streamed degridding");
+  degrid_to(image, wts, vis, nullptr, s, done);
+  // The streamed binning serves this pass only (its chunk offsets stay on
+  // the device): the layout goes, and later passes report its absence.
+  key_.release();
+  starts_.release();
+  sorted_.release();
+  rec_.release();
+}
+
+template <class T>
 void Plan<T>::degrid_to(const T* image, const Inputs& wts, T* vis, const void* fused, cudaStream_t s,
                         cudaEvent_t* done) {
   if (vis) check_cuda(cudaMemsetAsync(vis, 0, n_ * 2 * sizeof(T), s), "memset");
+  // A LAYOUT_STREAMED plan: bin each row chunk just before degridding it
+  // when the tensor-core degridder takes all planes at once, else bin now.
+  bool stream_bins = false;
+  if (streamed_ && nvis_ > 0) {
+    streamed_ = false;
+    const size_t nb = (size_t)g_.ntu * g_.ntv * (size_t)g_.nbuckets * (size_t)g_.nsub;
+    const size_t np = (size_t)std::max(g_.nplanes, 1), pl = (size_t)g_.nu * g_.nv;
+    const size_t npx = (size_t)o_.nx * o_.ny, tpl = (size_t)g_.ny * g_.nu;
+    stream_bins = sizeof(T) == 4 && !fused && g_.supp <= 8 && nchunk_ > 1 &&
+                  (size_t)nchunk_ * nb < 0xffffffffull &&
+                  plane_group(pl * sizeof(cplx<T>), tpl * sizeof(cplx<T>) + npx * sizeof(T)) >= np;
+    if (stream_bins) {
+      ntiles_ = (size_t)g_.ntu * g_.ntv;
+      nbins_ = nb;
+      key_.alloc(n_ * 4, s);
+      rec_.alloc(n_ * sizeof(fast::VisRecord), s);
+      starts_.alloc(((size_t)nchunk_ * nbins_ + 1) * 4, s);
+      sorted_.alloc(nvis_ * 4, s);
+      corrections(s);
+    } else {
+      build_layout(scan_in_, scan_vis_, bits_.as<uint32_t>(), s);
+    }
+  }
   if (nvis_ > 0 && !sorted_.get()) throw InvalidArgument("this plan was made without the visibility layout");
+  DevBuf counts, cursor, base;  // the streamed binning's scratch
+  if (stream_bins) {
+    counts.alloc((nbins_ + 1) * 4, s);
+    cursor.alloc(nbins_ * 4, s);
+    base.alloc(((size_t)nchunk_ + 1) * 4, s);
+    check_cuda(cudaMemsetAsync(base.get(), 0, ((size_t)nchunk_ + 1) * 4, s), "memset");
+  }
+  // Row chunk c's binning: its counts, its offsets after the earlier chunks'
+  // (base), its placement; the keys are the full plan's (chunk-major).
+  auto bin_chunk = [&](int c) {
+    const uint64_t i0 = (uint64_t)row_begin(c) * nchan_, i1 = (uint64_t)row_begin(c + 1) * nchan_;
+    const uint32_t koff = (uint32_t)((size_t)c * nbins_);
+    uint32_t* st = starts_.as<uint32_t>() + (size_t)c * nbins_;
+    check_cuda(cudaMemsetAsync(counts.get(), 0, (nbins_ + 1) * 4, s), "memset");
+    {
+      StageTimer timer_(ST_BIN_COUNT, s);
+      if constexpr (sizeof(T) == 4)
+        launch_count_rec(g_, uvw_.as<double>(), foc_.as<double>(), bits_.as<uint32_t>(), key_.as<uint32_t>(),
+                         counts.as<uint32_t>(), rec_.as<fast::VisRecord>(), (uint32_t)rows_per_chunk_,
+                         (uint32_t)nbins_, i1, s, i0, koff);
+    }
+    check_cuda(cudaGetLastError(), "bin count");
+    exclusive_scan(counts.as<uint32_t>(), st, nbins_ + 1, s);
+    {
+      StageTimer timer_(ST_PREFIX, s);
+      k_add_base<<<blocks_for(nbins_ + 1, 256), 256, 0, s>>>(st, nbins_ + 1, base.as<uint32_t>(), c);
+    }
+    check_cuda(cudaGetLastError(), "offsets");
+    check_cuda(cudaMemcpyAsync(cursor.get(), st, nbins_ * 4, cudaMemcpyDeviceToDevice, s), "copy");
+    {
+      StageTimer timer_(ST_BIN_SCATTER, s);
+      k_bin_scatter<<<blocks_for(i1 - i0, 256), 256, 0, s>>>(i1, key_.as<uint32_t>(), cursor.as<uint32_t>(),
+                                                              sorted_.as<uint32_t>(), i0, koff);
+    }
+    check_cuda(cudaGetLastError(), "bin scatter");
+  };
   if (nvis_ == 0) {
     if (done)
       for (int c = 0; c < nchunk_; c++) check_cuda(cudaEventRecord(done[c], s), "record");
@@ -2819,10 +2910,19 @@ void Plan<T>::degrid_to(const T* image, const Inputs& wts, T* vis, const void* f
           } else {
             out.vis = reinterpret_cast<cplx<float>*>(vis);
           }
-          launch_degrid_h<SV>(s, g_, wts, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(), chunk_sorted_[c],
-                              chunk_sorted_[c + 1], (uint32_t)nbins_,
-                              reinterpret_cast<const cplx<float>*>(grids.as<cplx<T>>()), (int)pg0, n, out, first,
-                              last);
+          if (stream_bins) {  // the chunk's sorted range is on the device: at most its rows' visibilities
+            if (pg0 == 0) bin_chunk(c);
+            const uint32_t* st = starts_.as<uint32_t>() + (size_t)c * nbins_;
+            launch_degrid_h<SV>(s, g_, wts, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(), 0,
+                                (uint64_t)(row_begin(c + 1) - row_begin(c)) * nchan_, (uint32_t)nbins_,
+                                reinterpret_cast<const cplx<float>*>(grids.as<cplx<T>>()), (int)pg0, n, out, first,
+                                last, st, st + nbins_);
+          } else {
+            launch_degrid_h<SV>(s, g_, wts, rec_.as<fast::VisRecord>(), sorted_.as<uint32_t>(), chunk_sorted_[c],
+                                chunk_sorted_[c + 1], (uint32_t)nbins_,
+                                reinterpret_cast<const cplx<float>*>(grids.as<cplx<T>>()), (int)pg0, n, out, first,
+                                last);
+          }
           fast_path = true;
         }
         if (!fast_path && fused) throw DeviceError("stored values need the tensor-core degridder");

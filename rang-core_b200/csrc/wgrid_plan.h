@@ -81,11 +81,22 @@ class Plan {
   // the sorted order is chunk-major (each range's visibilities contiguous,
   // binned among themselves), so that gridding can start on the rows that
   // have arrived and degridding can hand out finished rows early.
-  // `layout` false stops after the kernel and grid choice (the reference's
-  // `plan` and `gridding_footprint`): such a plan reports `info` and
-  // `footprint` but cannot grid.
+  // `layout` LAYOUT_NONE stops after the kernel and grid choice (the
+  // reference's `plan` and `gridding_footprint`): such a plan reports `info`
+  // and `footprint` but cannot grid. LAYOUT_STREAMED defers the binning to
+  // degrid_streamed, which bins each row chunk just before degridding it.
+  enum Layout : int { LAYOUT_NONE = 0, LAYOUT_FULL = 1, LAYOUT_STREAMED = 2 };
   Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double* uvw_dev, const double* freq_host,
-       const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks = 1, bool layout = true);
+       const Inputs& act, bool with_vis, cudaStream_t s, int row_chunks = 1, int layout = LAYOUT_FULL);
+
+  // dirty2vis of a LAYOUT_STREAMED plan, its only pass: the image's planes
+  // are transformed, then row chunk c is binned (count, offsets after the
+  // earlier chunks' on the device, placement) and degridded before chunk
+  // c + 1 is binned, so done[c] is recorded long before the whole binning
+  // would end. The results equal degrid's bit for bit. Plans the streamed
+  // form does not serve (double precision, supports above 8, one chunk,
+  // plane groups) are binned whole and degridded as by degrid.
+  void degrid_streamed(const T* image, const Inputs& wts, T* vis, cudaStream_t s, cudaEvent_t* done);
 
   bool empty() const { return nvis_ == 0; }
   const PlanInfo& info() const { return info_; }
@@ -204,6 +215,8 @@ class Plan {
   std::vector<uint32_t> chunk_tasks_;   // nchunk_ + 1 offsets into the task list
   unsigned long long scan_[4] = {0, 0, 0, 0};  // count, finite count, |w| min and max bits
   bool foc_finite_ = true;  // every channel's f / c finite
+  bool streamed_ = false;   // LAYOUT_STREAMED, not yet binned
+  DevBuf bits_;             // LAYOUT_STREAMED: the scan's active set, one bit per visibility
   // The arrays of the scan whose value maxima bound_ holds (with the
   // visibilities when scan_vis_), to tell whether a gridding pass's data
   // need their own bound.
