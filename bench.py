@@ -1141,7 +1141,17 @@ def run_b200(args):
                             "fp32_fma_peak_tflops": fp32_peak, "peak_kind": "nominal (148 SMs x 128 FMA x 1965 MHz)",
                             "frac": flops / per_launch_s / 1e12 / fp32_peak}}
 
+    # Between legs (outside every timed region) the library's cached device
+    # buffers of the previous leg go back to the device: the next leg is a
+    # workload of other shapes, partly on PyTorch's allocator, which cannot
+    # use memory the library holds.
+    def release_cached():
+        torch.cuda.synchronize()
+        assert ext.wgridder_release_cached() == 0, ext.wgridder_last_error()
+        torch.cuda.empty_cache()
+
     # End to end through the C ABI with pinned host arrays.
+    release_cached()
     e2e = None
     pinned = None
     reason = "pinned host memory refused on another rank"
@@ -1194,10 +1204,12 @@ def run_b200(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te / args.steps}
         del vis_h, mask_h, out_h, dirty_h
 
+    release_cached()
     accuracy = None
     if world == 1 and not args.no_accuracy:
         accuracy = run_accuracy(dev, ext, wl, uvw, uvw_np, freq, vis, mask, common, args)
 
+    release_cached()
     fst = None
     if world == 1 and not args.no_fista:
         learn = None if args.no_learned else {"patches": args.learned_patches, "steps": args.learned_steps, "batch": 16}
@@ -1233,10 +1245,12 @@ def run_b200(args):
                 "note": "fixed cost (plan, FFTs of the full grid) and per-visibility cost fitted to two samples"}
             del vis2, mask2
 
+    release_cached()
     config1 = None
     if world == 1 and not args.no_config1:
         config1 = run_config1(dev, args)
 
+    release_cached()
     weights_leg = None
     if world == 1 and not args.no_weights:
         weights_leg = run_imaging_weights(wl, uvw_np, freq, mask, args)
