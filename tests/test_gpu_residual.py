@@ -270,10 +270,11 @@ def test_cached_buffers_are_reused_and_released():
     from rang import core, gridder as cw
 
     ext = core.extension()
-    uvw, freq = meerkat_like(nant=64, ntime=16, nchan=64, seed=3)  # 2 M visibilities: 64 MB of records
+    uvw, freq = meerkat_like(nant=64, ntime=32, nchan=64, seed=3)  # 4.1 M visibilities: 132 MB of records
     rng = np.random.default_rng(3)
     vis = (rng.standard_normal((uvw.shape[0], freq.size)) + 1j).astype(np.complex64)
     kw = dict(uvw=uvw, freq=freq, npix_x=256, npix_y=256, pixsize_x=3e-5, pixsize_y=3e-5, epsilon=1e-5)
+    assert ext.wgridder_release_cached() == 0  # the earlier tests' buffers
     first = cw.vis2dirty(vis=vis, **kw)
     held = ext.wgridder_cached_bytes()
     assert held >= 64 << 20
