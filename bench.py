@@ -95,6 +95,9 @@ def parse():
     ap.add_argument("--no-msv4", action="store_true")
     ap.add_argument("--learned-patches", type=int, default=20000)
     ap.add_argument("--learned-steps", type=int, default=2500)
+    ap.add_argument("--trace-e2e", default=None, metavar="PATH",
+                    help="after the e2e leg, one more e2e step under the PyTorch profiler (CUDA activity), "
+                         "its trace written to PATH (Chrome trace JSON)")
     return ap.parse_args()
 
 
@@ -1202,6 +1205,12 @@ def run_b200(args):
         d2h = dirty_np.nbytes + out_np.nbytes
         e2e = {"value": job_rate(world, nvis, args.steps, te), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * te / args.steps}
+        if args.trace_e2e and rank == 0:  # untimed: the copies' and kernels' timeline of one step
+            from torch.profiler import ProfilerActivity, profile
+
+            with profile(activities=[ProfilerActivity.CUDA]) as tprof:
+                e2e_step()
+            tprof.export_chrome_trace(args.trace_e2e)
         del vis_h, mask_h, out_h, dirty_h
 
     release_cached()
