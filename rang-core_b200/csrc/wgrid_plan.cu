@@ -138,30 +138,31 @@ struct Quad {
   uint32_t m;  // the four mask bytes, visibility e in the low byte
 };
 
-template <class T>
-__device__ __forceinline__ void load_quad(const Inputs& in, bool with_vis, bool vec, uint64_t e, uint64_t n,
-                                          Quad<T>& q) {
+// VIS: the values read (0 none, 1 complex64, 2 complex128); WGT: weights read.
+template <class T, int VIS, bool WGT>
+__device__ __forceinline__ void load_quad(const Inputs& in, bool vec, uint64_t e, uint64_t n, Quad<T>& q) {
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     q.v[k] = {(T)1, (T)0};
     q.w[k] = (T)1;
   }
   if (vec && e + 4 <= n) {
-    if (with_vis && in.vis_kind == VIS_C64) {
+    if (VIS == 1) {
       const float4 a = reinterpret_cast<const float4*>(in.vis)[e / 2];
       const float4 b = reinterpret_cast<const float4*>(in.vis)[e / 2 + 1];
       q.v[0] = {(T)a.x, (T)a.y};
       q.v[1] = {(T)a.z, (T)a.w};
       q.v[2] = {(T)b.x, (T)b.y};
       q.v[3] = {(T)b.z, (T)b.w};
-    } else if (with_vis && in.vis_kind == VIS_C128) {
+    } else if (VIS == 2) {
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         const double2 d = reinterpret_cast<const double2*>(in.vis)[e + k];
         q.v[k] = {(T)d.x, (T)d.y};
       }
     }
-    if (in.wgt_kind == WGT_F32 || in.wgt_kind == WGT_F32_PRODUCT) {
+    if (!WGT) {
+    } else if (in.wgt_kind == WGT_F32 || in.wgt_kind == WGT_F32_PRODUCT) {
       float4 a = reinterpret_cast<const float4*>(in.wgt)[e / 4];
       if (in.wgt_kind == WGT_F32_PRODUCT) {
         const float4 b = reinterpret_cast<const float4*>(in.wgt2)[e / 4];
@@ -186,8 +187,8 @@ __device__ __forceinline__ void load_quad(const Inputs& in, bool with_vis, bool 
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     if (e + k < n) {
-      if (with_vis) q.v[k] = vis_get<T>(in, e + k);
-      q.w[k] = wgt_get<T>(in, e + k);
+      if (VIS) q.v[k] = vis_get<T>(in, e + k);
+      if (WGT) q.w[k] = wgt_get<T>(in, e + k);
       q.m |= (in.mask ? (uint32_t)in.mask[e + k] : 1u) << (8 * k);
     }
   }
@@ -239,9 +240,9 @@ constexpr int SCAN_GROUPS = 2;
 // smallest and largest |w| of the group's active visibilities are those of
 // its first and last active channel, and each is NaN exactly when
 // fw w_row is.
-template <class T>
+template <class T, int VIS, bool WGT>
 __global__ void __launch_bounds__(256, 3) k_scan(uint32_t nrow, uint32_t nchan, const double* __restrict__ uvw,
-                       const double* __restrict__ foc, double fw, Inputs in, int with_vis, int vec, int clean,
+                       const double* __restrict__ foc, double fw, Inputs in, int vec, int clean,
                        ScanOut* out, uint32_t* __restrict__ bits) {
   const uint64_t n = (uint64_t)nrow * nchan;
   constexpr int G = sizeof(T) == 4 ? SCAN_GROUPS : SCAN_GROUPS / 2;
@@ -258,7 +259,7 @@ __global__ void __launch_bounds__(256, 3) k_scan(uint32_t nrow, uint32_t nchan, 
   for (; b0 < n; b0 += wstride, rc.next(nchan)) {
     Quad<T> q[G];
 #pragma unroll
-    for (int g = 0; g < G; g++) load_quad<T>(in, with_vis != 0, vec != 0, b0 + 128 * g + 4 * lane, n, q[g]);
+    for (int g = 0; g < G; g++) load_quad<T, VIS, WGT>(in, vec != 0, b0 + 128 * g + 4 * lane, n, q[g]);
     uint32_t row = rc.row, ch = rc.ch;
 #pragma unroll
     for (int g = 0; g < G; g++) {
@@ -266,14 +267,14 @@ __global__ void __launch_bounds__(256, 3) k_scan(uint32_t nrow, uint32_t nchan, 
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         // is_active, keeping the magnitudes for the value bound
-        const T vn = with_vis ? q[g].v[k].re * q[g].v[k].re + q[g].v[k].im * q[g].v[k].im : (T)1;
+        const T vn = VIS ? q[g].v[k].re * q[g].v[k].re + q[g].v[k].im * q[g].v[k].im : (T)1;
         if (active_of(vn, q[g].w[k], (q[g].m >> (8 * k)) & 0xffu)) {
           nib |= 1u << k;
           const T awt = fabs(q[g].w[k]);
           wm = awt > wm ? awt : wm;
           // |vis|^2 |wgt|^2, the value bound's square (value_bound_sq)
           const double aw = (double)awt;
-          const double av = with_vis ? value_bound_sq(q[g].v[k], aw) : aw * aw;
+          const double av = VIS ? value_bound_sq(q[g].v[k], aw) : aw * aw;
           vm = av > vm ? av : vm;
         }
       }
@@ -338,6 +339,31 @@ __global__ void __launch_bounds__(256, 3) k_scan(uint32_t nrow, uint32_t nchan, 
       atomicMin(&out->lo_bits, (unsigned long long)__double_as_longlong(lo));
       atomicMax(&out->hi_bits, (unsigned long long)__double_as_longlong(hi));
     }
+  }
+}
+
+// k_scan for the activity inputs present: the values (with_vis, of kind
+// complex64 or complex128) and the weights, each a template argument so that
+// a scan of the mask alone tests a byte per visibility and no more.
+template <class T>
+void launch_scan(uint32_t nrow, uint32_t nchan, const double* uvw, const double* foc, double fw, const Inputs& in,
+                 bool with_vis, bool clean, ScanOut* out, uint32_t* bits, cudaStream_t s) {
+  const uint64_t n = (uint64_t)nrow * nchan;
+  const int vec = scan_vectors(in, with_vis) ? 1 : 0;
+  const int vis = !with_vis ? 0 : in.vis_kind == VIS_C64 ? 1 : in.vis_kind == VIS_C128 ? 2 : 0;
+  const bool wgt = in.wgt_kind != WGT_NONE;
+  auto go = [&](auto kv, auto kw) {
+    k_scan<T, decltype(kv)::value, decltype(kw)::value><<<blocks_for(n, 256), 256, 0, s>>>(
+        nrow, nchan, uvw, foc, fw, in, vec, clean ? 1 : 0, out, bits);
+  };
+  using W1 = std::true_type;
+  using W0 = std::false_type;
+  if (vis == 1) {
+    if (wgt) go(std::integral_constant<int, 1>{}, W1{}); else go(std::integral_constant<int, 1>{}, W0{});
+  } else if (vis == 2) {
+    if (wgt) go(std::integral_constant<int, 2>{}, W1{}); else go(std::integral_constant<int, 2>{}, W0{});
+  } else {
+    if (wgt) go(std::integral_constant<int, 0>{}, W1{}); else go(std::integral_constant<int, 0>{}, W0{});
   }
 }
 
@@ -2292,10 +2318,8 @@ Plan<T>::Plan(const WgridderOptions& o, size_t nrow, size_t nchan, const double*
   if (n_) {
     {
       StageTimer timer_(ST_SCAN, s);
-      k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw_.as<double>(),
-                                                    foc_.as<double>(), fw, act, with_vis ? 1 : 0,
-                                                    scan_vectors(act, with_vis) ? 1 : 0, foc_finite_ ? 1 : 0,
-                                                    so.as<ScanOut>(), bits.as<uint32_t>());
+      launch_scan<T>((uint32_t)nrow, (uint32_t)nchan, uvw_.as<double>(), foc_.as<double>(), fw, act, with_vis,
+                     foc_finite_, so.as<ScanOut>(), bits.as<uint32_t>(), s);
       k_umax<<<blocks_for(nrow, 256, 148u * 8u), 256, 0, s>>>((uint32_t)nrow, uvw_.as<double>(), so.as<ScanOut>());
     }
     check_cuda(cudaGetLastError(), "scan kernel");
@@ -2462,10 +2486,8 @@ bool Plan<T>::same_scan(const Inputs& act, bool with_vis, cudaStream_t s) const 
   if (n_) {
     {
       StageTimer timer_(ST_SCAN, s);
-      k_scan<T><<<blocks_for(n_, 256), 256, 0, s>>>((uint32_t)nrow_, (uint32_t)nchan_, uvw_.as<double>(),
-                                                    foc_.as<double>(), o_.flip_w ? 1.0 : -1.0, act, with_vis ? 1 : 0,
-                                                    scan_vectors(act, with_vis) ? 1 : 0, foc_finite_ ? 1 : 0,
-                                                    so.as<ScanOut>(), nullptr);
+      launch_scan<T>((uint32_t)nrow_, (uint32_t)nchan_, uvw_.as<double>(), foc_.as<double>(),
+                     o_.flip_w ? 1.0 : -1.0, act, with_vis, foc_finite_, so.as<ScanOut>(), nullptr, s);
     }
     check_cuda(cudaGetLastError(), "scan kernel");
   }
@@ -3263,9 +3285,7 @@ void bin_noalloc(const WgridderOptions& o, size_t nrow, size_t nchan, const doub
   check_cuda(cudaMemcpyAsync(dfoc, foc.data(), nchan * sizeof(double), cudaMemcpyHostToDevice, s), "copy");
   const double fw = o.flip_w ? 1.0 : -1.0;
   if (n) {
-    k_scan<T><<<blocks_for(n, 256), 256, 0, s>>>((uint32_t)nrow, (uint32_t)nchan, uvw, dfoc, fw, act, 0,
-                                                  scan_vectors(act, false) ? 1 : 0, all_finite(foc) ? 1 : 0, so,
-                                                  nullptr);
+    launch_scan<T>((uint32_t)nrow, (uint32_t)nchan, uvw, dfoc, fw, act, false, all_finite(foc), so, nullptr, s);
     check_cuda(cudaGetLastError(), "scan kernel");
   }
   ScanOut r;
