@@ -265,17 +265,30 @@ static_assert(sizeof(VisRecord) == 32, "records are one 32-byte sector");
 // iteration ahead of their use (the pass otherwise waited on them).
 struct CountIn {
   uint32_t word = 0;
-  double u = 0.0, v = 0.0, w = 0.0, f = 0.0;
+  double4 b = {0.0, 0.0, 0.0, 1.0};  // the row's coordinates and sign (k_row_coords)
+  double f = 0.0;
 };
-__device__ __forceinline__ CountIn count_in(const uint32_t* __restrict__ bits, const double* __restrict__ uvw,
+__device__ __forceinline__ CountIn count_in(const uint32_t* __restrict__ bits, const double4* __restrict__ rowc,
                                             const double* __restrict__ foc, uint64_t i, uint32_t row, uint32_t ch) {
   CountIn c;
   c.word = bits[i >> 5];
-  c.u = uvw[3 * (uint64_t)row];
-  c.v = uvw[3 * (uint64_t)row + 1];
-  c.w = uvw[3 * (uint64_t)row + 2];
+  c.b = rowc[row];
   c.f = foc[ch];
   return c;
+}
+
+// Each row's coordinates as the binning uses them (row_coord: flips,
+// recentring, w made non-negative) and the sign of that flip, once per row:
+// the count pass then reads them instead of forming them for every channel
+// (the same doubles, so the same keys and records).
+__global__ void k_row_coords(uint64_t nrow, const double* __restrict__ uvw, double fu, double fv, double fw,
+                             double r_l, double r_m, double4* __restrict__ out) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nrow;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    double b[3];
+    const double sgn = row_coord(uvw, r, fu, fv, fw, r_l, r_m, b);
+    out[r] = make_double4(b[0], b[1], b[2], sgn);
+  }
 }
 
 // The count pass of the counting sort (k_bin_count) for single precision,
@@ -291,7 +304,7 @@ __device__ __forceinline__ CountIn count_in(const uint32_t* __restrict__ bits, c
 constexpr int COUNT_BLOCKS = 3;
 template <bool WPL, bool SHIFT, bool CHUNKED>
 __global__ void __launch_bounds__(256, COUNT_BLOCKS)
-    k_bin_count_rec(const __grid_constant__ Geom<float> g, const double* __restrict__ uvw,
+    k_bin_count_rec(const __grid_constant__ Geom<float> g, const double4* __restrict__ rowc,
                     const double* __restrict__ foc, const uint32_t* __restrict__ bits, uint32_t* __restrict__ key,
                     uint32_t* __restrict__ counts, VisRecord* __restrict__ rec, uint32_t rows_per_chunk,
                     uint32_t nbins, uint64_t i0, uint64_t n, uint32_t koff) {
@@ -302,18 +315,18 @@ __global__ void __launch_bounds__(256, COUNT_BLOCKS)
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint64_t i = i0 + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   RowCh rc(i, (uint32_t)g.nchan, stride);
-  CountIn cur = i < n ? count_in(bits, uvw, foc, i, rc.row, rc.ch) : CountIn{};
+  CountIn cur = i < n ? count_in(bits, rowc, foc, i, rc.row, rc.ch) : CountIn{};
   for (; i < nround; i += stride) {
     RowCh nrc = rc;
     nrc.next((uint32_t)g.nchan);
-    const CountIn nxt = i + stride < n ? count_in(bits, uvw, foc, i + stride, nrc.row, nrc.ch) : CountIn{};
+    const CountIn nxt = i + stride < n ? count_in(bits, rowc, foc, i + stride, nrc.row, nrc.ch) : CountIn{};
     bool act = false;
     uint32_t k = INACTIVE;
     if (i < n) {
       act = ((cur.word >> (i & 31)) & 1u) != 0;
       if (act) {
-        double b[3];
-        const double imflip = row_coord_of(cur.u, cur.v, cur.w, g.fu, g.fv, g.fw, g.r_l, g.r_m, b);
+        const double b[3] = {cur.b.x, cur.b.y, cur.b.z};
+        const double imflip = cur.b.w;
         const double f = cur.f;
         const double u = b[0] * f, v = b[1] * f, w = b[2] * f;
         double uf, vf;

@@ -1915,12 +1915,12 @@ void launch_grid_bf16(cudaStream_t s, const Geom<float>& g, const Inputs& in, in
 }
 
 // The record count pass for the plan's w-planes, shift and row chunks.
-void launch_count_rec(const Geom<float>& g, const double* uvw, const double* foc, const uint32_t* bits, uint32_t* key,
+void launch_count_rec(const Geom<float>& g, const double4* rowc, const double* foc, const uint32_t* bits, uint32_t* key,
                       uint32_t* counts, fast::VisRecord* rec, uint32_t rows_per_chunk, uint32_t nbins, uint64_t n,
                       cudaStream_t s, uint64_t i0 = 0, uint32_t koff = 0) {
   auto go = [&](auto wpl, auto shift, auto chunked) {
     fast::k_bin_count_rec<decltype(wpl)::value, decltype(shift)::value, decltype(chunked)::value>
-        <<<blocks_for(n - i0, 256), 256, 0, s>>>(g, uvw, foc, bits, key, counts, rec, rows_per_chunk, nbins, i0, n,
+        <<<blocks_for(n - i0, 256), 256, 0, s>>>(g, rowc, foc, bits, key, counts, rec, rows_per_chunk, nbins, i0, n,
                                                  koff);
   };
   using T_ = std::true_type;
@@ -2376,6 +2376,14 @@ int Plan<T>::touched_rows(double umax, double wmax) const {
 }
 
 template <class T>
+void Plan<T>::row_coords(DevBuf& out, cudaStream_t s) const {
+  if (nrow_ == 0) return;
+  fast::k_row_coords<<<blocks_for(nrow_, 256, 148u * 8u), 256, 0, s>>>(nrow_, uvw_.as<double>(), g_.fu, g_.fv, g_.fw,
+                                                                       g_.r_l, g_.r_m, out.as<double4>());
+  check_cuda(cudaGetLastError(), "row coordinates");
+}
+
+template <class T>
 void Plan<T>::build_layout(const Inputs& act, bool with_vis, const uint32_t* bits, cudaStream_t s) {
   ntiles_ = (size_t)g_.ntu * g_.ntv;
   nbins_ = ntiles_ * (size_t)g_.nbuckets * (size_t)g_.nsub;
@@ -2390,8 +2398,10 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, const uint32_t* bit
   check_cuda(cudaMemsetAsync(starts_.get(), 0, (nkeys + 1) * 4, s), "memset");
   if constexpr (sizeof(T) == 4) {  // with the records of the tensor-core kernels
     rec_.alloc(n_ * sizeof(fast::VisRecord), s);
+    DevBuf rowc(nrow_ * sizeof(double4), s);
     StageTimer timer_(ST_BIN_COUNT, s);
-    launch_count_rec(g_, uvw_.as<double>(), foc_.as<double>(), bits, key_.as<uint32_t>(), starts_.as<uint32_t>(),
+    row_coords(rowc, s);
+    launch_count_rec(g_, rowc.as<double4>(), foc_.as<double>(), bits, key_.as<uint32_t>(), starts_.as<uint32_t>(),
                      rec_.as<fast::VisRecord>(), K > 1 ? (uint32_t)rows_per_chunk_ : 0u, (uint32_t)nbins_, n_, s);
   } else {
     StageTimer timer_(ST_BIN_COUNT, s);
@@ -2836,8 +2846,10 @@ void Plan<T>::degrid_to(const T* image, const Inputs& wts, T* vis, const void* f
     }
   }
   if (nvis_ > 0 && !sorted_.get()) throw InvalidArgument("this plan was made without the visibility layout");
-  DevBuf counts, cursor, base;  // the streamed binning's scratch
+  DevBuf counts, cursor, base, rowc;  // the streamed binning's scratch
   if (stream_bins) {
+    rowc.alloc(nrow_ * sizeof(double4), s);
+    row_coords(rowc, s);
     counts.alloc((nbins_ + 1) * 4, s);
     cursor.alloc(nbins_ * 4, s);
     base.alloc(((size_t)nchunk_ + 1) * 4, s);
@@ -2853,7 +2865,7 @@ void Plan<T>::degrid_to(const T* image, const Inputs& wts, T* vis, const void* f
     {
       StageTimer timer_(ST_BIN_COUNT, s);
       if constexpr (sizeof(T) == 4)
-        launch_count_rec(g_, uvw_.as<double>(), foc_.as<double>(), bits_.as<uint32_t>(), key_.as<uint32_t>(),
+        launch_count_rec(g_, rowc.as<double4>(), foc_.as<double>(), bits_.as<uint32_t>(), key_.as<uint32_t>(),
                          counts.as<uint32_t>(), rec_.as<fast::VisRecord>(), (uint32_t)rows_per_chunk_,
                          (uint32_t)nbins_, i1, s, i0, koff);
     }

@@ -171,6 +171,8 @@ class Plan {
 
  private:
   void build_layout(const Inputs& act, bool with_vis, const uint32_t* bits, cudaStream_t s);
+  // Per row the binning's coordinates and sign (double4, nrow_ of them).
+  void row_coords(DevBuf& out, cudaStream_t s) const;
   // Degridding into `vis` (by visibility index), or, with `fused` (a
   // fast::DegridOut), into the stored values by sorted position.
   void degrid_to(const T* image, const Inputs& wts, T* vis, const void* fused, cudaStream_t s, cudaEvent_t* done);
