@@ -2126,18 +2126,11 @@ struct CachedBuf {
   size_t bytes;
   int dev;
   cudaEvent_t ready;
-  uint64_t tick;  // g_tick when released
 };
 std::mutex g_cache_mu;
 std::vector<CachedBuf> g_cache;  // oldest first
-uint64_t g_tick = 0;             // requests of CACHED_MIN bytes or more so far (under g_cache_mu)
 
 constexpr size_t CACHED_MAX = 128;
-// A buffer not taken within this many later requests of CACHED_MIN bytes or
-// more goes back to the pool: a workload's buffers come back within one of
-// its steps (about 30 such requests for a vis2dirty + dirty2vis), while those
-// of a workload no longer run would otherwise stay held.
-constexpr uint64_t CACHED_AGE = 256;
 
 // The device's memory in bytes (looked up once per device).
 size_t device_bytes(int dev) {
@@ -2190,7 +2183,6 @@ void DevBuf::alloc(size_t bytes, cudaStream_t s) {
     CachedBuf b{};
     {
       std::lock_guard<std::mutex> lock(g_cache_mu);
-      g_tick++;
       for (size_t i = g_cache.size(); i-- > 0;)  // the most recent of this size
         if (g_cache[i].dev == dev && g_cache[i].bytes == bytes) {
           b = g_cache[i];
@@ -2237,7 +2229,7 @@ void DevBuf::release() {
         // memory per device (a step of two plans holds about 100 GB at 1 G
         // visibilities); the oldest go back to the pool.
         std::lock_guard<std::mutex> lock(g_cache_mu);
-        g_cache.push_back(CachedBuf{p_, n_, dev, ev, g_tick});
+        g_cache.push_back(CachedBuf{p_, n_, dev, ev});
         size_t count = 0, bytes = 0;
         for (const CachedBuf& b : g_cache)
           if (b.dev == dev) {
@@ -2245,9 +2237,8 @@ void DevBuf::release() {
             bytes += b.bytes;
           }
         const size_t cap = device_bytes(dev) / 4 * 3;
-        for (size_t i = 0; i < g_cache.size();) {
-          const bool stale = g_tick - g_cache[i].tick > CACHED_AGE;
-          if (g_cache[i].dev != dev || !(stale || count > CACHED_MAX || bytes > cap)) {
+        for (size_t i = 0; i < g_cache.size() && (count > CACHED_MAX || bytes > cap);) {
+          if (g_cache[i].dev != dev) {
             i++;
             continue;
           }
