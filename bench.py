@@ -1059,6 +1059,18 @@ def run_b200(args):
     svis = vis if single else vis.to(torch.complex128)
     torch.cuda.synchronize()
 
+    # Between phases and legs (outside every timed region) the library's
+    # cached device buffers of the previous phase go back to the device: the
+    # next is a workload of other shapes (here the data's making at epsilon
+    # 1e-6), partly on PyTorch's allocator, which cannot use memory the
+    # library holds.
+    def release_cached():
+        torch.cuda.synchronize()
+        assert ext.wgridder_release_cached() == 0, ext.wgridder_last_error()
+        torch.cuda.empty_cache()
+
+    release_cached()
+
     def step():
         p1 = wgrid_torch.DevicePlan(uvw, freq, vis=svis, mask=mask, epsilon=eps, single=single, **common)
         dirty = p1.grid(svis, scanned=True)
@@ -1143,15 +1155,6 @@ def run_b200(args):
                 "compute": {"useful_tflop_per_launch": flops / 1e12, "achieved_tflops": flops / per_launch_s / 1e12,
                             "fp32_fma_peak_tflops": fp32_peak, "peak_kind": "nominal (148 SMs x 128 FMA x 1965 MHz)",
                             "frac": flops / per_launch_s / 1e12 / fp32_peak}}
-
-    # Between legs (outside every timed region) the library's cached device
-    # buffers of the previous leg go back to the device: the next leg is a
-    # workload of other shapes, partly on PyTorch's allocator, which cannot
-    # use memory the library holds.
-    def release_cached():
-        torch.cuda.synchronize()
-        assert ext.wgridder_release_cached() == 0, ext.wgridder_last_error()
-        torch.cuda.empty_cache()
 
     # End to end through the C ABI with pinned host arrays.
     release_cached()
