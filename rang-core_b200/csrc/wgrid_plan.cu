@@ -2380,9 +2380,12 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, const uint32_t* bit
   ntiles_ = (size_t)g_.ntu * g_.ntv;
   nbins_ = ntiles_ * (size_t)g_.nbuckets * (size_t)g_.nsub;
   if (nbins_ >= 0xffffffffull) throw InvalidArgument("too many uv tiles and w-planes for one call");
-  if ((size_t)nchunk_ * nbins_ >= 0xffffffffull) {  // row chunks are an optimisation: drop them
-    nchunk_ = 1;
-    rows_per_chunk_ = std::max<size_t>(nrow_, 1);
+  if ((size_t)nchunk_ * nbins_ >= 0xffffffffull) {
+    // Row chunks are an optimisation: as many as the 32-bit key space holds
+    // (chunks x bins keys, below the inactive key), down to one.
+    const size_t kmax = std::max<size_t>(1, (0xffffffffull - 1) / nbins_);
+    rows_per_chunk_ = chunk_rows(nrow_, (int)std::min<size_t>(kmax, (size_t)nchunk_));
+    nchunk_ = (int)((std::max<size_t>(nrow_, 1) + rows_per_chunk_ - 1) / rows_per_chunk_);
   }
   const size_t K = (size_t)nchunk_, nkeys = K * nbins_, nvt = K * ntiles_;
   key_.alloc(n_ * 4, s);
