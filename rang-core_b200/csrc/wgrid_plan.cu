@@ -466,6 +466,28 @@ __global__ void k_iota(uint64_t n, uint32_t* __restrict__ out) {
     out[i] = (uint32_t)i;
 }
 
+// The active bits of each 32-visibility word.
+__global__ void k_word_counts(const uint32_t* __restrict__ bits, uint64_t nwords, uint32_t* __restrict__ out) {
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < nwords; w += (uint64_t)gridDim.x * blockDim.x)
+    out[w] = (uint32_t)__popc(bits[w]);
+}
+
+// The active visibilities' keys and indices, in index order: visibility i
+// goes to its word's offset (woff, the exclusive scan of k_word_counts) plus
+// the active bits below it in its word.
+__global__ void k_compact_active(uint64_t n, const uint32_t* __restrict__ bits, const uint32_t* __restrict__ woff,
+                                 const uint32_t* __restrict__ key, uint32_t* __restrict__ kc,
+                                 uint32_t* __restrict__ ic) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t w = bits[i >> 5], b = 1u << (i & 31);
+    if (w & b) {
+      const uint32_t pos = woff[i >> 5] + (uint32_t)__popc(w & (b - 1u));
+      kc[pos] = key[i];
+      ic[pos] = (uint32_t)i;
+    }
+  }
+}
+
 // Each thread takes four indices a grid-stride apart per round, so that four
 // independent atomics (each returning its run's base) are in flight at once:
 // the kernel is bound by their latency. The order within a bin is free.
@@ -2412,26 +2434,51 @@ void Plan<T>::build_layout(const Inputs& act, bool with_vis, const uint32_t* bit
     // the visibilities keep their index order (the reference's layout
     // order), so the double-precision gridder's sums, which follow this
     // order, come out the same on every call. Inactive keys (all ones in
-    // the sorted bits: 2^bits - 1 exceeds every bin key) sort last.
-    int bits = 1;
-    while (bits < 32 && ((1ull << bits) - 1ull) < (unsigned long long)nkeys) bits++;
-    DevBuf iota(n_ * 4, s), keys_out(n_ * 4, s), vals_out(n_ * 4, s);
-    {
+    // the sorted bits: 2^nbits - 1 exceeds every bin key) would sort last.
+    int nbits = 1;
+    while (nbits < 32 && ((1ull << nbits) - 1ull) < (unsigned long long)nkeys) nbits++;
+    if (bits) {
+      // Only the active visibilities' (key, index) pairs, compacted in index
+      // order through the scan's bits (a bit count per word, its exclusive
+      // scan, a place per active bit), are sorted: the radix sort is stable.
+      const size_t nwords = (n_ + 31) / 32;
+      DevBuf woff(nwords * 4, s), kc(nvis_ * 4, s), ic(nvis_ * 4, s), keys_out(nvis_ * 4, s);
+      sorted_.alloc(nvis_ * 4, s);
       StageTimer timer_(ST_BIN_SCATTER, s);
-      k_iota<<<blocks_for(n_, 256), 256, 0, s>>>(n_, iota.as<uint32_t>());
+      k_word_counts<<<blocks_for(nwords, 256), 256, 0, s>>>(bits, nwords, woff.as<uint32_t>());
+      exclusive_scan(woff.as<uint32_t>(), woff.as<uint32_t>(), nwords, s);
+      k_compact_active<<<blocks_for(n_, 256), 256, 0, s>>>(n_, bits, woff.as<uint32_t>(), key_.as<uint32_t>(),
+                                                            kc.as<uint32_t>(), ic.as<uint32_t>());
+      check_cuda(cudaGetLastError(), "compaction");
       size_t temp = 0;
-      check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, temp, key_.as<uint32_t>(), keys_out.as<uint32_t>(),
-                                                 iota.as<uint32_t>(), vals_out.as<uint32_t>(), (long long)n_, 0, bits,
-                                                 s),
+      check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, temp, kc.as<uint32_t>(), keys_out.as<uint32_t>(),
+                                                 ic.as<uint32_t>(), sorted_.as<uint32_t>(), (long long)nvis_, 0,
+                                                 nbits, s),
                  "radix sort");
       DevBuf work(temp, s);
-      check_cuda(cub::DeviceRadixSort::SortPairs(work.get(), temp, key_.as<uint32_t>(), keys_out.as<uint32_t>(),
-                                                 iota.as<uint32_t>(), vals_out.as<uint32_t>(), (long long)n_, 0, bits,
-                                                 s),
+      check_cuda(cub::DeviceRadixSort::SortPairs(work.get(), temp, kc.as<uint32_t>(), keys_out.as<uint32_t>(),
+                                                 ic.as<uint32_t>(), sorted_.as<uint32_t>(), (long long)nvis_, 0,
+                                                 nbits, s),
                  "radix sort");
+    } else {  // every visibility's key, inactive ones sorting last
+      DevBuf iota(n_ * 4, s), keys_out(n_ * 4, s), vals_out(n_ * 4, s);
+      {
+        StageTimer timer_(ST_BIN_SCATTER, s);
+        k_iota<<<blocks_for(n_, 256), 256, 0, s>>>(n_, iota.as<uint32_t>());
+        size_t temp = 0;
+        check_cuda(cub::DeviceRadixSort::SortPairs(nullptr, temp, key_.as<uint32_t>(), keys_out.as<uint32_t>(),
+                                                   iota.as<uint32_t>(), vals_out.as<uint32_t>(), (long long)n_, 0,
+                                                   nbits, s),
+                   "radix sort");
+        DevBuf work(temp, s);
+        check_cuda(cub::DeviceRadixSort::SortPairs(work.get(), temp, key_.as<uint32_t>(), keys_out.as<uint32_t>(),
+                                                   iota.as<uint32_t>(), vals_out.as<uint32_t>(), (long long)n_, 0,
+                                                   nbits, s),
+                   "radix sort");
+      }
+      sorted_.alloc(nvis_ * 4, s);
+      check_cuda(cudaMemcpyAsync(sorted_.get(), vals_out.get(), nvis_ * 4, cudaMemcpyDeviceToDevice, s), "copy");
     }
-    sorted_.alloc(nvis_ * 4, s);
-    check_cuda(cudaMemcpyAsync(sorted_.get(), vals_out.get(), nvis_ * 4, cudaMemcpyDeviceToDevice, s), "copy");
   } else {
     DevBuf cursor((nkeys + 1) * 4, s);
     check_cuda(cudaMemcpyAsync(cursor.get(), starts_.get(), (nkeys + 1) * 4, cudaMemcpyDeviceToDevice, s), "copy");
